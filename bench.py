@@ -1,0 +1,350 @@
+"""Benchmark of the one-sided Jacobi SVD on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload tall|square512|batch|serve] [--path auto|plain|blocked]
+
+One step = one pass of the hot path over one batch of synthetic input (for the
+single-matrix workloads: one full SVD).  `value` is whole-job SVDs/s with the
+input resident in HBM; `e2e` repeats the measurement through the host-buffer
+C-ABI call (H2D of A and D2H of U, sigma, V inside the timed region).  Under
+torchrun every rank solves its own replica (no collective on the data path):
+`scaling` is "weak" and the time is the max over ranks.
+
+`--impl reference` times the reference's CPU arithmetic - the FP64 host
+oracle, a restatement of the reference's kernels (the reference has no CPU
+path of its own) - on the host cores, on a bounded sample of the same
+workload, extrapolated to SVDs/s.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "jacobi-svd-cuda_b200"))
+
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+# Sweep counts of the plain path on the seeded inputs (identical in the oracle,
+# which reproduces the GPU arithmetic bit for bit); used to extrapolate the
+# bounded CPU samples to whole SVDs.
+PLAIN_SWEEPS = {"tall": 12, "square512": 11}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workloads
+
+
+def make_workload(name: str):
+    import workloads as W
+
+    if name == "tall":
+        a, s = W.tall_case(seed=2)
+        return {"name": name, "a": a, "sigma_true": s, "eps": 1e-14,
+                "desc": "4096x1024 FP64, A = U diag(sigma) V^T, Haar U,V (seed 2), sigma geometric 1..1e-6"}
+    if name == "square512":
+        a = W.gaussian_splitmix(512, 512, 1)
+        return {"name": name, "a": a, "sigma_true": None, "eps": 1e-14,
+                "desc": "512x512 FP64 N(0,1) (SplitMix64 seed 1)"}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def algorithmic_round_bytes(m: int, n: int) -> float:
+    """Per launch of the fused round kernel: every pair reads its two A columns
+    and writes them back (2 reads + 2 writes of m doubles)."""
+    return (n // 2) * 4.0 * m * 8.0
+
+
+def run_ours(args, rank: int, world: int, device):
+    import torch
+    import jsvd
+
+    wl = make_workload(args.workload)
+    a = wl["a"]
+    m, n = a.shape
+    cfg = jsvd.default_config(epsilon=wl["eps"])
+    da = torch.from_numpy(a).to(device)
+    du = torch.empty((m, n), dtype=torch.float64, device=device)
+    ds = torch.empty(n, dtype=torch.float64, device=device)
+    dv = torch.empty((n, n), dtype=torch.float64, device=device)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    torch.cuda.synchronize(device)
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
+
+    def step():
+        return jsvd.plain_svd_device(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg,
+                                     stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(device)
+
+    # correctness guard on the timed configuration (sigma vs the analytic spectrum)
+    sig = np.sort(ds.cpu().numpy())[::-1]
+    guard = None
+    if wl["sigma_true"] is not None:
+        t = np.sort(wl["sigma_true"])[::-1]
+        guard = {"sigma_max_rel_vs_analytic": float(np.max(np.abs(sig - t) / t)),
+                 "sigma_normwise_vs_analytic": float(np.max(np.abs(sig - t)) / t[0])}
+
+    jsvd.plain_stats_reset()
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    sampler.start()
+    total_ms = 0.0
+    sweeps = []
+    for _ in range(args.steps):
+        flush.zero_()  # evict A, V and the working copies from L2 between steps
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sweeps.append(step())
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize(device)
+    clocks = sampler.stop()
+    st = jsvd.plain_stats()
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1e3)
+    launches = int(st.round_launches + st.vpass_launches + st.other_launches)
+
+    # e2e through the host-buffer C-ABI call, pinned host memory
+    ha = torch.from_numpy(a).pin_memory().numpy()
+    hu = torch.empty((m, n), dtype=torch.float64).pin_memory().numpy()
+    hs = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    hv = torch.empty((n, n), dtype=torch.float64).pin_memory().numpy()
+    import ctypes
+    lib = jsvd.lib()
+    sw = ctypes.c_int(0)
+    for _ in range(max(1, args.warmup)):
+        jsvd.check(lib.jsvd_plain_svd(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data,
+                                      hv.ctypes.data, ctypes.byref(sw)))
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        jsvd.check(lib.jsvd_plain_svd(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data,
+                                      hv.ctypes.data, ctypes.byref(sw)))
+        e2e_s += time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * args.steps / e2e_s
+
+    hbm_peak, _, peak_kind = peaks()
+    avg_round_ms = st.round_ms / max(1, st.round_launches)
+    achieved = algorithmic_round_bytes(m, n) / (avg_round_ms * 1e-3) / 1e9
+    line = {
+        "metric": "SVDs/s",
+        "value": value,
+        "unit": "SVD/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["desc"], "path": "plain FP64 drop-in (reference arithmetic, round-robin)",
+                   "epsilon": wl["eps"], "sweeps_per_svd": sweeps[0] if sweeps else None,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "SVD/s", "h2d_bytes_per_step": a.nbytes,
+                "d2h_bytes_per_step": (m * n + n + n * n) * 8, "timer": "host wall clock around the synchronous call"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "plain_round_kernel", "achieved": achieved, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                     "traffic": None, "avg_launch_us": avg_round_ms * 1e3,
+                     "algorithmic_bytes_per_launch": algorithmic_round_bytes(m, n),
+                     "round_share_of_step": st.round_ms / max(total_ms / world, 1e-9),
+                     "vpass_ms_per_sweep": st.vpass_ms / max(1, st.vpass_launches)},
+        "clocks": clocks,
+        "check": guard,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl, sweeps[0] if sweeps else PLAIN_SWEEPS.get(wl["name"], 12),
+                                            budget_s=args.cpu_budget)
+    return line
+
+
+def cpu_baseline(wl, sweeps: int, budget_s: float = 12.0, threads: int | None = None) -> dict:
+    """Oracle (reference arithmetic) on the host cores: a bounded number of
+    rounds of one sweep, extrapolated to a whole SVD with `sweeps` sweeps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    a = wl["a"]
+    m, n = a.shape
+    threads = threads or os.cpu_count() or 1
+    rounds_total = n - 1 if n % 2 == 0 else n
+    probe = min(4, rounds_total)
+    t0 = time.perf_counter()
+    O.partial_sweep(a, wl["eps"], rounds=probe, threads=threads)
+    per_round = (time.perf_counter() - t0) / probe
+    r = int(max(probe, min(rounds_total, budget_s / max(per_round, 1e-9))))
+    t0 = time.perf_counter()
+    O.partial_sweep(a, wl["eps"], rounds=r, threads=threads)
+    dt = time.perf_counter() - t0
+    per_svd = dt / r * rounds_total * sweeps
+    return {"value": 1.0 / per_svd, "unit": "SVD/s", "cores": threads, "kind": "port",
+            "sample": f"{r} of {rounds_total} rounds of one sweep of the same {m}x{n} input "
+                      f"({dt:.1f} s), extrapolated x{rounds_total / r:.2f} rounds x {sweeps} sweeps"}
+
+
+def run_reference(args):
+    wl = make_workload(args.workload)
+    m, n = wl["a"].shape
+    sweeps = PLAIN_SWEEPS.get(wl["name"], 12)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(wl, sweeps, budget_s=args.cpu_budget)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    value = statistics.mean(vals)
+    cb["value"] = value
+    return {
+        "impl": "reference",
+        "metric": "SVDs/s",
+        "value": value,
+        "unit": "SVD/s",
+        "n_gpus": 0,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["desc"], "path": "FP64 host oracle (reference arithmetic; the reference has "
+                                                   "no CPU path)", "epsilon": wl["eps"]},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "SVD/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="tall")
+    ap.add_argument("--path", default="auto")
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    import torch
+
+    device = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        line = run_ours(args, rank, world, device)
+    finally:
+        if world > 1:
+            torch.distributed.barrier()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,69 @@
+// Host-side helpers shared by the C-ABI translation units: the per-thread
+// last-error string, CUDA status checks and argument validation that mirror
+// the reference's exception messages (kleedaisuki/jacobi-svd-cuda
+// src/kernels.cu:29-46, 338-356, 807-833).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <sstream>
+#include <string>
+
+#include "jsvd.h"
+
+namespace jsvd {
+
+void set_last_error(int code, const std::string &message);
+const std::string &last_error_message();
+
+// Formats a CUDA failure like the reference's JACOBI_CUDA_CHECK:
+// "CUDA call failed: <expr> @ <file>:<line>, code=<n>, message=<text>".
+inline int cuda_failure(cudaError_t status, const char *expr, const char *file, int line)
+{
+    std::ostringstream os;
+    os << "CUDA call failed: " << expr << " @ " << file << ':' << line << ", code=" << static_cast<int>(status)
+       << ", message=" << cudaGetErrorString(status);
+    set_last_error(JSVD_ERR_CUDA, os.str());
+    return JSVD_ERR_CUDA;
+}
+
+inline int invalid_argument(const char *message)
+{
+    set_last_error(JSVD_ERR_INVALID_ARGUMENT, message);
+    return JSVD_ERR_INVALID_ARGUMENT;
+}
+
+// Validates a plain-path request exactly as the reference does, in the same
+// order and with the same messages.  Returns JSVD_OK or an error code.
+int validate_plain_request(const void *input, std::size_t rows, std::size_t columns, const jsvd_config &cfg);
+
+// Threads-per-block normalisation of the reference (kernels.cu:685-690):
+// clamp to [32, 1024] and round up to a multiple of 32.
+inline int normalize_threads_per_block(int raw)
+{
+    int c = raw < 32 ? 32 : (raw > 1024 ? 1024 : raw);
+    int a = ((c + 31) / 32) * 32;
+    return a > 1024 ? 1024 : a;
+}
+
+// Reduction width actually used: the largest power of two not above the
+// normalised thread count (identical to it for every power of two, which
+// includes the default 256).
+inline int reduction_lanes(int raw_threads)
+{
+    int t = normalize_threads_per_block(raw_threads);
+    int p = 32;
+    while (p * 2 <= t) p *= 2;
+    return p;
+}
+
+}  // namespace jsvd
+
+#define JSVD_CUDA_TRY(EXPR)                                                          \
+    do {                                                                             \
+        cudaError_t jsvd_status_ = (EXPR);                                           \
+        if (jsvd_status_ != cudaSuccess)                                             \
+            return ::jsvd::cuda_failure(jsvd_status_, #EXPR, __FILE__, __LINE__);    \
+    } while (0)

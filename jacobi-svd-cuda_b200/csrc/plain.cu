@@ -1,0 +1,479 @@
+// Plain FP64 one-sided Jacobi SVD for sm_100a: the drop-in for
+// jacobi::svd::one_sided_jacobi_svd (kleedaisuki/jacobi-svd-cuda
+// src/kernels.cu:844-1004, 1066-1076).
+//
+// Same arithmetic and cyclic round-robin order as the reference; different
+// execution:
+//   * A lives in a column-major working copy (lda = m), so every pair reads two
+//     contiguous columns with fully coalesced accesses.
+//   * One fused kernel per round: Gram dot products (fma chains over T virtual
+//     lanes + the reference's halving tree, warp shuffles for the in-warp
+//     levels), Rutishauser angle in registers, rotation of the register-held
+//     column tiles written back in place.  The reference needs three launches
+//     and three blocking host transfers per round.
+//   * V never sits on the round-to-round critical path.  Each round records
+//     its (c, s); after the sweep one row-parallel pass applies the whole
+//     sweep to V, rows held in shared memory.  Per element the sequence of
+//     rotations is the reference's, so V is bit-identical.
+//   * A sweep (n-1 round kernels + the V pass) is captured once into a CUDA
+//     graph per (device, m, n, T, eps) and replayed; the host reads one
+//     rotation counter per sweep.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.hpp"
+#include "plain.hpp"
+
+namespace jsvd {
+namespace {
+
+constexpr int kTile = 32;
+constexpr int kTileRows = 8;
+
+// row-major src (rows x cols) -> column-major dst (leading dimension ldd).
+__global__ void __launch_bounds__(kTile *kTileRows)
+    rowmajor_to_colmajor_kernel(const double *__restrict__ src, int rows, int cols, double *__restrict__ dst,
+                                long ldd)
+{
+    __shared__ double tile[kTile][kTile + 1];
+    const int c0 = blockIdx.x * kTile, r0 = blockIdx.y * kTile;
+    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[k][threadIdx.x] = src[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) dst[(size_t)c * ldd + r] = tile[threadIdx.x][k];
+    }
+}
+
+// column-major src (rows x cols, leading dimension lds) -> row-major dst.
+// With sigma != nullptr each column is divided by sigma[c], or zeroed when
+// sigma[c] <= eps (src/kernels.cu:622-627).
+__global__ void __launch_bounds__(kTile *kTileRows)
+    colmajor_to_rowmajor_kernel(const double *__restrict__ src, long lds, int rows, int cols,
+                                double *__restrict__ dst, const double *__restrict__ sigma, double eps)
+{
+    __shared__ double tile[kTile][kTile + 1];
+    const int r0 = blockIdx.x * kTile, c0 = blockIdx.y * kTile;
+    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) tile[k][threadIdx.x] = src[(size_t)c * lds + r];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) {
+            double val = tile[threadIdx.x][k];
+            if (sigma != nullptr) {
+                const double sg = sigma[c];
+                val = (sg > eps) ? (val / sg) : 0.0;
+            }
+            dst[(size_t)r * cols + c] = val;
+        }
+    }
+}
+
+__global__ void identity_colmajor_kernel(double *__restrict__ v, int n, long ldv)
+{
+    const size_t total = (size_t)n * ldv;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const size_t col = idx / ldv, row = idx % ldv;
+        v[idx] = (row == col) ? 1.0 : 0.0;
+    }
+}
+
+// Block-wide reference tree over T lanes for three quantities; result valid in
+// thread 0.  `red` holds 3*T doubles.
+template <int T>
+__device__ __forceinline__ void block_tree3(double &pp, double &qq, double &pq, double *red)
+{
+    if constexpr (T == 32) {
+        pp = warp_tree1(pp);
+        qq = warp_tree1(qq);
+        pq = warp_tree1(pq);
+    } else {
+        constexpr int W = T / 32;
+        const int t = threadIdx.x;
+        red[t] = pp;
+        red[T + t] = qq;
+        red[2 * T + t] = pq;
+        __syncthreads();
+        if (t < 32) {
+            double y[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) y[w] = red[w * 32 + t];
+            pp = warp_tree<W>(y);
+#pragma unroll
+            for (int w = 0; w < W; ++w) y[w] = red[T + w * 32 + t];
+            qq = warp_tree<W>(y);
+#pragma unroll
+            for (int w = 0; w < W; ++w) y[w] = red[2 * T + w * 32 + t];
+            pq = warp_tree<W>(y);
+        }
+    }
+}
+
+// One round of the sweep: blockIdx.x = pair slot.  T threads = T virtual
+// lanes; thread t owns rows t + k*T.  K > 0: the K row-tiles of both columns
+// stay in registers between the dot products and the rotation.  K == 0: the
+// columns are streamed twice (m > K_max * T).
+template <int T, int K>
+__global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, long lda, int m,
+                                                         const int2 *__restrict__ pairs,
+                                                         double2 *__restrict__ cs, double eps,
+                                                         unsigned *__restrict__ counter)
+{
+    __shared__ double red[T == 32 ? 1 : 3 * T];
+    __shared__ double2 rot;
+    const int t = threadIdx.x;
+    const int2 pq_idx = pairs[blockIdx.x];
+    double *__restrict__ ap = a + (size_t)pq_idx.x * lda;
+    double *__restrict__ aq = a + (size_t)pq_idx.y * lda;
+
+    double spp = 0.0, sqq = 0.0, spq = 0.0;
+    double xp[K > 0 ? K : 1], xq[K > 0 ? K : 1];
+    if constexpr (K > 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int r = t + k * T;
+            xp[k] = (r < m) ? ap[r] : 0.0;
+            xq[k] = (r < m) ? aq[r] : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (t + k * T < m) {
+                spp = fma(xp[k], xp[k], spp);
+                sqq = fma(xq[k], xq[k], sqq);
+                spq = fma(xp[k], xq[k], spq);
+            }
+        }
+    } else {
+        for (int r = t; r < m; r += T) {
+            const double x = ap[r], y = aq[r];
+            spp = fma(x, x, spp);
+            sqq = fma(y, y, sqq);
+            spq = fma(x, y, spq);
+        }
+    }
+    block_tree3<T>(spp, sqq, spq, red);
+    if (t == 0) {
+        double c, s;
+        const bool rotates = rotation_params(spp, sqq, spq, eps, c, s);
+        cs[blockIdx.x] = make_double2(c, s);
+        if (rotates) atomicAdd(counter, 1u);
+        rot = make_double2(c, s);
+    }
+    __syncthreads();
+    const double c = rot.x, s = rot.y;
+    if (c == 0.0) return;  // no rotation: columns unchanged
+    if constexpr (K > 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int r = t + k * T;
+            if (r < m) {
+                ap[r] = rot_p(c, s, xp[k], xq[k]);
+                aq[r] = rot_q(c, s, xp[k], xq[k]);
+            }
+        }
+    } else {
+        for (int r = t; r < m; r += T) {
+            const double x = ap[r], y = aq[r];
+            ap[r] = rot_p(c, s, x, y);
+            aq[r] = rot_q(c, s, x, y);
+        }
+    }
+}
+
+// Deferred V update: applies every rotation of one sweep to R rows of V.
+// V is column-major (element (row, col) at col*ldv + row); the CTA stages its
+// rows as sv[col*R + rr] in shared memory, so the round-to-round dependency
+// never leaves the SM.
+__global__ void __launch_bounds__(256) plain_vpass_kernel(double *__restrict__ v, long ldv, int n, int R,
+                                                          const int2 *__restrict__ pairs,
+                                                          const double2 *__restrict__ cs, int rounds, int npairs)
+{
+    extern __shared__ double sv[];
+    const int r0 = blockIdx.x * R;
+    const int rows = min(R, n - r0);
+    const int total = n * R;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int col = idx / R, rr = idx - col * R;
+        sv[idx] = (rr < rows) ? v[(size_t)col * ldv + r0 + rr] : 0.0;
+    }
+    __syncthreads();
+    const int items = npairs * R;
+    for (int r = 0; r < rounds; ++r) {
+        const double2 *__restrict__ csr = cs + (size_t)r * npairs;
+        const int2 *__restrict__ pr = pairs + (size_t)r * npairs;
+        for (int idx = threadIdx.x; idx < items; idx += blockDim.x) {
+            const int i = idx / R, rr = idx - i * R;
+            const double2 g = csr[i];
+            if (g.x != 0.0) {
+                const int2 pq = pr[i];
+                const double x = sv[pq.x * R + rr], y = sv[pq.y * R + rr];
+                sv[pq.x * R + rr] = rot_p(g.x, g.y, x, y);
+                sv[pq.y * R + rr] = rot_q(g.x, g.y, x, y);
+            }
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int col = idx / R, rr = idx - col * R;
+        if (rr < rows) v[(size_t)col * ldv + r0 + rr] = sv[idx];
+    }
+}
+
+// sigma_j = sqrt(max(||a_j||^2, 0)) with the reference's T-lane order
+// (src/kernels.cu:586-629).
+template <int T>
+__global__ void __launch_bounds__(T) plain_sigma_kernel(const double *__restrict__ a, long lda, int m,
+                                                        double *__restrict__ sigma)
+{
+    __shared__ double red[T == 32 ? 1 : T];
+    const int t = threadIdx.x;
+    const double *__restrict__ col = a + (size_t)blockIdx.x * lda;
+    double acc = 0.0;
+    for (int r = t; r < m; r += T) acc = fma(col[r], col[r], acc);
+    if constexpr (T == 32) {
+        acc = warp_tree1(acc);
+    } else {
+        constexpr int W = T / 32;
+        red[t] = acc;
+        __syncthreads();
+        if (t < 32) {
+            double y[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) y[w] = red[w * 32 + t];
+            acc = warp_tree<W>(y);
+        }
+    }
+    if (t == 0) sigma[blockIdx.x] = sqrt(fmax(acc, 0.0));
+}
+
+using RoundFn = void (*)(double *, long, int, const int2 *, double2 *, double, unsigned *);
+using SigmaFn = void (*)(const double *, long, int, double *);
+
+template <int T>
+RoundFn pick_round_t(int m)
+{
+    constexpr int kmax = T <= 256 ? 16 : (T == 512 ? 8 : 4);
+    if (m <= 1 * T) return plain_round_kernel<T, 1>;
+    if (m <= 2 * T) return plain_round_kernel<T, 2>;
+    if (m <= 4 * T) return plain_round_kernel<T, 4>;
+    if (kmax >= 8 && m <= 8 * T) return plain_round_kernel<T, (kmax >= 8 ? 8 : 4)>;
+    if (kmax >= 16 && m <= 16 * T) return plain_round_kernel<T, (kmax >= 16 ? 16 : 4)>;
+    return plain_round_kernel<T, 0>;
+}
+
+RoundFn pick_round(int T, int m)
+{
+    switch (T) {
+    case 32: return pick_round_t<32>(m);
+    case 64: return pick_round_t<64>(m);
+    case 128: return pick_round_t<128>(m);
+    case 256: return pick_round_t<256>(m);
+    case 512: return pick_round_t<512>(m);
+    default: return pick_round_t<1024>(m);
+    }
+}
+
+SigmaFn pick_sigma(int T)
+{
+    switch (T) {
+    case 32: return plain_sigma_kernel<32>;
+    case 64: return plain_sigma_kernel<64>;
+    case 128: return plain_sigma_kernel<128>;
+    case 256: return plain_sigma_kernel<256>;
+    case 512: return plain_sigma_kernel<512>;
+    default: return plain_sigma_kernel<1024>;
+    }
+}
+
+// Round-robin schedule, identical to src/kernels.cu:637-678 (fixed head,
+// dummy column for odd n, pair i = (circle[i], circle[ne-1-i])).  Every round
+// has the same number of real pairs, floor(n/2).
+void build_schedule(int n, std::vector<int2> &pairs, int &rounds, int &npairs)
+{
+    pairs.clear();
+    if (n < 2) {
+        rounds = 0;
+        npairs = 0;
+        return;
+    }
+    const int ne = (n % 2) ? n + 1 : n;
+    std::vector<int> circle(ne, -1);
+    for (int i = 0; i < n; ++i) circle[i] = i;
+    rounds = ne - 1;
+    npairs = n / 2;
+    pairs.reserve((size_t)rounds * npairs);
+    for (int r = 0; r < rounds; ++r) {
+        for (int i = 0; i < ne / 2; ++i) {
+            const int lhs = circle[i], rhs = circle[ne - 1 - i];
+            if (lhs >= 0 && rhs >= 0) pairs.push_back(make_int2(lhs, rhs));
+        }
+        const int last = circle[ne - 1];
+        for (int i = ne - 1; i > 1; --i) circle[i] = circle[i - 1];
+        circle[1] = last;
+    }
+}
+
+}  // namespace
+
+PlainStats &plain_stats()
+{
+    thread_local PlainStats stats;
+    return stats;
+}
+
+PlainPlan::~PlainPlan()
+{
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (device >= 0) cudaSetDevice(device);
+    if (sweep_exec) cudaGraphExecDestroy(sweep_exec);
+    for (cudaEvent_t e : {ev_round_begin, ev_round_end, ev_vpass_end})
+        if (e) cudaEventDestroy(e);
+    for (void *p : {(void *)a_w, (void *)v_w, (void *)pairs, (void *)cs, (void *)counter, (void *)d_in,
+                    (void *)d_u, (void *)d_sigma, (void *)d_v, (void *)sigma_w})
+        if (p) cudaFree(p);
+    if (h_counter) cudaFreeHost(h_counter);
+    if (prev >= 0) cudaSetDevice(prev);
+}
+
+int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaStream_t stream,
+                      std::unique_ptr<PlainPlan> &out)
+{
+    auto plan = std::make_unique<PlainPlan>();
+    plan->device = dev;
+    plan->m = m_;
+    plan->n = n_;
+    plan->T = T_;
+    plan->eps = eps_;
+    plan->lda = (long)m_;
+    plan->ldv = (long)n_;
+    std::vector<int2> host_pairs;
+    build_schedule((int)n_, host_pairs, plan->rounds, plan->npairs);
+    JSVD_CUDA_TRY(cudaMalloc(&plan->a_w, sizeof(double) * m_ * n_));
+    JSVD_CUDA_TRY(cudaMalloc(&plan->v_w, sizeof(double) * n_ * n_));
+    JSVD_CUDA_TRY(cudaMalloc(&plan->sigma_w, sizeof(double) * n_));
+    JSVD_CUDA_TRY(cudaMalloc(&plan->counter, sizeof(unsigned)));
+    JSVD_CUDA_TRY(cudaMallocHost(&plan->h_counter, sizeof(unsigned)));
+    if (plan->rounds > 0) {
+        const size_t np = (size_t)plan->rounds * plan->npairs;
+        JSVD_CUDA_TRY(cudaMalloc(&plan->pairs, sizeof(int2) * np));
+        JSVD_CUDA_TRY(cudaMalloc(&plan->cs, sizeof(double2) * np));
+        JSVD_CUDA_TRY(cudaMemcpyAsync(plan->pairs, host_pairs.data(), sizeof(int2) * np, cudaMemcpyHostToDevice,
+                                      stream));
+        // V pass geometry: enough CTAs to cover the SMs, rows capped by shared memory.
+        const size_t smem_cap = 200 * 1024;
+        int rmax = (int)std::max<size_t>(1, smem_cap / (sizeof(double) * n_));
+        int R = std::max(1, (int)(n_ / 128));
+        R = std::min(std::min(R, rmax), 16);
+        plan->vpass_rows = R;
+        plan->vpass_smem = (int)(sizeof(double) * n_ * R);
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(plain_vpass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           plan->vpass_smem));
+        // Capture one sweep.
+        RoundFn round_fn = pick_round(T_, (int)m_);
+        JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_begin));
+        JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_end));
+        JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_vpass_end));
+        cudaGraph_t graph = nullptr;
+        JSVD_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        JSVD_CUDA_TRY(cudaEventRecordWithFlags(plan->ev_round_begin, stream, cudaEventRecordExternal));
+        for (int r = 0; r < plan->rounds; ++r) {
+            const size_t off = (size_t)r * plan->npairs;
+            round_fn<<<plan->npairs, T_, 0, stream>>>(plan->a_w, plan->lda, (int)m_, plan->pairs + off,
+                                                      plan->cs + off, eps_, plan->counter);
+        }
+        JSVD_CUDA_TRY(cudaEventRecordWithFlags(plan->ev_round_end, stream, cudaEventRecordExternal));
+        const int vgrid = (int)((n_ + R - 1) / R);
+        plain_vpass_kernel<<<vgrid, 256, plan->vpass_smem, stream>>>(plan->v_w, plan->ldv, (int)n_, R, plan->pairs,
+                                                                    plan->cs, plan->rounds, plan->npairs);
+        JSVD_CUDA_TRY(cudaEventRecordWithFlags(plan->ev_vpass_end, stream, cudaEventRecordExternal));
+        cudaError_t cap = cudaStreamEndCapture(stream, &graph);
+        if (cap != cudaSuccess) return cuda_failure(cap, "cudaStreamEndCapture", __FILE__, __LINE__);
+        cudaError_t inst = cudaGraphInstantiate(&plan->sweep_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (inst != cudaSuccess) return cuda_failure(inst, "cudaGraphInstantiate", __FILE__, __LINE__);
+    }
+    plan->bytes = sizeof(double) * (m_ * n_ + n_ * n_ + n_) +
+                  (sizeof(int2) + sizeof(double2)) * (size_t)plan->rounds * plan->npairs;
+    out = std::move(plan);
+    return JSVD_OK;
+}
+
+int PlainPlan::ensure_host_staging()
+{
+    if (d_in) return JSVD_OK;
+    JSVD_CUDA_TRY(cudaMalloc(&d_in, sizeof(double) * m * n));
+    JSVD_CUDA_TRY(cudaMalloc(&d_u, sizeof(double) * m * n));
+    JSVD_CUDA_TRY(cudaMalloc(&d_sigma, sizeof(double) * n));
+    JSVD_CUDA_TRY(cudaMalloc(&d_v, sizeof(double) * n * n));
+    bytes += sizeof(double) * (2 * m * n + n + n * n);
+    return JSVD_OK;
+}
+
+int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *out_v, int max_sweeps, int *sweeps,
+                   cudaStream_t stream)
+{
+    const int im = (int)m, in = (int)n;
+    {
+        dim3 block(kTile, kTileRows);
+        dim3 grid((in + kTile - 1) / kTile, (im + kTile - 1) / kTile);
+        rowmajor_to_colmajor_kernel<<<grid, block, 0, stream>>>(d_a, im, in, a_w, lda);
+        JSVD_CUDA_TRY(cudaGetLastError());
+    }
+    identity_colmajor_kernel<<<std::min<size_t>(1184, (n * n + 255) / 256), 256, 0, stream>>>(v_w, in, ldv);
+    JSVD_CUDA_TRY(cudaGetLastError());
+
+    PlainStats &st = plain_stats();
+    int executed = 0;
+    if (rounds == 0) {
+        executed = 1;  // n == 1: one empty sweep, as the reference reports
+    } else {
+        for (int s = 0; s < max_sweeps; ++s) {
+            JSVD_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), stream));
+            JSVD_CUDA_TRY(cudaGraphLaunch(sweep_exec, stream));
+            JSVD_CUDA_TRY(cudaMemcpyAsync(h_counter, counter, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+            JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
+            executed = s + 1;
+            float r_ms = 0.f, v_ms = 0.f;
+            if (cudaEventElapsedTime(&r_ms, ev_round_begin, ev_round_end) == cudaSuccess) st.round_ms += r_ms;
+            if (cudaEventElapsedTime(&v_ms, ev_round_end, ev_vpass_end) == cudaSuccess) st.vpass_ms += v_ms;
+            st.round_launches += (unsigned long long)rounds;
+            st.vpass_launches += 1;
+            if (*h_counter == 0) break;
+        }
+    }
+    st.solves += 1;
+    st.sweeps += (unsigned long long)executed;
+    st.other_launches += 3 + (out_u ? 1 : 0) + (out_v ? 1 : 0);
+    double *sig = out_sigma ? out_sigma : sigma_w;
+    pick_sigma(T)<<<in, T, 0, stream>>>(a_w, lda, im, sig);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    dim3 block(kTile, kTileRows);
+    if (out_u) {
+        dim3 grid((im + kTile - 1) / kTile, (in + kTile - 1) / kTile);
+        colmajor_to_rowmajor_kernel<<<grid, block, 0, stream>>>(a_w, lda, im, in, out_u, sig, eps);
+        JSVD_CUDA_TRY(cudaGetLastError());
+    }
+    if (out_v) {
+        dim3 grid((in + kTile - 1) / kTile, (in + kTile - 1) / kTile);
+        colmajor_to_rowmajor_kernel<<<grid, block, 0, stream>>>(v_w, ldv, in, in, out_v, nullptr, 0.0);
+        JSVD_CUDA_TRY(cudaGetLastError());
+    }
+    if (sweeps) *sweeps = executed;
+    return JSVD_OK;
+}
+
+}  // namespace jsvd

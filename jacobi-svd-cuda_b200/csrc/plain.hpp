@@ -1,0 +1,63 @@
+// Host-side plan of the plain FP64 sweep: device workspace for one shape and
+// the captured sweep graph.  Plans are cached per thread (see abi.cu), so a
+// caller that solves many matrices of one shape pays for allocation and
+// graph instantiation once.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <memory>
+
+namespace jsvd {
+
+struct PlainPlan {
+    int device = -1;
+    size_t m = 0, n = 0;
+    int T = 256;
+    double eps = 0.0;
+    long lda = 0, ldv = 0;
+    int rounds = 0, npairs = 0;
+    int vpass_rows = 1, vpass_smem = 0;
+    size_t bytes = 0;
+
+    double *a_w = nullptr;      // column-major working copy of A (m x n)
+    double *v_w = nullptr;      // column-major V (n x n)
+    double *sigma_w = nullptr;  // sigma when the caller does not want it
+    int2 *pairs = nullptr;      // rounds x npairs schedule
+    double2 *cs = nullptr;      // (c, s) of every pair of the current sweep
+    unsigned *counter = nullptr;
+    unsigned *h_counter = nullptr;  // pinned
+    // staging for host-buffer calls
+    double *d_in = nullptr, *d_u = nullptr, *d_sigma = nullptr, *d_v = nullptr;
+
+    cudaGraphExec_t sweep_exec = nullptr;
+    // Event-record nodes inside the sweep graph: before the first round,
+    // after the last round, after the V pass (live kernel timing).
+    cudaEvent_t ev_round_begin = nullptr, ev_round_end = nullptr, ev_vpass_end = nullptr;
+
+    PlainPlan() = default;
+    ~PlainPlan();
+    PlainPlan(const PlainPlan &) = delete;
+    PlainPlan &operator=(const PlainPlan &) = delete;
+
+    static int create(int dev, size_t m, size_t n, int T, double eps, cudaStream_t stream,
+                      std::unique_ptr<PlainPlan> &out);
+    int ensure_host_staging();
+    // Runs the whole solve on device buffers; outputs may be null.
+    int run(const double *d_a, double *out_u, double *out_sigma, double *out_v, int max_sweeps, int *sweeps,
+            cudaStream_t stream);
+};
+
+// Cumulative per-thread counters of the plain path (jsvd_plain_stats).
+struct PlainStats {
+    unsigned long long solves = 0, sweeps = 0, round_launches = 0, vpass_launches = 0, other_launches = 0;
+    double round_ms = 0.0, vpass_ms = 0.0;
+};
+PlainStats &plain_stats();
+
+// Per-thread plan cache and stream.
+int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t stream, PlainPlan **plan);
+cudaStream_t thread_stream(int device);
+
+}  // namespace jsvd

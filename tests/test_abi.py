@@ -1,0 +1,82 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol
+declared in include/jsvd.h, and rejects invalid requests with the reference's
+messages (validation runs before any CUDA call)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import jsvd
+from conftest import ROOT
+
+
+def _declared_functions():
+    names = []
+    for hdr in ("jsvd.h",):
+        text = open(os.path.join(ROOT, "include", hdr)).read()
+        names += re.findall(r"^\s*(?:const\s+)?\w[\w\s\*]*?\b(jsvd_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_loads_and_exports_declared_symbols():
+    lib = jsvd.lib()
+    declared = _declared_functions()
+    assert len(declared) >= 8
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in include/jsvd.h but not exported"
+    assert set(jsvd.exported_symbols()) <= set(declared)
+
+
+def test_version_and_variant():
+    assert b"sm_100a" in jsvd.lib().jsvd_version()
+    assert jsvd.arith_variant() in (5, 9, 6, 10, 0, 1, 2, 4, 8)
+
+
+def test_default_config_matches_reference():
+    c = jsvd.default_config()
+    assert c.epsilon == 1e-9 and c.max_sweeps == 128 and c.threads_per_block == 256
+    assert c.layout_transpose_mode == jsvd.LAYOUT_AUTO
+    assert c.layout_transpose_min_columns == 16 and c.layout_transpose_min_elements == 4096
+    assert c.layout_transpose_auto_tune == 0
+    assert c.layout_transpose_benchmark_repetitions == 2 and c.layout_transpose_benchmark_sweeps == 8
+
+
+@pytest.mark.parametrize(
+    "shape,overrides,message",
+    [
+        ((0, 3), {}, "Input matrix shape must be non-zero."),
+        ((3, 0), {}, "Input matrix shape must be non-zero."),
+        ((2, 3), {}, "One-sided Jacobi SVD requires rows >= columns in this implementation."),
+        ((4, 3), {"epsilon": 0.0}, "epsilon must be positive."),
+        ((4, 3), {"epsilon": -1.0}, "epsilon must be positive."),
+        ((4, 3), {"max_sweeps": 0}, "max_sweeps must be positive."),
+        ((4, 3), {"layout_transpose_min_columns": 0}, "layout_transpose_min_columns must be positive."),
+        ((4, 3), {"layout_transpose_min_elements": 0}, "layout_transpose_min_elements must be positive."),
+        ((4, 3), {"layout_transpose_benchmark_repetitions": 0},
+         "layout_transpose_benchmark_repetitions must be positive."),
+        ((4, 3), {"layout_transpose_benchmark_sweeps": 0}, "layout_transpose_benchmark_sweeps must be positive."),
+    ],
+)
+def test_invalid_arguments(shape, overrides, message):
+    cfg = jsvd.default_config(**overrides)
+    m, n = shape
+    buf = np.zeros(max(1, m * n))
+    rc = jsvd.lib().jsvd_plain_svd(buf.ctypes.data, m, n, ctypes.byref(cfg), None, None, None, None)
+    assert rc == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    code, msg = jsvd.last_error()
+    assert code == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert msg == message
+
+
+def test_null_input_is_rejected():
+    cfg = jsvd.default_config()
+    rc = jsvd.lib().jsvd_plain_svd(None, 4, 3, ctypes.byref(cfg), None, None, None, None)
+    assert rc == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == "Input buffer size mismatch."
+
+
+def test_python_wrapper_raises_invalid_argument():
+    with pytest.raises(jsvd.InvalidArgument, match="rows >= columns"):
+        jsvd.plain_svd(np.zeros((2, 5)))

@@ -1,0 +1,122 @@
+"""Oracle checks that need no GPU: schedule invariants, agreement with LAPACK,
+thread invariance, and (when present) the reference's own golden outputs."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import workloads as W
+from conftest import GOLDEN, golden_input
+
+
+@pytest.mark.parametrize("n", list(range(1, 34)) + [64, 127, 128])
+def test_schedule_covers_every_pair_once(n):
+    rounds = O.schedule(n)
+    if n < 2:
+        assert rounds == []
+        return
+    ne = n + (n % 2)
+    assert len(rounds) == ne - 1
+    seen = set()
+    for pairs in rounds:
+        assert len(pairs) == n // 2
+        cols = [c for pq in pairs for c in pq]
+        assert len(cols) == len(set(cols)), "pairs of a round must be disjoint"
+        for p, q in pairs:
+            key = (min(p, q), max(p, q))
+            assert key not in seen
+            seen.add(key)
+    assert len(seen) == n * (n - 1) // 2
+
+
+def test_schedule_orientation_first_rounds():
+    # Round 0 pairs (i, ne-1-i); round 1 after one rotation of circle[1:]
+    # (kernels.cu:661-674): circle = [0, 5, 1, 2, 3, 4] for n = 6.
+    r = O.schedule(6)
+    assert r[0] == [(0, 5), (1, 4), (2, 3)]
+    assert r[1] == [(0, 4), (5, 3), (1, 2)]
+    # odd n: dummy column -1 occupies the last slot, its pair is dropped
+    r5 = O.schedule(5)
+    assert r5[0] == [(1, 4), (2, 3)]
+
+
+@pytest.mark.parametrize("m,n", [(1, 1), (2, 2), (3, 2), (9, 9), (20, 7), (64, 33), (150, 150)])
+def test_oracle_matches_lapack(m, n):
+    a = W.gaussian_splitmix(m, n, seed=100 + m + n)
+    u, s, v, sw = O.plain_svd(a, eps=1e-14, threads=2)
+    ref = np.linalg.svd(a, compute_uv=False)
+    err = O.sigma_errors(s, ref)
+    assert err["max_rel"] <= 1e-13 * n
+    r = O.residuals(a, u, s, v)
+    assert r["rho_A"] < 1e-13 * max(1, n)
+    assert r["rho_V"] < 1e-13 * max(1, n)
+    assert 1 <= sw < 128
+
+
+def test_oracle_thread_invariance():
+    a = W.gaussian_splitmix(80, 40, seed=5)
+    r1 = O.plain_svd(a, eps=1e-13, threads=1)
+    r4 = O.plain_svd(a, eps=1e-13, threads=4)
+    for x, y in zip(r1[:3], r4[:3]):
+        assert np.array_equal(x, y)
+    assert r1[3] == r4[3]
+
+
+def test_oracle_unsorted_sigma_and_eps_cut():
+    # U columns are zeroed when sigma <= eps (absolute cut, kernels.cu:622-627)
+    a = W.gaussian_splitmix(30, 10, seed=9)
+    a[:, 4] = 0.0
+    u, s, v, _ = O.plain_svd(a, eps=1e-12)
+    k = int(np.argmin(s))
+    assert s[k] == 0.0
+    assert np.all(u[:, k] == 0.0)
+
+
+def test_identity_converges_in_one_sweep():
+    u, s, v, sw = O.plain_svd(np.eye(12), eps=1e-9)
+    assert sw == 1
+    assert np.array_equal(s, np.ones(12))
+    assert np.array_equal(v, np.eye(12))
+
+
+def _golden_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def _summary():
+    p = os.path.join(GOLDEN, "summary.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
+
+
+def test_golden_fixtures_present():
+    assert _summary() is not None, "tests/golden/summary.json missing (run tests/golden/make_golden.py on a GPU)"
+    assert len(_golden_cases()) >= 10
+
+
+@pytest.mark.parametrize("path", _golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_reproduces_reference_outputs(path):
+    """The oracle under the pinned FMA variant reproduces the reference's own
+    outputs bit for bit (small cases keep full U/V; large ones SHA-256)."""
+    summ = _summary()
+    name = os.path.basename(path)[:-4]
+    rec = summ["cases"][name]
+    variant = summ["pinned_variant"]
+    g = np.load(path)
+    a = golden_input(name, g)
+    u, s, v, sw = O.plain_svd(a, eps=float(g["eps"]), lanes=int(g["T"]), variant=O.VARIANTS[variant],
+                              threads=os.cpu_count() or 1)
+    assert sw == int(g["sweeps"])
+    assert np.array_equal(s, g["sigma"])
+    if "u" in g:
+        assert np.array_equal(u, g["u"])
+        assert np.array_equal(v, g["v"])
+    else:
+        import hashlib
+        assert hashlib.sha256(u.tobytes()).hexdigest() == rec["u_sha256"]
+        assert hashlib.sha256(v.tobytes()).hexdigest() == rec["v_sha256"]
