@@ -92,6 +92,26 @@ int jsvd_plain_svd_device(const double *d_a, size_t rows, size_t columns, const 
                           double *d_sigma, double *d_v, int *sweeps, void *stream);
 
 /*
+ * Allocation-free variant of jsvd_plain_svd_device.  It has no counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc once they
+ * are running (a framework that reserved the device for its own pool,
+ * latency-critical code that cannot afford the device synchronisation of
+ * cudaMalloc/cudaFree, plugin hosts that forbid device allocation).
+ * It allocates nothing: the caller passes device buffers for A, U, sigma and
+ * V (U, sigma, V may be NULL), work runs on `stream` as given (NULL = the
+ * legacy default stream), and the working copies live in one fixed 16 MiB
+ * device array inside the library, so rows*columns + columns*columns +
+ * columns + 1 must not exceed 2097152 (larger requests fail with
+ * JSVD_ERR_INVALID_ARGUMENT).  That array is held by every GPU that loads the
+ * library until exit and is shared by all calls: calls that overlap on the GPU
+ * race and must be serialised by the caller.  The first call on a device looks
+ * up the array's device address; make it before any stream capture begins.
+ * Results are bit-identical to jsvd_plain_svd_device.
+ */
+int jsvd_plain_svd_noalloc(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,
+                           double *d_sigma, double *d_v, int *sweeps, void *stream);
+
+/*
  * Replaces jacobi::svd::auto_tune_layout_transpose_threshold
  * (include/kernels.hpp:306-307, src/kernels.cu:1078-1126): scans
  * n in {8,12,16,24,32,48,64,96}, m = 2n, on the reference's deterministic
