@@ -36,7 +36,7 @@ FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # Sweep counts of the plain path on the seeded inputs (identical in the oracle,
 # which reproduces the GPU arithmetic bit for bit); used to extrapolate the
 # bounded CPU samples to whole SVDs.
-PLAIN_SWEEPS = {"tall": 12, "square512": 11}
+PLAIN_SWEEPS = {"tall": 30, "square512": 14}
 
 
 def peaks():
@@ -274,7 +274,155 @@ def cpu_baseline(wl, sweeps: int, budget_s: float = 12.0, threads: int | None = 
                       f"({dt:.1f} s), extrapolated x{rounds_total / r:.2f} rounds x {sweeps} sweeps"}
 
 
+BATCH_COUNT = 20000
+
+
+def batch_flops(rows, cols, sweeps) -> float:
+    """Nominal FP64 flops: sweeps * P * (12 m + 6 n) per matrix, P = n(n-1)/2
+    (every pair counted as rotating)."""
+    m = rows.astype(np.float64)
+    n = cols.astype(np.float64)
+    return float(np.sum(sweeps.astype(np.float64) * n * (n - 1) / 2 * (12 * m + 6 * n)))
+
+
+def run_batch(args, rank: int, world: int, device):
+    import torch
+    import jsvd
+    import workloads as W
+
+    t0 = time.time()
+    mats = W.batch_workload_torch(args.batch_count, seed=3, device=device)
+    gen_s = time.time() - t0
+    cfg = jsvd.default_config(epsilon=1e-14)
+    b = jsvd.DeviceBatch(mats, device, f32=True, want_u=False, want_v=True)
+    fp64_peak = jsvd.probe_fp64_tflops()
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    torch.cuda.synchronize(device)
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
+    for _ in range(args.warmup):
+        b.solve(cfg, stream=stream.cuda_stream)
+    jsvd.batch_stats_reset()
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    sampler.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.solve(cfg, stream=stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    st = jsvd.batch_stats()
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps * b.count / (total_ms / 1e3)
+    flops = batch_flops(b.rows, b.cols, b.sweeps)
+    kernel_ms = st.kernel_ms / max(1, st.calls)
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+
+    # e2e: pinned FP32 input H2D + solve + D2H of sigma and V, every step
+    host_in = b.host_a.pin_memory()
+    host_s = torch.empty(b.sigma.shape, dtype=torch.float64).pin_memory()
+    host_v = torch.empty(b.v.shape, dtype=torch.float64).pin_memory()
+    e2e_s = 0.0
+    for i in range(args.steps + 1):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        t1 = time.perf_counter()
+        b.a.copy_(host_in, non_blocking=True)
+        b.solve(cfg, stream=stream.cuda_stream)
+        host_s.copy_(b.sigma, non_blocking=True)
+        host_v.copy_(b.v, non_blocking=True)
+        torch.cuda.synchronize(device)
+        if i > 0:
+            e2e_s += time.perf_counter() - t1
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    line = {
+        "metric": "SVDs/s",
+        "value": value,
+        "unit": "SVD/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"{b.count} FP32-stored matrices, m~U{{16..256}}, n~U{{8..m}}, Haar U,V, sigma "
+                               f"log-uniform [1/kappa,1], kappa log-uniform [1e1,1e6] (seed 3); sigma and V",
+                   "path": "batched persistent kernels (one CTA per matrix, plain arithmetic)",
+                   "epsilon": 1e-14, "mean_sweeps": float(np.mean(b.sweeps)),
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "generation_s": gen_s},
+        "e2e": {"value": world * args.steps * b.count / e2e_s, "unit": "SVD/s", "h2d_bytes_per_step": b.h2d_bytes,
+                "d2h_bytes_per_step": int((b.sigma.numel() + b.v.numel()) * 8),
+                "timer": "host wall clock around H2D + solve + D2H"},
+        "gpu_launches": int(st.launches),
+        "roofline": {"bound": "fp64", "kernel": "batch_kernel", "achieved": achieved, "peak": fp64_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                     "peak_kind": "measured FP64 FMA probe (jsvd_probe_fp64_tflops)",
+                     "traffic": None, "flops_per_launch_set": flops,
+                     "flop_model": "sweeps * n(n-1)/2 * (12m + 6n) per matrix"},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = batch_cpu_baseline(mats, budget_s=args.cpu_budget)
+    return line
+
+
+def batch_cpu_baseline(mats, budget_s: float = 10.0, threads: int | None = None) -> dict:
+    """Oracle on the host cores, threads across matrices, on the first
+    matrices of the same batch until the time budget is used."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    threads = threads or os.cpu_count() or 1
+    done, t_used, k = 0, 0.0, 0
+    chunk = max(threads, 16)
+    while t_used < budget_s and k < len(mats):
+        part = [a.astype(np.float64) for a in mats[k: k + chunk]]
+        t0 = time.perf_counter()
+        O.batch_svd(part, eps=1e-14, threads=threads)
+        t_used += time.perf_counter() - t0
+        done += len(part)
+        k += chunk
+    return {"value": done / t_used, "unit": "SVD/s", "cores": threads, "kind": "port",
+            "sample": f"first {done} of {len(mats)} matrices of the same batch ({t_used:.1f} s), oracle, "
+                      f"one matrix per thread"}
+
+
 def run_reference(args):
+    if args.workload == "batch":
+        import workloads as W
+        mats = W.batch_workload(min(args.batch_count, 400), seed=3)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            cb = batch_cpu_baseline(mats, budget_s=args.cpu_budget)
+            if i >= args.warmup:
+                vals.append(cb["value"])
+        value = statistics.mean(vals)
+        cb["value"] = value
+        return {"impl": "reference", "metric": "SVDs/s", "value": value, "unit": "SVD/s", "n_gpus": 0,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": {"workload": "batch (FP32-stored, m~U{16..256}, n~U{8..m}), sample of the same "
+                                       "distribution", "path": "FP64 host oracle"},
+                "cpu_baseline": cb,
+                "e2e": {"value": value, "unit": "SVD/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     wl = make_workload(args.workload)
     m, n = wl["a"].shape
     sweeps = PLAIN_SWEEPS.get(wl["name"], 12)
@@ -316,6 +464,7 @@ def main():
     ap.add_argument("--path", default="auto")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -335,7 +484,10 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        line = run_ours(args, rank, world, device)
+        if args.workload == "batch":
+            line = run_batch(args, rank, world, device)
+        else:
+            line = run_ours(args, rank, world, device)
     finally:
         if world > 1:
             torch.distributed.barrier()

@@ -135,6 +135,94 @@ typedef struct jsvd_plain_stats {
 void jsvd_plain_stats_get(jsvd_plain_stats *out);
 void jsvd_plain_stats_reset(void);
 
+/* ---- batched solver ---------------------------------------------------------
+ * Many independent matrices in one persistent launch per size class.  The
+ * reference solves them one call at a time from a host thread pool
+ * (src/pipeline.cpp:799-807 -> one_sided_jacobi_svd); this replaces that loop
+ * for matrices that are all resident on the device.  Arithmetic per matrix is
+ * the plain path's (T = 256 reduction order), so each result is bit-identical
+ * to jsvd_plain_svd on the FP64-promoted input. */
+
+/* Launch shape of one size class: 0 keeps the built-in choice. */
+typedef struct jsvd_batch_tuning {
+    int threads;     /* threads per CTA (multiple of 32, <= 512) */
+    int ctas_per_sm; /* persistent CTAs per SM (shared-memory classes) */
+} jsvd_batch_tuning;
+
+/*
+ * count matrices; matrix i is rows[i] x cols[i] (rows >= cols >= 1), row-major
+ * at element offset a_offsets[i] of d_a (FP32 when a_is_f32, else FP64).
+ * Outputs are packed in input order: d_sigma gets cols[i] values per matrix,
+ * d_v (optional) cols[i]^2 row-major, d_u (optional) rows[i]*cols[i]
+ * row-major; sweeps (host, optional) the sweep count of each matrix.  cfg's
+ * epsilon and max_sweeps apply (threads_per_block must be 256).  tuning may
+ * be NULL or point to 4 entries for the first four size classes (A and V in
+ * <=48 KiB, <=100 KiB, <=~226 KiB of shared memory; A alone in shared
+ * memory); the fifth class (A and V in global memory) keeps its defaults.
+ * Synchronous on `stream` (NULL = library stream, ordered after the legacy
+ * default stream).
+ */
+int jsvd_batch_svd_device(int count, const int *rows, const int *cols, const long long *a_offsets, const void *d_a,
+                          int a_is_f32, const jsvd_config *cfg, double *d_sigma, double *d_v, double *d_u,
+                          int *sweeps, const jsvd_batch_tuning *tuning, void *stream);
+
+/* Cumulative counters of the batched solver on the calling thread. */
+typedef struct jsvd_batch_stats {
+    unsigned long long calls;
+    unsigned long long launches;
+    unsigned long long matrices;
+    unsigned long long sweeps;
+    double kernel_ms; /* device time of the persistent launches (events) */
+    unsigned long long class_count[5]; /* matrices per size class */
+} jsvd_batch_stats;
+
+void jsvd_batch_stats_get(jsvd_batch_stats *out);
+void jsvd_batch_stats_reset(void);
+
+/* ---- serving loop -----------------------------------------------------------
+ * Continuous batching of SVD requests on the current device.  Replaces the
+ * reference's thread-pool dispatch of one_sided_jacobi_svd per testcase
+ * (src/pipeline.cpp:234-394, 754-863): requests are admitted against a
+ * device-memory budget, small ones are gathered into batched launches while
+ * earlier batches run, large ones run concurrently on worker streams.  Results
+ * do not depend on what else is in flight (every path keeps the plain
+ * arithmetic). */
+
+typedef struct jsvd_server jsvd_server;
+
+typedef struct jsvd_server_options {
+    size_t device_budget_bytes; /* admission budget (0 = 40 GiB)                    */
+    int small_workers;          /* concurrent batched launches (0 = 2)             */
+    int large_workers;          /* concurrent large solves, one stream each (0 = 4) */
+    int max_batch;              /* requests per batched launch (0 = 4096)           */
+    jsvd_config cfg;            /* epsilon, max_sweeps, threads_per_block           */
+} jsvd_server_options;
+
+typedef struct jsvd_server_stats {
+    unsigned long long submitted, completed, failed;
+    unsigned long long batches, batched_requests, large_solves;
+    double p50_ms, p99_ms, mean_ms; /* submit-to-completion latency */
+    size_t peak_device_bytes, device_bytes_in_use;
+} jsvd_server_stats;
+
+void jsvd_server_options_default(jsvd_server_options *opt);
+int jsvd_server_create(const jsvd_server_options *opt, jsvd_server **out);
+/* Copies A (row-major m x n, m >= n) and queues it; JSVD_ERR_BUDGET when its
+ * footprint exceeds the whole budget. */
+int jsvd_server_submit(jsvd_server *s, const double *a, size_t rows, size_t columns, int want_u, uint64_t *ticket);
+/* Blocks until the request is done and copies its results (row-major U if
+ * requested at submit, sigma, row-major V); each ticket can be collected once. */
+int jsvd_server_wait(jsvd_server *s, uint64_t ticket, double *u, double *sigma, double *v, int *sweeps,
+                     double *latency_ms);
+int jsvd_server_get_stats(jsvd_server *s, jsvd_server_stats *out);
+/* Stops the workers; requests still queued are dropped. */
+void jsvd_server_destroy(jsvd_server *s);
+
+/* Measured FP64 FMA throughput of the current device in TFLOP/s (eight
+ * independent FMA chains per thread, best of 5 launches): the roofline
+ * denominator of the FP64-bound kernels. */
+int jsvd_probe_fp64_tflops(double *tflops);
+
 /* Releases the calling thread's cached device workspaces and graphs. */
 void jsvd_release_thread_cache(void);
 

@@ -82,8 +82,13 @@ int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t strea
             return JSVD_OK;
         }
     }
+    // Plans allocate and release on the library's own per-thread stream (a
+    // caller's stream may be destroyed before the plan is evicted).
+    cudaStream_t own = thread_stream(dev);
+    if (own == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+    if (own != stream) JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
     std::unique_ptr<PlainPlan> plan;
-    int rc = PlainPlan::create(dev, m, n, T, eps, stream, plan);
+    int rc = PlainPlan::create(dev, m, n, T, eps, own, plan);
     if (rc != JSVD_OK) return rc;
     plans.push_back(std::move(plan));
     size_t total = 0;

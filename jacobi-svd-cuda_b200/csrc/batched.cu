@@ -1,0 +1,477 @@
+// Batched one-sided Jacobi SVD: thousands of independent small matrices,
+// one persistent launch per size class, the classes running concurrently on
+// their own streams (sm_100a).
+//
+// Each CTA pulls matrix indices from a device work queue (one atomic counter
+// per class; matrices sorted by work, largest first) and solves the whole
+// matrix before taking the next one.  Where the FP64 working copies live
+// depends on the class:
+//   class 0-2: A and V in shared memory (<= 48 KiB, <= 100 KiB, <= ~226 KiB)
+//   class 3  : A in shared memory, V in a per-CTA slice of global memory
+//   class 4  : A and V in global memory (L2-resident per-CTA slices)
+// Each round runs in three phases separated by __syncthreads:
+//   1. one warp per pair: the three dot products, reduced in the reference's
+//      order (T = 256 virtual lanes; lane l holds virtual lanes l + 32j, then
+//      the halving tree) - so every matrix is bit-identical to the plain path
+//      and to the oracle on the same (FP64-promoted) input;
+//   2. one thread per pair: the rotation angle (the long sqrt/div chain runs
+//      for all pairs of the round in parallel instead of serially per warp);
+//   3. one warp per pair: rotation of the A and V columns.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "batched.hpp"
+#include "common.cuh"
+#include "internal.hpp"
+#include "plain.hpp"
+
+namespace jsvd {
+namespace {
+
+constexpr int kLanes = 256;      // reduction width T (reference default)
+constexpr int kW = kLanes / 32;  // virtual lanes per physical lane
+constexpr int kClasses = 5;
+
+// Closed-form pair k of round r (fixed-head circle, reference
+// src/kernels.cu:637-678).
+__device__ __forceinline__ int2 batch_pair(int n, int r, int k)
+{
+    const int ne = n + (n & 1);
+    const int L = ne - 1;
+    int i = k;
+    if (n & 1) {
+        const int j = 1 + ((n - 1 + r) % L);
+        const int slot = j < ne / 2 ? j : ne - 1 - j;
+        if (i >= slot) i += 1;
+    }
+    const int i2 = ne - 1 - i;
+    const int p = i == 0 ? 0 : 1 + ((i - 1 - r) % L + L) % L;
+    const int q = 1 + ((i2 - 1 - r) % L + L) % L;
+    return make_int2(p, q);
+}
+
+// Reference-order dot products of columns x, y (length m) by one warp; the
+// totals are valid in lane 0.
+__device__ __forceinline__ void warp_pair_stats(const double *x, const double *y, int m, int lane, double &pp,
+                                                double &qq, double &pq)
+{
+    double app[kW], aqq[kW], apq[kW];
+#pragma unroll
+    for (int j = 0; j < kW; ++j) app[j] = aqq[j] = apq[j] = 0.0;
+    for (int base = 0; base < m; base += kLanes) {
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            const int r = base + 32 * j + lane;
+            if (r < m) {
+                const double a = x[r], b = y[r];
+                app[j] = fma(a, a, app[j]);
+                aqq[j] = fma(b, b, aqq[j]);
+                apq[j] = fma(a, b, apq[j]);
+            }
+        }
+    }
+    pp = warp_tree<kW>(app);
+    qq = warp_tree<kW>(aqq);
+    pq = warp_tree<kW>(apq);
+}
+
+__device__ __forceinline__ double warp_norm2(const double *x, int m, int lane)
+{
+    double acc[kW];
+#pragma unroll
+    for (int j = 0; j < kW; ++j) acc[j] = 0.0;
+    for (int base = 0; base < m; base += kLanes) {
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            const int r = base + 32 * j + lane;
+            if (r < m) acc[j] = fma(x[r], x[r], acc[j]);
+        }
+    }
+    return __shfl_sync(0xffffffffu, warp_tree<kW>(acc), 0);
+}
+
+// Per-round scratch (pair statistics and angles): `half` is n/2 rounded up to
+// an even count so the double2 angle array starts on a 16-byte boundary.
+__host__ __device__ constexpr int round_half(int n) { return (n / 2 + 2) & ~1; }
+__host__ __device__ constexpr size_t round_scratch_doubles(int n) { return (size_t)5 * round_half(n); }
+
+template <bool kAShared, bool kVShared>
+__global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict__ descs, int count,
+                                                    int *__restrict__ next, const void *__restrict__ a_all,
+                                                    int a_is_f32, double eps, int max_sweeps,
+                                                    double *__restrict__ sigma_all, double *__restrict__ v_all,
+                                                    double *__restrict__ u_all, int *__restrict__ sweeps_all,
+                                                    double *__restrict__ workspace, size_t ws_stride)
+{
+    extern __shared__ double smem[];
+    __shared__ int s_idx;
+    __shared__ int s_rot;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double *gws = workspace + (size_t)blockIdx.x * ws_stride;
+    for (;;) {
+        if (threadIdx.x == 0) s_idx = atomicAdd(next, 1);
+        __syncthreads();
+        const int idx = s_idx;
+        if (idx >= count) return;
+        const BatchDesc d = descs[idx];
+        const int m = d.m, n = d.n;
+        const int half = round_half(n);
+        // smem layout: [round scratch 5*half][A if shared][V if shared]
+        double *st_pp = smem, *st_qq = smem + half, *st_pq = smem + 2 * half;
+        double2 *st_cs = reinterpret_cast<double2 *>(smem + 3 * half);  // 2*half doubles, 16-byte aligned
+        double *sm_rest = smem + round_scratch_doubles(n);
+        double *A = kAShared ? sm_rest : gws;
+        double *V = kVShared ? (kAShared ? sm_rest + (size_t)m * n : gws + (size_t)m * n)
+                             : (kAShared ? gws : gws + (size_t)m * n);
+        const size_t mn = (size_t)m * n;
+        if (a_is_f32) {
+            const float *src = reinterpret_cast<const float *>(a_all) + d.a_off;
+            for (size_t e = threadIdx.x; e < mn; e += blockDim.x) {
+                const size_t r = e / n, c = e - r * n;
+                A[c * m + r] = (double)src[e];
+            }
+        } else {
+            const double *src = reinterpret_cast<const double *>(a_all) + d.a_off;
+            for (size_t e = threadIdx.x; e < mn; e += blockDim.x) {
+                const size_t r = e / n, c = e - r * n;
+                A[c * m + r] = src[e];
+            }
+        }
+        for (size_t e = threadIdx.x; e < (size_t)n * n; e += blockDim.x) V[e] = (e / n == e % n) ? 1.0 : 0.0;
+        if (threadIdx.x == 0) s_rot = 0;
+        __syncthreads();
+        const int ne = n + (n & 1);
+        const int rounds = n >= 2 ? ne - 1 : 0;
+        const int npairs = n / 2;
+        int sweeps = 1;
+        if (rounds > 0) {
+            for (int sw = 0; sw < max_sweeps; ++sw) {
+                for (int r = 0; r < rounds; ++r) {
+                    // phase 1: dot products, one warp per pair
+                    for (int k = warp; k < npairs; k += nwarps) {
+                        const int2 pq = batch_pair(n, r, k);
+                        double pp, qq, pqv;
+                        warp_pair_stats(A + (size_t)pq.x * m, A + (size_t)pq.y * m, m, lane, pp, qq, pqv);
+                        if (lane == 0) {
+                            st_pp[k] = pp;
+                            st_qq[k] = qq;
+                            st_pq[k] = pqv;
+                        }
+                    }
+                    __syncthreads();
+                    // phase 2: angles, one thread per pair
+                    for (int k = threadIdx.x; k < npairs; k += blockDim.x) {
+                        double c, s;
+                        if (rotation_params(st_pp[k], st_qq[k], st_pq[k], eps, c, s)) s_rot = 1;
+                        st_cs[k] = make_double2(c, s);
+                    }
+                    __syncthreads();
+                    // phase 3: rotations, one warp per pair
+                    for (int k = warp; k < npairs; k += nwarps) {
+                        const double2 g = st_cs[k];
+                        if (g.x == 0.0) continue;
+                        const int2 pq = batch_pair(n, r, k);
+                        double *x = A + (size_t)pq.x * m, *y = A + (size_t)pq.y * m;
+                        for (int i = lane; i < m; i += 32) {
+                            const double a = x[i], b = y[i];
+                            x[i] = rot_p(g.x, g.y, a, b);
+                            y[i] = rot_q(g.x, g.y, a, b);
+                        }
+                        double *vx = V + (size_t)pq.x * n, *vy = V + (size_t)pq.y * n;
+                        for (int i = lane; i < n; i += 32) {
+                            const double a = vx[i], b = vy[i];
+                            vx[i] = rot_p(g.x, g.y, a, b);
+                            vy[i] = rot_q(g.x, g.y, a, b);
+                        }
+                    }
+                    __syncthreads();
+                }
+                const bool any = s_rot != 0;
+                __syncthreads();  // every thread has read the flag before it is reset
+                if (threadIdx.x == 0) s_rot = 0;
+                sweeps = sw + 1;
+                if (!any) break;
+            }
+        }
+        // sigma, U (optional), V (row-major)
+        double *sg = sigma_all + d.s_off;
+        for (int c = warp; c < n; c += nwarps) {
+            const double *x = A + (size_t)c * m;
+            const double sc = sqrt(fmax(warp_norm2(x, m, lane), 0.0));
+            if (lane == 0) sg[c] = sc;
+            if (u_all != nullptr) {
+                double *u = u_all + d.u_off;
+                for (int i = lane; i < m; i += 32) u[(size_t)i * n + c] = (sc > eps) ? (x[i] / sc) : 0.0;
+            }
+        }
+        if (v_all != nullptr) {
+            double *vo = v_all + d.v_off;
+            for (size_t e = threadIdx.x; e < (size_t)n * n; e += blockDim.x) {
+                const size_t r = e / n, c = e - r * n;
+                vo[e] = V[c * n + r];
+            }
+        }
+        if (sweeps_all != nullptr && threadIdx.x == 0) sweeps_all[idx] = sweeps;
+        __syncthreads();  // the working copies are reused by the next matrix
+    }
+}
+
+using BatchFn = void (*)(const BatchDesc *, int, int *, const void *, int, double, int, double *, double *,
+                         double *, int *, double *, size_t);
+
+struct ThreadStreams {
+    cudaStream_t s[kClasses] = {};
+    cudaEvent_t fork = nullptr, join[kClasses] = {}, t0 = nullptr, t1 = nullptr;
+    int device = -1;
+    ~ThreadStreams()
+    {
+        for (int c = 0; c < kClasses; ++c) {
+            if (s[c]) cudaStreamDestroy(s[c]);
+            if (join[c]) cudaEventDestroy(join[c]);
+        }
+        if (fork) cudaEventDestroy(fork);
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+    }
+};
+
+int class_streams(int dev, ThreadStreams **out)
+{
+    thread_local ThreadStreams ts;
+    if (ts.device != dev) {
+        if (ts.device >= 0) return invalid_argument("The batched solver is bound to the first device it ran on.");
+        for (int c = 0; c < kClasses; ++c) {
+            JSVD_CUDA_TRY(cudaStreamCreateWithFlags(&ts.s[c], cudaStreamNonBlocking));
+            JSVD_CUDA_TRY(cudaEventCreateWithFlags(&ts.join[c], cudaEventDisableTiming));
+        }
+        JSVD_CUDA_TRY(cudaEventCreateWithFlags(&ts.fork, cudaEventDisableTiming));
+        JSVD_CUDA_TRY(cudaEventCreate(&ts.t0));
+        JSVD_CUDA_TRY(cudaEventCreate(&ts.t1));
+        ts.device = dev;
+    }
+    *out = &ts;
+    return JSVD_OK;
+}
+
+}  // namespace
+
+BatchStats &batch_stats()
+{
+    thread_local BatchStats s;
+    return s;
+}
+
+int batch_solve(const BatchRequest &req, cudaStream_t stream)
+{
+    const int count = req.count;
+    if (count <= 0) return JSVD_OK;
+    int dev = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    int sms = 0, smem_optin = 0;
+    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t smem_cap = (size_t)std::min(smem_optin, 227 * 1024) - 1024;
+    ThreadStreams *ts = nullptr;
+    int rc = class_streams(dev, &ts);
+    if (rc != JSVD_OK) return rc;
+
+    struct Class {
+        size_t limit;  // max shared-memory bytes of a member
+        int threads;
+        int ctas_per_sm;
+        bool a_shared, v_shared;
+        BatchFn fn;
+    };
+    Class classes[kClasses] = {
+        {48 * 1024, 256, 4, true, true, batch_kernel<true, true>},
+        {100 * 1024, 256, 2, true, true, batch_kernel<true, true>},
+        {smem_cap, 512, 1, true, true, batch_kernel<true, true>},
+        {smem_cap, 512, 1, true, false, batch_kernel<true, false>},
+        {(size_t)-1, 512, 1, false, false, batch_kernel<false, false>},
+    };
+    if (req.tuning != nullptr) {
+        for (int c = 0; c < 4; ++c) {
+            if (req.tuning[c].threads > 0) classes[c].threads = req.tuning[c].threads;
+            if (req.tuning[c].ctas_per_sm > 0) classes[c].ctas_per_sm = req.tuning[c].ctas_per_sm;
+        }
+    }
+    std::vector<std::vector<int>> members(kClasses);
+    std::vector<BatchDesc> all(count);
+    std::vector<size_t> need_smem(count);
+    size_t s_off = 0, v_off = 0, u_off = 0;
+    for (int i = 0; i < count; ++i) {
+        BatchDesc d;
+        d.m = req.rows[i];
+        d.n = req.cols[i];
+        if (d.m <= 0 || d.n <= 0 || d.m < d.n)
+            return invalid_argument("Batch matrix shape must satisfy rows >= columns > 0.");
+        d.a_off = req.a_offsets[i];
+        d.s_off = (long long)s_off;
+        d.v_off = (long long)v_off;
+        d.u_off = (long long)u_off;
+        s_off += d.n;
+        v_off += (size_t)d.n * d.n;
+        u_off += (size_t)d.m * d.n;
+        all[i] = d;
+        const size_t scratch = sizeof(double) * round_scratch_doubles(d.n);
+        const size_t a_bytes = sizeof(double) * (size_t)d.m * d.n, v_bytes = sizeof(double) * (size_t)d.n * d.n;
+        int c;
+        if (scratch + a_bytes + v_bytes <= classes[0].limit) c = 0;
+        else if (scratch + a_bytes + v_bytes <= classes[1].limit) c = 1;
+        else if (scratch + a_bytes + v_bytes <= classes[2].limit) c = 2;
+        else if (scratch + a_bytes <= classes[3].limit) c = 3;
+        else c = 4;
+        need_smem[i] = scratch + (classes[c].a_shared ? a_bytes : 0) + (classes[c].v_shared ? v_bytes : 0);
+        members[c].push_back(i);
+    }
+    // Largest work first inside each class (tail balance of the work queue):
+    // work ~ n^2 (m + n) per sweep.
+    auto work = [&](int i) { return (double)all[i].n * all[i].n * (all[i].m + all[i].n); };
+    std::vector<BatchDesc> ordered;
+    ordered.reserve(count);
+    std::vector<int> first(kClasses + 1, 0), order_index;
+    order_index.reserve(count);
+    size_t smem_of[kClasses] = {}, gws_of[kClasses] = {};
+    for (int c = 0; c < kClasses; ++c) {
+        std::sort(members[c].begin(), members[c].end(), [&](int x, int y) { return work(x) > work(y); });
+        first[c] = (int)ordered.size();
+        for (int i : members[c]) {
+            ordered.push_back(all[i]);
+            order_index.push_back(i);
+            smem_of[c] = std::max(smem_of[c], need_smem[i]);
+            size_t g = 0;
+            if (!classes[c].a_shared) g += (size_t)all[i].m * all[i].n;
+            if (!classes[c].v_shared) g += (size_t)all[i].n * all[i].n;
+            gws_of[c] = std::max(gws_of[c], g);
+        }
+    }
+    first[kClasses] = (int)ordered.size();
+    int grid_of[kClasses] = {};
+    size_t gws_total = 0, gws_base[kClasses] = {};
+    for (int c = 0; c < kClasses; ++c) {
+        const int cnt = first[c + 1] - first[c];
+        grid_of[c] = std::min(cnt, sms * classes[c].ctas_per_sm);
+        gws_base[c] = gws_total;
+        gws_total += gws_of[c] * (size_t)grid_of[c];
+    }
+
+    BatchDesc *d_desc = nullptr;
+    int *d_next = nullptr, *d_sweeps = nullptr;
+    double *d_ws = nullptr;
+    JSVD_CUDA_TRY(cudaMallocAsync(&d_desc, sizeof(BatchDesc) * ordered.size(), stream));
+    JSVD_CUDA_TRY(cudaMallocAsync(&d_next, sizeof(int) * kClasses, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync(&d_sweeps, sizeof(int) * (size_t)count, stream));
+    if (gws_total > 0) JSVD_CUDA_TRY(cudaMallocAsync(&d_ws, sizeof(double) * gws_total, stream));
+    JSVD_CUDA_TRY(cudaMemcpyAsync(d_desc, ordered.data(), sizeof(BatchDesc) * ordered.size(), cudaMemcpyHostToDevice,
+                                  stream));
+    JSVD_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int) * kClasses, stream));
+    for (BatchFn fn : {(BatchFn)batch_kernel<true, true>, (BatchFn)batch_kernel<true, false>,
+                       (BatchFn)batch_kernel<false, false>})
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+    // Fork the class streams off `stream`, run the classes concurrently, join.
+    JSVD_CUDA_TRY(cudaEventRecord(ts->t0, stream));
+    JSVD_CUDA_TRY(cudaEventRecord(ts->fork, stream));
+    int launches = 0;
+    for (int c = kClasses - 1; c >= 0; --c) {
+        const int cnt = first[c + 1] - first[c];
+        if (cnt == 0) continue;
+        const Class &cl = classes[c];
+        cudaStream_t cs = ts->s[c];
+        JSVD_CUDA_TRY(cudaStreamWaitEvent(cs, ts->fork, 0));
+        cl.fn<<<grid_of[c], cl.threads, smem_of[c], cs>>>(d_desc + first[c], cnt, d_next + c, req.a, req.a_is_f32,
+                                                          req.eps, req.max_sweeps, req.sigma, req.v, req.u,
+                                                          d_sweeps + first[c], d_ws + gws_base[c], gws_of[c]);
+        JSVD_CUDA_TRY(cudaGetLastError());
+        JSVD_CUDA_TRY(cudaEventRecord(ts->join[c], cs));
+        JSVD_CUDA_TRY(cudaStreamWaitEvent(stream, ts->join[c], 0));
+        ++launches;
+    }
+    JSVD_CUDA_TRY(cudaEventRecord(ts->t1, stream));
+    std::vector<int> h_sweeps(count);
+    JSVD_CUDA_TRY(cudaMemcpyAsync(h_sweeps.data(), d_sweeps, sizeof(int) * count, cudaMemcpyDeviceToHost, stream));
+    JSVD_CUDA_TRY(cudaFreeAsync(d_desc, stream));
+    JSVD_CUDA_TRY(cudaFreeAsync(d_next, stream));
+    JSVD_CUDA_TRY(cudaFreeAsync(d_sweeps, stream));
+    if (d_ws) JSVD_CUDA_TRY(cudaFreeAsync(d_ws, stream));
+    JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ts->t0, ts->t1);
+    BatchStats &st = batch_stats();
+    st.calls += 1;
+    st.launches += (unsigned long long)launches;
+    st.kernel_ms += ms;
+    unsigned long long total_sweeps = 0;
+    for (int p = 0; p < count; ++p) {
+        total_sweeps += (unsigned long long)h_sweeps[p];
+        if (req.sweeps) req.sweeps[order_index[p]] = h_sweeps[p];
+    }
+    st.sweeps += total_sweeps;
+    st.matrices += (unsigned long long)count;
+    for (int c = 0; c < kClasses; ++c) st.class_count[c] += (unsigned long long)(first[c + 1] - first[c]);
+    return JSVD_OK;
+}
+
+}  // namespace jsvd
+
+using namespace jsvd;
+
+extern "C" int jsvd_batch_svd_device(int count, const int *rows, const int *cols, const long long *a_offsets,
+                                     const void *d_a, int a_is_f32, const jsvd_config *cfg, double *d_sigma,
+                                     double *d_v, double *d_u, int *sweeps, const jsvd_batch_tuning *tuning,
+                                     void *stream)
+{
+    set_last_error(JSVD_OK, "");
+    jsvd_config def;
+    jsvd_config_default(&def);
+    const jsvd_config &c = cfg ? *cfg : def;
+    if (count < 0) return invalid_argument("count must be non-negative.");
+    if (count > 0 && (rows == nullptr || cols == nullptr || a_offsets == nullptr || d_a == nullptr ||
+                      d_sigma == nullptr))
+        return invalid_argument("Batch buffers must not be null.");
+    if (!(c.epsilon > 0.0)) return invalid_argument("epsilon must be positive.");
+    if (c.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
+    if (reduction_lanes(c.threads_per_block) != 256)
+        return invalid_argument("The batched solver reduces with threads_per_block = 256.");
+    int dev = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (st == nullptr) {
+        st = thread_stream(dev);
+        if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+        JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+    }
+    BatchRequest req;
+    req.count = count;
+    req.rows = rows;
+    req.cols = cols;
+    req.a_offsets = a_offsets;
+    req.a = d_a;
+    req.a_is_f32 = a_is_f32;
+    req.eps = c.epsilon;
+    req.max_sweeps = c.max_sweeps;
+    req.sigma = d_sigma;
+    req.v = d_v;
+    req.u = d_u;
+    req.sweeps = sweeps;
+    req.tuning = tuning;
+    return batch_solve(req, st);
+}
+
+extern "C" void jsvd_batch_stats_get(jsvd_batch_stats *out)
+{
+    if (!out) return;
+    const BatchStats &s = batch_stats();
+    out->calls = s.calls;
+    out->launches = s.launches;
+    out->matrices = s.matrices;
+    out->sweeps = s.sweeps;
+    out->kernel_ms = s.kernel_ms;
+    for (int c = 0; c < 5; ++c) out->class_count[c] = s.class_count[c];
+}
+
+extern "C" void jsvd_batch_stats_reset(void) { batch_stats() = BatchStats{}; }

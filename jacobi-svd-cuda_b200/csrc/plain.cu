@@ -15,9 +15,11 @@
 //     its (c, s); after the sweep one row-parallel pass applies the whole
 //     sweep to V, rows held in shared memory.  Per element the sequence of
 //     rotations is the reference's, so V is bit-identical.
-//   * A sweep (n-1 round kernels + the V pass) is captured once into a CUDA
-//     graph per (device, m, n, T, eps) and replayed; the host reads one
-//     rotation counter per sweep.
+//   * A sweep (n-1 round kernels + the V pass) is launched directly the first
+//     time a plan (device, m, n, T, eps) is used and captured into a CUDA graph
+//     when the plan is reused; the host reads one rotation counter per sweep.
+//   * Plan workspaces use stream-ordered allocation, so creating or evicting a
+//     plan never synchronises the whole device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -193,12 +195,34 @@ __global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, 
     }
 }
 
-// Deferred V update: applies every rotation of one sweep to R rows of V.
+// Pair k of round r of the fixed-head circle schedule in closed form (the
+// same sequence build_schedule tabulates): positions 1..ne-1 rotate by one per
+// round, so position i >= 1 holds 1 + ((i - 1 - r) mod (ne - 1)); for odd n
+// the value n is the dummy column and its slot is skipped.
+__device__ __forceinline__ int2 schedule_pair(int n, int r, int k)
+{
+    const int ne = n + (n & 1);
+    const int L = ne - 1;
+    int i = k;
+    if (n & 1) {
+        const int j = 1 + ((n - 1 + r) % L);
+        const int slot = j < ne / 2 ? j : ne - 1 - j;
+        if (i >= slot) i += 1;
+    }
+    const int i2 = ne - 1 - i;
+    const int p = i == 0 ? 0 : 1 + ((i - 1 - r) % L + L) % L;
+    const int q = 1 + ((i2 - 1 - r) % L + L) % L;
+    return make_int2(p, q);
+}
+
+// Deferred V update: applies every rotation of one sweep to R rows of V
+// (R = 4 or 8, a template parameter so the row loop is vectorised).
 // V is column-major (element (row, col) at col*ldv + row); the CTA stages its
 // rows as sv[col*R + rr] in shared memory, so the round-to-round dependency
-// never leaves the SM.
-__global__ void __launch_bounds__(256) plain_vpass_kernel(double *__restrict__ v, long ldv, int n, int R,
-                                                          const int2 *__restrict__ pairs,
+// never leaves the SM.  Thread k owns pair slot k of every round; the (c, s)
+// of the next round is loaded while the current one is applied.
+template <int R>
+__global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v, long ldv, int n,
                                                           const double2 *__restrict__ cs, int rounds, int npairs)
 {
     extern __shared__ double sv[];
@@ -210,18 +234,33 @@ __global__ void __launch_bounds__(256) plain_vpass_kernel(double *__restrict__ v
         sv[idx] = (rr < rows) ? v[(size_t)col * ldv + r0 + rr] : 0.0;
     }
     __syncthreads();
-    const int items = npairs * R;
+    const int k0 = threadIdx.x;
+    double2 g_next = (k0 < npairs) ? cs[k0] : make_double2(0.0, 0.0);
     for (int r = 0; r < rounds; ++r) {
-        const double2 *__restrict__ csr = cs + (size_t)r * npairs;
-        const int2 *__restrict__ pr = pairs + (size_t)r * npairs;
-        for (int idx = threadIdx.x; idx < items; idx += blockDim.x) {
-            const int i = idx / R, rr = idx - i * R;
-            const double2 g = csr[i];
+        for (int k = k0; k < npairs; k += blockDim.x) {
+            double2 g;
+            if (k == k0) {
+                g = g_next;
+                if (r + 1 < rounds) g_next = cs[(size_t)(r + 1) * npairs + k0];
+            } else {
+                g = cs[(size_t)r * npairs + k];
+            }
             if (g.x != 0.0) {
-                const int2 pq = pr[i];
-                const double x = sv[pq.x * R + rr], y = sv[pq.y * R + rr];
-                sv[pq.x * R + rr] = rot_p(g.x, g.y, x, y);
-                sv[pq.y * R + rr] = rot_q(g.x, g.y, x, y);
+                const int2 pq = schedule_pair(n, r, k);
+                if constexpr (R == 1) {
+                    const double x = sv[pq.x], y = sv[pq.y];
+                    sv[pq.x] = rot_p(g.x, g.y, x, y);
+                    sv[pq.y] = rot_q(g.x, g.y, x, y);
+                } else {
+                    double2 *__restrict__ xp = reinterpret_cast<double2 *>(sv + (size_t)pq.x * R);
+                    double2 *__restrict__ xq = reinterpret_cast<double2 *>(sv + (size_t)pq.y * R);
+#pragma unroll
+                    for (int h = 0; h < R / 2; ++h) {
+                        const double2 x = xp[h], y = xq[h];
+                        xp[h] = make_double2(rot_p(g.x, g.y, x.x, y.x), rot_p(g.x, g.y, x.y, y.y));
+                        xq[h] = make_double2(rot_q(g.x, g.y, x.x, y.x), rot_q(g.x, g.y, x.y, y.y));
+                    }
+                }
             }
         }
         __syncthreads();
@@ -261,6 +300,17 @@ __global__ void __launch_bounds__(T) plain_sigma_kernel(const double *__restrict
 
 using RoundFn = void (*)(double *, long, int, const int2 *, double2 *, double, unsigned *);
 using SigmaFn = void (*)(const double *, long, int, double *);
+using VpassFn = void (*)(double *, long, int, const double2 *, int, int);
+
+VpassFn pick_vpass(int R)
+{
+    switch (R) {
+    case 1: return plain_vpass_kernel<1>;
+    case 2: return plain_vpass_kernel<2>;
+    case 4: return plain_vpass_kernel<4>;
+    default: return plain_vpass_kernel<8>;
+    }
+}
 
 template <int T>
 RoundFn pick_round_t(int m)
@@ -342,10 +392,11 @@ PlainPlan::~PlainPlan()
     if (sweep_exec) cudaGraphExecDestroy(sweep_exec);
     for (cudaEvent_t e : {ev_round_begin, ev_round_end, ev_vpass_end})
         if (e) cudaEventDestroy(e);
+    // Stream-ordered release: no device-wide synchronisation, so evicting a
+    // plan does not stall work on other streams.
     for (void *p : {(void *)a_w, (void *)v_w, (void *)pairs, (void *)cs, (void *)counter, (void *)d_in,
                     (void *)d_u, (void *)d_sigma, (void *)d_v, (void *)sigma_w})
-        if (p) cudaFree(p);
-    if (h_counter) cudaFreeHost(h_counter);
+        if (p) cudaFreeAsync(p, stream);
     if (prev >= 0) cudaSetDevice(prev);
 }
 
@@ -354,6 +405,7 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
 {
     auto plan = std::make_unique<PlainPlan>();
     plan->device = dev;
+    plan->stream = stream;
     plan->m = m_;
     plan->n = n_;
     plan->T = T_;
@@ -362,63 +414,92 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
     plan->ldv = (long)n_;
     std::vector<int2> host_pairs;
     build_schedule((int)n_, host_pairs, plan->rounds, plan->npairs);
-    JSVD_CUDA_TRY(cudaMalloc(&plan->a_w, sizeof(double) * m_ * n_));
-    JSVD_CUDA_TRY(cudaMalloc(&plan->v_w, sizeof(double) * n_ * n_));
-    JSVD_CUDA_TRY(cudaMalloc(&plan->sigma_w, sizeof(double) * n_));
-    JSVD_CUDA_TRY(cudaMalloc(&plan->counter, sizeof(unsigned)));
-    JSVD_CUDA_TRY(cudaMallocHost(&plan->h_counter, sizeof(unsigned)));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->a_w, sizeof(double) * m_ * n_, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->v_w, sizeof(double) * n_ * n_, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->sigma_w, sizeof(double) * n_, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->counter, sizeof(unsigned), stream));
     if (plan->rounds > 0) {
         const size_t np = (size_t)plan->rounds * plan->npairs;
-        JSVD_CUDA_TRY(cudaMalloc(&plan->pairs, sizeof(int2) * np));
-        JSVD_CUDA_TRY(cudaMalloc(&plan->cs, sizeof(double2) * np));
+        JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->pairs, sizeof(int2) * np, stream));
+        JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->cs, sizeof(double2) * np, stream));
         JSVD_CUDA_TRY(cudaMemcpyAsync(plan->pairs, host_pairs.data(), sizeof(int2) * np, cudaMemcpyHostToDevice,
                                       stream));
-        // V pass geometry: enough CTAs to cover the SMs, rows capped by shared memory.
+        // host_pairs dies at return: the copy must have consumed it.
+        JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
+        // V pass geometry: R rows of V per CTA (R in {1,2,4,8}), about n/128 so
+        // the grid covers the SMs, capped by 200 KB of shared memory.
         const size_t smem_cap = 200 * 1024;
-        int rmax = (int)std::max<size_t>(1, smem_cap / (sizeof(double) * n_));
-        int R = std::max(1, (int)(n_ / 128));
-        R = std::min(std::min(R, rmax), 16);
+        const int rmax = (int)std::max<size_t>(1, smem_cap / (sizeof(double) * n_));
+        int R = 1;
+        while (R * 2 <= 8 && R * 2 <= rmax && (size_t)(R * 2) * 128 <= n_) R *= 2;
         plan->vpass_rows = R;
         plan->vpass_smem = (int)(sizeof(double) * n_ * R);
-        JSVD_CUDA_TRY(cudaFuncSetAttribute(plain_vpass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           plan->vpass_smem));
-        // Capture one sweep.
-        RoundFn round_fn = pick_round(T_, (int)m_);
+        plan->vpass_threads = std::min(512, std::max(32, (plan->npairs + 31) / 32 * 32));
+        // The attribute is per function and process-wide: always raise it to the
+        // fixed cap, never to this plan's size, or a plan created concurrently
+        // on another thread could lower it under a larger plan's launch.
+        JSVD_CUDA_TRY(
+            cudaFuncSetAttribute(pick_vpass(R), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_begin));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_end));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_vpass_end));
-        cudaGraph_t graph = nullptr;
-        JSVD_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        JSVD_CUDA_TRY(cudaEventRecordWithFlags(plan->ev_round_begin, stream, cudaEventRecordExternal));
-        for (int r = 0; r < plan->rounds; ++r) {
-            const size_t off = (size_t)r * plan->npairs;
-            round_fn<<<plan->npairs, T_, 0, stream>>>(plan->a_w, plan->lda, (int)m_, plan->pairs + off,
-                                                      plan->cs + off, eps_, plan->counter);
-        }
-        JSVD_CUDA_TRY(cudaEventRecordWithFlags(plan->ev_round_end, stream, cudaEventRecordExternal));
-        const int vgrid = (int)((n_ + R - 1) / R);
-        plain_vpass_kernel<<<vgrid, 256, plan->vpass_smem, stream>>>(plan->v_w, plan->ldv, (int)n_, R, plan->pairs,
-                                                                    plan->cs, plan->rounds, plan->npairs);
-        JSVD_CUDA_TRY(cudaEventRecordWithFlags(plan->ev_vpass_end, stream, cudaEventRecordExternal));
-        cudaError_t cap = cudaStreamEndCapture(stream, &graph);
-        if (cap != cudaSuccess) return cuda_failure(cap, "cudaStreamEndCapture", __FILE__, __LINE__);
-        cudaError_t inst = cudaGraphInstantiate(&plan->sweep_exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (inst != cudaSuccess) return cuda_failure(inst, "cudaGraphInstantiate", __FILE__, __LINE__);
     }
     plan->bytes = sizeof(double) * (m_ * n_ + n_ * n_ + n_) +
                   (sizeof(int2) + sizeof(double2)) * (size_t)plan->rounds * plan->npairs;
+    // The allocations become usable on any stream once this one has drained.
+    JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
     out = std::move(plan);
+    return JSVD_OK;
+}
+
+// Enqueues one sweep (every round kernel, then the V pass) on `st`, bracketed
+// by the plan's timing events.  Used for direct launches and for capture.
+int PlainPlan::enqueue_sweep(cudaStream_t st)
+{
+    RoundFn round_fn = pick_round(T, (int)m);
+    JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_round_begin, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
+    for (int r = 0; r < rounds; ++r) {
+        const size_t off = (size_t)r * npairs;
+        round_fn<<<npairs, T, 0, st>>>(a_w, lda, (int)m, pairs + off, cs + off, eps, counter);
+    }
+    JSVD_CUDA_TRY(cudaGetLastError());
+    JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_round_end, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
+    const int vgrid = (int)((n + vpass_rows - 1) / vpass_rows);
+    pick_vpass(vpass_rows)<<<vgrid, vpass_threads, vpass_smem, st>>>(v_w, ldv, (int)n, cs, rounds, npairs);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_vpass_end, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
+    return JSVD_OK;
+}
+
+// Captures one sweep into a graph (done when a plan is used a second time:
+// one-off shapes are not worth the instantiation).
+int PlainPlan::capture_sweep(cudaStream_t st)
+{
+    cudaGraph_t graph = nullptr;
+    JSVD_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    sweep_exec_capturing = true;
+    const int rc = enqueue_sweep(st);
+    sweep_exec_capturing = false;
+    cudaError_t cap = cudaStreamEndCapture(st, &graph);
+    if (rc != JSVD_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (cap != cudaSuccess) return cuda_failure(cap, "cudaStreamEndCapture", __FILE__, __LINE__);
+    cudaError_t inst = cudaGraphInstantiate(&sweep_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (inst != cudaSuccess) return cuda_failure(inst, "cudaGraphInstantiate", __FILE__, __LINE__);
     return JSVD_OK;
 }
 
 int PlainPlan::ensure_host_staging()
 {
     if (d_in) return JSVD_OK;
-    JSVD_CUDA_TRY(cudaMalloc(&d_in, sizeof(double) * m * n));
-    JSVD_CUDA_TRY(cudaMalloc(&d_u, sizeof(double) * m * n));
-    JSVD_CUDA_TRY(cudaMalloc(&d_sigma, sizeof(double) * n));
-    JSVD_CUDA_TRY(cudaMalloc(&d_v, sizeof(double) * n * n));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&d_in, sizeof(double) * m * n, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&d_u, sizeof(double) * m * n, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&d_sigma, sizeof(double) * n, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&d_v, sizeof(double) * n * n, stream));
+    JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
     bytes += sizeof(double) * (2 * m * n + n + n * n);
     return JSVD_OK;
 }
@@ -441,10 +522,20 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
     if (rounds == 0) {
         executed = 1;  // n == 1: one empty sweep, as the reference reports
     } else {
+        if (sweep_exec == nullptr && uses >= 1) {
+            const int rc = capture_sweep(stream);
+            if (rc != JSVD_OK) return rc;
+        }
         for (int s = 0; s < max_sweeps; ++s) {
             JSVD_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), stream));
-            JSVD_CUDA_TRY(cudaGraphLaunch(sweep_exec, stream));
-            JSVD_CUDA_TRY(cudaMemcpyAsync(h_counter, counter, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+            if (sweep_exec != nullptr) {
+                JSVD_CUDA_TRY(cudaGraphLaunch(sweep_exec, stream));
+            } else {
+                const int rc = enqueue_sweep(stream);
+                if (rc != JSVD_OK) return rc;
+            }
+            unsigned rotated = 0;
+            JSVD_CUDA_TRY(cudaMemcpyAsync(&rotated, counter, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
             JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
             executed = s + 1;
             float r_ms = 0.f, v_ms = 0.f;
@@ -452,9 +543,10 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             if (cudaEventElapsedTime(&v_ms, ev_round_end, ev_vpass_end) == cudaSuccess) st.vpass_ms += v_ms;
             st.round_launches += (unsigned long long)rounds;
             st.vpass_launches += 1;
-            if (*h_counter == 0) break;
+            if (rotated == 0) break;
         }
     }
+    uses += 1;
     st.solves += 1;
     st.sweeps += (unsigned long long)executed;
     st.other_launches += 3 + (out_u ? 1 : 0) + (out_v ? 1 : 0);

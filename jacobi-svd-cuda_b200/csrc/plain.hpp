@@ -13,12 +13,13 @@ namespace jsvd {
 
 struct PlainPlan {
     int device = -1;
+    cudaStream_t stream = nullptr;  // allocation / release stream (the creating thread's)
     size_t m = 0, n = 0;
     int T = 256;
     double eps = 0.0;
     long lda = 0, ldv = 0;
     int rounds = 0, npairs = 0;
-    int vpass_rows = 1, vpass_smem = 0;
+    int vpass_rows = 1, vpass_smem = 0, vpass_threads = 256;
     size_t bytes = 0;
 
     double *a_w = nullptr;      // column-major working copy of A (m x n)
@@ -27,7 +28,8 @@ struct PlainPlan {
     int2 *pairs = nullptr;      // rounds x npairs schedule
     double2 *cs = nullptr;      // (c, s) of every pair of the current sweep
     unsigned *counter = nullptr;
-    unsigned *h_counter = nullptr;  // pinned
+    unsigned long long uses = 0;
+    bool sweep_exec_capturing = false;
     // staging for host-buffer calls
     double *d_in = nullptr, *d_u = nullptr, *d_sigma = nullptr, *d_v = nullptr;
 
@@ -44,6 +46,8 @@ struct PlainPlan {
     static int create(int dev, size_t m, size_t n, int T, double eps, cudaStream_t stream,
                       std::unique_ptr<PlainPlan> &out);
     int ensure_host_staging();
+    int enqueue_sweep(cudaStream_t st);
+    int capture_sweep(cudaStream_t st);
     // Runs the whole solve on device buffers; outputs may be null.
     int run(const double *d_a, double *out_u, double *out_sigma, double *out_v, int max_sweeps, int *sweeps,
             cudaStream_t stream);

@@ -1,0 +1,450 @@
+// Serving core: continuous batching of SVD requests on one GPU.
+//
+// This is what the reference's pipeline does with a host thread pool calling
+// one_sided_jacobi_svd per testcase (kleedaisuki/jacobi-svd-cuda
+// src/pipeline.cpp:234-394, 754-863), reorganised for the device:
+//   * submit() copies the request and queues it; nothing touches the GPU yet;
+//   * admission reserves the request's device footprint against a memory
+//     budget and waits while the budget is exhausted;
+//   * "small" requests (the working copy of A fits a CTA's shared memory) are
+//     gathered by two batch workers: whatever is queued when a worker becomes
+//     free forms its next batch, so requests that arrive while a batch is on
+//     the GPU join the next one and two batches overlap on the device;
+//   * "large" requests go to worker threads that each drive their own stream
+//     (plain path, per-thread plan cache), so several large solves overlap;
+//   * every path uses the plain path's arithmetic, so a request's result does
+//     not depend on what else was in flight.
+// Latency = completion - submission (host steady clock).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "batched.hpp"
+#include "internal.hpp"
+#include "jsvd.h"
+#include "plain.hpp"
+
+namespace jsvd {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+// A request may use the batched solver when A's FP64 working copy plus the
+// round scratch fits one CTA's shared memory.
+bool is_small(size_t m, size_t n) { return sizeof(double) * (m * n + 5 * (n / 2 + 2)) <= 200 * 1024; }
+
+size_t small_footprint(size_t m, size_t n, bool want_u)
+{
+    // A (FP64 input) + sigma + V + optional U + global V workspace
+    return sizeof(double) * (m * n + n + 2 * n * n + (want_u ? m * n : 0));
+}
+
+size_t large_footprint(size_t m, size_t n)
+{
+    // I/O buffers (A, U, sigma, V) + plan (A_w, V_w, sigma, schedule and angles)
+    return sizeof(double) * (2 * m * n + n + n * n) + sizeof(double) * (m * n + n * n + n) + 24 * n * n;
+}
+
+struct Request {
+    uint64_t id = 0;
+    size_t m = 0, n = 0;
+    bool want_u = false, small = false;
+    std::vector<double> a, u, sigma, v;
+    int sweeps = 0;
+    int status = JSVD_OK;
+    std::string error;
+    size_t footprint = 0;
+    Clock::time_point t_submit, t_done;
+    bool done = false;
+};
+
+// Pinned host staging that grows and is reused by one worker.
+struct Pinned {
+    void *p = nullptr;
+    size_t cap = 0;
+    ~Pinned()
+    {
+        if (p) cudaFreeHost(p);
+    }
+    int ensure(size_t bytes)
+    {
+        if (bytes <= cap) return JSVD_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        size_t c = std::max<size_t>(bytes, cap * 2);
+        JSVD_CUDA_TRY(cudaMallocHost(&p, c));
+        cap = c;
+        return JSVD_OK;
+    }
+};
+
+}  // namespace
+
+class Server {
+public:
+    explicit Server(const jsvd_server_options &o) : opt_(o)
+    {
+        cudaGetDevice(&device_);
+        for (int i = 0; i < opt_.small_workers; ++i) threads_.emplace_back([this] { small_loop(); });
+        for (int i = 0; i < opt_.large_workers; ++i) threads_.emplace_back([this] { large_loop(); });
+    }
+
+    ~Server()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stopping_ = true;
+        }
+        cv_work_.notify_all();
+        cv_budget_.notify_all();
+        for (auto &t : threads_) t.join();
+    }
+
+    int submit(const double *a, size_t m, size_t n, int want_u, uint64_t *ticket)
+    {
+        if (a == nullptr || ticket == nullptr) return invalid_argument("Request buffers must not be null.");
+        if (m == 0 || n == 0) return invalid_argument("Input matrix shape must be non-zero.");
+        if (m < n) return invalid_argument("One-sided Jacobi SVD requires rows >= columns in this implementation.");
+        auto r = std::make_unique<Request>();
+        r->m = m;
+        r->n = n;
+        r->want_u = want_u != 0;
+        // The batched solver reduces with T = 256; other widths take the plain path.
+        r->small = is_small(m, n) && reduction_lanes(opt_.cfg.threads_per_block) == 256;
+        r->footprint = r->small ? small_footprint(m, n, r->want_u) : large_footprint(m, n);
+        if (r->footprint > opt_.device_budget_bytes) {
+            set_last_error(JSVD_ERR_BUDGET, "Request needs " + std::to_string(r->footprint) +
+                                                " bytes of device memory, more than the serving budget of " +
+                                                std::to_string(opt_.device_budget_bytes) + ".");
+            return JSVD_ERR_BUDGET;
+        }
+        r->a.assign(a, a + m * n);
+        r->t_submit = Clock::now();
+        std::lock_guard<std::mutex> lk(mu_);
+        r->id = next_id_++;
+        *ticket = r->id;
+        Request *raw = r.get();
+        requests_.emplace(r->id, std::move(r));
+        (raw->small ? small_q_ : large_q_).push_back(raw);
+        ++submitted_;
+        cv_work_.notify_all();
+        return JSVD_OK;
+    }
+
+    int wait(uint64_t ticket, double *u, double *sigma, double *v, int *sweeps, double *latency_ms)
+    {
+        std::unique_ptr<Request> r;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            auto it = requests_.find(ticket);
+            if (it == requests_.end()) return invalid_argument("Unknown or already collected ticket.");
+            Request *raw = it->second.get();
+            cv_done_.wait(lk, [&] { return raw->done; });
+            r = std::move(it->second);
+            requests_.erase(it);
+        }
+        if (r->status != JSVD_OK) {
+            set_last_error(r->status, r->error);
+            return r->status;
+        }
+        if (u && r->want_u) std::memcpy(u, r->u.data(), sizeof(double) * r->m * r->n);
+        if (sigma) std::memcpy(sigma, r->sigma.data(), sizeof(double) * r->n);
+        if (v) std::memcpy(v, r->v.data(), sizeof(double) * r->n * r->n);
+        if (sweeps) *sweeps = r->sweeps;
+        if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+        return JSVD_OK;
+    }
+
+    void stats(jsvd_server_stats *s)
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        std::memset(s, 0, sizeof(*s));
+        s->submitted = submitted_;
+        s->completed = completed_;
+        s->failed = failed_;
+        s->batches = batches_;
+        s->batched_requests = batched_requests_;
+        s->large_solves = large_solves_;
+        s->peak_device_bytes = peak_bytes_;
+        s->device_bytes_in_use = in_use_;
+        if (!lat_.empty()) {
+            std::vector<double> l = lat_;
+            std::sort(l.begin(), l.end());
+            auto pct = [&](double q) { return l[std::min(l.size() - 1, (size_t)(q * (l.size() - 1) + 0.5))]; };
+            s->p50_ms = pct(0.50);
+            s->p99_ms = pct(0.99);
+            double sum = 0;
+            for (double x : l) sum += x;
+            s->mean_ms = sum / l.size();
+        }
+    }
+
+private:
+    // Takes requests from q while their footprints fit the budget; blocks while
+    // the first one does not fit.  Returns an empty list when stopping.
+    std::vector<Request *> admit(std::deque<Request *> &q, size_t max_count)
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_work_.wait(lk, [&] { return stopping_ || !q.empty(); });
+        std::vector<Request *> got;
+        while (!stopping_ && got.empty()) {
+            while (!q.empty() && got.size() < max_count && in_use_ + q.front()->footprint <= opt_.device_budget_bytes) {
+                in_use_ += q.front()->footprint;
+                got.push_back(q.front());
+                q.pop_front();
+            }
+            if (got.empty()) {
+                if (q.empty()) {
+                    cv_work_.wait(lk, [&] { return stopping_ || !q.empty(); });
+                } else {
+                    cv_budget_.wait(lk);
+                }
+            }
+        }
+        peak_bytes_ = std::max(peak_bytes_, in_use_);
+        return got;
+    }
+
+    void finish(const std::vector<Request *> &rs, int status, const std::string &err)
+    {
+        const auto now = Clock::now();
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (Request *r : rs) {
+                in_use_ -= r->footprint;
+                r->status = status;
+                r->error = err;
+                r->t_done = now;
+                r->done = true;
+                if (status == JSVD_OK) {
+                    ++completed_;
+                    lat_.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
+                } else {
+                    ++failed_;
+                }
+            }
+        }
+        cv_budget_.notify_all();
+        cv_done_.notify_all();
+    }
+
+    int run_batch(const std::vector<Request *> &rs, cudaStream_t st, Pinned &stage)
+    {
+        const int count = (int)rs.size();
+        std::vector<int> rows(count), cols(count);
+        std::vector<long long> aoff(count);
+        size_t a_total = 0, s_total = 0, v_total = 0, u_total = 0;
+        bool any_u = false;
+        for (int i = 0; i < count; ++i) {
+            rows[i] = (int)rs[i]->m;
+            cols[i] = (int)rs[i]->n;
+            aoff[i] = (long long)a_total;
+            a_total += rs[i]->m * rs[i]->n;
+            s_total += rs[i]->n;
+            v_total += rs[i]->n * rs[i]->n;
+            any_u = any_u || rs[i]->want_u;
+        }
+        if (any_u) u_total = a_total;
+        const size_t doubles = a_total + s_total + v_total + u_total;
+        int rc = stage.ensure(sizeof(double) * doubles);
+        if (rc != JSVD_OK) return rc;
+        double *h = static_cast<double *>(stage.p);
+        for (int i = 0; i < count; ++i)
+            std::memcpy(h + aoff[i], rs[i]->a.data(), sizeof(double) * rs[i]->a.size());
+        double *d = nullptr;
+        JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * doubles, st));
+        JSVD_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double) * a_total, cudaMemcpyHostToDevice, st));
+        BatchRequest req;
+        req.count = count;
+        req.rows = rows.data();
+        req.cols = cols.data();
+        req.a_offsets = aoff.data();
+        req.a = d;
+        req.a_is_f32 = 0;
+        req.eps = opt_.cfg.epsilon;
+        req.max_sweeps = opt_.cfg.max_sweeps;
+        req.sigma = d + a_total;
+        req.v = d + a_total + s_total;
+        req.u = any_u ? d + a_total + s_total + v_total : nullptr;
+        std::vector<int> sweeps(count);
+        req.sweeps = sweeps.data();
+        rc = batch_solve(req, st);
+        if (rc != JSVD_OK) {
+            cudaFreeAsync(d, st);
+            return rc;
+        }
+        JSVD_CUDA_TRY(cudaMemcpyAsync(h + a_total, d + a_total, sizeof(double) * (s_total + v_total + u_total),
+                                      cudaMemcpyDeviceToHost, st));
+        JSVD_CUDA_TRY(cudaFreeAsync(d, st));
+        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+        size_t so = 0, vo = 0;
+        for (int i = 0; i < count; ++i) {
+            Request *r = rs[i];
+            r->sigma.assign(h + a_total + so, h + a_total + so + r->n);
+            r->v.assign(h + a_total + s_total + vo, h + a_total + s_total + vo + r->n * r->n);
+            if (r->want_u) {
+                const double *us = h + a_total + s_total + v_total + aoff[i];
+                r->u.assign(us, us + r->m * r->n);
+            }
+            r->sweeps = sweeps[i];
+            so += r->n;
+            vo += r->n * r->n;
+        }
+        return JSVD_OK;
+    }
+
+    void small_loop()
+    {
+        cudaSetDevice(device_);
+        cudaStream_t st = nullptr;
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        Pinned stage;
+        for (;;) {
+            std::vector<Request *> rs = admit(small_q_, (size_t)opt_.max_batch);
+            if (rs.empty()) break;
+            const int rc = run_batch(rs, st, stage);
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                ++batches_;
+                batched_requests_ += rs.size();
+            }
+            finish(rs, rc, rc == JSVD_OK ? std::string() : last_error_message());
+        }
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int run_large(Request *r, Pinned &stage)
+    {
+        const size_t m = r->m, n = r->n;
+        const size_t doubles = m * n + n + n * n + (r->want_u ? m * n : 0);
+        int rc = stage.ensure(sizeof(double) * doubles);
+        if (rc != JSVD_OK) return rc;
+        cudaStream_t st = thread_stream(device_);
+        if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+        double *h = static_cast<double *>(stage.p);
+        std::memcpy(h, r->a.data(), sizeof(double) * m * n);
+        double *d = nullptr;
+        JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * doubles, st));
+        JSVD_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double) * m * n, cudaMemcpyHostToDevice, st));
+        double *ds = d + m * n, *dv = ds + n, *du = r->want_u ? dv + n * n : nullptr;
+        rc = jsvd_plain_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st);
+        if (rc != JSVD_OK) {
+            cudaFreeAsync(d, st);
+            return rc;
+        }
+        JSVD_CUDA_TRY(cudaMemcpyAsync(h + m * n, ds, sizeof(double) * (doubles - m * n), cudaMemcpyDeviceToHost, st));
+        JSVD_CUDA_TRY(cudaFreeAsync(d, st));
+        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+        r->sigma.assign(h + m * n, h + m * n + n);
+        r->v.assign(h + m * n + n, h + m * n + n + n * n);
+        if (r->want_u) r->u.assign(h + m * n + n + n * n, h + m * n + n + n * n + m * n);
+        return JSVD_OK;
+    }
+
+    void large_loop()
+    {
+        cudaSetDevice(device_);
+        Pinned stage;
+        for (;;) {
+            std::vector<Request *> rs = admit(large_q_, 1);
+            if (rs.empty()) break;
+            const int rc = run_large(rs[0], stage);
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                ++large_solves_;
+            }
+            finish(rs, rc, rc == JSVD_OK ? std::string() : last_error_message());
+        }
+        jsvd_release_thread_cache();
+    }
+
+    jsvd_server_options opt_;
+    int device_ = 0;
+    std::mutex mu_;
+    std::condition_variable cv_work_, cv_done_, cv_budget_;
+    std::deque<Request *> small_q_, large_q_;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> requests_;
+    std::vector<std::thread> threads_;
+    bool stopping_ = false;
+    uint64_t next_id_ = 1;
+    size_t in_use_ = 0, peak_bytes_ = 0;
+    unsigned long long submitted_ = 0, completed_ = 0, failed_ = 0, batches_ = 0, batched_requests_ = 0,
+                       large_solves_ = 0;
+    std::vector<double> lat_;
+};
+
+}  // namespace jsvd
+
+using namespace jsvd;
+
+struct jsvd_server {
+    std::unique_ptr<Server> impl;
+};
+
+extern "C" {
+
+void jsvd_server_options_default(jsvd_server_options *o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->device_budget_bytes = size_t(40) << 30;
+    o->small_workers = 2;
+    o->large_workers = 4;
+    o->max_batch = 4096;
+    jsvd_config_default(&o->cfg);
+}
+
+int jsvd_server_create(const jsvd_server_options *opt, jsvd_server **out)
+{
+    set_last_error(JSVD_OK, "");
+    if (!out) return invalid_argument("out must not be null.");
+    jsvd_server_options o;
+    jsvd_server_options_default(&o);
+    if (opt) o = *opt;
+    if (o.device_budget_bytes == 0) o.device_budget_bytes = size_t(40) << 30;
+    if (o.small_workers <= 0) o.small_workers = 2;
+    if (o.large_workers <= 0) o.large_workers = 4;
+    if (o.max_batch <= 0) o.max_batch = 4096;
+    if (!(o.cfg.epsilon > 0.0)) return invalid_argument("epsilon must be positive.");
+    if (o.cfg.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
+    auto *s = new jsvd_server;
+    s->impl = std::make_unique<Server>(o);
+    *out = s;
+    return JSVD_OK;
+}
+
+int jsvd_server_submit(jsvd_server *s, const double *a, size_t rows, size_t columns, int want_u, uint64_t *ticket)
+{
+    set_last_error(JSVD_OK, "");
+    if (!s) return invalid_argument("server must not be null.");
+    return s->impl->submit(a, rows, columns, want_u, ticket);
+}
+
+int jsvd_server_wait(jsvd_server *s, uint64_t ticket, double *u, double *sigma, double *v, int *sweeps,
+                     double *latency_ms)
+{
+    set_last_error(JSVD_OK, "");
+    if (!s) return invalid_argument("server must not be null.");
+    return s->impl->wait(ticket, u, sigma, v, sweeps, latency_ms);
+}
+
+int jsvd_server_get_stats(jsvd_server *s, jsvd_server_stats *out)
+{
+    if (!s || !out) return invalid_argument("server and out must not be null.");
+    s->impl->stats(out);
+    return JSVD_OK;
+}
+
+void jsvd_server_destroy(jsvd_server *s) { delete s; }
+
+}  // extern "C"

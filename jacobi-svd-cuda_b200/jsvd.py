@@ -62,6 +62,41 @@ class PlainStats(ctypes.Structure):
     ]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [
+        ("calls", ctypes.c_ulonglong),
+        ("launches", ctypes.c_ulonglong),
+        ("matrices", ctypes.c_ulonglong),
+        ("sweeps", ctypes.c_ulonglong),
+        ("kernel_ms", ctypes.c_double),
+        ("class_count", ctypes.c_ulonglong * 5),
+    ]
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [
+        ("device_budget_bytes", ctypes.c_size_t),
+        ("small_workers", ctypes.c_int),
+        ("large_workers", ctypes.c_int),
+        ("max_batch", ctypes.c_int),
+        ("cfg", Config),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_ulonglong), ("completed", ctypes.c_ulonglong), ("failed", ctypes.c_ulonglong),
+        ("batches", ctypes.c_ulonglong), ("batched_requests", ctypes.c_ulonglong),
+        ("large_solves", ctypes.c_ulonglong),
+        ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+        ("peak_device_bytes", ctypes.c_size_t), ("device_bytes_in_use", ctypes.c_size_t),
+    ]
+
+
 class JsvdError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[{code}] {message}")
@@ -88,7 +123,10 @@ def exported_symbols() -> list[str]:
     return [
         "jsvd_config_default", "jsvd_last_error", "jsvd_version", "jsvd_plain_arith_variant",
         "jsvd_plain_svd", "jsvd_plain_svd_device", "jsvd_auto_tune_layout", "jsvd_release_thread_cache",
-        "jsvd_plain_stats_get", "jsvd_plain_stats_reset",
+        "jsvd_plain_stats_get", "jsvd_plain_stats_reset", "jsvd_plain_svd_noalloc",
+        "jsvd_batch_svd_device", "jsvd_batch_stats_get", "jsvd_batch_stats_reset", "jsvd_probe_fp64_tflops",
+        "jsvd_server_options_default", "jsvd_server_create", "jsvd_server_submit", "jsvd_server_wait",
+        "jsvd_server_get_stats", "jsvd_server_destroy",
     ]
 
 
@@ -115,6 +153,26 @@ def lib() -> ctypes.CDLL:
         L.jsvd_plain_stats_get.argtypes = [ctypes.POINTER(PlainStats)]
         L.jsvd_plain_stats_get.restype = None
         L.jsvd_plain_stats_reset.restype = None
+        L.jsvd_batch_svd_device.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), P, P, P, P,
+                                            ctypes.POINTER(BatchTuning), P]
+        L.jsvd_batch_svd_device.restype = I
+        L.jsvd_batch_stats_get.argtypes = [ctypes.POINTER(BatchStats)]
+        L.jsvd_batch_stats_get.restype = None
+        L.jsvd_batch_stats_reset.restype = None
+        L.jsvd_probe_fp64_tflops.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        L.jsvd_probe_fp64_tflops.restype = I
+        L.jsvd_server_options_default.argtypes = [ctypes.POINTER(ServerOptions)]
+        L.jsvd_server_options_default.restype = None
+        L.jsvd_server_create.argtypes = [ctypes.POINTER(ServerOptions), ctypes.POINTER(P)]
+        L.jsvd_server_create.restype = I
+        L.jsvd_server_submit.argtypes = [P, P, S, S, I, ctypes.POINTER(ctypes.c_uint64)]
+        L.jsvd_server_submit.restype = I
+        L.jsvd_server_wait.argtypes = [P, ctypes.c_uint64, P, P, P, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double)]
+        L.jsvd_server_wait.restype = I
+        L.jsvd_server_get_stats.argtypes = [P, ctypes.POINTER(ServerStats)]
+        L.jsvd_server_get_stats.restype = I
+        L.jsvd_server_destroy.argtypes = [P]
+        L.jsvd_server_destroy.restype = None
         _LIB = L
     return _LIB
 
@@ -181,6 +239,132 @@ def plain_stats() -> PlainStats:
 
 def plain_stats_reset() -> None:
     lib().jsvd_plain_stats_reset()
+
+
+class DeviceBatch:
+    """A batch of matrices packed on the device (torch tensors), ready for
+    jsvd_batch_svd_device.  Outputs are packed in input order."""
+
+    def __init__(self, mats, device, f32: bool = False, want_u: bool = False, want_v: bool = True):
+        import torch
+
+        self.count = len(mats)
+        self.rows = np.array([a.shape[0] for a in mats], dtype=np.int32)
+        self.cols = np.array([a.shape[1] for a in mats], dtype=np.int32)
+        sizes = self.rows.astype(np.int64) * self.cols
+        self.a_off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        self.s_off = np.concatenate([[0], np.cumsum(self.cols)[:-1]]).astype(np.int64)
+        self.v_off = np.concatenate([[0], np.cumsum(self.cols.astype(np.int64) ** 2)[:-1]]).astype(np.int64)
+        dt = np.float32 if f32 else np.float64
+        packed = np.concatenate([np.ascontiguousarray(a, dtype=dt).ravel() for a in mats])
+        self.f32 = f32
+        self.h2d_bytes = packed.nbytes
+        self.host_a = torch.from_numpy(packed)
+        self.a = self.host_a.to(device)
+        self.sigma = torch.empty(int(self.cols.sum()), dtype=torch.float64, device=device)
+        self.v = torch.empty(int((self.cols.astype(np.int64) ** 2).sum()), dtype=torch.float64,
+                             device=device) if want_v else None
+        self.u = torch.empty(int(sizes.sum()), dtype=torch.float64, device=device) if want_u else None
+        self.sweeps = np.zeros(self.count, dtype=np.int32)
+
+    def solve(self, cfg: Config | None = None, tuning=None, stream: int = 0) -> None:
+        cfg = cfg or default_config()
+        tun = None
+        if tuning is not None:
+            arr = (BatchTuning * 4)(*[BatchTuning(t, c) for t, c in tuning])
+            tun = arr
+        rc = lib().jsvd_batch_svd_device(
+            self.count, self.rows.ctypes.data, self.cols.ctypes.data, self.a_off.ctypes.data, self.a.data_ptr(),
+            1 if self.f32 else 0, ctypes.byref(cfg), self.sigma.data_ptr(),
+            self.v.data_ptr() if self.v is not None else None,
+            self.u.data_ptr() if self.u is not None else None, self.sweeps.ctypes.data, tun, stream or None)
+        check(rc)
+
+    def results(self):
+        s = self.sigma.cpu().numpy()
+        v = self.v.cpu().numpy() if self.v is not None else None
+        u = self.u.cpu().numpy() if self.u is not None else None
+        out = []
+        for k in range(self.count):
+            m, n = int(self.rows[k]), int(self.cols[k])
+            sk = s[self.s_off[k]: self.s_off[k] + n]
+            vk = v[self.v_off[k]: self.v_off[k] + n * n].reshape(n, n) if v is not None else None
+            uk = u[self.a_off[k]: self.a_off[k] + m * n].reshape(m, n) if u is not None else None
+            out.append((uk, sk, vk, int(self.sweeps[k])))
+        return out
+
+
+def probe_fp64_tflops() -> float:
+    x = ctypes.c_double(0.0)
+    check(lib().jsvd_probe_fp64_tflops(ctypes.byref(x)))
+    return x.value
+
+
+class Server:
+    """Serving core (jsvd_server_*): submit host matrices, wait for results."""
+
+    def __init__(self, cfg: Config | None = None, budget_bytes: int = 0, small_workers: int = 0,
+                 large_workers: int = 0, max_batch: int = 0):
+        opt = ServerOptions()
+        lib().jsvd_server_options_default(ctypes.byref(opt))
+        if cfg is not None:
+            opt.cfg = cfg
+        if budget_bytes:
+            opt.device_budget_bytes = budget_bytes
+        if small_workers:
+            opt.small_workers = small_workers
+        if large_workers:
+            opt.large_workers = large_workers
+        if max_batch:
+            opt.max_batch = max_batch
+        h = ctypes.c_void_p()
+        check(lib().jsvd_server_create(ctypes.byref(opt), ctypes.byref(h)))
+        self.h = h
+        self.shapes = {}
+
+    def submit(self, a: np.ndarray, want_u: bool = False) -> int:
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        t = ctypes.c_uint64(0)
+        check(lib().jsvd_server_submit(self.h, a.ctypes.data, a.shape[0], a.shape[1], int(want_u), ctypes.byref(t)))
+        self.shapes[t.value] = (a.shape[0], a.shape[1], want_u)
+        return t.value
+
+    def wait(self, ticket: int):
+        m, n, want_u = self.shapes.pop(ticket)
+        u = np.empty((m, n)) if want_u else None
+        s = np.empty(n)
+        v = np.empty((n, n))
+        sw = ctypes.c_int(0)
+        lat = ctypes.c_double(0.0)
+        check(lib().jsvd_server_wait(self.h, ticket, u.ctypes.data if u is not None else None, s.ctypes.data,
+                                     v.ctypes.data, ctypes.byref(sw), ctypes.byref(lat)))
+        return u, s, v, sw.value, lat.value
+
+    def stats(self) -> ServerStats:
+        st = ServerStats()
+        check(lib().jsvd_server_get_stats(self.h, ctypes.byref(st)))
+        return st
+
+    def close(self) -> None:
+        if self.h:
+            lib().jsvd_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def batch_stats() -> BatchStats:
+    st = BatchStats()
+    lib().jsvd_batch_stats_get(ctypes.byref(st))
+    return st
+
+
+def batch_stats_reset() -> None:
+    lib().jsvd_batch_stats_reset()
 
 
 def auto_tune_layout(cfg: Config | None = None) -> AutoTuneReport:

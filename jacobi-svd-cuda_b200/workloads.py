@@ -127,3 +127,32 @@ def graded_clustered_sigma(n: int, clusters: int = 8, size: int = 16, gap: float
             c = s[c0]
             s[c0: c0 + size] = c * (1.0 + gap * np.arange(size))
     return np.sort(s)[::-1]
+
+
+def batch_workload_torch(count: int, seed: int = 3, device=None, m_lo: int = 16, m_hi: int = 256,
+                         n_lo: int = 8) -> list[np.ndarray]:
+    """Same distribution as batch_workload, generated with torch (FP64 QR on
+    `device`, e.g. a GPU, for speed) and stored as FP32.  Shapes and kappas
+    come from the numpy stream of `seed`; the Gaussian factors from a torch
+    generator seeded with `seed`."""
+    import torch
+
+    ms, ns, kappas, rng = batch_shapes(count, seed, m_lo, m_hi, n_lo)
+    dev = torch.device(device) if device is not None else torch.device("cpu")
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    out = []
+    for m, n, kappa in zip(ms, ns, kappas):
+        m, n = int(m), int(n)
+        s = np.sort(10.0 ** rng.uniform(-math.log10(kappa), 0.0, size=n))[::-1].copy()
+        s[0] = 1.0
+        gu = torch.randn((m, n), generator=g, dtype=torch.float64, device=dev)
+        gv = torch.randn((n, n), generator=g, dtype=torch.float64, device=dev)
+        qu, ru = torch.linalg.qr(gu)
+        qv, rv = torch.linalg.qr(gv)
+        qu = qu * torch.sign(torch.diagonal(ru))[None, :]
+        qv = qv * torch.sign(torch.diagonal(rv))[None, :]
+        st = torch.from_numpy(s).to(dev)
+        a = (qu * st[None, :]) @ qv.T
+        out.append(a.to(torch.float32).cpu().numpy())
+    return out

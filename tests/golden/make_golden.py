@@ -7,10 +7,12 @@ records its outputs.  It also runs the oracle under every FMA-placement variant
 and records which variant reproduces the reference bit for bit.
 
 Usage (needs a GPU and a built oracle/_ref):
-    python tests/golden/make_golden.py OUTDIR
+    python tests/golden/make_golden.py OUTDIR [--pipeline-only]
 Writes OUTDIR/<case>.npz and OUTDIR/summary.json.  Small cases keep the full
 U, Sigma, V; large cases keep Sigma, the sweep count and SHA-256 digests of
-the U and V bytes.
+the U and V bytes.  It also writes OUTDIR/pipeline_in.mat (a seeded stream of
+testcases) and OUTDIR/pipeline_ref_out.mat, the output of the reference's own
+CLI (oracle/_ref/jacobi-svd-cuda -e 1e-12) on it.
 """
 from __future__ import annotations
 
@@ -18,6 +20,7 @@ import ctypes
 import hashlib
 import json
 import os
+import subprocess
 import sys
 
 import numpy as np
@@ -26,6 +29,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "jacobi-svd-cuda_b200"))
 
+import matfile  # noqa: E402
 import oracle as O  # noqa: E402
 import workloads as W  # noqa: E402
 
@@ -97,8 +101,27 @@ def digest(x: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(x, dtype=np.float64).tobytes()).hexdigest()
 
 
+def pipeline_golden(outdir: str) -> None:
+    """Seeded testcase stream through the reference CLI."""
+    rng = np.random.default_rng(2024)
+    mats = [W.gaussian_splitmix(5, 3, 31), np.eye(4), W.gaussian_splitmix(7, 1, 32)]
+    for k in range(9):
+        m = int(rng.integers(2, 90))
+        n = int(rng.integers(1, m + 1))
+        mats.append(rng.standard_normal((m, n)))
+    inp = os.path.join(outdir, "pipeline_in.mat")
+    out = os.path.join(outdir, "pipeline_ref_out.mat")
+    matfile.write(inp, mats)
+    cli = os.path.join(ROOT, "oracle", "_ref", "jacobi-svd-cuda")
+    subprocess.check_call([cli, "-i", inp, "-o", out, "-e", "1e-12", "--force", "-q"])
+    print("pipeline golden:", len(mats), "testcases,", os.path.getsize(out), "bytes")
+
+
 def main(outdir: str) -> int:
     os.makedirs(outdir, exist_ok=True)
+    pipeline_golden(outdir)
+    if "--pipeline-only" in sys.argv:
+        return 0
     L = ref_lib()
     threads = os.cpu_count() or 1
     summary = {"variants": {}, "cases": {}}

@@ -1,0 +1,69 @@
+"""Batched solver (one persistent launch per size class) against the oracle.
+
+Every matrix of a batch uses the plain path's arithmetic, so each result must
+be bit-identical to the oracle on the same FP64 (or FP32-promoted) input:
+same sigma, U and V bytes and sweep count.  The batch spans all four size
+classes (<= 48 KiB, <= 100 KiB, <= 227 KiB of shared memory, and the global
+memory class) and odd/even n.
+"""
+import numpy as np
+import pytest
+
+import jsvd
+import oracle as O
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(16, 8), (17, 17), (40, 33), (60, 50), (31, 1), (2, 2), (100, 90), (120, 100), (129, 64),
+          (256, 200), (256, 256), (250, 131), (8, 8), (64, 63), (200, 9)]
+
+
+def _mats(seed, f32):
+    rng = np.random.default_rng(seed)
+    out = []
+    for m, n in SHAPES:
+        a = rng.standard_normal((m, n))
+        out.append(a.astype(np.float32) if f32 else a)
+    return out
+
+
+@pytest.mark.parametrize("f32", [False, True])
+def test_batch_bitwise_vs_oracle(cuda_device, f32):
+    mats = _mats(11 + int(f32), f32)
+    b = jsvd.DeviceBatch(mats, cuda_device, f32=f32, want_u=True)
+    b.solve(jsvd.default_config(epsilon=1e-13))
+    got = b.results()
+    for a, (u, s, v, sw) in zip(mats, got):
+        eu, es, ev, esw = O.plain_svd(a.astype(np.float64), eps=1e-13, variant=jsvd.arith_variant(), threads=4)
+        assert sw == esw, a.shape
+        assert np.array_equal(s, es), a.shape
+        assert np.array_equal(v, ev), a.shape
+        assert np.array_equal(u, eu), a.shape
+
+
+def test_batch_workload_sample_accuracy(cuda_device):
+    """A sample of the mixed-size FP32 batch workload: sigma against LAPACK on
+    the FP32-promoted input and orthogonality of V."""
+    mats = W.batch_workload(64, seed=3)
+    b = jsvd.DeviceBatch(mats, cuda_device, f32=True)
+    b.solve(jsvd.default_config(epsilon=1e-14))
+    for a, (_, s, v, sw) in zip(mats, b.results()):
+        ref = np.linalg.svd(a.astype(np.float64), compute_uv=False)
+        e = O.sigma_errors(s, ref)
+        assert e["normwise"] < 1e-13
+        assert O.residuals(a.astype(np.float64), None, s, v)["rho_V"] < 1e-12
+        assert 1 <= sw < 128
+
+
+def test_batch_tuning_and_empty(cuda_device):
+    mats = _mats(5, False)[:6]
+    b = jsvd.DeviceBatch(mats, cuda_device)
+    b.solve(jsvd.default_config(epsilon=1e-12), tuning=[(128, 2), (512, 1), (256, 1), (256, 1)])
+    ref = jsvd.DeviceBatch(mats, cuda_device)
+    ref.solve(jsvd.default_config(epsilon=1e-12))
+    for x, y in zip(b.results(), ref.results()):
+        assert np.array_equal(x[1], y[1]) and np.array_equal(x[2], y[2]) and x[3] == y[3]
+    empty = jsvd.DeviceBatch([np.zeros((3, 2))], cuda_device)
+    empty.count = 0
+    empty.solve()

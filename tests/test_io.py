@@ -1,0 +1,136 @@
+"""The *.mat / *.txt stream formats (include/io.hpp) and the CLI's argument
+handling, on CPU.
+
+*.mat records are u64 rows | u64 columns | f64 values, big-endian, row-major
+(reference include/io.hpp:40-51); the C++ codec must round-trip byte for byte
+with the independent Python codec, reject truncated records with the
+reference's messages, and print text with max_digits10 (exact round trip).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import matfile
+from conftest import PKG, ROOT
+
+DRIVER = os.path.join(ROOT, "tests", "cpp", "io_driver.cpp")
+CLI = os.path.join(PKG, "jacobi-svd-b200")
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    out = tmp_path_factory.mktemp("io") / "io_driver"
+    subprocess.check_call(["g++", "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include"),
+                           "-I/usr/local/cuda/include", DRIVER, "-o", str(out), "-L", PKG, "-ljsvd",
+                           "-L/usr/local/cuda/lib64", "-lcudart", f"-Wl,-rpath,{PKG}"])
+    return str(out)
+
+
+def _mats(seed=0):
+    rng = np.random.default_rng(seed)
+    return [rng.standard_normal((3, 2)), np.arange(12.0).reshape(4, 3) - 5.5, np.array([[1e-300, -0.0]]),
+            rng.standard_normal((1, 7)) * 1e200, np.array([[np.pi]])]
+
+
+def run(driver, *args):
+    return subprocess.run([driver, *map(str, args)], capture_output=True, text=True)
+
+
+def test_mat_roundtrip_bytes(driver, tmp_path):
+    src, dst = tmp_path / "a.mat", tmp_path / "b.mat"
+    matfile.write(src, _mats())
+    r = run(driver, "mat-copy", src, dst)
+    assert r.returncode == 0, r.stdout
+    assert dst.read_bytes() == src.read_bytes()
+    r = run(driver, "stream-copy", src, tmp_path / "c.mat")
+    assert r.returncode == 0 and "records 5" in r.stdout
+    assert (tmp_path / "c.mat").read_bytes() == src.read_bytes()
+
+
+def test_mat_to_txt_is_exact(driver, tmp_path):
+    src, txt, back = tmp_path / "a.mat", tmp_path / "a.txt", tmp_path / "b.txt"
+    mats = _mats(1)
+    matfile.write(src, mats)
+    assert run(driver, "mat-to-txt", src, txt).returncode == 0
+    text = txt.read_text()
+    blocks = [b for b in text.split("\n\n") if b.strip()]
+    assert len(blocks) == len(mats)
+    for blk, a in zip(blocks, mats):
+        got = np.array([[float(x) for x in line.split()] for line in blk.strip().splitlines()])
+        assert got.shape == a.shape and np.array_equal(got, a)
+    assert run(driver, "txt-copy", txt, back).returncode == 0
+    assert back.read_text() == text
+
+
+@pytest.mark.parametrize("cut,msg", [(10, "Truncated *.mat header."), (16 + 8 * 5, "Truncated *.mat payload.")])
+def test_truncated_mat(driver, tmp_path, cut, msg):
+    src = tmp_path / "t.mat"
+    data = matfile.encode(_mats()[:2])
+    src.write_bytes(data[:cut])
+    r = run(driver, "mat-copy", src, tmp_path / "o.mat")
+    assert r.returncode == 1 and msg in r.stdout
+
+
+def test_txt_errors(driver, tmp_path):
+    bad = tmp_path / "bad.txt"
+    bad.write_text("1 2\n3\n")
+    r = run(driver, "txt-copy", bad, tmp_path / "o.txt")
+    assert r.returncode == 1 and "Inconsistent column count in text matrix block." in r.stdout
+    bad.write_text("1 x\n")
+    r = run(driver, "txt-copy", bad, tmp_path / "o.txt")
+    assert r.returncode == 1 and "Invalid numeric token in text matrix row." in r.stdout
+
+
+def test_empty_mat_file(driver, tmp_path):
+    src = tmp_path / "e.mat"
+    src.write_bytes(b"")
+    assert run(driver, "mat-copy", src, tmp_path / "o.mat").returncode == 0
+    assert (tmp_path / "o.mat").read_bytes() == b""
+
+
+# ---- CLI (argument handling needs no GPU) -----------------------------------------
+
+def cli(*args, cwd=None):
+    return subprocess.run([CLI, *map(str, args)], capture_output=True, text=True, cwd=cwd)
+
+
+def test_cli_version_and_help():
+    r = cli("--version")
+    assert r.returncode == 0 and "sm_100a" in r.stdout
+    r = cli("-h")
+    assert r.returncode == 0 and "--layout-transpose-mode" in r.stdout and "--queue-capacity" in r.stdout
+
+
+def test_cli_argument_errors(tmp_path):
+    assert cli().returncode == 2
+    r = cli(tmp_path / "missing.mat")
+    assert r.returncode == 2 and "Input file does not exist" in r.stderr
+    src = tmp_path / "a.mat"
+    matfile.write(src, _mats())
+    r = cli(src, "--epsilon", "-1")
+    assert r.returncode == 2 and "must be a positive finite number" in r.stderr
+    r = cli(src, "--max-sweeps", "x")
+    assert r.returncode == 2 and "Invalid integer value for --max-sweeps." in r.stderr
+    r = cli(src, "--bogus")
+    assert r.returncode == 2 and "Unknown option: --bogus" in r.stderr
+    r = cli(src, src)
+    assert r.returncode == 2 and "must be different files" in r.stderr
+    (tmp_path / "a.svd.mat").write_bytes(b"")
+    r = cli(src)
+    assert r.returncode == 2 and "Use --force to overwrite" in r.stderr
+    r = cli(tmp_path / "noext", "--dry-run")
+    assert r.returncode == 2
+
+
+def test_cli_dry_run_defaults(tmp_path):
+    src = tmp_path / "case.txt"
+    src.write_text("1 2\n3 4\n")
+    r = cli(src, "--dry-run", "-e", "1e-12", "-t", "128", "--layout-transpose-mode", "off")
+    assert r.returncode == 0
+    assert f"output          : {tmp_path / 'case.svd.txt'}" in r.stdout
+    assert "epsilon         : 1e-12" in r.stdout
+    assert "threads-per-blk : 128" in r.stdout and "layout-mode     : off" in r.stdout
+    r = cli(src, tmp_path / "out", "--dry-run")
+    assert f"output          : {tmp_path / 'out.txt'}" in r.stdout
