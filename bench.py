@@ -127,11 +127,12 @@ def algorithmic_round_bytes(m: int, n: int) -> float:
     return (n // 2) * 4.0 * m * 8.0
 
 
-def run_ours(args, rank: int, world: int, device):
+def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
+    """Device-timed SVDs of one workload matrix through one path; returns
+    (total_ms, sweeps list, per-path stats, last sigma)."""
     import torch
     import jsvd
 
-    wl = make_workload(args.workload)
     a = wl["a"]
     m, n = a.shape
     cfg = jsvd.default_config(epsilon=wl["eps"])
@@ -139,36 +140,22 @@ def run_ours(args, rank: int, world: int, device):
     du = torch.empty((m, n), dtype=torch.float64, device=device)
     ds = torch.empty(n, dtype=torch.float64, device=device)
     dv = torch.empty((n, n), dtype=torch.float64, device=device)
-    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
-    torch.cuda.synchronize(device)
-    stream = torch.cuda.Stream(device)
-    torch.cuda.set_stream(stream)
+    fn = {"precond": jsvd.precond_svd_device, "blocked": jsvd.blocked_svd_device}.get(path, jsvd.plain_svd_device)
 
     def step():
-        return jsvd.plain_svd_device(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg,
-                                     stream.cuda_stream)
+        return fn(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg, stream.cuda_stream)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize(device)
-
-    # correctness guard on the timed configuration (sigma vs the analytic spectrum)
-    sig = np.sort(ds.cpu().numpy())[::-1]
-    guard = None
-    if wl["sigma_true"] is not None:
-        t = np.sort(wl["sigma_true"])[::-1]
-        guard = {"sigma_max_rel_vs_analytic": float(np.max(np.abs(sig - t) / t)),
-                 "sigma_normwise_vs_analytic": float(np.max(np.abs(sig - t)) / t[0])}
-
     jsvd.plain_stats_reset()
-    sampler = ClockSampler(device.index if device.index is not None else 0)
+    jsvd.precond_stats_reset()
+    jsvd.blocked_stats_reset()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(device)
-    sampler.start()
-    total_ms = 0.0
-    sweeps = []
-    for _ in range(args.steps):
+    total_ms, sweeps = 0.0, []
+    for _ in range(steps):
         flush.zero_()  # evict A, V and the working copies from L2 between steps
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -178,34 +165,84 @@ def run_ours(args, rank: int, world: int, device):
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
     torch.cuda.synchronize(device)
-    clocks = sampler.stop()
-    st = jsvd.plain_stats()
     if world > 1:
         t = torch.tensor([total_ms], dtype=torch.float64, device=device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
+    return total_ms, sweeps, (jsvd.plain_stats(), jsvd.precond_stats(), jsvd.blocked_stats()), ds.cpu().numpy(), \
+        (du, dv)
+
+
+def blocked_sweep_flops(rows: int, n: int, b: int = 32) -> float:
+    """FP64 flops of one blocked sweep: for every block pair, the panel Gram
+    (2 rows w^2) and the panel update of X and V (2 (rows + n) w^2), w = 2b."""
+    nb = -(-n // b)
+    w = 2 * b
+    return nb * (nb - 1) / 2 * (2.0 * rows * w * w + 2.0 * (rows + n) * w * w)
+
+
+def run_ours(args, rank: int, world: int, device):
+    import ctypes
+
+    import torch
+    import jsvd
+
+    wl = make_workload(args.workload)
+    a = wl["a"]
+    m, n = a.shape
+    path = args.path if args.path != "auto" else "precond"
+    cfg = jsvd.default_config(epsilon=wl["eps"])
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    torch.cuda.synchronize(device)
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
+
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    sampler.start()
+    total_ms, sweeps, (pst, cst, bst), sig, (du, dv) = time_single(args, wl, path, device, stream, args.steps,
+                                                                  args.warmup, flush, world)
+    clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms / 1e3)
-    launches = int(st.round_launches + st.vpass_launches + st.other_launches)
+    launches = int(pst.round_launches + pst.vpass_launches + pst.other_launches)
+    if path == "precond":
+        # per solve: layout kernel, 3 passes x (shift?, ceil(n/64) x (chol + trsm) + ceil(n/64) trsm + 1), status
+        blocks = (n + 63) // 64
+        launches += args.steps * (1 + 3 * (3 * blocks + 1) + 1)
+
+    # accuracy guard on the timed configuration (sigma vs the analytic spectrum,
+    # and the reference's residual metrics on the returned factors)
+    sig_cols = sig.copy()
+    sig = np.sort(sig)[::-1]
+    guard = None
+    if wl["sigma_true"] is not None:
+        t = np.sort(wl["sigma_true"])[::-1]
+        guard = {"sigma_max_rel_vs_analytic": float(np.max(np.abs(sig - t) / t)),
+                 "sigma_normwise_vs_analytic": float(np.max(np.abs(sig - t)) / t[0])}
+    if m * n <= (1 << 22):
+        import sys as _s
+        _s.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        guard = dict(guard or {}, **O.residuals(a, du.cpu().numpy(), sig_cols, dv.cpu().numpy()))
 
     # e2e through the host-buffer C-ABI call, pinned host memory
     ha = torch.from_numpy(a).pin_memory().numpy()
     hu = torch.empty((m, n), dtype=torch.float64).pin_memory().numpy()
     hs = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
     hv = torch.empty((n, n), dtype=torch.float64).pin_memory().numpy()
-    import ctypes
     lib = jsvd.lib()
+    entry = lib.jsvd_precond_svd if path in ("precond", "blocked") else lib.jsvd_plain_svd
     sw = ctypes.c_int(0)
     for _ in range(max(1, args.warmup)):
-        jsvd.check(lib.jsvd_plain_svd(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data,
-                                      hv.ctypes.data, ctypes.byref(sw)))
+        jsvd.check(entry(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data, hv.ctypes.data,
+                         ctypes.byref(sw)))
     e2e_s = 0.0
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
-        jsvd.check(lib.jsvd_plain_svd(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data,
-                                      hv.ctypes.data, ctypes.byref(sw)))
+        jsvd.check(entry(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data, hv.ctypes.data,
+                         ctypes.byref(sw)))
         e2e_s += time.perf_counter() - t0
     if world > 1:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
@@ -213,9 +250,41 @@ def run_ours(args, rank: int, world: int, device):
         e2e_s = float(t.item())
     e2e_value = world * args.steps / e2e_s
 
+    # the plain drop-in on the same input, for the speed-up of the fast path
+    plain = None
+    if path != "plain" and not args.no_plain_compare:
+        p_ms, p_sw, _, _, _ = time_single(args, wl, "plain", device, stream, 2, 1, flush, world)
+        plain = {"value": world * 2 / (p_ms / 1e3), "ms_per_step": p_ms / 2, "sweeps_per_svd": p_sw[0]}
+
     hbm_peak, _, peak_kind = peaks()
-    avg_round_ms = st.round_ms / max(1, st.round_launches)
-    achieved = algorithmic_round_bytes(m, n) / (avg_round_ms * 1e-3) / 1e9
+    mx = n if path == "precond" else m  # rows of the swept matrix
+    if pst.round_launches:
+        avg_round_ms = pst.round_ms / pst.round_launches
+        roof = {"bound": "hbm", "kernel": "plain_round_kernel",
+                "achieved": algorithmic_round_bytes(mx, n) / (avg_round_ms * 1e-3) / 1e9, "peak": hbm_peak,
+                "unit": "GB/s", "peak_kind": peak_kind, "traffic": None, "avg_launch_us": avg_round_ms * 1e3,
+                "algorithmic_bytes_per_launch": algorithmic_round_bytes(mx, n),
+                "round_share_of_step": pst.round_ms / max(total_ms / world, 1e-9),
+                "vpass_ms_per_sweep": pst.vpass_ms / max(1, pst.vpass_launches)}
+    else:
+        # blocked sweep: FP64 work of the Gram and apply kernels against the
+        # measured FP64 FMA peak
+        fp64_peak = jsvd.probe_fp64_tflops()
+        flops = blocked_sweep_flops(mx, n) * bst.sweeps
+        roof = {"bound": "fp64", "kernel": "blk_gram + blk_solve + blk_apply",
+                "achieved": flops / (bst.sweep_ms * 1e-3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                "peak_kind": "measured FP64 FMA probe (jsvd_probe_fp64_tflops)", "traffic": None,
+                "flops_per_sweep": blocked_sweep_flops(mx, n),
+                "sweep_share_of_step": bst.sweep_ms / max(total_ms / world, 1e-9)}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    phases = None
+    if path == "precond" and cst.solves:
+        phases = {"qr_ms": cst.qr_ms / cst.solves, "jacobi_ms": cst.jacobi_ms / cst.solves,
+                  "u_ms": cst.u_ms / cst.solves, "fallbacks": int(cst.fallbacks)}
+    if bst.solves:
+        phases = dict(phases or {}, blocked_sweeps=bst.sweeps / bst.solves,
+                      blocked_sweep_ms=bst.sweep_ms / max(1, bst.sweeps),
+                      block_rounds_per_sweep=bst.block_rounds / max(1, bst.sweeps))
     line = {
         "metric": "SVDs/s",
         "value": value,
@@ -229,24 +298,23 @@ def run_ours(args, rank: int, world: int, device):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded)",
-        "config": {"workload": wl["desc"], "path": "plain FP64 drop-in (reference arithmetic, round-robin)",
+        "config": {"workload": wl["desc"],
+                   "path": {"precond": "QR-preconditioned: shifted CholeskyQR3 + blocked FP64 Jacobi on R^T",
+                            "blocked": "blocked FP64 one-sided Jacobi on A (32-column blocks)"}.get(
+                       path, "plain FP64 drop-in (reference arithmetic, round-robin)"),
                    "epsilon": wl["eps"], "sweeps_per_svd": sweeps[0] if sweeps else None,
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "phases_ms": phases},
+        "plain_path": plain,
         "e2e": {"value": e2e_value, "unit": "SVD/s", "h2d_bytes_per_step": a.nbytes,
                 "d2h_bytes_per_step": (m * n + n + n * n) * 8, "timer": "host wall clock around the synchronous call"},
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "plain_round_kernel", "achieved": achieved, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": None, "avg_launch_us": avg_round_ms * 1e3,
-                     "algorithmic_bytes_per_launch": algorithmic_round_bytes(m, n),
-                     "round_share_of_step": st.round_ms / max(total_ms / world, 1e-9),
-                     "vpass_ms_per_sweep": st.vpass_ms / max(1, st.vpass_launches)},
+        "roofline": roof,
         "clocks": clocks,
         "check": guard,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(wl, sweeps[0] if sweeps else PLAIN_SWEEPS.get(wl["name"], 12),
-                                            budget_s=args.cpu_budget)
+        line["cpu_baseline"] = cpu_baseline(wl, PLAIN_SWEEPS.get(wl["name"], 12), budget_s=args.cpu_budget)
     return line
 
 
@@ -465,6 +533,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
+    ap.add_argument("--no-plain-compare", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -179,6 +179,45 @@ typedef struct jsvd_batch_stats {
 void jsvd_batch_stats_get(jsvd_batch_stats *out);
 void jsvd_batch_stats_reset(void);
 
+/* ---- QR-preconditioned path -------------------------------------------------
+ * The fast path for tall and ill-conditioned matrices (no counterpart in the
+ * reference, which always sweeps A directly): A = Q R by shifted CholeskyQR3,
+ * one-sided Jacobi (the plain sweep) on X = R^T, then V_A = normalised columns
+ * of the rotated X, U_A = Q V_x.  Same inputs, outputs and validation as
+ * jsvd_plain_svd / jsvd_plain_svd_device; sigma is unsorted; *sweeps is the
+ * sweep count on X.  Falls back to the plain path if a Cholesky pivot is not
+ * positive.  Results agree with the plain path to working accuracy
+ * (normwise sigma error ~1e-14, orthogonality ~1e-13), not bit for bit. */
+int jsvd_precond_svd(const double *a, size_t rows, size_t columns, const jsvd_config *cfg, double *u,
+                     double *sigma, double *v, int *sweeps);
+int jsvd_precond_svd_device(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,
+                            double *d_sigma, double *d_v, int *sweeps, void *stream);
+
+/* Blocked FP64 one-sided Jacobi (no counterpart in the reference): column
+ * blocks of 32, block pairs in the round-robin order, per pair a panel Gram,
+ * a two-sided Jacobi solve of the 64 x 64 Gram and the panel update P <- P W.
+ * Same arguments and outputs as jsvd_plain_svd_device; accurate to working
+ * precision, not bit-identical to the plain path.  Below 64 columns (fewer
+ * than two blocks) it runs the plain sweep. */
+int jsvd_blocked_svd_device(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,
+                            double *d_sigma, double *d_v, int *sweeps, void *stream);
+
+typedef struct jsvd_blocked_stats {
+    unsigned long long solves, sweeps, block_rounds;
+    double sweep_ms; /* device time of the sweeps (events) */
+} jsvd_blocked_stats;
+
+void jsvd_blocked_stats_get(jsvd_blocked_stats *out);
+void jsvd_blocked_stats_reset(void);
+
+typedef struct jsvd_precond_stats {
+    unsigned long long solves, fallbacks;
+    double qr_ms, jacobi_ms, u_ms; /* device time per phase (events) */
+} jsvd_precond_stats;
+
+void jsvd_precond_stats_get(jsvd_precond_stats *out);
+void jsvd_precond_stats_reset(void);
+
 /* ---- serving loop -----------------------------------------------------------
  * Continuous batching of SVD requests on the current device.  Replaces the
  * reference's thread-pool dispatch of one_sided_jacobi_svd per testcase
@@ -196,6 +235,7 @@ typedef struct jsvd_server_options {
     int large_workers;          /* concurrent large solves, one stream each (0 = 4) */
     int max_batch;              /* requests per batched launch (0 = 4096)           */
     jsvd_config cfg;            /* epsilon, max_sweeps, threads_per_block           */
+    int large_path;             /* 0 = plain sweep, 1 = QR-preconditioned           */
 } jsvd_server_options;
 
 typedef struct jsvd_server_stats {

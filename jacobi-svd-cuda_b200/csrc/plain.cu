@@ -216,11 +216,14 @@ __device__ __forceinline__ int2 schedule_pair(int n, int r, int k)
 }
 
 // Deferred V update: applies every rotation of one sweep to R rows of V
-// (R = 4 or 8, a template parameter so the row loop is vectorised).
+// (R in {1, 2, 4, 8}, a template parameter so the row loop unrolls).
 // V is column-major (element (row, col) at col*ldv + row); the CTA stages its
-// rows as sv[col*R + rr] in shared memory, so the round-to-round dependency
-// never leaves the SM.  Thread k owns pair slot k of every round; the (c, s)
-// of the next round is loaded while the current one is applied.
+// R rows row by row in shared memory, sv[rr*n + col], so the round-to-round
+// dependency never leaves the SM and the 32 lanes of a warp, which rotate 32
+// unrelated column pairs, spread over the banks instead of all starting at the
+// same bank (which a column-by-column staging with R = 8 would cause).
+// Thread k owns pair slot k of every round; the (c, s) of the next round is
+// loaded while the current one is applied.
 template <int R>
 __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v, long ldv, int n,
                                                           const double2 *__restrict__ cs, int rounds, int npairs)
@@ -231,7 +234,7 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
     const int total = n * R;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         const int col = idx / R, rr = idx - col * R;
-        sv[idx] = (rr < rows) ? v[(size_t)col * ldv + r0 + rr] : 0.0;
+        sv[rr * n + col] = (rr < rows) ? v[(size_t)col * ldv + r0 + rr] : 0.0;
     }
     __syncthreads();
     const int k0 = threadIdx.x;
@@ -247,19 +250,16 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
             }
             if (g.x != 0.0) {
                 const int2 pq = schedule_pair(n, r, k);
-                if constexpr (R == 1) {
-                    const double x = sv[pq.x], y = sv[pq.y];
-                    sv[pq.x] = rot_p(g.x, g.y, x, y);
-                    sv[pq.y] = rot_q(g.x, g.y, x, y);
-                } else {
-                    double2 *__restrict__ xp = reinterpret_cast<double2 *>(sv + (size_t)pq.x * R);
-                    double2 *__restrict__ xq = reinterpret_cast<double2 *>(sv + (size_t)pq.y * R);
+                double x[R], y[R];
 #pragma unroll
-                    for (int h = 0; h < R / 2; ++h) {
-                        const double2 x = xp[h], y = xq[h];
-                        xp[h] = make_double2(rot_p(g.x, g.y, x.x, y.x), rot_p(g.x, g.y, x.y, y.y));
-                        xq[h] = make_double2(rot_q(g.x, g.y, x.x, y.x), rot_q(g.x, g.y, x.y, y.y));
-                    }
+                for (int h = 0; h < R; ++h) {
+                    x[h] = sv[h * n + pq.x];
+                    y[h] = sv[h * n + pq.y];
+                }
+#pragma unroll
+                for (int h = 0; h < R; ++h) {
+                    sv[h * n + pq.x] = rot_p(g.x, g.y, x[h], y[h]);
+                    sv[h * n + pq.y] = rot_q(g.x, g.y, x[h], y[h]);
                 }
             }
         }
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
     }
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         const int col = idx / R, rr = idx - col * R;
-        if (rr < rows) v[(size_t)col * ldv + r0 + rr] = sv[idx];
+        if (rr < rows) v[(size_t)col * ldv + r0 + rr] = sv[rr * n + col];
     }
 }
 

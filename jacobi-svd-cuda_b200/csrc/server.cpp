@@ -51,8 +51,10 @@ size_t small_footprint(size_t m, size_t n, bool want_u)
 
 size_t large_footprint(size_t m, size_t n)
 {
-    // I/O buffers (A, U, sigma, V) + plan (A_w, V_w, sigma, schedule and angles)
-    return sizeof(double) * (2 * m * n + n + n * n) + sizeof(double) * (m * n + n * n + n) + 24 * n * n;
+    // I/O buffers (A, U, sigma, V) + plan (A_w, V_w, sigma, schedule and
+    // angles) + the preconditioned path's Q and seven n x n scratch matrices
+    return sizeof(double) * (2 * m * n + n + n * n) + sizeof(double) * (m * n + n * n + n) + 24 * n * n +
+           sizeof(double) * (m * n + 7 * n * n);
 }
 
 struct Request {
@@ -337,7 +339,8 @@ private:
         JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * doubles, st));
         JSVD_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double) * m * n, cudaMemcpyHostToDevice, st));
         double *ds = d + m * n, *dv = ds + n, *du = r->want_u ? dv + n * n : nullptr;
-        rc = jsvd_plain_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st);
+        rc = opt_.large_path == 1 ? jsvd_precond_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st)
+                                  : jsvd_plain_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st);
         if (rc != JSVD_OK) {
             cudaFreeAsync(d, st);
             return rc;

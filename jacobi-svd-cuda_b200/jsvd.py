@@ -84,6 +84,7 @@ class ServerOptions(ctypes.Structure):
         ("large_workers", ctypes.c_int),
         ("max_batch", ctypes.c_int),
         ("cfg", Config),
+        ("large_path", ctypes.c_int),
     ]
 
 
@@ -95,6 +96,16 @@ class ServerStats(ctypes.Structure):
         ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
         ("peak_device_bytes", ctypes.c_size_t), ("device_bytes_in_use", ctypes.c_size_t),
     ]
+
+
+class PrecondStats(ctypes.Structure):
+    _fields_ = [("solves", ctypes.c_ulonglong), ("fallbacks", ctypes.c_ulonglong), ("qr_ms", ctypes.c_double),
+                ("jacobi_ms", ctypes.c_double), ("u_ms", ctypes.c_double)]
+
+
+class BlockedStats(ctypes.Structure):
+    _fields_ = [("solves", ctypes.c_ulonglong), ("sweeps", ctypes.c_ulonglong),
+                ("block_rounds", ctypes.c_ulonglong), ("sweep_ms", ctypes.c_double)]
 
 
 class JsvdError(RuntimeError):
@@ -126,7 +137,9 @@ def exported_symbols() -> list[str]:
         "jsvd_plain_stats_get", "jsvd_plain_stats_reset", "jsvd_plain_svd_noalloc",
         "jsvd_batch_svd_device", "jsvd_batch_stats_get", "jsvd_batch_stats_reset", "jsvd_probe_fp64_tflops",
         "jsvd_server_options_default", "jsvd_server_create", "jsvd_server_submit", "jsvd_server_wait",
-        "jsvd_server_get_stats", "jsvd_server_destroy",
+        "jsvd_server_get_stats", "jsvd_server_destroy", "jsvd_precond_svd", "jsvd_precond_svd_device",
+        "jsvd_precond_stats_get", "jsvd_precond_stats_reset", "jsvd_blocked_svd_device",
+        "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset",
     ]
 
 
@@ -173,6 +186,18 @@ def lib() -> ctypes.CDLL:
         L.jsvd_server_get_stats.restype = I
         L.jsvd_server_destroy.argtypes = [P]
         L.jsvd_server_destroy.restype = None
+        L.jsvd_precond_svd.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P]
+        L.jsvd_precond_svd.restype = I
+        L.jsvd_precond_svd_device.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P, P]
+        L.jsvd_precond_svd_device.restype = I
+        L.jsvd_precond_stats_get.argtypes = [ctypes.POINTER(PrecondStats)]
+        L.jsvd_precond_stats_get.restype = None
+        L.jsvd_precond_stats_reset.restype = None
+        L.jsvd_blocked_svd_device.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P, P]
+        L.jsvd_blocked_svd_device.restype = I
+        L.jsvd_blocked_stats_get.argtypes = [ctypes.POINTER(BlockedStats)]
+        L.jsvd_blocked_stats_get.restype = None
+        L.jsvd_blocked_stats_reset.restype = None
         _LIB = L
     return _LIB
 
@@ -219,6 +244,56 @@ def plain_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, wan
                               v.ctypes.data if v is not None else None, ctypes.byref(sw))
     check(rc)
     return u, s, v, sw.value
+
+
+def precond_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, want_v: bool = True):
+    """Host-buffer QR-preconditioned solve -> (U or None, sigma, V or None, sweeps on R^T)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    m, n = a.shape
+    cfg = cfg or default_config()
+    u = np.empty((m, n)) if want_u else None
+    s = np.empty(n)
+    v = np.empty((n, n)) if want_v else None
+    sw = ctypes.c_int(0)
+    check(lib().jsvd_precond_svd(a.ctypes.data, m, n, ctypes.byref(cfg), u.ctypes.data if u is not None else None,
+                                 s.ctypes.data, v.ctypes.data if v is not None else None, ctypes.byref(sw)))
+    return u, s, v, sw.value
+
+
+def precond_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:
+    cfg = cfg or default_config()
+    sw = ctypes.c_int(0)
+    check(lib().jsvd_precond_svd_device(d_a, m, n, ctypes.byref(cfg), d_u, d_sigma, d_v, ctypes.byref(sw),
+                                        stream or None))
+    return sw.value
+
+
+def blocked_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:
+    cfg = cfg or default_config()
+    sw = ctypes.c_int(0)
+    check(lib().jsvd_blocked_svd_device(d_a, m, n, ctypes.byref(cfg), d_u, d_sigma, d_v, ctypes.byref(sw),
+                                        stream or None))
+    return sw.value
+
+
+def blocked_stats() -> BlockedStats:
+    st = BlockedStats()
+    lib().jsvd_blocked_stats_get(ctypes.byref(st))
+    return st
+
+
+def blocked_stats_reset() -> None:
+    lib().jsvd_blocked_stats_reset()
+
+
+def precond_stats() -> PrecondStats:
+    st = PrecondStats()
+    lib().jsvd_precond_stats_get(ctypes.byref(st))
+    return st
+
+
+def precond_stats_reset() -> None:
+    lib().jsvd_precond_stats_reset()
 
 
 def plain_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:
@@ -304,7 +379,7 @@ class Server:
     """Serving core (jsvd_server_*): submit host matrices, wait for results."""
 
     def __init__(self, cfg: Config | None = None, budget_bytes: int = 0, small_workers: int = 0,
-                 large_workers: int = 0, max_batch: int = 0):
+                 large_workers: int = 0, max_batch: int = 0, large_path: int = 0):
         opt = ServerOptions()
         lib().jsvd_server_options_default(ctypes.byref(opt))
         if cfg is not None:
@@ -317,6 +392,7 @@ class Server:
             opt.large_workers = large_workers
         if max_batch:
             opt.max_batch = max_batch
+        opt.large_path = large_path
         h = ctypes.c_void_p()
         check(lib().jsvd_server_create(ctypes.byref(opt), ctypes.byref(h)))
         self.h = h
