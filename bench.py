@@ -473,6 +473,109 @@ def batch_cpu_baseline(mats, budget_s: float = 10.0, threads: int | None = None)
                       f"one matrix per thread"}
 
 
+def serve_requests(count: int, seed: int, device):
+    """Matrices of the serving workload (shapes and kappas from
+    workloads.serving_requests, Haar factors from FP64 QR on the GPU)."""
+    import torch
+    import workloads as W
+
+    t, ms, ns, kappas, rng = W.serving_requests(count, 1.0, seed=seed)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    mats = []
+    for m, n, kappa in zip(ms, ns, kappas):
+        m, n = int(m), int(n)
+        s = np.sort(10.0 ** rng.uniform(-np.log10(kappa), 0.0, size=n))[::-1].copy()
+        s[0] = 1.0
+        qu, ru = torch.linalg.qr(torch.randn((m, n), generator=g, dtype=torch.float64, device=device))
+        qv, rv = torch.linalg.qr(torch.randn((n, n), generator=g, dtype=torch.float64, device=device))
+        qu = qu * torch.sign(torch.diagonal(ru))[None, :]
+        qv = qv * torch.sign(torch.diagonal(rv))[None, :]
+        a = (qu * torch.from_numpy(s).to(device)[None, :]) @ qv.T
+        mats.append(np.ascontiguousarray(a.cpu().numpy()))
+    return t, mats
+
+
+def run_serve(args, rank: int, world: int, device):
+    """Poisson arrivals at several rates through the serving core; one step =
+    one arrival trace.  value = completed SVDs/s at the highest rate."""
+    import torch
+    import jsvd
+
+    rates = [float(r) for r in args.rates.split(",")]
+    t_unit, mats = serve_requests(args.serve_count, seed=4, device=device)
+    cfg = jsvd.default_config(epsilon=1e-14)
+    budget = 40 << 30
+    per_rate = []
+    sampler = ClockSampler(device.index if device.index is not None else 0)
+    sampler.start()
+    for rate in rates:
+        arrivals = t_unit / rate
+        with jsvd.Server(cfg, budget_bytes=budget, large_path=1) as srv:
+            # warm the worker plans and kernels
+            srv.wait(srv.submit(mats[0]))
+            tickets = [None] * len(mats)
+            lat = [0.0] * len(mats)
+            sweeps = [0] * len(mats)
+
+            def collect():
+                for i in range(len(mats)):
+                    while tickets[i] is None:
+                        time.sleep(0.0002)
+                    _, _, _, sweeps[i], lat[i] = srv.wait(tickets[i])
+
+            th = threading.Thread(target=collect)
+            th.start()
+            t0 = time.perf_counter()
+            for i, a in enumerate(mats):
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets[i] = srv.submit(a)
+            th.join()
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+        lat_sorted = np.sort(np.array(lat))
+        per_rate.append({"rate_req_s": rate, "requests": len(mats), "svd_s": len(mats) / wall,
+                         "p50_ms": float(np.percentile(lat_sorted, 50)), "p99_ms": float(np.percentile(lat_sorted, 99)),
+                         "batches": int(st.batches), "batched_requests": int(st.batched_requests),
+                         "large_solves": int(st.large_solves), "peak_device_gb": st.peak_device_bytes / 2**30})
+    clocks = sampler.stop()
+    # the plain drop-in, one request at a time, on a sample of the same trace
+    k = min(len(mats), args.serve_plain_sample)
+    t0 = time.perf_counter()
+    for a in mats[:k]:
+        jsvd.plain_svd(a, cfg)
+    plain_rate = k / (time.perf_counter() - t0)
+    top = per_rate[-1]
+    in_bytes = sum(a.nbytes for a in mats)
+    out_bytes = sum((a.shape[1] + a.shape[1] ** 2) * 8 for a in mats)
+    return {
+        "metric": "SVDs/s",
+        "value": top["svd_s"],
+        "unit": "SVD/s",
+        "n_gpus": world,
+        "steps": len(rates),
+        "warmup": 1,
+        "ms_per_step": 1e3 * top["requests"] / top["svd_s"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"serving: Poisson arrivals, {args.serve_count} requests per rate, m log-uniform "
+                               f"32..2048, n = m*U(0.25,1), FP64, kappa log-uniform [1e2,1e8], 40 GB budget (seed 4)",
+                   "path": "serving core: batched small requests + QR-preconditioned large requests",
+                   "epsilon": 1e-14, "per_rate": per_rate,
+                   "plain_one_at_a_time_svd_s": plain_rate, "plain_sample": k},
+        "e2e": {"value": top["svd_s"], "unit": "SVD/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": out_bytes, "timer": "host wall clock, submit of the first request to "
+                                                          "completion of the last (host buffers in and out)"},
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+
+
 def run_reference(args):
     if args.workload == "batch":
         import workloads as W
@@ -534,6 +637,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     ap.add_argument("--no-plain-compare", action="store_true")
+    ap.add_argument("--rates", default="50,200,1000")
+    ap.add_argument("--serve-count", type=int, default=300)
+    ap.add_argument("--serve-plain-sample", type=int, default=40)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -555,6 +661,8 @@ def main():
     try:
         if args.workload == "batch":
             line = run_batch(args, rank, world, device)
+        elif args.workload == "serve":
+            line = run_serve(args, rank, world, device)
         else:
             line = run_ours(args, rank, world, device)
     finally:

@@ -13,8 +13,10 @@
 //     and three blocking host transfers per round.
 //   * V never sits on the round-to-round critical path.  Each round records
 //     its (c, s); after the sweep one row-parallel pass applies the whole
-//     sweep to V, rows held in shared memory.  Per element the sequence of
-//     rotations is the reference's, so V is bit-identical.
+//     sweep to V, rows held in shared memory, on a second stream while the
+//     next sweep's rounds run (the angle tables alternate between sweeps).
+//     Per element the sequence of rotations is the reference's, so V is
+//     bit-identical.
 //   * A sweep (n-1 round kernels + the V pass) is launched directly the first
 //     time a plan (device, m, n, T, eps) is used and captured into a CUDA graph
 //     when the plan is reused; the host reads one rotation counter per sweep.
@@ -93,34 +95,35 @@ __global__ void identity_colmajor_kernel(double *__restrict__ v, int n, long ldv
     }
 }
 
-// Block-wide reference tree over T lanes for three quantities; result valid in
-// thread 0.  `red` holds 3*T doubles.
+// Block-wide reference tree over T lanes for three quantities.  Every warp
+// reads all T partial sums and reduces them in the reference's order itself,
+// so every thread ends with the totals after a single barrier (no second
+// barrier to broadcast a result computed by one thread).  `red` holds 3*T
+// doubles.
 template <int T>
-__device__ __forceinline__ void block_tree3(double &pp, double &qq, double &pq, double *red)
+__device__ __forceinline__ void block_tree3_all(double &pp, double &qq, double &pq, double *red)
 {
     if constexpr (T == 32) {
-        pp = warp_tree1(pp);
-        qq = warp_tree1(qq);
-        pq = warp_tree1(pq);
+        pp = __shfl_sync(0xffffffffu, warp_tree1(pp), 0);
+        qq = __shfl_sync(0xffffffffu, warp_tree1(qq), 0);
+        pq = __shfl_sync(0xffffffffu, warp_tree1(pq), 0);
     } else {
         constexpr int W = T / 32;
-        const int t = threadIdx.x;
+        const int t = threadIdx.x, lane = t & 31;
         red[t] = pp;
         red[T + t] = qq;
         red[2 * T + t] = pq;
         __syncthreads();
-        if (t < 32) {
-            double y[W];
+        double y[W];
 #pragma unroll
-            for (int w = 0; w < W; ++w) y[w] = red[w * 32 + t];
-            pp = warp_tree<W>(y);
+        for (int w = 0; w < W; ++w) y[w] = red[w * 32 + lane];
+        pp = __shfl_sync(0xffffffffu, warp_tree<W>(y), 0);
 #pragma unroll
-            for (int w = 0; w < W; ++w) y[w] = red[T + w * 32 + t];
-            qq = warp_tree<W>(y);
+        for (int w = 0; w < W; ++w) y[w] = red[T + w * 32 + lane];
+        qq = __shfl_sync(0xffffffffu, warp_tree<W>(y), 0);
 #pragma unroll
-            for (int w = 0; w < W; ++w) y[w] = red[2 * T + w * 32 + t];
-            pq = warp_tree<W>(y);
-        }
+        for (int w = 0; w < W; ++w) y[w] = red[2 * T + w * 32 + lane];
+        pq = __shfl_sync(0xffffffffu, warp_tree<W>(y), 0);
     }
 }
 
@@ -135,7 +138,6 @@ __global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, 
                                                          unsigned *__restrict__ counter)
 {
     __shared__ double red[T == 32 ? 1 : 3 * T];
-    __shared__ double2 rot;
     const int t = threadIdx.x;
     const int2 pq_idx = pairs[blockIdx.x];
     double *__restrict__ ap = a + (size_t)pq_idx.x * lda;
@@ -166,17 +168,15 @@ __global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, 
             spq = fma(x, y, spq);
         }
     }
-    block_tree3<T>(spp, sqq, spq, red);
+    block_tree3_all<T>(spp, sqq, spq, red);
+    // every thread derives the same angle from the same totals
+    double c, s;
+    const bool rotates = rotation_params(spp, sqq, spq, eps, c, s);
     if (t == 0) {
-        double c, s;
-        const bool rotates = rotation_params(spp, sqq, spq, eps, c, s);
         cs[blockIdx.x] = make_double2(c, s);
         if (rotates) atomicAdd(counter, 1u);
-        rot = make_double2(c, s);
     }
-    __syncthreads();
-    const double c = rot.x, s = rot.y;
-    if (c == 0.0) return;  // no rotation: columns unchanged
+    if (!rotates) return;  // no rotation: columns unchanged
     if constexpr (K > 0) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -390,11 +390,20 @@ PlainPlan::~PlainPlan()
     cudaGetDevice(&prev);
     if (device >= 0) cudaSetDevice(device);
     if (sweep_exec) cudaGraphExecDestroy(sweep_exec);
-    for (cudaEvent_t e : {ev_round_begin, ev_round_end, ev_vpass_end})
+    for (cudaEvent_t e : {ev_round_begin, ev_round_end})
         if (e) cudaEventDestroy(e);
     // Stream-ordered release: no device-wide synchronisation, so evicting a
     // plan does not stall work on other streams.
-    for (void *p : {(void *)a_w, (void *)v_w, (void *)pairs, (void *)cs, (void *)counter, (void *)d_in,
+    if (vstream) {
+        cudaStreamSynchronize(vstream);
+        cudaStreamDestroy(vstream);
+    }
+    for (cudaGraphExec_t g : {sweep_exec2})
+        if (g) cudaGraphExecDestroy(g);
+    for (int p = 0; p < 2; ++p)
+        for (cudaEvent_t e : {ev_rounds_done[p], ev_vpass_done[p], ev_v0[p], ev_v1[p]})
+            if (e) cudaEventDestroy(e);
+    for (void *p : {(void *)a_w, (void *)v_w, (void *)pairs, (void *)cs, (void *)cs2, (void *)counter, (void *)d_in,
                     (void *)d_u, (void *)d_sigma, (void *)d_v, (void *)sigma_w})
         if (p) cudaFreeAsync(p, stream);
     if (prev >= 0) cudaSetDevice(prev);
@@ -422,6 +431,14 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
         const size_t np = (size_t)plan->rounds * plan->npairs;
         JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->pairs, sizeof(int2) * np, stream));
         JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->cs, sizeof(double2) * np, stream));
+        JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->cs2, sizeof(double2) * np, stream));
+        JSVD_CUDA_TRY(cudaStreamCreateWithFlags(&plan->vstream, cudaStreamNonBlocking));
+        for (int p = 0; p < 2; ++p) {
+            JSVD_CUDA_TRY(cudaEventCreateWithFlags(&plan->ev_rounds_done[p], cudaEventDisableTiming));
+            JSVD_CUDA_TRY(cudaEventCreateWithFlags(&plan->ev_vpass_done[p], cudaEventDisableTiming));
+            JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_v0[p]));
+            JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_v1[p]));
+        }
         JSVD_CUDA_TRY(cudaMemcpyAsync(plan->pairs, host_pairs.data(), sizeof(int2) * np, cudaMemcpyHostToDevice,
                                       stream));
         // host_pairs dies at return: the copy must have consumed it.
@@ -442,43 +459,51 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
             cudaFuncSetAttribute(pick_vpass(R), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_begin));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_end));
-        JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_vpass_end));
     }
     plan->bytes = sizeof(double) * (m_ * n_ + n_ * n_ + n_) +
-                  (sizeof(int2) + sizeof(double2)) * (size_t)plan->rounds * plan->npairs;
+                  (sizeof(int2) + 2 * sizeof(double2)) * (size_t)plan->rounds * plan->npairs;
     // The allocations become usable on any stream once this one has drained.
     JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
     out = std::move(plan);
     return JSVD_OK;
 }
 
-// Enqueues one sweep (every round kernel, then the V pass) on `st`, bracketed
-// by the plan's timing events.  Used for direct launches and for capture.
-int PlainPlan::enqueue_sweep(cudaStream_t st)
+// Enqueues the round kernels of one sweep on `st`, writing their angles into
+// the (c, s) table of `parity`, bracketed by the plan's timing events.  Used
+// for direct launches and for capture.
+int PlainPlan::enqueue_rounds(cudaStream_t st, int parity)
 {
     RoundFn round_fn = pick_round(T, (int)m);
+    double2 *tab = parity ? cs2 : cs;
     JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_round_begin, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
     for (int r = 0; r < rounds; ++r) {
         const size_t off = (size_t)r * npairs;
-        round_fn<<<npairs, T, 0, st>>>(a_w, lda, (int)m, pairs + off, cs + off, eps, counter);
+        round_fn<<<npairs, T, 0, st>>>(a_w, lda, (int)m, pairs + off, tab + off, eps, counter);
     }
     JSVD_CUDA_TRY(cudaGetLastError());
     JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_round_end, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
-    const int vgrid = (int)((n + vpass_rows - 1) / vpass_rows);
-    pick_vpass(vpass_rows)<<<vgrid, vpass_threads, vpass_smem, st>>>(v_w, ldv, (int)n, cs, rounds, npairs);
-    JSVD_CUDA_TRY(cudaGetLastError());
-    JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_vpass_end, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
     return JSVD_OK;
 }
 
-// Captures one sweep into a graph (done when a plan is used a second time:
-// one-off shapes are not worth the instantiation).
-int PlainPlan::capture_sweep(cudaStream_t st)
+// The V pass of a sweep (all rows of V, angles of `parity`) on `st`.
+int PlainPlan::enqueue_vpass(cudaStream_t st, int parity)
+{
+    const int vgrid = (int)((n + vpass_rows - 1) / vpass_rows);
+    pick_vpass(vpass_rows)<<<vgrid, vpass_threads, vpass_smem, st>>>(v_w, ldv, (int)n, parity ? cs2 : cs, rounds,
+                                                                      npairs);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    return JSVD_OK;
+}
+
+// Captures the rounds of a sweep for one parity of the angle table into a
+// graph (done when a plan is used a second time: one-off shapes are not worth
+// the instantiation).
+int PlainPlan::capture_rounds(cudaStream_t st, int parity)
 {
     cudaGraph_t graph = nullptr;
     JSVD_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     sweep_exec_capturing = true;
-    const int rc = enqueue_sweep(st);
+    const int rc = enqueue_rounds(st, parity);
     sweep_exec_capturing = false;
     cudaError_t cap = cudaStreamEndCapture(st, &graph);
     if (rc != JSVD_OK) {
@@ -486,7 +511,8 @@ int PlainPlan::capture_sweep(cudaStream_t st)
         return rc;
     }
     if (cap != cudaSuccess) return cuda_failure(cap, "cudaStreamEndCapture", __FILE__, __LINE__);
-    cudaError_t inst = cudaGraphInstantiate(&sweep_exec, graph, 0);
+    cudaGraphExec_t *dst = parity ? &sweep_exec2 : &sweep_exec;
+    cudaError_t inst = cudaGraphInstantiate(dst, graph, 0);
     cudaGraphDestroy(graph);
     if (inst != cudaSuccess) return cuda_failure(inst, "cudaGraphInstantiate", __FILE__, __LINE__);
     return JSVD_OK;
@@ -523,27 +549,61 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
         executed = 1;  // n == 1: one empty sweep, as the reference reports
     } else {
         if (sweep_exec == nullptr && uses >= 1) {
-            const int rc = capture_sweep(stream);
+            int rc = capture_rounds(stream, 0);
+            if (rc == JSVD_OK) rc = capture_rounds(stream, 1);
             if (rc != JSVD_OK) return rc;
         }
+        // The V pass of sweep s runs on vstream while the rounds of sweep s + 1
+        // run on `stream`; the (c, s) tables alternate between sweeps, and the
+        // rounds of sweep s + 2 wait for the V pass of sweep s.
+        bool vpending[2] = {false, false};
+        auto collect_v = [&](int p) -> int {
+            if (!vpending[p]) return JSVD_OK;
+            JSVD_CUDA_TRY(cudaEventSynchronize(ev_v1[p]));
+            float v_ms = 0.f;
+            if (cudaEventElapsedTime(&v_ms, ev_v0[p], ev_v1[p]) == cudaSuccess) st.vpass_ms += v_ms;
+            vpending[p] = false;
+            return JSVD_OK;
+        };
         for (int s = 0; s < max_sweeps; ++s) {
-            JSVD_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), stream));
-            if (sweep_exec != nullptr) {
-                JSVD_CUDA_TRY(cudaGraphLaunch(sweep_exec, stream));
-            } else {
-                const int rc = enqueue_sweep(stream);
+            const int p = s & 1;
+            if (vpending[p]) {
+                JSVD_CUDA_TRY(cudaStreamWaitEvent(stream, ev_vpass_done[p], 0));
+                const int rc = collect_v(p);
                 if (rc != JSVD_OK) return rc;
             }
+            JSVD_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), stream));
+            cudaGraphExec_t g = p ? sweep_exec2 : sweep_exec;
+            if (g != nullptr) {
+                JSVD_CUDA_TRY(cudaGraphLaunch(g, stream));
+            } else {
+                const int rc = enqueue_rounds(stream, p);
+                if (rc != JSVD_OK) return rc;
+            }
+            JSVD_CUDA_TRY(cudaEventRecord(ev_rounds_done[p], stream));
+            JSVD_CUDA_TRY(cudaStreamWaitEvent(vstream, ev_rounds_done[p], 0));
+            JSVD_CUDA_TRY(cudaEventRecord(ev_v0[p], vstream));
+            {
+                const int rc = enqueue_vpass(vstream, p);
+                if (rc != JSVD_OK) return rc;
+            }
+            JSVD_CUDA_TRY(cudaEventRecord(ev_v1[p], vstream));
+            JSVD_CUDA_TRY(cudaEventRecord(ev_vpass_done[p], vstream));
+            vpending[p] = true;
             unsigned rotated = 0;
             JSVD_CUDA_TRY(cudaMemcpyAsync(&rotated, counter, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
             JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
             executed = s + 1;
-            float r_ms = 0.f, v_ms = 0.f;
+            float r_ms = 0.f;
             if (cudaEventElapsedTime(&r_ms, ev_round_begin, ev_round_end) == cudaSuccess) st.round_ms += r_ms;
-            if (cudaEventElapsedTime(&v_ms, ev_round_end, ev_vpass_end) == cudaSuccess) st.vpass_ms += v_ms;
             st.round_launches += (unsigned long long)rounds;
             st.vpass_launches += 1;
             if (rotated == 0) break;
+        }
+        for (int p = 0; p < 2; ++p) {
+            if (vpending[p]) JSVD_CUDA_TRY(cudaStreamWaitEvent(stream, ev_vpass_done[p], 0));
+            const int rc = collect_v(p);
+            if (rc != JSVD_OK) return rc;
         }
     }
     uses += 1;

@@ -26,17 +26,21 @@ struct PlainPlan {
     double *v_w = nullptr;      // column-major V (n x n)
     double *sigma_w = nullptr;  // sigma when the caller does not want it
     int2 *pairs = nullptr;      // rounds x npairs schedule
-    double2 *cs = nullptr;      // (c, s) of every pair of the current sweep
+    double2 *cs = nullptr;      // (c, s) of every pair of even sweeps
+    double2 *cs2 = nullptr;     // (c, s) of every pair of odd sweeps
     unsigned *counter = nullptr;
     unsigned long long uses = 0;
     bool sweep_exec_capturing = false;
     // staging for host-buffer calls
     double *d_in = nullptr, *d_u = nullptr, *d_sigma = nullptr, *d_v = nullptr;
 
-    cudaGraphExec_t sweep_exec = nullptr;
+    cudaGraphExec_t sweep_exec = nullptr;   // rounds of even sweeps
+    cudaGraphExec_t sweep_exec2 = nullptr;  // rounds of odd sweeps
+    cudaStream_t vstream = nullptr;         // the deferred V passes
+    cudaEvent_t ev_rounds_done[2] = {}, ev_vpass_done[2] = {}, ev_v0[2] = {}, ev_v1[2] = {};
     // Event-record nodes inside the sweep graph: before the first round,
     // after the last round, after the V pass (live kernel timing).
-    cudaEvent_t ev_round_begin = nullptr, ev_round_end = nullptr, ev_vpass_end = nullptr;
+    cudaEvent_t ev_round_begin = nullptr, ev_round_end = nullptr;
 
     PlainPlan() = default;
     ~PlainPlan();
@@ -46,8 +50,9 @@ struct PlainPlan {
     static int create(int dev, size_t m, size_t n, int T, double eps, cudaStream_t stream,
                       std::unique_ptr<PlainPlan> &out);
     int ensure_host_staging();
-    int enqueue_sweep(cudaStream_t st);
-    int capture_sweep(cudaStream_t st);
+    int enqueue_rounds(cudaStream_t st, int parity);
+    int enqueue_vpass(cudaStream_t st, int parity);
+    int capture_rounds(cudaStream_t st, int parity);
     // Runs the whole solve on device buffers; outputs may be null.
     int run(const double *d_a, double *out_u, double *out_sigma, double *out_v, int max_sweeps, int *sweeps,
             cudaStream_t stream);

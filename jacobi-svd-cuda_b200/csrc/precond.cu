@@ -96,70 +96,66 @@ __global__ void __launch_bounds__(256) pc_shift_diagonal(double *__restrict__ G,
     for (int i = threadIdx.x; i < n; i += blockDim.x) G[(size_t)i * n + i] += shift;
 }
 
-// In-place Cholesky of the kb x kb diagonal block at (k0, k0) of the lower
-// triangle of G (column-major, ld = n), one CTA; status <- 1 on a pivot that
-// is not positive and finite.
-__global__ void __launch_bounds__(256) pc_chol_diag(double *__restrict__ G, int n, int k0, int kb,
-                                                    int *__restrict__ status)
+// Cholesky of the kb x kb diagonal block at (k0, k0) of the lower triangle of
+// G (column-major, ld = n) into the same block of Lm, and the inverse of that
+// factor into Linv (column-major, ld = kNb).  1024 threads; thread t owns row
+// t / 16, columns 4 (t % 16) .. 4 (t % 16) + 3 of the block, so the
+// right-looking update needs no index arithmetic beyond that.  status <- 1
+// on a pivot that is not positive and finite.
+constexpr size_t kDiagSmem = sizeof(double) * 2 * kNb * (kNb + 1);
+
+__global__ void __launch_bounds__(1024) pc_chol_inv_diag(const double *__restrict__ G, double *__restrict__ Lm,
+                                                         int n, int k0, int kb, double *__restrict__ Linv,
+                                                         int *__restrict__ status)
 {
-    __shared__ double a[kNb][kNb + 1];
-    const int tid = threadIdx.x;
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        const int i = e % kb, j = e / kb;
-        a[i][j] = (i >= j) ? G[(size_t)(k0 + j) * n + k0 + i] : 0.0;
+    extern __shared__ double dsm[];
+    double(*a)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);
+    double(*x)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm + kNb * (kNb + 1));
+    const int t = threadIdx.x, i = t >> 4, kq = (t & 15) * 4;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int k = kq + u;
+        a[i][k] = (i < kb && k < kb) ? (i >= k ? G[(size_t)(k0 + k) * n + k0 + i] : 0.0) : (i == k ? 1.0 : 0.0);
     }
     __syncthreads();
     for (int j = 0; j < kb; ++j) {
         const double d = a[j][j];
         const bool ok = d > 0.0 && d < INFINITY;
         const double r = ok ? sqrt(d) : 1.0;
-        __syncthreads();
-        if (tid == 0) {
-            a[j][j] = r;
-            if (!ok) atomicExch(status, 1);
+        if (t == 0 && !ok) atomicExch(status, 1);
+        __syncthreads();  // every thread has read a[j][j]
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = kq + u;
+            if (k == j && i >= j) a[i][j] = (i == j) ? r : a[i][j] / r;
         }
-        for (int i = j + 1 + tid; i < kb; i += blockDim.x) a[i][j] /= r;
         __syncthreads();
-        // trailing update of the lower triangle
-        const int t = kb - j - 1;
-        for (int e = tid; e < t * t; e += blockDim.x) {
-            const int i = j + 1 + e % t, k = j + 1 + e / t;
-            if (i >= k) a[i][k] = fma(-a[i][j], a[k][j], a[i][k]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = kq + u;
+            if (k > j && i >= k) a[i][k] = fma(-a[i][j], a[k][j], a[i][k]);
         }
         __syncthreads();
     }
-    for (int e = tid; e < kb * kb; e += blockDim.x) {
-        const int i = e % kb, j = e / kb;
-        if (i >= j) G[(size_t)(k0 + j) * n + k0 + i] = a[i][j];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int k = kq + u;
+        if (i < kb && k < kb && i >= k) Lm[(size_t)(k0 + k) * n + k0 + i] = a[i][k];
     }
-}
-
-// Forward substitution on rows: for every row r of B (column-major, ld = ldb,
-// columns [c0, c0 + kb)), solve x L^T = b with L the kb x kb lower block at
-// (l0, l0) of Lm (column-major, ld = ldl):  x_j = (b_j - sum_{l<j} x_l L_jl) / L_jj.
-// Dynamic shared memory: the block of L, then the solved x of each thread.
-constexpr int kTrsmThreads = 64;
-constexpr size_t kTrsmSmem = sizeof(double) * (kNb * (kNb + 1) + kNb * kTrsmThreads);
-
-__global__ void __launch_bounds__(kTrsmThreads) pc_trsm_rows(double *__restrict__ B, long ldb, int rows, int c0,
-                                                             const double *__restrict__ Lm, long ldl, int l0, int kb)
-{
-    extern __shared__ double dsm[];
-    double(*L)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);
-    double(*xs)[kTrsmThreads] = reinterpret_cast<double(*)[kTrsmThreads]>(dsm + kNb * (kNb + 1));
-    for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-        const int i = e % kb, j = e / kb;
-        L[i][j] = (i >= j) ? Lm[(size_t)(l0 + j) * ldl + l0 + i] : 0.0;
+    // inverse by columns: thread c solves L x = e_c (forward substitution)
+    if (t < kb) {
+        const int c = t;
+        for (int rr = 0; rr < c; ++rr) x[rr][c] = 0.0;
+        for (int rr = c; rr < kb; ++rr) {
+            double acc = (rr == c) ? 1.0 : 0.0;
+            for (int k = c; k < rr; ++k) acc = fma(-a[rr][k], x[k][c], acc);
+            x[rr][c] = acc / a[rr][rr];
+        }
     }
     __syncthreads();
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows) return;
-    for (int j = 0; j < kb; ++j) {
-        double acc = B[(size_t)(c0 + j) * ldb + r];
-        for (int l = 0; l < j; ++l) acc = fma(-xs[l][threadIdx.x], L[j][l], acc);
-        const double x = acc / L[j][j];
-        xs[j][threadIdx.x] = x;
-        B[(size_t)(c0 + j) * ldb + r] = x;
+    for (int e = t; e < kNb * kNb; e += blockDim.x) {
+        const int rr = e % kNb, c = e / kNb;
+        Linv[e] = (rr < kb && c < kb) ? x[rr][c] : 0.0;
     }
 }
 
@@ -196,49 +192,48 @@ int thread_cublas(int dev, cudaStream_t st, cublasHandle_t *out)
     return JSVD_OK;
 }
 
-// One Cholesky QR pass on Q (m x n column-major, in place): G = Q^T Q (+ shift),
-// G = L L^T, Q <- Q L^{-T}, R = L^T.  G is n x n scratch.
-int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Q, int m, int n, double *G, double *R, bool shift,
-                 int *d_status)
+// One Cholesky QR pass: G = Qin^T Qin (+ shift), G = L L^T (blocked,
+// right-looking, diagonal blocks factored and inverted by pc_chol_inv_diag,
+// panels and trailing updates as DGEMM/DSYRK), Qout = Qin L^{-T} (blocked
+// right-looking solve: Qout_J = Qin_J Linv_J^T, Qin_{>J} -= Qout_J L_{>J,J}^T;
+// Qin is overwritten), R = L^T.
+int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Qin, double *Qout, int m, int n, double *G, double *Lm,
+                 double *Linv, double *R, bool shift, int *d_status)
 {
     const double one = 1.0, zero = 0.0, mone = -1.0;
-    JSVD_CUDA_TRY(cudaFuncSetAttribute(pc_trsm_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
-    JSVD_CUBLAS_TRY(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, m, &one, Q, m, &zero, G, n));
+    JSVD_CUDA_TRY(cudaFuncSetAttribute(pc_chol_inv_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
+    JSVD_CUBLAS_TRY(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, m, &one, Qin, m, &zero, G, n));
     if (shift) {
         pc_shift_diagonal<<<1, 256, 0, st>>>(G, n, m);
         JSVD_CUDA_TRY(cudaGetLastError());
     }
-    // Blocked right-looking Cholesky (lower).
-    for (int k0 = 0; k0 < n; k0 += kNb) {
+    for (int k0 = 0, blk = 0; k0 < n; k0 += kNb, ++blk) {
         const int kb = std::min(kNb, n - k0);
-        pc_chol_diag<<<1, 256, 0, st>>>(G, n, k0, kb, d_status);
+        double *li = Linv + (size_t)blk * kNb * kNb;
+        pc_chol_inv_diag<<<1, 1024, kDiagSmem, st>>>(G, Lm, n, k0, kb, li, d_status);
         JSVD_CUDA_TRY(cudaGetLastError());
         const int rest = n - k0 - kb;
         if (rest > 0) {
-            // L21 = G21 L11^{-T}: rows of G below the block, columns [k0, k0+kb)
-            pc_trsm_rows<<<(rest + kTrsmThreads - 1) / kTrsmThreads, kTrsmThreads, kTrsmSmem, st>>>(
-                G + (k0 + kb), n, rest, k0, G, n, k0, kb);
-            JSVD_CUDA_TRY(cudaGetLastError());
+            // L21 = G21 L11^{-T}
+            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, rest, kb, kb, &one, G + (size_t)k0 * n + k0 + kb,
+                                        n, li, kNb, &zero, Lm + (size_t)k0 * n + k0 + kb, n));
             // G22 -= L21 L21^T (lower)
             JSVD_CUBLAS_TRY(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, rest, kb, &mone,
-                                        G + (size_t)k0 * n + (k0 + kb), n, &one,
-                                        G + (size_t)(k0 + kb) * n + (k0 + kb), n));
+                                        Lm + (size_t)k0 * n + k0 + kb, n, &one, G + (size_t)(k0 + kb) * n + k0 + kb,
+                                        n));
         }
     }
-    // Q <- Q L^{-T}: blocked right-looking over column blocks.
-    for (int j0 = 0; j0 < n; j0 += kNb) {
+    for (int j0 = 0, blk = 0; j0 < n; j0 += kNb, ++blk) {
         const int kb = std::min(kNb, n - j0);
-        pc_trsm_rows<<<(m + kTrsmThreads - 1) / kTrsmThreads, kTrsmThreads, kTrsmSmem, st>>>(Q, m, m, j0, G, n,
-                                                                                              j0, kb);
-        JSVD_CUDA_TRY(cudaGetLastError());
+        const double *li = Linv + (size_t)blk * kNb * kNb;
+        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, kb, kb, &one, Qin + (size_t)j0 * m, m, li, kNb,
+                                    &zero, Qout + (size_t)j0 * m, m));
         const int rest = n - j0 - kb;
-        if (rest > 0) {
-            // Q[:, j0+kb:] -= Q[:, j0:j0+kb] * L[j0+kb:, j0:j0+kb]^T
-            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, rest, kb, &mone, Q + (size_t)j0 * m, m,
-                                        G + (size_t)j0 * n + (j0 + kb), n, &one, Q + (size_t)(j0 + kb) * m, m));
-        }
+        if (rest > 0)
+            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, rest, kb, &mone, Qout + (size_t)j0 * m, m,
+                                        Lm + (size_t)j0 * n + j0 + kb, n, &one, Qin + (size_t)(j0 + kb) * m, m));
     }
-    pc_lower_to_upper<<<std::min<size_t>(1184, ((size_t)n * n + 255) / 256), 256, 0, st>>>(G, R, n);
+    pc_lower_to_upper<<<std::min<size_t>(1184, ((size_t)n * n + 255) / 256), 256, 0, st>>>(Lm, R, n);
     JSVD_CUDA_TRY(cudaGetLastError());
     return JSVD_OK;
 }
@@ -265,13 +260,15 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     int rc = thread_cublas(dev, st, &hb);
     if (rc != JSVD_OK) return rc;
     const size_t mn = (size_t)m * n, nn = (size_t)n * n;
-    // workspace: Q (m x n) | G | R1 | R2 | R3 | T | Vx (n x n each) | Ux (if the caller skips V) | sigma | status
+    // workspace: Qa, Qb (m x n) | G | Lm | R1 | R2 | R3 | T | Vx | Ux (n x n) | Linv (blocks x 64 x 64) | sigma | status
+    const int nblk = (n + kNb - 1) / kNb;
     double *ws = nullptr;
-    const size_t ws_doubles = mn + 7 * nn + n + 1;
+    const size_t ws_doubles = 2 * mn + 8 * nn + (size_t)nblk * kNb * kNb + n + 1;
     JSVD_CUDA_TRY(cudaMallocAsync((void **)&ws, sizeof(double) * ws_doubles, st));
-    double *Q = ws, *G = Q + mn, *R1 = G + nn, *R2 = R1 + nn, *R3 = R2 + nn, *Tm = R3 + nn, *Vx = Tm + nn,
-           *Ux = Vx + nn, *sg = Ux + nn;
+    double *Qa = ws, *Qb = Qa + mn, *G = Qb + mn, *Lm = G + nn, *R1 = Lm + nn, *R2 = R1 + nn, *R3 = R2 + nn,
+           *Tm = R3 + nn, *Vx = Tm + nn, *Ux = Vx + nn, *Linv = Ux + nn, *sg = Linv + (size_t)nblk * kNb * kNb;
     int *d_status = reinterpret_cast<int *>(sg + n);
+    double *Q = Qb;  // after three passes (Qa -> Qb -> Qa -> Qb) the factor is in Qb
     cudaEvent_t e0, e1, e2, e3;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -287,11 +284,11 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     cudaEventRecord(e0, st);
     JSVD_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     pc_to_colmajor<<<dim3((n + kTile - 1) / kTile, (m + kTile - 1) / kTile), dim3(kTile, kTileRows), 0, st>>>(
-        d_a, m, n, Q);
+        d_a, m, n, Qa);
     JSVD_CUDA_TRY(cudaGetLastError());
-    rc = chol_qr_pass(hb, st, Q, m, n, G, R1, true, d_status);
-    if (rc == JSVD_OK) rc = chol_qr_pass(hb, st, Q, m, n, G, R2, false, d_status);
-    if (rc == JSVD_OK) rc = chol_qr_pass(hb, st, Q, m, n, G, R3, false, d_status);
+    rc = chol_qr_pass(hb, st, Qa, Qb, m, n, G, Lm, Linv, R1, true, d_status);
+    if (rc == JSVD_OK) rc = chol_qr_pass(hb, st, Qb, Qa, m, n, G, Lm, Linv, R2, false, d_status);
+    if (rc == JSVD_OK) rc = chol_qr_pass(hb, st, Qa, Qb, m, n, G, Lm, Linv, R3, false, d_status);
     if (rc != JSVD_OK) {
         cleanup();
         return rc;
