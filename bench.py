@@ -1,7 +1,7 @@
 """Benchmark of the one-sided Jacobi SVD on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tall|square512|batch|serve] [--path auto|plain|blocked]
+                    [--workload tall|square512|batch|serve|large] [--path auto|plain|precond|blocked]
 
 One step = one pass of the hot path over one batch of synthetic input (for the
 single-matrix workloads: one full SVD).  `value` is whole-job SVDs/s with the
@@ -71,6 +71,11 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi's start-up (NVML initialisation) stalls CUDA calls of this
+        # process for a few hundred ms: let it finish before the timed region.
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -377,6 +382,7 @@ def run_batch(args, rank: int, world: int, device):
     torch.cuda.synchronize(device)
     sampler.start()
     total_ms = 0.0
+    step_ms = []
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -385,7 +391,8 @@ def run_batch(args, rank: int, world: int, device):
         b.solve(cfg, stream=stream.cuda_stream)
         e1.record(stream)
         e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
+        step_ms.append(e0.elapsed_time(e1))
+        total_ms += step_ms[-1]
     clocks = sampler.stop()
     st = jsvd.batch_stats()
     if world > 1:
@@ -435,7 +442,9 @@ def run_batch(args, rank: int, world: int, device):
                    "path": "batched persistent kernels (one CTA per matrix, plain arithmetic)",
                    "epsilon": 1e-14, "mean_sweeps": float(np.mean(b.sweeps)),
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "generation_s": gen_s},
+                   "generation_s": gen_s, "step_ms": step_ms,
+                   "classes": {"count": [int(x) for x in st.class_count],
+                               "ms_per_step": [x / max(1, st.calls) for x in st.class_ms]}},
         "e2e": {"value": world * args.steps * b.count / e2e_s, "unit": "SVD/s", "h2d_bytes_per_step": b.h2d_bytes,
                 "d2h_bytes_per_step": int((b.sigma.numel() + b.v.numel()) * 8),
                 "timer": "host wall clock around H2D + solve + D2H"},
@@ -576,6 +585,85 @@ def run_serve(args, rank: int, world: int, device):
     }
 
 
+def run_large(args, rank: int, world: int, device):
+    """Large streamed case: an m x n FP64 matrix with sigma_i = 10^(-10 i / n)
+    and 8 clusters of 16 values with relative gaps 1e-10, Haar U and V, written
+    to disk in the *.mat format and solved by the CLI pipeline (mmap reader,
+    serving core, QR-preconditioned solver, mmap writer).  One step = one run
+    of the CLI on the file; timed on the host wall clock (file in, file out)."""
+    import torch
+    import workloads as W
+
+    m, n = args.large_m, args.large_n
+    sig = np.ascontiguousarray(W.graded_clustered_sigma(n))
+    g = torch.Generator(device=device)
+    g.manual_seed(5)
+    t0 = time.time()
+    qu, ru = torch.linalg.qr(torch.randn((m, n), generator=g, dtype=torch.float64, device=device))
+    qu *= torch.sign(torch.diagonal(ru))[None, :]
+    del ru
+    qv, rv = torch.linalg.qr(torch.randn((n, n), generator=g, dtype=torch.float64, device=device))
+    qv *= torch.sign(torch.diagonal(rv))[None, :]
+    del rv
+    qu *= torch.from_numpy(sig).to(device)[None, :]
+    a = (qu @ qv.T).cpu().numpy()
+    del qu, qv
+    torch.cuda.empty_cache()
+    gen_s = time.time() - t0
+    work = args.large_dir or "/tmp/jsvd_large"
+    os.makedirs(work, exist_ok=True)
+    src, dst = os.path.join(work, "large_in.mat"), os.path.join(work, "large_out.mat")
+    with open(src, "wb") as f:
+        f.write(np.array([m, n], dtype=">u8").tobytes())
+        a.astype(">f8").tofile(f)
+    del a
+    cli = os.path.join(ROOT, "jacobi-svd-cuda_b200", "jacobi-svd-b200")
+    cmd = [cli, src, dst, "-e", "1e-14", "--solver", "precond", "--force", "-q", "--json-report"]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t1 = time.perf_counter()
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        dt = time.perf_counter() - t1
+        if out.returncode != 0:
+            raise SystemExit(f"CLI failed: {out.stderr}")
+        if i >= args.warmup:
+            times.append(dt)
+    report = json.loads(out.stdout[out.stdout.index("{"):])
+    # sigma is the second record of the output stream: U (m x n), Sigma (1 x n), V
+    with open(dst, "rb") as f:
+        f.seek(16 + 8 * m * n)
+        hdr = np.frombuffer(f.read(16), dtype=">u8")
+        got = np.frombuffer(f.read(8 * n), dtype=">f8").astype(np.float64)
+    got = np.sort(got)[::-1]
+    ref = np.sort(sig)[::-1]
+    err = np.abs(got - ref)
+    elapsed = float(np.mean(times))
+    return {
+        "metric": "SVDs/s",
+        "value": 1.0 / elapsed,
+        "unit": "SVD/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * elapsed,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"{m}x{n} FP64, sigma_i = 10^(-10 i/n) with 8 clusters of 16 (gaps 1e-10), Haar U,V "
+                               f"(seed 5), streamed from a *.mat file through the CLI pipeline",
+                   "path": "CLI pipeline -> serving core -> QR-preconditioned solver", "epsilon": 1e-14,
+                   "pipeline_report": report, "generation_s": gen_s, "sigma_header": hdr.tolist()},
+        "e2e": {"value": 1.0 / elapsed, "unit": "SVD/s", "h2d_bytes_per_step": 8 * m * n,
+                "d2h_bytes_per_step": 8 * (m * n + n + n * n), "timer": "host wall clock around the CLI process"},
+        "check": {"sigma_normwise_vs_analytic": float(err.max() / ref[0]),
+                  "sigma_max_rel_vs_analytic": float(np.max(err / ref)),
+                  "sigma_max_rel_top_half": float(np.max((err / ref)[: n // 2]))},
+        "gpu_launches": None,
+    }
+
+
 def run_reference(args):
     if args.workload == "batch":
         import workloads as W
@@ -640,6 +728,11 @@ def main():
     ap.add_argument("--rates", default="50,200,1000")
     ap.add_argument("--serve-count", type=int, default=300)
     ap.add_argument("--serve-plain-sample", type=int, default=40)
+    ap.add_argument("--large-m", type=int, default=16384)
+    ap.add_argument("--large-n", type=int, default=8192)
+    ap.add_argument("--large-dir", default="")
+    ap.add_argument("--sweep-mode", type=int, default=0, choices=[0, 1],
+                    help="0: per-round kernels replayed from a graph; 1: persistent sweep kernel")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -655,6 +748,8 @@ def main():
 
     device = torch.device(f"cuda:{local}")
     torch.cuda.set_device(device)
+    import jsvd
+    jsvd.set_sweep_mode(args.sweep_mode)
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
@@ -663,6 +758,8 @@ def main():
             line = run_batch(args, rank, world, device)
         elif args.workload == "serve":
             line = run_serve(args, rank, world, device)
+        elif args.workload == "large":
+            line = run_large(args, rank, world, device)
         else:
             line = run_ours(args, rank, world, device)
     finally:

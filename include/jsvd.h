@@ -133,6 +133,14 @@ typedef struct jsvd_plain_stats {
 } jsvd_plain_stats;
 
 void jsvd_plain_stats_get(jsvd_plain_stats *out);
+
+/* How the plain path launches a sweep (process-wide, read when a plan is
+ * created): 0 = one kernel per round, replayed from a CUDA graph (default);
+ * 1 = one persistent cooperative kernel per sweep whose CTAs synchronise with
+ * their neighbours through per-CTA round counters (bounded waits).  Both give
+ * bit-identical results. */
+void jsvd_plain_set_sweep_mode(int mode);
+int jsvd_plain_get_sweep_mode(void);
 void jsvd_plain_stats_reset(void);
 
 /* ---- batched solver ---------------------------------------------------------
@@ -146,7 +154,8 @@ void jsvd_plain_stats_reset(void);
 /* Launch shape of one size class: 0 keeps the built-in choice. */
 typedef struct jsvd_batch_tuning {
     int threads;     /* threads per CTA (multiple of 32, <= 512) */
-    int ctas_per_sm; /* persistent CTAs per SM (shared-memory classes) */
+    int ctas_per_sm; /* persistent CTAs per SM */
+    int max_ctas;    /* upper bound on the class's grid (bounds the L2 working set of the global classes) */
 } jsvd_batch_tuning;
 
 /*
@@ -156,9 +165,9 @@ typedef struct jsvd_batch_tuning {
  * d_v (optional) cols[i]^2 row-major, d_u (optional) rows[i]*cols[i]
  * row-major; sweeps (host, optional) the sweep count of each matrix.  cfg's
  * epsilon and max_sweeps apply (threads_per_block must be 256).  tuning may
- * be NULL or point to 4 entries for the first four size classes (A and V in
- * <=48 KiB, <=100 KiB, <=~226 KiB of shared memory; A alone in shared
- * memory); the fifth class (A and V in global memory) keeps its defaults.
+ * be NULL or point to 5 entries, one per size class: A and V in <= 48 KiB,
+ * <= 100 KiB, <= ~226 KiB of shared memory; A alone in shared memory; A and V
+ * in global memory.
  * Synchronous on `stream` (NULL = library stream, ordered after the legacy
  * default stream).
  */
@@ -174,6 +183,7 @@ typedef struct jsvd_batch_stats {
     unsigned long long sweeps;
     double kernel_ms; /* device time of the persistent launches (events) */
     unsigned long long class_count[5]; /* matrices per size class */
+    double class_ms[5];                /* device time of each class's launch */
 } jsvd_batch_stats;
 
 void jsvd_batch_stats_get(jsvd_batch_stats *out);

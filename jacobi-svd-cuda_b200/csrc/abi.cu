@@ -76,7 +76,7 @@ int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t strea
     auto &plans = thread_cache().plans;
     for (size_t i = 0; i < plans.size(); ++i) {
         PlainPlan *p = plans[i].get();
-        if (p->device == dev && p->m == m && p->n == n && p->T == T && p->eps == eps) {
+        if (p->device == dev && p->m == m && p->n == n && p->T == T && p->eps == eps && p->mode == sweep_mode()) {
             std::rotate(plans.begin() + i, plans.begin() + i + 1, plans.end());
             *out = plans.back().get();
             return JSVD_OK;
@@ -90,6 +90,7 @@ int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t strea
     std::unique_ptr<PlainPlan> plan;
     int rc = PlainPlan::create(dev, m, n, T, eps, own, plan);
     if (rc != JSVD_OK) return rc;
+    plan->mode = sweep_mode();
     plans.push_back(std::move(plan));
     size_t total = 0;
     for (auto &p : plans) total += p->bytes;
@@ -320,6 +321,10 @@ void jsvd_plain_stats_get(jsvd_plain_stats *out)
 }
 
 void jsvd_plain_stats_reset(void) { plain_stats() = PlainStats{}; }
+
+void jsvd_plain_set_sweep_mode(int mode) { set_sweep_mode(mode); }
+
+int jsvd_plain_get_sweep_mode(void) { return sweep_mode(); }
 
 void jsvd_release_thread_cache(void)
 {

@@ -1,6 +1,5 @@
 // Batched one-sided Jacobi SVD: thousands of independent small matrices,
-// one persistent launch per size class, the classes running concurrently on
-// their own streams (sm_100a).
+// one persistent launch per size class, largest class first (sm_100a).
 //
 // Each CTA pulls matrix indices from a device work queue (one atomic counter
 // per class; matrices sorted by work, largest first) and solves the whole
@@ -78,6 +77,44 @@ __device__ __forceinline__ void warp_pair_stats(const double *x, const double *y
     pp = warp_tree<kW>(app);
     qq = warp_tree<kW>(aqq);
     pq = warp_tree<kW>(apq);
+}
+
+// Rotation of one column pair of A (length m) and of V (length n) by one
+// warp.  Each 256-row chunk of all four columns is loaded into registers
+// before any store: with the working copies in global memory a load -> rotate
+// -> store loop pays one L2 round trip per 32 rows, because the compiler cannot
+// move a load past a store to a possibly aliasing column.
+__device__ __forceinline__ void warp_rotate(double *x, double *y, int m, double *vx, double *vy, int n, int lane,
+                                            double c, double s)
+{
+    const int len = m > n ? m : n;
+    for (int base = 0; base < len; base += kLanes) {
+        double xa[kW], ya[kW], xv[kW], yv[kW];
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            const int r = base + 32 * j + lane;
+            if (r < m) {
+                xa[j] = x[r];
+                ya[j] = y[r];
+            }
+            if (r < n) {
+                xv[j] = vx[r];
+                yv[j] = vy[r];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            const int r = base + 32 * j + lane;
+            if (r < m) {
+                x[r] = rot_p(c, s, xa[j], ya[j]);
+                y[r] = rot_q(c, s, xa[j], ya[j]);
+            }
+            if (r < n) {
+                vx[r] = rot_p(c, s, xv[j], yv[j]);
+                vy[r] = rot_q(c, s, xv[j], yv[j]);
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ double warp_norm2(const double *x, int m, int lane)
@@ -176,18 +213,8 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
                         const double2 g = st_cs[k];
                         if (g.x == 0.0) continue;
                         const int2 pq = batch_pair(n, r, k);
-                        double *x = A + (size_t)pq.x * m, *y = A + (size_t)pq.y * m;
-                        for (int i = lane; i < m; i += 32) {
-                            const double a = x[i], b = y[i];
-                            x[i] = rot_p(g.x, g.y, a, b);
-                            y[i] = rot_q(g.x, g.y, a, b);
-                        }
-                        double *vx = V + (size_t)pq.x * n, *vy = V + (size_t)pq.y * n;
-                        for (int i = lane; i < n; i += 32) {
-                            const double a = vx[i], b = vy[i];
-                            vx[i] = rot_p(g.x, g.y, a, b);
-                            vy[i] = rot_q(g.x, g.y, a, b);
-                        }
+                        warp_rotate(A + (size_t)pq.x * m, A + (size_t)pq.y * m, m, V + (size_t)pq.x * n,
+                                    V + (size_t)pq.y * n, n, lane, g.x, g.y);
                     }
                     __syncthreads();
                 }
@@ -224,32 +251,31 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
 using BatchFn = void (*)(const BatchDesc *, int, int *, const void *, int, double, int, double *, double *,
                          double *, int *, double *, size_t);
 
-struct ThreadStreams {
-    cudaStream_t s[kClasses] = {};
-    cudaEvent_t fork = nullptr, join[kClasses] = {}, t0 = nullptr, t1 = nullptr;
+// Per-thread timing events: whole call and one pair per size class.
+struct ThreadEvents {
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaEvent_t c0[kClasses] = {}, c1[kClasses] = {};
     int device = -1;
-    ~ThreadStreams()
+    ~ThreadEvents()
     {
         for (int c = 0; c < kClasses; ++c) {
-            if (s[c]) cudaStreamDestroy(s[c]);
-            if (join[c]) cudaEventDestroy(join[c]);
+            if (c0[c]) cudaEventDestroy(c0[c]);
+            if (c1[c]) cudaEventDestroy(c1[c]);
         }
-        if (fork) cudaEventDestroy(fork);
         if (t0) cudaEventDestroy(t0);
         if (t1) cudaEventDestroy(t1);
     }
 };
 
-int class_streams(int dev, ThreadStreams **out)
+int thread_events(int dev, ThreadEvents **out)
 {
-    thread_local ThreadStreams ts;
+    thread_local ThreadEvents ts;
     if (ts.device != dev) {
         if (ts.device >= 0) return invalid_argument("The batched solver is bound to the first device it ran on.");
         for (int c = 0; c < kClasses; ++c) {
-            JSVD_CUDA_TRY(cudaStreamCreateWithFlags(&ts.s[c], cudaStreamNonBlocking));
-            JSVD_CUDA_TRY(cudaEventCreateWithFlags(&ts.join[c], cudaEventDisableTiming));
+            JSVD_CUDA_TRY(cudaEventCreate(&ts.c0[c]));
+            JSVD_CUDA_TRY(cudaEventCreate(&ts.c1[c]));
         }
-        JSVD_CUDA_TRY(cudaEventCreateWithFlags(&ts.fork, cudaEventDisableTiming));
         JSVD_CUDA_TRY(cudaEventCreate(&ts.t0));
         JSVD_CUDA_TRY(cudaEventCreate(&ts.t1));
         ts.device = dev;
@@ -276,8 +302,8 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t smem_cap = (size_t)std::min(smem_optin, 227 * 1024) - 1024;
-    ThreadStreams *ts = nullptr;
-    int rc = class_streams(dev, &ts);
+    ThreadEvents *ts = nullptr;
+    int rc = thread_events(dev, &ts);
     if (rc != JSVD_OK) return rc;
 
     struct Class {
@@ -294,10 +320,15 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         {smem_cap, 512, 1, true, false, batch_kernel<true, false>},
         {(size_t)-1, 512, 1, false, false, batch_kernel<false, false>},
     };
+    int max_ctas[kClasses] = {};
     if (req.tuning != nullptr) {
-        for (int c = 0; c < 4; ++c) {
-            if (req.tuning[c].threads > 0) classes[c].threads = req.tuning[c].threads;
-            if (req.tuning[c].ctas_per_sm > 0) classes[c].ctas_per_sm = req.tuning[c].ctas_per_sm;
+        for (int c = 0; c < kClasses; ++c) {
+            const jsvd_batch_tuning &t = req.tuning[c];
+            if (t.threads < 0 || t.threads > 512 || t.threads % 32 != 0 || t.ctas_per_sm < 0 || t.max_ctas < 0)
+                return invalid_argument("Batch tuning: threads must be a multiple of 32 up to 512, counts >= 0.");
+            if (t.threads > 0) classes[c].threads = t.threads;
+            if (t.ctas_per_sm > 0) classes[c].ctas_per_sm = t.ctas_per_sm;
+            max_ctas[c] = t.max_ctas;
         }
     }
     std::vector<std::vector<int>> members(kClasses);
@@ -356,6 +387,7 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     for (int c = 0; c < kClasses; ++c) {
         const int cnt = first[c + 1] - first[c];
         grid_of[c] = std::min(cnt, sms * classes[c].ctas_per_sm);
+        if (max_ctas[c] > 0) grid_of[c] = std::min(grid_of[c], max_ctas[c]);
         gws_base[c] = gws_total;
         gws_total += gws_of[c] * (size_t)grid_of[c];
     }
@@ -373,22 +405,22 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     for (BatchFn fn : {(BatchFn)batch_kernel<true, true>, (BatchFn)batch_kernel<true, false>,
                        (BatchFn)batch_kernel<false, false>})
         JSVD_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
-    // Fork the class streams off `stream`, run the classes concurrently, join.
     JSVD_CUDA_TRY(cudaEventRecord(ts->t0, stream));
-    JSVD_CUDA_TRY(cudaEventRecord(ts->fork, stream));
     int launches = 0;
     for (int c = kClasses - 1; c >= 0; --c) {
         const int cnt = first[c + 1] - first[c];
         if (cnt == 0) continue;
         const Class &cl = classes[c];
-        cudaStream_t cs = ts->s[c];
-        JSVD_CUDA_TRY(cudaStreamWaitEvent(cs, ts->fork, 0));
-        cl.fn<<<grid_of[c], cl.threads, smem_of[c], cs>>>(d_desc + first[c], cnt, d_next + c, req.a, req.a_is_f32,
+        // The classes run one after another on one stream: persistent CTAs of
+        // a class hold their SMs until its queue drains, and concurrent classes
+        // starved each other (a 512-thread CTA of the global class fills an
+        // SM's register file).
+        JSVD_CUDA_TRY(cudaEventRecord(ts->c0[c], stream));
+        cl.fn<<<grid_of[c], cl.threads, smem_of[c], stream>>>(d_desc + first[c], cnt, d_next + c, req.a, req.a_is_f32,
                                                           req.eps, req.max_sweeps, req.sigma, req.v, req.u,
                                                           d_sweeps + first[c], d_ws + gws_base[c], gws_of[c]);
         JSVD_CUDA_TRY(cudaGetLastError());
-        JSVD_CUDA_TRY(cudaEventRecord(ts->join[c], cs));
-        JSVD_CUDA_TRY(cudaStreamWaitEvent(stream, ts->join[c], 0));
+        JSVD_CUDA_TRY(cudaEventRecord(ts->c1[c], stream));
         ++launches;
     }
     JSVD_CUDA_TRY(cudaEventRecord(ts->t1, stream));
@@ -412,7 +444,12 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     }
     st.sweeps += total_sweeps;
     st.matrices += (unsigned long long)count;
-    for (int c = 0; c < kClasses; ++c) st.class_count[c] += (unsigned long long)(first[c + 1] - first[c]);
+    for (int c = 0; c < kClasses; ++c) {
+        st.class_count[c] += (unsigned long long)(first[c + 1] - first[c]);
+        float cms = 0.f;
+        if (first[c + 1] > first[c] && cudaEventElapsedTime(&cms, ts->c0[c], ts->c1[c]) == cudaSuccess)
+            st.class_ms[c] += cms;
+    }
     return JSVD_OK;
 }
 
@@ -471,7 +508,10 @@ extern "C" void jsvd_batch_stats_get(jsvd_batch_stats *out)
     out->matrices = s.matrices;
     out->sweeps = s.sweeps;
     out->kernel_ms = s.kernel_ms;
-    for (int c = 0; c < 5; ++c) out->class_count[c] = s.class_count[c];
+    for (int c = 0; c < 5; ++c) {
+        out->class_count[c] = s.class_count[c];
+        out->class_ms[c] = s.class_ms[c];
+    }
 }
 
 extern "C" void jsvd_batch_stats_reset(void) { batch_stats() = BatchStats{}; }

@@ -28,13 +28,14 @@ struct BatchRequest {
     double *v = nullptr;      // device, packed n*n row-major, or null
     double *u = nullptr;      // device, packed m*n row-major, or null
     int *sweeps = nullptr;    // host, per matrix, or null
-    const jsvd_batch_tuning *tuning = nullptr;  // 4 classes, or null
+    const jsvd_batch_tuning *tuning = nullptr;  // one entry per class, or null
 };
 
 struct BatchStats {
     unsigned long long calls = 0, launches = 0, matrices = 0, sweeps = 0;
     double kernel_ms = 0.0;
     unsigned long long class_count[5] = {};
+    double class_ms[5] = {};
 };
 
 BatchStats &batch_stats();

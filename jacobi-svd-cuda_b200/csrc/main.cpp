@@ -17,6 +17,7 @@
 
 #include "kernels.hpp"
 #include "pipeline.hpp"
+#include "pipeline_ext.hpp"
 
 namespace
 {
@@ -45,6 +46,7 @@ namespace
         std::size_t queue_capacity = 4;
         bool force = false, dry_run = false, print_config = false, json = false, quiet = false;
         bool help = false, version = false;
+        bool precond = false;
     };
 
     struct Flag
@@ -77,6 +79,7 @@ namespace
         {"print-config", '\0', false, "", "Print effective config before execution."},
         {"json-report", '\0', false, "", "Print execution report in JSON."},
         {"quiet", 'q', false, "", "Suppress text report."},
+        {"solver", '\0', true, "NAME", "Large-testcase solver: plain (bit-identical, default) | precond."},
         {"help", 'h', false, "", "Show this help message."},
         {"version", 'v', false, "", "Show version information."},
     };
@@ -175,6 +178,13 @@ namespace
         else if (n == "print-config") o.print_config = true;
         else if (n == "json-report") o.json = true;
         else if (n == "quiet") o.quiet = true;
+        else if (n == "solver")
+        {
+            const std::string l = lower(v);
+            if (l != "plain" && l != "precond")
+                throw ArgError("Invalid value for --solver: expected plain|precond.");
+            o.precond = l == "precond";
+        }
         else if (n == "help") o.help = true;
         else if (n == "version") o.version = true;
     }
@@ -359,7 +369,8 @@ namespace
                   << "layout-bench-rep: " << o.layout_bench_reps << '\n'
                   << "layout-bench-swp: " << o.layout_bench_sweeps << '\n'
                   << "queue-capacity  : " << o.queue_capacity << '\n'
-                  << "force-overwrite : " << (o.force ? "true" : "false") << '\n';
+                  << "force-overwrite : " << (o.force ? "true" : "false") << '\n'
+                  << "solver          : " << (o.precond ? "precond" : "plain") << '\n';
     }
 } // namespace
 
@@ -392,6 +403,8 @@ int main(int argc, char **argv)
             print_config(o);
             std::cout << '\n';
         }
+        jacobi::svd::pipeline::set_large_solver(o.precond ? jacobi::svd::pipeline::LargeSolver::precond
+                                                          : jacobi::svd::pipeline::LargeSolver::plain);
         jacobi::svd::pipeline::PipelineConfig cfg;
         cfg.input_path = o.input;
         cfg.output_path = o.output;

@@ -26,6 +26,7 @@
 
 #include "io.hpp"
 #include "jsvd.h"
+#include "pipeline_ext.hpp"
 
 namespace jacobi::svd::pipeline
 {
@@ -147,6 +148,18 @@ namespace jacobi::svd::pipeline
         };
     } // namespace
 
+    namespace
+    {
+        std::atomic<int> g_large_solver{0};
+    }
+
+    void set_large_solver(LargeSolver solver) noexcept { g_large_solver.store(solver == LargeSolver::precond ? 1 : 0); }
+
+    LargeSolver large_solver() noexcept
+    {
+        return g_large_solver.load() == 1 ? LargeSolver::precond : LargeSolver::plain;
+    }
+
     JacobiSvdPipeline::JacobiSvdPipeline(PipelineConfig config) : config_(std::move(config)) {}
 
     PipelineReport JacobiSvdPipeline::run() const
@@ -178,6 +191,7 @@ namespace jacobi::svd::pipeline
         jsvd_server_options opt;
         jsvd_server_options_default(&opt);
         opt.cfg = to_c(kernel);
+        opt.large_path = large_solver() == LargeSolver::precond ? 1 : 0;
         ServerHandle server;
         if (const int rc = jsvd_server_create(&opt, &server.s); rc != JSVD_OK)
             rethrow_status(rc);

@@ -25,9 +25,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -298,6 +300,182 @@ __global__ void __launch_bounds__(T) plain_sigma_kernel(const double *__restrict
     if (t == 0) sigma[blockIdx.x] = sqrt(fmax(acc, 0.0));
 }
 
+// ---- persistent sweep ---------------------------------------------------------
+// One launch per sweep instead of one per round.  CTA c owns the contiguous
+// pair slots [c*S, c*S + S) of the circle (slot k = positions k and ne-1-k) and
+// runs every round of the sweep; a slot's two columns in round r+1 come only
+// from slots k-1 (0 for k <= 1), k and k+1 (k for the last slot) of round r,
+// so CTAs synchronise point to point: after a round a CTA publishes the number
+// of rounds it has completed (flags[c], release at GPU scope) and before a
+// round it waits (acquire) for the CTAs owning its slots' sources.  All CTAs
+// are co-resident (cooperative launch).  Waits are bounded: after
+// kSpinLimitNs the CTA records kDevWaitTimeout in *status and returns.
+// Column loads and stores bypass L1 (other SMs write the columns).  The
+// arithmetic of a pair is the round kernel's, so results are bit-identical.
+
+constexpr long long kSpinLimitNs = 2000000000LL;  // 2 s
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ long long global_ns()
+{
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Column of circle position pos in round r (-1 for the dummy of an odd n).
+__device__ __forceinline__ int circle_col(int n, int L, int r, int pos)
+{
+    if (pos == 0) return 0;
+    const int c = 1 + ((pos - 1 - r) % L + L) % L;
+    return c == n ? -1 : c;
+}
+
+template <int T, int K>
+__global__ void __launch_bounds__(T) plain_sweep_persistent(double *__restrict__ a, long lda, int m, int n,
+                                                             int rounds, int slots_per_cta, double2 *__restrict__ cs,
+                                                             int npairs, double eps, unsigned *__restrict__ counter,
+                                                             int *__restrict__ flags, int g0,
+                                                             int *__restrict__ status)
+{
+    __shared__ double red[T == 32 ? 1 : 3 * T];
+    __shared__ int s_ok;
+    const int t = threadIdx.x;
+    const int ne = n + (n & 1), half = ne / 2, L = ne - 1;
+    const int k_lo = blockIdx.x * slots_per_cta;
+    const int k_hi = min(half, k_lo + slots_per_cta);
+    // CTAs owning the sources of this CTA's slots (besides itself)
+    const int dep_lo = (k_lo <= 1 ? 0 : k_lo - 1) / slots_per_cta;
+    const int dep_hi = (k_hi - 1 < half - 1 ? k_hi : k_hi - 1) / slots_per_cta;
+    for (int r = 0; r < rounds; ++r) {
+        const int g = g0 + r;
+        if (r > 0) {
+            if (t == 0) {
+                int ok = 1;
+                const long long t0 = global_ns();
+                for (;;) {
+                    const int f1 = ld_acquire_gpu(flags + dep_lo);
+                    const int f2 = ld_acquire_gpu(flags + dep_hi);
+                    const int f3 = ld_acquire_gpu(flags + 0);
+                    if (f1 >= g && f2 >= g && (k_lo != 1 || f3 >= g)) break;
+                    if (global_ns() - t0 > kSpinLimitNs) {
+                        atomicExch(status, (int)kDevWaitTimeout);
+                        ok = 0;
+                        break;
+                    }
+                }
+                s_ok = ok;
+            }
+            __syncthreads();
+            if (!s_ok) return;
+        }
+        // position of the dummy column (odd n) in this round and its slot
+        int dummy_slot = -1;
+        if (n & 1) {
+            const int j = 1 + ((n - 1 + r) % L);
+            dummy_slot = j < half ? j : ne - 1 - j;
+        }
+        for (int k = k_lo; k < k_hi; ++k) {
+            if (k == dummy_slot) continue;
+            const int p = circle_col(n, L, r, k), q = circle_col(n, L, r, ne - 1 - k);
+            const int pair = (dummy_slot >= 0 && k > dummy_slot) ? k - 1 : k;
+            double *__restrict__ ap = a + (size_t)p * lda;
+            double *__restrict__ aq = a + (size_t)q * lda;
+            double spp = 0.0, sqq = 0.0, spq = 0.0;
+            double xp[K > 0 ? K : 1], xq[K > 0 ? K : 1];
+            if constexpr (K > 0) {
+#pragma unroll
+                for (int kk = 0; kk < K; ++kk) {
+                    const int row = t + kk * T;
+                    xp[kk] = (row < m) ? __ldcg(ap + row) : 0.0;
+                    xq[kk] = (row < m) ? __ldcg(aq + row) : 0.0;
+                }
+#pragma unroll
+                for (int kk = 0; kk < K; ++kk) {
+                    if (t + kk * T < m) {
+                        spp = fma(xp[kk], xp[kk], spp);
+                        sqq = fma(xq[kk], xq[kk], sqq);
+                        spq = fma(xp[kk], xq[kk], spq);
+                    }
+                }
+            } else {
+                for (int row = t; row < m; row += T) {
+                    const double x = __ldcg(ap + row), y = __ldcg(aq + row);
+                    spp = fma(x, x, spp);
+                    sqq = fma(y, y, sqq);
+                    spq = fma(x, y, spq);
+                }
+            }
+            block_tree3_all<T>(spp, sqq, spq, red);
+            double c, s;
+            const bool rotates = rotation_params(spp, sqq, spq, eps, c, s);
+            if (t == 0) {
+                cs[(size_t)r * npairs + pair] = make_double2(c, s);
+                if (rotates) atomicAdd(counter, 1u);
+            }
+            if (rotates) {
+                if constexpr (K > 0) {
+#pragma unroll
+                    for (int kk = 0; kk < K; ++kk) {
+                        const int row = t + kk * T;
+                        if (row < m) {
+                            __stcg(ap + row, rot_p(c, s, xp[kk], xq[kk]));
+                            __stcg(aq + row, rot_q(c, s, xp[kk], xq[kk]));
+                        }
+                    }
+                } else {
+                    for (int row = t; row < m; row += T) {
+                        const double x = __ldcg(ap + row), y = __ldcg(aq + row);
+                        __stcg(ap + row, rot_p(c, s, x, y));
+                        __stcg(aq + row, rot_q(c, s, x, y));
+                    }
+                }
+            }
+            __syncthreads();  // red[] is reused by the next slot
+        }
+        // bar.sync above orders the CTA's column stores before thread 0's
+        // release, which is cumulative at GPU scope.
+        if (t == 0) st_release_gpu(flags + blockIdx.x, g + 1);
+    }
+}
+
+using SweepFn = void (*)(double *, long, int, int, int, int, double2 *, int, double, unsigned *, int *, int, int *);
+
+template <int T>
+SweepFn pick_sweep_t(int m)
+{
+    constexpr int kmax = T <= 256 ? 16 : (T == 512 ? 8 : 4);
+    if (m <= 1 * T) return plain_sweep_persistent<T, 1>;
+    if (m <= 2 * T) return plain_sweep_persistent<T, 2>;
+    if (m <= 4 * T) return plain_sweep_persistent<T, 4>;
+    if (kmax >= 8 && m <= 8 * T) return plain_sweep_persistent<T, (kmax >= 8 ? 8 : 4)>;
+    if (kmax >= 16 && m <= 16 * T) return plain_sweep_persistent<T, (kmax >= 16 ? 16 : 4)>;
+    return plain_sweep_persistent<T, 0>;
+}
+
+SweepFn pick_sweep(int T, int m)
+{
+    switch (T) {
+    case 32: return pick_sweep_t<32>(m);
+    case 64: return pick_sweep_t<64>(m);
+    case 128: return pick_sweep_t<128>(m);
+    case 256: return pick_sweep_t<256>(m);
+    case 512: return pick_sweep_t<512>(m);
+    default: return pick_sweep_t<1024>(m);
+    }
+}
+
 using RoundFn = void (*)(double *, long, int, const int2 *, double2 *, double, unsigned *);
 using SigmaFn = void (*)(const double *, long, int, double *);
 using VpassFn = void (*)(double *, long, int, const double2 *, int, int);
@@ -378,6 +556,13 @@ void build_schedule(int n, std::vector<int2> &pairs, int &rounds, int &npairs)
 
 }  // namespace
 
+namespace {
+std::atomic<int> g_sweep_mode{0};
+}
+
+int sweep_mode() { return g_sweep_mode.load(); }
+void set_sweep_mode(int mode) { g_sweep_mode.store(mode == 1 ? 1 : 0); }
+
 PlainStats &plain_stats()
 {
     thread_local PlainStats stats;
@@ -403,7 +588,8 @@ PlainPlan::~PlainPlan()
     for (int p = 0; p < 2; ++p)
         for (cudaEvent_t e : {ev_rounds_done[p], ev_vpass_done[p], ev_v0[p], ev_v1[p]})
             if (e) cudaEventDestroy(e);
-    for (void *p : {(void *)a_w, (void *)v_w, (void *)pairs, (void *)cs, (void *)cs2, (void *)counter, (void *)d_in,
+    for (void *p : {(void *)a_w, (void *)v_w, (void *)pairs, (void *)cs, (void *)cs2, (void *)counter, (void *)flags,
+                    (void *)d_in,
                     (void *)d_u, (void *)d_sigma, (void *)d_v, (void *)sigma_w})
         if (p) cudaFreeAsync(p, stream);
     if (prev >= 0) cudaSetDevice(prev);
@@ -426,7 +612,7 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
     JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->a_w, sizeof(double) * m_ * n_, stream));
     JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->v_w, sizeof(double) * n_ * n_, stream));
     JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->sigma_w, sizeof(double) * n_, stream));
-    JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->counter, sizeof(unsigned), stream));
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->counter, 2 * sizeof(unsigned), stream));  // rotations, status
     if (plan->rounds > 0) {
         const size_t np = (size_t)plan->rounds * plan->npairs;
         JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->pairs, sizeof(int2) * np, stream));
@@ -459,6 +645,20 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
             cudaFuncSetAttribute(pick_vpass(R), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_begin));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_end));
+        // Persistent sweep when the whole grid can be co-resident.
+        int coop = 0, sms = 0, per_sm = 0;
+        JSVD_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        SweepFn sfn = pick_sweep(T_, (int)m_);
+        JSVD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sfn, T_, 0));
+        const int half = (int)((n_ + (n_ & 1)) / 2);
+        if (coop && per_sm > 0 && sweep_mode() == 1) {
+            const int max_ctas = per_sm * sms;
+            plan->slots_per_cta = (half + max_ctas - 1) / max_ctas;
+            plan->sweep_grid = (half + plan->slots_per_cta - 1) / plan->slots_per_cta;
+            JSVD_CUDA_TRY(cudaMallocAsync((void **)&plan->flags, sizeof(int) * (plan->sweep_grid + 1), stream));
+            plan->persistent = true;
+        }
     }
     plan->bytes = sizeof(double) * (m_ * n_ + n_ * n_ + n_) +
                   (sizeof(int2) + 2 * sizeof(double2)) * (size_t)plan->rounds * plan->npairs;
@@ -518,6 +718,26 @@ int PlainPlan::capture_rounds(cudaStream_t st, int parity)
     return JSVD_OK;
 }
 
+// One persistent launch for all rounds of a sweep (angles of `parity`).
+int PlainPlan::enqueue_persistent(cudaStream_t st, int parity, int g0)
+{
+    SweepFn sfn = pick_sweep(T, (int)m);
+    double *a_arg = a_w;
+    long lda_arg = lda;
+    int m_arg = (int)m, n_arg = (int)n, rounds_arg = rounds, spc = slots_per_cta, np = npairs, g0_arg = g0;
+    double2 *tab = parity ? cs2 : cs;
+    double eps_arg = eps;
+    unsigned *cnt = counter;
+    int *fl = flags;
+    int *status = reinterpret_cast<int *>(counter + 1);
+    void *args[] = {&a_arg, &lda_arg, &m_arg, &n_arg, &rounds_arg, &spc, &tab, &np, &eps_arg, &cnt, &fl, &g0_arg,
+                    &status};
+    JSVD_CUDA_TRY(cudaEventRecord(ev_round_begin, st));
+    JSVD_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)sfn, dim3(sweep_grid), dim3(T), args, 0, st));
+    JSVD_CUDA_TRY(cudaEventRecord(ev_round_end, st));
+    return JSVD_OK;
+}
+
 int PlainPlan::ensure_host_staging()
 {
     if (d_in) return JSVD_OK;
@@ -548,7 +768,11 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
     if (rounds == 0) {
         executed = 1;  // n == 1: one empty sweep, as the reference reports
     } else {
-        if (sweep_exec == nullptr && uses >= 1) {
+        if (persistent) {
+            JSVD_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int) * (sweep_grid + 1), stream));
+            JSVD_CUDA_TRY(cudaMemsetAsync(counter + 1, 0, sizeof(unsigned), stream));
+        }
+        if (!persistent && sweep_exec == nullptr && uses >= 1) {
             int rc = capture_rounds(stream, 0);
             if (rc == JSVD_OK) rc = capture_rounds(stream, 1);
             if (rc != JSVD_OK) return rc;
@@ -573,26 +797,42 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
                 if (rc != JSVD_OK) return rc;
             }
             JSVD_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), stream));
-            cudaGraphExec_t g = p ? sweep_exec2 : sweep_exec;
-            if (g != nullptr) {
-                JSVD_CUDA_TRY(cudaGraphLaunch(g, stream));
+            if (persistent) {
+                const int rc = enqueue_persistent(stream, p, s * rounds);
+                if (rc != JSVD_OK) return rc;
             } else {
-                const int rc = enqueue_rounds(stream, p);
-                if (rc != JSVD_OK) return rc;
+                cudaGraphExec_t g = p ? sweep_exec2 : sweep_exec;
+                if (g != nullptr) {
+                    JSVD_CUDA_TRY(cudaGraphLaunch(g, stream));
+                } else {
+                    const int rc = enqueue_rounds(stream, p);
+                    if (rc != JSVD_OK) return rc;
+                }
             }
-            JSVD_CUDA_TRY(cudaEventRecord(ev_rounds_done[p], stream));
-            JSVD_CUDA_TRY(cudaStreamWaitEvent(vstream, ev_rounds_done[p], 0));
-            JSVD_CUDA_TRY(cudaEventRecord(ev_v0[p], vstream));
+            // A persistent sweep needs all of its CTAs resident: its V pass runs
+            // after it on the same stream instead of beside the next sweep.
+            cudaStream_t vs = persistent ? stream : vstream;
+            if (!persistent) {
+                JSVD_CUDA_TRY(cudaEventRecord(ev_rounds_done[p], stream));
+                JSVD_CUDA_TRY(cudaStreamWaitEvent(vstream, ev_rounds_done[p], 0));
+            }
+            JSVD_CUDA_TRY(cudaEventRecord(ev_v0[p], vs));
             {
-                const int rc = enqueue_vpass(vstream, p);
+                const int rc = enqueue_vpass(vs, p);
                 if (rc != JSVD_OK) return rc;
             }
-            JSVD_CUDA_TRY(cudaEventRecord(ev_v1[p], vstream));
-            JSVD_CUDA_TRY(cudaEventRecord(ev_vpass_done[p], vstream));
+            JSVD_CUDA_TRY(cudaEventRecord(ev_v1[p], vs));
+            JSVD_CUDA_TRY(cudaEventRecord(ev_vpass_done[p], vs));
             vpending[p] = true;
-            unsigned rotated = 0;
-            JSVD_CUDA_TRY(cudaMemcpyAsync(&rotated, counter, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+            unsigned cnt[2] = {0, 0};
+            JSVD_CUDA_TRY(cudaMemcpyAsync(cnt, counter, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
             JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
+            const unsigned rotated = cnt[0];
+            if (persistent && cnt[1] != 0) {
+                set_last_error(JSVD_ERR_RUNTIME, "A persistent sweep stopped at its wait limit (device status " +
+                                                     std::to_string(cnt[1]) + ").");
+                return JSVD_ERR_RUNTIME;
+            }
             executed = s + 1;
             float r_ms = 0.f;
             if (cudaEventElapsedTime(&r_ms, ev_round_begin, ev_round_end) == cudaSuccess) st.round_ms += r_ms;

@@ -28,7 +28,11 @@ struct PlainPlan {
     int2 *pairs = nullptr;      // rounds x npairs schedule
     double2 *cs = nullptr;      // (c, s) of every pair of even sweeps
     double2 *cs2 = nullptr;     // (c, s) of every pair of odd sweeps
-    unsigned *counter = nullptr;
+    unsigned *counter = nullptr;  // [0] rotations in the sweep, [1] device status
+    int *flags = nullptr;         // persistent sweep: rounds completed per CTA
+    bool persistent = false;      // one cooperative launch per sweep
+    int slots_per_cta = 1, sweep_grid = 0;
+    int mode = 0;  // sweep_mode() at creation
     unsigned long long uses = 0;
     bool sweep_exec_capturing = false;
     // staging for host-buffer calls
@@ -52,6 +56,7 @@ struct PlainPlan {
     int ensure_host_staging();
     int enqueue_rounds(cudaStream_t st, int parity);
     int enqueue_vpass(cudaStream_t st, int parity);
+    int enqueue_persistent(cudaStream_t st, int parity, int g0);
     int capture_rounds(cudaStream_t st, int parity);
     // Runs the whole solve on device buffers; outputs may be null.
     int run(const double *d_a, double *out_u, double *out_sigma, double *out_v, int max_sweeps, int *sweeps,
@@ -64,6 +69,12 @@ struct PlainStats {
     double round_ms = 0.0, vpass_ms = 0.0;
 };
 PlainStats &plain_stats();
+
+// Process-wide choice of how a sweep is launched: 0 = one kernel per round
+// (replayed CUDA graph, the default), 1 = one persistent cooperative kernel per
+// sweep.  Plans record the mode they were created with.
+int sweep_mode();
+void set_sweep_mode(int mode);
 
 // Per-thread plan cache and stream.
 int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t stream, PlainPlan **plan);

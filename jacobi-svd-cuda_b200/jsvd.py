@@ -63,7 +63,7 @@ class PlainStats(ctypes.Structure):
 
 
 class BatchTuning(ctypes.Structure):
-    _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int)]
+    _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("max_ctas", ctypes.c_int)]
 
 
 class BatchStats(ctypes.Structure):
@@ -74,6 +74,7 @@ class BatchStats(ctypes.Structure):
         ("sweeps", ctypes.c_ulonglong),
         ("kernel_ms", ctypes.c_double),
         ("class_count", ctypes.c_ulonglong * 5),
+        ("class_ms", ctypes.c_double * 5),
     ]
 
 
@@ -139,7 +140,8 @@ def exported_symbols() -> list[str]:
         "jsvd_server_options_default", "jsvd_server_create", "jsvd_server_submit", "jsvd_server_wait",
         "jsvd_server_get_stats", "jsvd_server_destroy", "jsvd_precond_svd", "jsvd_precond_svd_device",
         "jsvd_precond_stats_get", "jsvd_precond_stats_reset", "jsvd_blocked_svd_device",
-        "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset",
+        "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset", "jsvd_plain_set_sweep_mode",
+        "jsvd_plain_get_sweep_mode",
     ]
 
 
@@ -198,6 +200,9 @@ def lib() -> ctypes.CDLL:
         L.jsvd_blocked_stats_get.argtypes = [ctypes.POINTER(BlockedStats)]
         L.jsvd_blocked_stats_get.restype = None
         L.jsvd_blocked_stats_reset.restype = None
+        L.jsvd_plain_set_sweep_mode.argtypes = [I]
+        L.jsvd_plain_set_sweep_mode.restype = None
+        L.jsvd_plain_get_sweep_mode.restype = I
         _LIB = L
     return _LIB
 
@@ -306,6 +311,11 @@ def plain_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None 
     return sw.value
 
 
+def set_sweep_mode(mode: int) -> None:
+    """0 = per-round kernels in a replayed graph (default), 1 = persistent sweep."""
+    lib().jsvd_plain_set_sweep_mode(mode)
+
+
 def plain_stats() -> PlainStats:
     st = PlainStats()
     lib().jsvd_plain_stats_get(ctypes.byref(st))
@@ -346,8 +356,9 @@ class DeviceBatch:
         cfg = cfg or default_config()
         tun = None
         if tuning is not None:
-            arr = (BatchTuning * 4)(*[BatchTuning(t, c) for t, c in tuning])
-            tun = arr
+            # one (threads, ctas_per_sm[, max_ctas]) tuple per size class; missing classes keep defaults
+            ents = [BatchTuning(*t) for t in tuning] + [BatchTuning(0, 0, 0)] * (5 - len(tuning))
+            tun = (BatchTuning * 5)(*ents[:5])
         rc = lib().jsvd_batch_svd_device(
             self.count, self.rows.ctypes.data, self.cols.ctypes.data, self.a_off.ctypes.data, self.a.data_ptr(),
             1 if self.f32 else 0, ctypes.byref(cfg), self.sigma.data_ptr(),

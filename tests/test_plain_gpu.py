@@ -137,3 +137,17 @@ def test_plain_vs_reference_golden(cuda_device, path):
         assert O.sigma_errors(s, g["sigma"])["max_rel"] <= 1e-13 * n
         if "u" in g:
             assert O.columns_match_up_to_sign(v, g["v"], 1e-9) <= 1e-9
+
+
+@pytest.mark.parametrize("m,n", [(2, 2), (17, 9), (257, 64), (600, 257), (2100, 24)])
+def test_plain_persistent_sweep_bitwise(cuda_device, m, n):
+    """The persistent cooperative sweep (one launch per sweep, neighbour
+    round counters) gives the same bytes as the per-round graph path."""
+    a = W.gaussian_splitmix(m, n, seed=4242 + m + 3 * n)
+    eps = 1e-13
+    jsvd.set_sweep_mode(1)
+    try:
+        got = jsvd.plain_svd(a, jsvd.default_config(epsilon=eps))
+    finally:
+        jsvd.set_sweep_mode(0)
+    _assert_bitwise(got, _oracle(a, eps))
