@@ -731,8 +731,9 @@ def main():
     ap.add_argument("--large-m", type=int, default=16384)
     ap.add_argument("--large-n", type=int, default=8192)
     ap.add_argument("--large-dir", default="")
-    ap.add_argument("--sweep-mode", type=int, default=0, choices=[0, 1],
-                    help="0: per-round kernels replayed from a graph; 1: persistent sweep kernel")
+    ap.add_argument("--sweep-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="0: per-round kernels replayed from a graph; 1: persistent sweep kernel; "
+                         "2: as 0 with programmatic dependent launch between rounds")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

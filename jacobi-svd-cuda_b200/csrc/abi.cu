@@ -91,6 +91,7 @@ int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t strea
     int rc = PlainPlan::create(dev, m, n, T, eps, own, plan);
     if (rc != JSVD_OK) return rc;
     plan->mode = sweep_mode();
+    plan->use_pdl = plan->mode == 2;
     plans.push_back(std::move(plan));
     size_t total = 0;
     for (auto &p : plans) total += p->bytes;

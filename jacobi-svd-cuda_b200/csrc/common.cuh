@@ -18,6 +18,13 @@
 
 namespace jsvd {
 
+// Programmatic dependent launch (sm_90+ PTX).  launch_dependents lets the next
+// kernel of the stream be scheduled before this one ends; wait blocks until
+// every prerequisite grid has completed and its memory operations are
+// visible.  Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // FMA placement for c*x - s*y and s*x + c*y.  nvcc contracts these two
 // expressions in the reference; the forms below are the ones pinned against
 // the reference binary's outputs (see oracle variant codes: p form | q form<<2).

@@ -141,9 +141,14 @@ __global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, 
 {
     __shared__ double red[T == 32 ? 1 : 3 * T];
     const int t = threadIdx.x;
-    const int2 pq_idx = pairs[blockIdx.x];
+    // Programmatic dependent launch: the next round may be scheduled now; its
+    // CTAs stop at pdl_wait() until this grid has completed and its stores
+    // are visible.
+    pdl_launch_dependents();
+    const int2 pq_idx = pairs[blockIdx.x];  // written once per plan
     double *__restrict__ ap = a + (size_t)pq_idx.x * lda;
     double *__restrict__ aq = a + (size_t)pq_idx.y * lda;
+    pdl_wait();  // the previous round's columns and counter
 
     double spp = 0.0, sqq = 0.0, spq = 0.0;
     double xp[K > 0 ? K : 1], xq[K > 0 ? K : 1];
@@ -561,7 +566,7 @@ std::atomic<int> g_sweep_mode{0};
 }
 
 int sweep_mode() { return g_sweep_mode.load(); }
-void set_sweep_mode(int mode) { g_sweep_mode.store(mode == 1 ? 1 : 0); }
+void set_sweep_mode(int mode) { g_sweep_mode.store(mode >= 0 && mode <= 2 ? mode : 0); }
 
 PlainStats &plain_stats()
 {
@@ -676,11 +681,24 @@ int PlainPlan::enqueue_rounds(cudaStream_t st, int parity)
     RoundFn round_fn = pick_round(T, (int)m);
     double2 *tab = parity ? cs2 : cs;
     JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_round_begin, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
+    // With use_pdl, rounds after the first are launched with programmatic
+    // stream serialisation, so each round's launch overlaps the previous
+    // round's tail.
+    cudaLaunchAttribute pdl[1];
+    pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    pdl[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(npairs);
+    lc.blockDim = dim3(T);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = st;
     for (int r = 0; r < rounds; ++r) {
         const size_t off = (size_t)r * npairs;
-        round_fn<<<npairs, T, 0, st>>>(a_w, lda, (int)m, pairs + off, tab + off, eps, counter);
+        lc.attrs = r > 0 && use_pdl ? pdl : nullptr;
+        lc.numAttrs = r > 0 && use_pdl ? 1 : 0;
+        JSVD_CUDA_TRY(cudaLaunchKernelEx(&lc, round_fn, a_w, lda, (int)m, (const int2 *)(pairs + off), tab + off, eps,
+                                         counter));
     }
-    JSVD_CUDA_TRY(cudaGetLastError());
     JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_round_end, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
     return JSVD_OK;
 }

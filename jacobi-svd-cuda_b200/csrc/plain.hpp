@@ -32,7 +32,8 @@ struct PlainPlan {
     int *flags = nullptr;         // persistent sweep: rounds completed per CTA
     bool persistent = false;      // one cooperative launch per sweep
     int slots_per_cta = 1, sweep_grid = 0;
-    int mode = 0;  // sweep_mode() at creation
+    int mode = 0;         // sweep_mode() at creation
+    bool use_pdl = false;  // programmatic dependent launch between rounds
     unsigned long long uses = 0;
     bool sweep_exec_capturing = false;
     // staging for host-buffer calls
@@ -70,9 +71,10 @@ struct PlainStats {
 };
 PlainStats &plain_stats();
 
-// Process-wide choice of how a sweep is launched: 0 = one kernel per round
-// (replayed CUDA graph, the default), 1 = one persistent cooperative kernel per
-// sweep.  Plans record the mode they were created with.
+// Process-wide choice of how a sweep is launched: 0 = one kernel per round,
+// replayed from a CUDA graph (the default), 1 = one persistent cooperative
+// kernel per sweep, 2 = as 0 with programmatic dependent launch between rounds.
+// Plans record the mode they were created with.
 int sweep_mode();
 void set_sweep_mode(int mode);
 

@@ -99,63 +99,77 @@ __global__ void __launch_bounds__(256) pc_shift_diagonal(double *__restrict__ G,
 // Cholesky of the kb x kb diagonal block at (k0, k0) of the lower triangle of
 // G (column-major, ld = n) into the same block of Lm, and the inverse of that
 // factor into Linv (column-major, ld = kNb).  1024 threads; thread t owns row
-// t / 16, columns 4 (t % 16) .. 4 (t % 16) + 3 of the block, so the
-// right-looking update needs no index arithmetic beyond that.  status <- 1
-// on a pivot that is not positive and finite.
+// i = t % 64 and columns 4 (t / 64) .. 4 (t / 64) + 3 of the block, so a warp
+// reads 32 consecutive rows of one column: coalesced in global memory and free
+// of bank conflicts in shared memory (row stride kNb + 1), and the column
+// group is uniform across the warp.
+//
+// Factorisation and inverse run in one right-looking loop with one barrier
+// per step j: every thread reads the unscaled column j (a[., j], x[j, .]) and
+// scales what it needs by 1/L(j,j) itself, so no value read in step j is
+// written in step j (the scaled column goes straight to Lm and Linv, the
+// updates touch columns > j of a and rows > j of x).  The pivot's square root
+// and reciprocal are computed once, by the thread that finishes the pivot's
+// last update, and published in shared memory before the barrier.  The
+// inverse is forward elimination of [L | I]: row j of L^{-1} is
+// x[j, .] / L(j,j), then x[i, .] -= L(i,j) L^{-1}[j, .] for i > j.
+// status <- 1 on a pivot that is not positive and finite.
 constexpr size_t kDiagSmem = sizeof(double) * 2 * kNb * (kNb + 1);
+
+__device__ __forceinline__ void pc_publish_pivot(double d, double *piv, int j, int *status)
+{
+    const bool ok = d > 0.0 && d < INFINITY;
+    const double r = ok ? sqrt(d) : 1.0;
+    if (!ok) atomicExch(status, 1);
+    piv[2 * j] = r;
+    piv[2 * j + 1] = 1.0 / r;
+}
 
 __global__ void __launch_bounds__(1024) pc_chol_inv_diag(const double *__restrict__ G, double *__restrict__ Lm,
                                                          int n, int k0, int kb, double *__restrict__ Linv,
                                                          int *__restrict__ status)
 {
     extern __shared__ double dsm[];
+    __shared__ double piv[2 * kNb];  // (L(j,j), 1 / L(j,j))
     double(*a)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);
     double(*x)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm + kNb * (kNb + 1));
-    const int t = threadIdx.x, i = t >> 4, kq = (t & 15) * 4;
+    const int t = threadIdx.x, i = t & (kNb - 1), kq = (t / kNb) * 4;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         const int k = kq + u;
-        a[i][k] = (i < kb && k < kb) ? (i >= k ? G[(size_t)(k0 + k) * n + k0 + i] : 0.0) : (i == k ? 1.0 : 0.0);
+        const double g =
+            (i < kb && k < kb) ? (i >= k ? G[(size_t)(k0 + k) * n + k0 + i] : 0.0) : (i == k ? 1.0 : 0.0);
+        a[i][k] = g;
+        x[i][k] = (i == k) ? 1.0 : 0.0;
+        if (i == 0 && k == 0) pc_publish_pivot(g, piv, 0, status);
+        // entries of L^{-1} that the loop below does not write
+        if (k > i || i >= kb || k >= kb) Linv[i + (size_t)k * kNb] = 0.0;
     }
     __syncthreads();
     for (int j = 0; j < kb; ++j) {
-        const double d = a[j][j];
-        const bool ok = d > 0.0 && d < INFINITY;
-        const double r = ok ? sqrt(d) : 1.0;
-        if (t == 0 && !ok) atomicExch(status, 1);
-        __syncthreads();  // every thread has read a[j][j]
+        const double r = piv[2 * j], rinv = piv[2 * j + 1];
+        if (i == j) {
+            if (kq <= j && j < kq + 4) Lm[(size_t)(k0 + j) * n + k0 + j] = r;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int k = kq + u;
-            if (k == j && i >= j) a[i][j] = (i == j) ? r : a[i][j] / r;
+            for (int u = 0; u < 4; ++u) {
+                const int c = kq + u;
+                if (c <= j) Linv[j + (size_t)c * kNb] = x[j][c] * rinv;
+            }
+        } else if (i > j && i < kb) {
+            const double lij = a[i][j] * rinv;
+            if (kq <= j && j < kq + 4) Lm[(size_t)(k0 + j) * n + k0 + i] = lij;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = kq + u;
+                if (k > j && k <= i) {
+                    const double v = fma(-lij, a[k][j] * rinv, a[i][k]);
+                    a[i][k] = v;
+                    if (k == i && i == j + 1) pc_publish_pivot(v, piv, j + 1, status);
+                }
+                if (k <= j) x[i][k] = fma(-lij, x[j][k] * rinv, x[i][k]);
+            }
         }
         __syncthreads();
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int k = kq + u;
-            if (k > j && i >= k) a[i][k] = fma(-a[i][j], a[k][j], a[i][k]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int k = kq + u;
-        if (i < kb && k < kb && i >= k) Lm[(size_t)(k0 + k) * n + k0 + i] = a[i][k];
-    }
-    // inverse by columns: thread c solves L x = e_c (forward substitution)
-    if (t < kb) {
-        const int c = t;
-        for (int rr = 0; rr < c; ++rr) x[rr][c] = 0.0;
-        for (int rr = c; rr < kb; ++rr) {
-            double acc = (rr == c) ? 1.0 : 0.0;
-            for (int k = c; k < rr; ++k) acc = fma(-a[rr][k], x[k][c], acc);
-            x[rr][c] = acc / a[rr][rr];
-        }
-    }
-    __syncthreads();
-    for (int e = t; e < kNb * kNb; e += blockDim.x) {
-        const int rr = e % kNb, c = e / kNb;
-        Linv[e] = (rr < kb && c < kb) ? x[rr][c] : 0.0;
     }
 }
 
@@ -192,17 +206,17 @@ int thread_cublas(int dev, cudaStream_t st, cublasHandle_t *out)
     return JSVD_OK;
 }
 
-// One Cholesky QR pass: G = Qin^T Qin (+ shift), G = L L^T (blocked,
-// right-looking, diagonal blocks factored and inverted by pc_chol_inv_diag,
-// panels and trailing updates as DGEMM/DSYRK), Qout = Qin L^{-T} (blocked
-// right-looking solve: Qout_J = Qin_J Linv_J^T, Qin_{>J} -= Qout_J L_{>J,J}^T;
-// Qin is overwritten), R = L^T.
-int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Qin, double *Qout, int m, int n, double *G, double *Lm,
+// One Cholesky QR pass: G = Q^T Q (+ shift), G = L L^T (blocked,
+// right-looking; diagonal blocks factored and inverted by pc_chol_inv_diag,
+// panels L21 = G21 L11^{-T} and trailing updates as DGEMM/DSYRK), then
+// Qout = Q L^{-T} by a blocked right-looking solve (Qout_J = Q_J Linv_J^T,
+// Q_{>J} -= Qout_J L_{>J,J}^T; Q is overwritten) and R = L^T.
+int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Q, double *Qout, int m, int n, double *G, double *Lm,
                  double *Linv, double *R, bool shift, int *d_status)
 {
     const double one = 1.0, zero = 0.0, mone = -1.0;
     JSVD_CUDA_TRY(cudaFuncSetAttribute(pc_chol_inv_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
-    JSVD_CUBLAS_TRY(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, m, &one, Qin, m, &zero, G, n));
+    JSVD_CUBLAS_TRY(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, m, &one, Q, m, &zero, G, n));
     if (shift) {
         pc_shift_diagonal<<<1, 256, 0, st>>>(G, n, m);
         JSVD_CUDA_TRY(cudaGetLastError());
@@ -226,12 +240,12 @@ int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Qin, double *Qout, 
     for (int j0 = 0, blk = 0; j0 < n; j0 += kNb, ++blk) {
         const int kb = std::min(kNb, n - j0);
         const double *li = Linv + (size_t)blk * kNb * kNb;
-        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, kb, kb, &one, Qin + (size_t)j0 * m, m, li, kNb,
+        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, kb, kb, &one, Q + (size_t)j0 * m, m, li, kNb,
                                     &zero, Qout + (size_t)j0 * m, m));
         const int rest = n - j0 - kb;
         if (rest > 0)
             JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, rest, kb, &mone, Qout + (size_t)j0 * m, m,
-                                        Lm + (size_t)j0 * n + j0 + kb, n, &one, Qin + (size_t)(j0 + kb) * m, m));
+                                        Lm + (size_t)j0 * n + j0 + kb, n, &one, Q + (size_t)(j0 + kb) * m, m));
     }
     pc_lower_to_upper<<<std::min<size_t>(1184, ((size_t)n * n + 255) / 256), 256, 0, st>>>(Lm, R, n);
     JSVD_CUDA_TRY(cudaGetLastError());
@@ -260,15 +274,18 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     int rc = thread_cublas(dev, st, &hb);
     if (rc != JSVD_OK) return rc;
     const size_t mn = (size_t)m * n, nn = (size_t)n * n;
-    // workspace: Qa, Qb (m x n) | G | Lm | R1 | R2 | R3 | T | Vx | Ux (n x n) | Linv (blocks x 64 x 64) | sigma | status
+    // workspace: Qa, Qb (m x n) | G | Lm | R1 | R2 | R3 | T | Vx | Ux | Sa | Sb | P1 (n x n)
+    //            | Linv (blocks x 64 x 64) | sigma | status
     const int nblk = (n + kNb - 1) / kNb;
     double *ws = nullptr;
-    const size_t ws_doubles = 2 * mn + 8 * nn + (size_t)nblk * kNb * kNb + n + 1;
+    const size_t ws_doubles = 2 * mn + 11 * nn + (size_t)nblk * kNb * kNb + n + 1;
     JSVD_CUDA_TRY(cudaMallocAsync((void **)&ws, sizeof(double) * ws_doubles, st));
     double *Qa = ws, *Qb = Qa + mn, *G = Qb + mn, *Lm = G + nn, *R1 = Lm + nn, *R2 = R1 + nn, *R3 = R2 + nn,
-           *Tm = R3 + nn, *Vx = Tm + nn, *Ux = Vx + nn, *Linv = Ux + nn, *sg = Linv + (size_t)nblk * kNb * kNb;
+           *Tm = R3 + nn, *Vx = Tm + nn, *Ux = Vx + nn, *Sa = Ux + nn, *Sb = Sa + nn, *P1 = Sb + nn,
+           *Linv = P1 + nn, *sg = Linv + (size_t)nblk * kNb * kNb;
     int *d_status = reinterpret_cast<int *>(sg + n);
-    double *Q = Qb;  // after three passes (Qa -> Qb -> Qa -> Qb) the factor is in Qb
+    double *Q = Qb;   // after three passes (Qa -> Qb -> Qa -> Qb) the factor is in Qb
+    double *Q1 = Sb;  // likewise for the second factorisation (Sa -> Sb -> Sa -> Sb)
     cudaEvent_t e0, e1, e2, e3;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -281,46 +298,86 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
         cudaEventDestroy(e2);
         cudaEventDestroy(e3);
     };
+    const double one = 1.0, zero = 0.0;
+    // Shifted CholeskyQR3 of Xa (rows x n, column-major, overwritten): the
+    // orthonormal factor ends in Xb, R = R3 R2 R1 in Ra (upper, column-major);
+    // Rb, Rc are scratch.
+    auto scqr3 = [&](double *Xa, double *Xb, int rows, double *Ra, double *Rb, double *Rc) -> int {
+        int r = chol_qr_pass(hb, st, Xa, Xb, rows, n, G, Lm, Linv, Ra, true, d_status);
+        if (r == JSVD_OK) r = chol_qr_pass(hb, st, Xb, Xa, rows, n, G, Lm, Linv, Rb, false, d_status);
+        if (r == JSVD_OK) r = chol_qr_pass(hb, st, Xa, Xb, rows, n, G, Lm, Linv, Rc, false, d_status);
+        if (r != JSVD_OK) return r;
+        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Rb, n, Ra, n, &zero, Tm, n));
+        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Rc, n, Tm, n, &zero, Ra, n));
+        return JSVD_OK;
+    };
+    auto read_status = [&](int *out) -> int {
+        JSVD_CUDA_TRY(cudaMemcpyAsync(out, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+        return JSVD_OK;
+    };
     cudaEventRecord(e0, st);
     JSVD_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     pc_to_colmajor<<<dim3((n + kTile - 1) / kTile, (m + kTile - 1) / kTile), dim3(kTile, kTileRows), 0, st>>>(
         d_a, m, n, Qa);
     JSVD_CUDA_TRY(cudaGetLastError());
-    rc = chol_qr_pass(hb, st, Qa, Qb, m, n, G, Lm, Linv, R1, true, d_status);
-    if (rc == JSVD_OK) rc = chol_qr_pass(hb, st, Qb, Qa, m, n, G, Lm, Linv, R2, false, d_status);
-    if (rc == JSVD_OK) rc = chol_qr_pass(hb, st, Qa, Qb, m, n, G, Lm, Linv, R3, false, d_status);
+    // A = Q R
+    rc = scqr3(Qa, Qb, m, R1, R2, R3);
+    int status = 0;
+    if (rc == JSVD_OK) rc = read_status(&status);
     if (rc != JSVD_OK) {
         cleanup();
         return rc;
     }
-    const double one = 1.0, zero = 0.0;
-    // R = R3 R2 R1  (upper)
-    JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, R2, n, R1, n, &zero, Tm, n));
-    JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, R3, n, Tm, n, &zero, R1, n));
-    int status = 0;
-    JSVD_CUDA_TRY(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
-    JSVD_CUDA_TRY(cudaStreamSynchronize(st));
-    cudaEventRecord(e1, st);
     PrecondStats &ps = precond_stats();
     if (status != 0) {
         // Gram not positive definite in floating point: plain path on A.
+        cudaEventRecord(e1, st);
         cleanup();
         ps.fallbacks += 1;
         return jsvd_plain_svd_device(d_a, rows, cols, &c, d_u, d_sigma, d_v, sweeps, st);
     }
-    // Jacobi on X = R^T: R's column-major buffer read as row-major is R^T.
-    double *vout = d_v ? d_v : Ux;  // V_A = U_x
-    double *sout = d_sigma ? d_sigma : sg;
-    rc = jsvd_plain_svd_device(R1, cols, cols, &c, vout, sout, Vx, sweeps, st);
+    // R^T = Q1 P (P upper): R1's column-major buffer read as row-major is R^T.
+    pc_to_colmajor<<<dim3((n + kTile - 1) / kTile, (n + kTile - 1) / kTile), dim3(kTile, kTileRows), 0, st>>>(
+        R1, n, n, Sa);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    rc = scqr3(Sa, Sb, n, P1, R2, R3);
+    int status2 = 0;
+    if (rc == JSVD_OK) rc = read_status(&status2);
     if (rc != JSVD_OK) {
         cleanup();
         return rc;
     }
-    cudaEventRecord(e2, st);
-    if (d_u) {
-        // U_A (row-major m x n) = Q V_x; as column-major it is (Q V_x)^T = V_x^T Q^T,
-        // and V_x's row-major buffer is V_x^T column-major.
-        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, n, m, n, &one, Vx, n, Q, m, &zero, d_u, n));
+    cudaEventRecord(e1, st);
+    double *sout = d_sigma ? d_sigma : sg;
+    if (status2 == 0) {
+        // A = Q R = Q P^T Q1^T.  Jacobi on X = P^T (P1's column-major buffer read
+        // as row-major): X = Ux S Vx^T, so U_A = Q Ux and V_A = Q1 Vx.
+        rc = jsvd_plain_svd_device(P1, cols, cols, &c, d_u ? Ux : nullptr, sout, d_v ? Vx : nullptr, sweeps, st);
+        if (rc != JSVD_OK) {
+            cleanup();
+            return rc;
+        }
+        cudaEventRecord(e2, st);
+        // Row-major U_A (m x n) is column-major U_A^T = Ux^T Q^T; Ux's row-major
+        // buffer is Ux^T column-major.  The same for V_A^T = Vx^T Q1^T.
+        if (d_u)
+            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, n, m, n, &one, Ux, n, Q, m, &zero, d_u, n));
+        if (d_v)
+            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, n, &one, Vx, n, Q1, n, &zero, d_v, n));
+    } else {
+        // Second factorisation failed: Jacobi on X = R^T, A = Q X^T =
+        // (Q Vx) S Ux^T, so U_A = Q Vx and V_A = Ux.
+        ps.fallbacks += 1;
+        double *vout = d_v ? d_v : Ux;
+        rc = jsvd_plain_svd_device(R1, cols, cols, &c, vout, sout, Vx, sweeps, st);
+        if (rc != JSVD_OK) {
+            cleanup();
+            return rc;
+        }
+        cudaEventRecord(e2, st);
+        if (d_u)
+            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, n, m, n, &one, Vx, n, Q, m, &zero, d_u, n));
     }
     cudaEventRecord(e3, st);
     JSVD_CUDA_TRY(cudaStreamSynchronize(st));

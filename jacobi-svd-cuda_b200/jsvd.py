@@ -312,7 +312,8 @@ def plain_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None 
 
 
 def set_sweep_mode(mode: int) -> None:
-    """0 = per-round kernels in a replayed graph (default), 1 = persistent sweep."""
+    """0 = per-round kernels in a replayed graph (default), 1 = persistent
+    sweep, 2 = as 0 with programmatic dependent launch between rounds."""
     lib().jsvd_plain_set_sweep_mode(mode)
 
 

@@ -151,3 +151,15 @@ def test_plain_persistent_sweep_bitwise(cuda_device, m, n):
     finally:
         jsvd.set_sweep_mode(0)
     _assert_bitwise(got, _oracle(a, eps))
+
+
+def test_plain_rounds_with_pdl_bitwise(cuda_device):
+    """Sweep mode 2 (programmatic dependent launch between rounds) gives the
+    same bytes."""
+    a = W.gaussian_splitmix(300, 120, seed=99)
+    jsvd.set_sweep_mode(2)
+    try:
+        got = jsvd.plain_svd(a, jsvd.default_config(epsilon=1e-13))
+    finally:
+        jsvd.set_sweep_mode(0)
+    _assert_bitwise(got, _oracle(a, 1e-13))
