@@ -145,7 +145,8 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
     du = torch.empty((m, n), dtype=torch.float64, device=device)
     ds = torch.empty(n, dtype=torch.float64, device=device)
     dv = torch.empty((n, n), dtype=torch.float64, device=device)
-    fn = {"precond": jsvd.precond_svd_device, "blocked": jsvd.blocked_svd_device}.get(path, jsvd.plain_svd_device)
+    fn = {"precond": jsvd.precond_svd_device, "blocked": jsvd.blocked_svd_device,
+          "blockpair": jsvd.blockpair_svd_device}.get(path, jsvd.plain_svd_device)
 
     def step():
         return fn(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg, stream.cuda_stream)
@@ -156,6 +157,7 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
     jsvd.plain_stats_reset()
     jsvd.precond_stats_reset()
     jsvd.blocked_stats_reset()
+    jsvd.blockpair_stats_reset()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(device)
@@ -174,8 +176,8 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
         t = torch.tensor([total_ms], dtype=torch.float64, device=device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-    return total_ms, sweeps, (jsvd.plain_stats(), jsvd.precond_stats(), jsvd.blocked_stats()), ds.cpu().numpy(), \
-        (du, dv)
+    return total_ms, sweeps, (jsvd.plain_stats(), jsvd.precond_stats(), jsvd.blocked_stats(),
+                              jsvd.blockpair_stats()), ds.cpu().numpy(), (du, dv)
 
 
 def blocked_sweep_flops(rows: int, n: int, b: int = 32) -> float:
@@ -204,12 +206,15 @@ def run_ours(args, rank: int, world: int, device):
 
     sampler = ClockSampler(device.index if device.index is not None else 0)
     sampler.start()
-    total_ms, sweeps, (pst, cst, bst), sig, (du, dv) = time_single(args, wl, path, device, stream, args.steps,
-                                                                  args.warmup, flush, world)
+    total_ms, sweeps, (pst, cst, bst, kst), sig, (du, dv) = time_single(args, wl, path, device, stream, args.steps,
+                                                                       args.warmup, flush, world)
     clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
     value = world * args.steps / (total_ms / 1e3)
     launches = int(pst.round_launches + pst.vpass_launches + pst.other_launches)
+    if kst.solves:
+        # outer rounds + per solve: layout in, identity, sigma, U and V layout out
+        launches += int(kst.round_launches) + 5 * int(kst.solves)
     if path == "precond":
         # per solve: layout kernel, 3 passes x (shift?, ceil(n/64) x (chol + trsm) + ceil(n/64) trsm + 1), status
         blocks = (n + 63) // 64
@@ -236,7 +241,8 @@ def run_ours(args, rank: int, world: int, device):
     hs = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
     hv = torch.empty((n, n), dtype=torch.float64).pin_memory().numpy()
     lib = jsvd.lib()
-    entry = lib.jsvd_precond_svd if path in ("precond", "blocked") else lib.jsvd_plain_svd
+    entry = {"precond": lib.jsvd_precond_svd, "blocked": lib.jsvd_precond_svd,
+             "blockpair": lib.jsvd_blockpair_svd}.get(path, lib.jsvd_plain_svd)
     sw = ctypes.c_int(0)
     for _ in range(max(1, args.warmup)):
         jsvd.check(entry(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data, hv.ctypes.data,
@@ -263,7 +269,17 @@ def run_ours(args, rank: int, world: int, device):
 
     hbm_peak, _, peak_kind = peaks()
     mx = n if path == "precond" else m  # rows of the swept matrix
-    if pst.round_launches:
+    if kst.round_launches:
+        # block-pair outer round: every column of X (mx rows) and of V (n rows)
+        # is read and written once per launch
+        avg_ms = kst.round_ms / kst.round_launches
+        bytes_per = 16.0 * n * (mx + n)
+        roof = {"bound": "hbm", "kernel": "bp_round_kernel", "achieved": bytes_per / (avg_ms * 1e-3) / 1e9,
+                "peak": hbm_peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
+                "avg_launch_us": avg_ms * 1e3, "algorithmic_bytes_per_launch": bytes_per,
+                "round_share_of_step": kst.round_ms / max(total_ms / world, 1e-9),
+                "outer_sweeps": kst.sweeps / max(1, kst.solves)}
+    elif pst.round_launches:
         avg_round_ms = pst.round_ms / pst.round_launches
         roof = {"bound": "hbm", "kernel": "plain_round_kernel",
                 "achieved": algorithmic_round_bytes(mx, n) / (avg_round_ms * 1e-3) / 1e9, "peak": hbm_peak,
@@ -304,8 +320,11 @@ def run_ours(args, rank: int, world: int, device):
         "dtype": "f64",
         "data": "synthetic (seeded)",
         "config": {"workload": wl["desc"],
-                   "path": {"precond": "QR-preconditioned: shifted CholeskyQR3 + blocked FP64 Jacobi on R^T",
-                            "blocked": "blocked FP64 one-sided Jacobi on A (32-column blocks)"}.get(
+                   "path": {"precond": "QR-preconditioned: two shifted CholeskyQR3 factorisations (A = QR, "
+                                       "R^T = Q1 P) + FP64 Jacobi on P^T (" +
+                                       ("block-pair" if kst.solves else "plain round-robin") + " sweep)",
+                            "blocked": "blocked FP64 one-sided Jacobi on A (32-column blocks)",
+                            "blockpair": "block-pair FP64 one-sided Jacobi on A"}.get(
                        path, "plain FP64 drop-in (reference arithmetic, round-robin)"),
                    "epsilon": wl["eps"], "sweeps_per_svd": sweeps[0] if sweeps else None,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
@@ -731,9 +750,12 @@ def main():
     ap.add_argument("--large-m", type=int, default=16384)
     ap.add_argument("--large-n", type=int, default=8192)
     ap.add_argument("--large-dir", default="")
-    ap.add_argument("--sweep-mode", type=int, default=0, choices=[0, 1, 2],
-                    help="0: per-round kernels replayed from a graph; 1: persistent sweep kernel; "
-                         "2: as 0 with programmatic dependent launch between rounds")
+    ap.add_argument("--sweep-mode", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="0: per-round kernels replayed from a graph, angle derived once per CTA; "
+                         "1: persistent sweep kernel; 2: as 0 with programmatic dependent launch; "
+                         "3: as 0 with every warp deriving the angle")
+    ap.add_argument("--precond-inner", type=int, default=1, choices=[0, 1],
+                    help="Jacobi stage of the QR-preconditioned path: 0 block-pair where it applies, 1 plain")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -751,6 +773,7 @@ def main():
     torch.cuda.set_device(device)
     import jsvd
     jsvd.set_sweep_mode(args.sweep_mode)
+    jsvd.precond_set_inner(args.precond_inner)
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))

@@ -135,13 +135,15 @@ typedef struct jsvd_plain_stats {
 void jsvd_plain_stats_get(jsvd_plain_stats *out);
 
 /* How the plain path launches a sweep (process-wide, read when a plan is
- * created): 0 = one kernel per round, replayed from a CUDA graph (default);
- * 1 = one persistent cooperative kernel per sweep whose CTAs synchronise with
- * their neighbours through per-CTA round counters (bounded waits); 2 = as 0
- * with programmatic dependent launch, each round scheduled while the previous
- * one drains.  All give bit-identical results; on B200 mode 0 measured
- * fastest (about 3.0 us per 512-row round against 3.9 for mode 2 and 6.9
- * for mode 1). */
+ * created): 0 = one kernel per round, replayed from a CUDA graph, each CTA
+ * reducing its pair's dot products and deriving the angle once, in one warp
+ * (default); 1 = one persistent cooperative kernel per sweep whose CTAs
+ * synchronise with their neighbours through per-CTA round counters (bounded
+ * waits); 2 = as 0 with programmatic dependent launch, each round scheduled
+ * while the previous one drains; 3 = as 0 with every warp reducing and
+ * deriving the angle itself (one barrier fewer, eight times the FP64 work).
+ * All give bit-identical results.  Measured per 512-row round on B200: mode 0
+ * 2.6 us, mode 3 2.9 us, mode 2 3.9 us, mode 1 6.9 us. */
 void jsvd_plain_set_sweep_mode(int mode);
 int jsvd_plain_get_sweep_mode(void);
 void jsvd_plain_stats_reset(void);
@@ -177,6 +179,45 @@ typedef struct jsvd_batch_tuning {
 int jsvd_batch_svd_device(int count, const int *rows, const int *cols, const long long *a_offsets, const void *d_a,
                           int a_is_f32, const jsvd_config *cfg, double *d_sigma, double *d_v, double *d_u,
                           int *sweeps, const jsvd_batch_tuning *tuning, void *stream);
+
+/*
+ * One-sided block-pair Jacobi on device buffers (same arguments and outputs as
+ * jsvd_plain_svd_device).  No single reference function corresponds: it
+ * replaces the cyclic sweep loop of run_one_sided_jacobi_svd_internal
+ * (src/kernels.cu:889-981) with an outer sweep over pairs of column blocks
+ * (B = 2, 4 or 8 columns), each block pair solved by one CTA with a full
+ * inner cyclic sweep over its 2B columns held in registers; V takes the
+ * product of a block pair's rotations once.  Rotation test, angle formula and
+ * stopping rule (an outer sweep without rotation) are the reference's; the
+ * ordering is not, so results agree with the plain path to working accuracy,
+ * not bit for bit.  Up to 4096 rows; taller inputs run the plain path.
+ */
+int jsvd_blockpair_svd_device(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,
+                              double *d_sigma, double *d_v, int *sweeps, void *stream);
+
+/* The same on host buffers (copies in and out on the library's stream). */
+int jsvd_blockpair_svd(const double *a, size_t rows, size_t columns, const jsvd_config *cfg, double *u, double *sigma,
+                       double *v, int *sweeps);
+
+/* Forces the block width (2, 4, 8) and threads per CTA (128, 256, 512) of
+ * block-pair plans created afterwards; 0 keeps the built-in choice for that
+ * parameter.  Process-wide; for tuning and tests. */
+void jsvd_blockpair_set_variant(int block_columns, int threads);
+
+/* Cumulative counters of the block-pair engine on the calling thread. */
+typedef struct jsvd_blockpair_stats {
+    unsigned long long solves;
+    unsigned long long sweeps;          /* outer sweeps */
+    unsigned long long round_launches;  /* outer-round kernels */
+    double round_ms;                    /* device time of the outer sweeps */
+} jsvd_blockpair_stats;
+void jsvd_blockpair_stats_get(jsvd_blockpair_stats *out);
+void jsvd_blockpair_stats_reset(void);
+
+/* Engine of the Jacobi stage inside jsvd_precond_svd*: 0 = block-pair sweep
+ * where it applies, else plain; 1 = the plain sweep (default, faster on B200
+ * for the shapes measured).  Process-wide. */
+void jsvd_precond_set_inner(int engine);
 
 /* Cumulative counters of the batched solver on the calling thread. */
 typedef struct jsvd_batch_stats {

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -11,6 +12,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "blockpair.hpp"
 #include "internal.hpp"
 #include "jsvd.h"
 #include "plain.hpp"
@@ -66,6 +68,19 @@ cudaStream_t thread_stream(int device)
     cudaStream_t st = nullptr;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
     cache.streams.emplace_back(device, st);
+    // The library's workspaces come from the device's default stream-ordered
+    // pool.  With the pool's default release threshold (0) every synchronise
+    // hands freed memory back to the driver and the next call maps it again
+    // (tens of ms for the workspace of a 4096 x 1024 solve); keep up to 4 GiB
+    // cached in this process instead.
+    static std::atomic<unsigned long long> pools_set{0};
+    if (device >= 0 && device < 64 && !(pools_set.fetch_or(1ull << device) & (1ull << device))) {
+        cudaMemPool_t pool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            unsigned long long keep = 4ull << 30;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     return st;
 }
 
@@ -92,6 +107,7 @@ int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t strea
     if (rc != JSVD_OK) return rc;
     plan->mode = sweep_mode();
     plan->use_pdl = plan->mode == 2;
+    plan->angle_once = plan->mode != 3;
     plans.push_back(std::move(plan));
     size_t total = 0;
     for (auto &p : plans) total += p->bytes;
@@ -332,6 +348,7 @@ void jsvd_release_thread_cache(void)
     auto &cache = thread_cache();
     for (auto &s : cache.streams) cudaStreamSynchronize(s.second);
     cache.plans.clear();
+    bp_release_thread_plans();
 }
 
 }  // extern "C"

@@ -34,68 +34,11 @@
 
 #include "common.cuh"
 #include "internal.hpp"
+#include "layout.cuh"
 #include "plain.hpp"
 
 namespace jsvd {
 namespace {
-
-constexpr int kTile = 32;
-constexpr int kTileRows = 8;
-
-// row-major src (rows x cols) -> column-major dst (leading dimension ldd).
-__global__ void __launch_bounds__(kTile *kTileRows)
-    rowmajor_to_colmajor_kernel(const double *__restrict__ src, int rows, int cols, double *__restrict__ dst,
-                                long ldd)
-{
-    __shared__ double tile[kTile][kTile + 1];
-    const int c0 = blockIdx.x * kTile, r0 = blockIdx.y * kTile;
-    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
-        const int r = r0 + k, c = c0 + threadIdx.x;
-        if (r < rows && c < cols) tile[k][threadIdx.x] = src[(size_t)r * cols + c];
-    }
-    __syncthreads();
-    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
-        const int c = c0 + k, r = r0 + threadIdx.x;
-        if (r < rows && c < cols) dst[(size_t)c * ldd + r] = tile[threadIdx.x][k];
-    }
-}
-
-// column-major src (rows x cols, leading dimension lds) -> row-major dst.
-// With sigma != nullptr each column is divided by sigma[c], or zeroed when
-// sigma[c] <= eps (src/kernels.cu:622-627).
-__global__ void __launch_bounds__(kTile *kTileRows)
-    colmajor_to_rowmajor_kernel(const double *__restrict__ src, long lds, int rows, int cols,
-                                double *__restrict__ dst, const double *__restrict__ sigma, double eps)
-{
-    __shared__ double tile[kTile][kTile + 1];
-    const int r0 = blockIdx.x * kTile, c0 = blockIdx.y * kTile;
-    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
-        const int c = c0 + k, r = r0 + threadIdx.x;
-        if (r < rows && c < cols) tile[k][threadIdx.x] = src[(size_t)c * lds + r];
-    }
-    __syncthreads();
-    for (int k = threadIdx.y; k < kTile; k += kTileRows) {
-        const int r = r0 + k, c = c0 + threadIdx.x;
-        if (r < rows && c < cols) {
-            double val = tile[threadIdx.x][k];
-            if (sigma != nullptr) {
-                const double sg = sigma[c];
-                val = (sg > eps) ? (val / sg) : 0.0;
-            }
-            dst[(size_t)r * cols + c] = val;
-        }
-    }
-}
-
-__global__ void identity_colmajor_kernel(double *__restrict__ v, int n, long ldv)
-{
-    const size_t total = (size_t)n * ldv;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const size_t col = idx / ldv, row = idx % ldv;
-        v[idx] = (row == col) ? 1.0 : 0.0;
-    }
-}
 
 // Block-wide reference tree over T lanes for three quantities.  Every warp
 // reads all T partial sums and reduces them in the reference's order itself,
@@ -129,17 +72,70 @@ __device__ __forceinline__ void block_tree3_all(double &pp, double &qq, double &
     }
 }
 
+// The same totals and angle computed once: the partial sums go to shared
+// memory, warp 0 reduces them in the reference's order and lane 0 derives
+// (c, s), which the other threads read after a second barrier.  The
+// arithmetic is block_tree3_all's followed by rotation_params, so the result
+// is bit-identical; the FP64 pipe does the reduction trees and the
+// square-root/division chain of the angle once per CTA instead of once per warp.
+template <int T>
+__device__ __forceinline__ bool block_angle_once(double pp, double qq, double pq, double *red, double2 *cs_sh,
+                                                 double eps, double &c, double &s)
+{
+    if constexpr (T == 32) {
+        pp = warp_tree1(pp);
+        qq = warp_tree1(qq);
+        pq = warp_tree1(pq);
+        double cc = 0.0, ss = 0.0;
+        if (threadIdx.x == 0) {
+            rotation_params(pp, qq, pq, eps, cc, ss);
+        }
+        c = __shfl_sync(0xffffffffu, cc, 0);
+        s = __shfl_sync(0xffffffffu, ss, 0);
+    } else {
+        constexpr int W = T / 32;
+        const int t = threadIdx.x, lane = t & 31;
+        red[t] = pp;
+        red[T + t] = qq;
+        red[2 * T + t] = pq;
+        __syncthreads();
+        if (t < 32) {
+            double y[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) y[w] = red[w * 32 + lane];
+            pp = warp_tree<W>(y);
+#pragma unroll
+            for (int w = 0; w < W; ++w) y[w] = red[T + w * 32 + lane];
+            qq = warp_tree<W>(y);
+#pragma unroll
+            for (int w = 0; w < W; ++w) y[w] = red[2 * T + w * 32 + lane];
+            pq = warp_tree<W>(y);
+            if (lane == 0) {
+                double cc, ss;
+                rotation_params(pp, qq, pq, eps, cc, ss);
+                *cs_sh = make_double2(cc, ss);
+            }
+        }
+        __syncthreads();
+        const double2 g = *cs_sh;
+        c = g.x;
+        s = g.y;
+    }
+    return c != 0.0;  // rotation_params gives c > 0 for a rotation, c = 0 otherwise
+}
+
 // One round of the sweep: blockIdx.x = pair slot.  T threads = T virtual
 // lanes; thread t owns rows t + k*T.  K > 0: the K row-tiles of both columns
 // stay in registers between the dot products and the rotation.  K == 0: the
 // columns are streamed twice (m > K_max * T).
-template <int T, int K>
+template <int T, int K, bool kOnce>
 __global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, long lda, int m,
                                                          const int2 *__restrict__ pairs,
                                                          double2 *__restrict__ cs, double eps,
                                                          unsigned *__restrict__ counter)
 {
     __shared__ double red[T == 32 ? 1 : 3 * T];
+    __shared__ double2 cs_sh;
     const int t = threadIdx.x;
     // Programmatic dependent launch: the next round may be scheduled now; its
     // CTAs stop at pdl_wait() until this grid has completed and its stores
@@ -175,10 +171,15 @@ __global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, 
             spq = fma(x, y, spq);
         }
     }
-    block_tree3_all<T>(spp, sqq, spq, red);
-    // every thread derives the same angle from the same totals
     double c, s;
-    const bool rotates = rotation_params(spp, sqq, spq, eps, c, s);
+    bool rotates;
+    if constexpr (kOnce) {
+        rotates = block_angle_once<T>(spp, sqq, spq, red, &cs_sh, eps, c, s);
+    } else {
+        block_tree3_all<T>(spp, sqq, spq, red);
+        // every thread derives the same angle from the same totals
+        rotates = rotation_params(spp, sqq, spq, eps, c, s);
+    }
     if (t == 0) {
         cs[blockIdx.x] = make_double2(c, s);
         if (rotates) atomicAdd(counter, 1u);
@@ -495,29 +496,32 @@ VpassFn pick_vpass(int R)
     }
 }
 
-template <int T>
+template <int T, bool kOnce>
 RoundFn pick_round_t(int m)
 {
     constexpr int kmax = T <= 256 ? 16 : (T == 512 ? 8 : 4);
-    if (m <= 1 * T) return plain_round_kernel<T, 1>;
-    if (m <= 2 * T) return plain_round_kernel<T, 2>;
-    if (m <= 4 * T) return plain_round_kernel<T, 4>;
-    if (kmax >= 8 && m <= 8 * T) return plain_round_kernel<T, (kmax >= 8 ? 8 : 4)>;
-    if (kmax >= 16 && m <= 16 * T) return plain_round_kernel<T, (kmax >= 16 ? 16 : 4)>;
-    return plain_round_kernel<T, 0>;
+    if (m <= 1 * T) return plain_round_kernel<T, 1, kOnce>;
+    if (m <= 2 * T) return plain_round_kernel<T, 2, kOnce>;
+    if (m <= 4 * T) return plain_round_kernel<T, 4, kOnce>;
+    if (kmax >= 8 && m <= 8 * T) return plain_round_kernel<T, (kmax >= 8 ? 8 : 4), kOnce>;
+    if (kmax >= 16 && m <= 16 * T) return plain_round_kernel<T, (kmax >= 16 ? 16 : 4), kOnce>;
+    return plain_round_kernel<T, 0, kOnce>;
 }
 
-RoundFn pick_round(int T, int m)
+template <bool kOnce>
+RoundFn pick_round_o(int T, int m)
 {
     switch (T) {
-    case 32: return pick_round_t<32>(m);
-    case 64: return pick_round_t<64>(m);
-    case 128: return pick_round_t<128>(m);
-    case 256: return pick_round_t<256>(m);
-    case 512: return pick_round_t<512>(m);
-    default: return pick_round_t<1024>(m);
+    case 32: return pick_round_t<32, kOnce>(m);
+    case 64: return pick_round_t<64, kOnce>(m);
+    case 128: return pick_round_t<128, kOnce>(m);
+    case 256: return pick_round_t<256, kOnce>(m);
+    case 512: return pick_round_t<512, kOnce>(m);
+    default: return pick_round_t<1024, kOnce>(m);
     }
 }
+
+RoundFn pick_round(int T, int m, bool once) { return once ? pick_round_o<true>(T, m) : pick_round_o<false>(T, m); }
 
 SigmaFn pick_sigma(int T)
 {
@@ -566,7 +570,7 @@ std::atomic<int> g_sweep_mode{0};
 }
 
 int sweep_mode() { return g_sweep_mode.load(); }
-void set_sweep_mode(int mode) { g_sweep_mode.store(mode >= 0 && mode <= 2 ? mode : 0); }
+void set_sweep_mode(int mode) { g_sweep_mode.store(mode >= 0 && mode <= 3 ? mode : 0); }
 
 PlainStats &plain_stats()
 {
@@ -678,7 +682,7 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
 // for direct launches and for capture.
 int PlainPlan::enqueue_rounds(cudaStream_t st, int parity)
 {
-    RoundFn round_fn = pick_round(T, (int)m);
+    RoundFn round_fn = pick_round(T, (int)m, angle_once);
     double2 *tab = parity ? cs2 : cs;
     JSVD_CUDA_TRY(cudaEventRecordWithFlags(ev_round_begin, st, sweep_exec_capturing ? cudaEventRecordExternal : 0));
     // With use_pdl, rounds after the first are launched with programmatic

@@ -33,7 +33,8 @@ struct PlainPlan {
     bool persistent = false;      // one cooperative launch per sweep
     int slots_per_cta = 1, sweep_grid = 0;
     int mode = 0;         // sweep_mode() at creation
-    bool use_pdl = false;  // programmatic dependent launch between rounds
+    bool use_pdl = false;     // programmatic dependent launch between rounds
+    bool angle_once = false;  // rounds reduce and derive the angle in one warp
     unsigned long long uses = 0;
     bool sweep_exec_capturing = false;
     // staging for host-buffer calls
@@ -72,9 +73,11 @@ struct PlainStats {
 PlainStats &plain_stats();
 
 // Process-wide choice of how a sweep is launched: 0 = one kernel per round,
-// replayed from a CUDA graph (the default), 1 = one persistent cooperative
-// kernel per sweep, 2 = as 0 with programmatic dependent launch between rounds.
-// Plans record the mode they were created with.
+// replayed from a CUDA graph, each CTA reducing the dot products and deriving
+// the angle in one warp (the default), 1 = one persistent cooperative kernel
+// per sweep, 2 = as 0 with programmatic dependent launch between rounds, 3 = as
+// 0 with every warp deriving the angle itself (one barrier fewer).  Plans
+// record the mode they were created with.
 int sweep_mode();
 void set_sweep_mode(int mode);
 

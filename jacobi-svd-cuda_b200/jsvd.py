@@ -62,6 +62,15 @@ class PlainStats(ctypes.Structure):
     ]
 
 
+class BlockPairStats(ctypes.Structure):
+    _fields_ = [
+        ("solves", ctypes.c_ulonglong),
+        ("sweeps", ctypes.c_ulonglong),
+        ("round_launches", ctypes.c_ulonglong),
+        ("round_ms", ctypes.c_double),
+    ]
+
+
 class BatchTuning(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("max_ctas", ctypes.c_int)]
 
@@ -141,7 +150,8 @@ def exported_symbols() -> list[str]:
         "jsvd_server_get_stats", "jsvd_server_destroy", "jsvd_precond_svd", "jsvd_precond_svd_device",
         "jsvd_precond_stats_get", "jsvd_precond_stats_reset", "jsvd_blocked_svd_device",
         "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset", "jsvd_plain_set_sweep_mode",
-        "jsvd_plain_get_sweep_mode",
+        "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
+        "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
     ]
 
 
@@ -203,6 +213,17 @@ def lib() -> ctypes.CDLL:
         L.jsvd_plain_set_sweep_mode.argtypes = [I]
         L.jsvd_plain_set_sweep_mode.restype = None
         L.jsvd_plain_get_sweep_mode.restype = I
+        L.jsvd_blockpair_svd_device.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P, P]
+        L.jsvd_blockpair_svd_device.restype = I
+        L.jsvd_blockpair_svd.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P]
+        L.jsvd_blockpair_svd.restype = I
+        L.jsvd_blockpair_set_variant.argtypes = [I, I]
+        L.jsvd_blockpair_set_variant.restype = None
+        L.jsvd_blockpair_stats_get.argtypes = [ctypes.POINTER(BlockPairStats)]
+        L.jsvd_blockpair_stats_get.restype = None
+        L.jsvd_blockpair_stats_reset.restype = None
+        L.jsvd_precond_set_inner.argtypes = [I]
+        L.jsvd_precond_set_inner.restype = None
         _LIB = L
     return _LIB
 
@@ -291,6 +312,51 @@ def blocked_stats_reset() -> None:
     lib().jsvd_blocked_stats_reset()
 
 
+def blockpair_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:
+    """Device-buffer block-pair Jacobi solve on raw pointers; returns outer sweeps."""
+    cfg = cfg or default_config()
+    sw = ctypes.c_int(0)
+    check(lib().jsvd_blockpair_svd_device(d_a, m, n, ctypes.byref(cfg), d_u, d_sigma, d_v, ctypes.byref(sw),
+                                          stream or None))
+    return sw.value
+
+
+def blockpair_svd(a: np.ndarray, cfg: Config | None = None, device=None):
+    """Block-pair solve of a host matrix through the device entry point
+    (torch buffers) -> (U, sigma, V, outer sweeps)."""
+    import torch
+
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    m, n = a.shape
+    da = torch.from_numpy(a).to(dev)
+    du = torch.empty((m, n), dtype=torch.float64, device=dev)
+    ds = torch.empty(n, dtype=torch.float64, device=dev)
+    dv = torch.empty((n, n), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+    sw = blockpair_svd_device(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg)
+    return du.cpu().numpy(), ds.cpu().numpy(), dv.cpu().numpy(), sw
+
+
+def blockpair_set_variant(block_columns: int = 0, threads: int = 0) -> None:
+    lib().jsvd_blockpair_set_variant(block_columns, threads)
+
+
+def blockpair_stats() -> BlockPairStats:
+    st = BlockPairStats()
+    lib().jsvd_blockpair_stats_get(ctypes.byref(st))
+    return st
+
+
+def blockpair_stats_reset() -> None:
+    lib().jsvd_blockpair_stats_reset()
+
+
+def precond_set_inner(engine: int) -> None:
+    """0 = block-pair Jacobi stage where it applies, 1 = plain sweep (default)."""
+    lib().jsvd_precond_set_inner(engine)
+
+
 def precond_stats() -> PrecondStats:
     st = PrecondStats()
     lib().jsvd_precond_stats_get(ctypes.byref(st))
@@ -312,8 +378,9 @@ def plain_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None 
 
 
 def set_sweep_mode(mode: int) -> None:
-    """0 = per-round kernels in a replayed graph (default), 1 = persistent
-    sweep, 2 = as 0 with programmatic dependent launch between rounds."""
+    """0 = per-round kernels in a replayed graph, angle derived once per CTA
+    (default), 1 = persistent sweep, 2 = as 0 with programmatic dependent
+    launch, 3 = as 0 with every warp deriving the angle."""
     lib().jsvd_plain_set_sweep_mode(mode)
 
 

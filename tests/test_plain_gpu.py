@@ -163,3 +163,16 @@ def test_plain_rounds_with_pdl_bitwise(cuda_device):
     finally:
         jsvd.set_sweep_mode(0)
     _assert_bitwise(got, _oracle(a, 1e-13))
+
+
+@pytest.mark.parametrize("T", [32, 256, 1024])
+def test_plain_angle_every_warp_bitwise(cuda_device, T):
+    """Sweep mode 3 (every warp reduces and derives the angle itself, the
+    single-barrier form) gives the same bytes as the oracle."""
+    a = W.gaussian_splitmix(700, 90, seed=123)
+    jsvd.set_sweep_mode(3)
+    try:
+        got = jsvd.plain_svd(a, jsvd.default_config(epsilon=1e-13, threads_per_block=T))
+    finally:
+        jsvd.set_sweep_mode(0)
+    _assert_bitwise(got, _oracle(a, 1e-13, T))
