@@ -115,6 +115,8 @@ class ClockSampler:
 # DRAM bytes (read + write) per launch measured by one ncu capture of the
 # named kernel at the named swept shape (rows, columns); caches are flushed
 # between ncu passes, so these are cold-cache figures.  Other shapes: null.
+L2_BYTES = 126e6  # B200 L2
+
 PROFILED_TRAFFIC = {("plain_round_kernel", 1024, 1024): 8408576.0}
 
 
@@ -247,7 +249,7 @@ def run_ours(args, rank: int, world: int, device):
     hs = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
     hv = torch.empty((n, n), dtype=torch.float64).pin_memory().numpy()
     lib = jsvd.lib()
-    entry = {"precond": lib.jsvd_precond_svd, "blocked": lib.jsvd_precond_svd,
+    entry = {"precond": lib.jsvd_precond_svd, "blocked": lib.jsvd_blocked_svd,
              "blockpair": lib.jsvd_blockpair_svd}.get(path, lib.jsvd_plain_svd)
     sw = ctypes.c_int(0)
     e2e_steps = 0 if args.no_e2e else args.steps
@@ -306,6 +308,10 @@ def run_ours(args, rank: int, world: int, device):
                 "flops_per_sweep": blocked_sweep_flops(mx, n),
                 "sweep_share_of_step": bst.sweep_ms / max(total_ms / world, 1e-9)}
     roof["frac"] = roof["achieved"] / roof["peak"]
+    # The swept matrix (and V) of these workloads fit in the 126 MB L2: the
+    # algorithmic bytes are served from L2, so `achieved` can pass the HBM
+    # copy rate and `frac` above 1 is expected there.
+    roof["l2_resident"] = bool(8.0 * (mx + n) * n <= L2_BYTES)
     phases = None
     if path == "precond" and cst.solves:
         phases = {"qr_ms": cst.qr_ms / cst.solves, "jacobi_ms": cst.jacobi_ms / cst.solves,

@@ -256,6 +256,10 @@ int jsvd_precond_svd_device(const double *d_a, size_t rows, size_t columns, cons
 int jsvd_blocked_svd_device(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,
                             double *d_sigma, double *d_v, int *sweeps, void *stream);
 
+/* The same on host buffers (copies in and out on the library's stream). */
+int jsvd_blocked_svd(const double *a, size_t rows, size_t columns, const jsvd_config *cfg, double *u, double *sigma,
+                     double *v, int *sweeps);
+
 typedef struct jsvd_blocked_stats {
     unsigned long long solves, sweeps, block_rounds;
     double sweep_ms; /* device time of the sweeps (events) */

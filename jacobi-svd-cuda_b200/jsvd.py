@@ -149,7 +149,7 @@ def exported_symbols() -> list[str]:
         "jsvd_server_options_default", "jsvd_server_create", "jsvd_server_submit", "jsvd_server_wait",
         "jsvd_server_get_stats", "jsvd_server_destroy", "jsvd_precond_svd", "jsvd_precond_svd_device",
         "jsvd_precond_stats_get", "jsvd_precond_stats_reset", "jsvd_blocked_svd_device",
-        "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset", "jsvd_plain_set_sweep_mode",
+        "jsvd_blocked_svd", "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset", "jsvd_plain_set_sweep_mode",
         "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
     ]
@@ -207,6 +207,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_precond_stats_reset.restype = None
         L.jsvd_blocked_svd_device.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P, P]
         L.jsvd_blocked_svd_device.restype = I
+        L.jsvd_blocked_svd.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P]
+        L.jsvd_blocked_svd.restype = I
         L.jsvd_blocked_stats_get.argtypes = [ctypes.POINTER(BlockedStats)]
         L.jsvd_blocked_stats_get.restype = None
         L.jsvd_blocked_stats_reset.restype = None

@@ -61,3 +61,22 @@ def test_blocked_deterministic_and_close_to_plain(cuda_device):
         assert np.array_equal(p, q)
     pu, ps, pv, _ = jsvd.plain_svd(a, jsvd.default_config(epsilon=1e-14))
     assert O.sigma_errors(x[1], ps)["normwise"] <= 4e-15 * 256
+
+
+@pytest.mark.parametrize("entry", ["jsvd_blocked_svd", "jsvd_blockpair_svd"])
+def test_host_buffer_entries_match_device(cuda_device, entry):
+    """The host-buffer entry points return the device entry points' bytes."""
+    import ctypes
+
+    a = W.gaussian_splitmix(300, 161, 67)
+    m, n = a.shape
+    cfg = jsvd.default_config(epsilon=1e-14)
+    u, s, v = np.empty((m, n)), np.empty(n), np.empty((n, n))
+    sw = ctypes.c_int(0)
+    jsvd.check(getattr(jsvd.lib(), entry)(a.ctypes.data, m, n, ctypes.byref(cfg), u.ctypes.data, s.ctypes.data,
+                                          v.ctypes.data, ctypes.byref(sw)))
+    if entry == "jsvd_blocked_svd":
+        du, ds, dv, dsw = _solve(a, cuda_device)
+    else:
+        du, ds, dv, dsw = jsvd.blockpair_svd(a, cfg)
+    assert sw.value == dsw and np.array_equal(s, ds) and np.array_equal(u, du) and np.array_equal(v, dv)
