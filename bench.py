@@ -148,7 +148,7 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
 
     a = wl["a"]
     m, n = a.shape
-    cfg = jsvd.default_config(epsilon=wl["eps"])
+    cfg = jsvd.default_config(epsilon=wl["eps"], **({"threads_per_block": args.threads} if args.threads else {}))
     da = torch.from_numpy(a).to(device)
     du = torch.empty((m, n), dtype=torch.float64, device=device)
     ds = torch.empty(n, dtype=torch.float64, device=device)
@@ -206,7 +206,7 @@ def run_ours(args, rank: int, world: int, device):
     a = wl["a"]
     m, n = a.shape
     path = args.path if args.path != "auto" else "precond"
-    cfg = jsvd.default_config(epsilon=wl["eps"])
+    cfg = jsvd.default_config(epsilon=wl["eps"], **({"threads_per_block": args.threads} if args.threads else {}))
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
     torch.cuda.synchronize(device)
     stream = torch.cuda.Stream(device)
@@ -553,7 +553,7 @@ def run_serve(args, rank: int, world: int, device):
     sampler.start()
     for rate in rates:
         arrivals = t_unit / rate
-        with jsvd.Server(cfg, budget_bytes=budget, large_path=1) as srv:
+        with jsvd.Server(cfg, budget_bytes=budget, large_path=1, large_workers=args.serve_large_workers) as srv:
             # warm the worker plans and kernels
             srv.wait(srv.submit(mats[0]))
             tickets = [None] * len(mats)
@@ -761,6 +761,7 @@ def main():
     ap.add_argument("--rates", default="50,200,1000")
     ap.add_argument("--serve-count", type=int, default=300)
     ap.add_argument("--serve-plain-sample", type=int, default=40)
+    ap.add_argument("--serve-large-workers", type=int, default=0, help="0 = the serving core's default")
     ap.add_argument("--large-m", type=int, default=16384)
     ap.add_argument("--large-n", type=int, default=8192)
     ap.add_argument("--large-dir", default="")
@@ -768,6 +769,8 @@ def main():
                     help="0: per-round kernels replayed from a graph, angle derived once per CTA; "
                          "1: persistent sweep kernel; 2: as 0 with programmatic dependent launch; "
                          "3: as 0 with every warp deriving the angle")
+    ap.add_argument("--threads", type=int, default=0,
+                    help="threads_per_block (reduction width T) of the config; 0 = the reference default 256")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the host-buffer leg (profiling runs: only the warm-up and timed solves launch)")
     ap.add_argument("--precond-inner", type=int, default=1, choices=[0, 1],

@@ -499,12 +499,15 @@ VpassFn pick_vpass(int R)
 template <int T, bool kOnce>
 RoundFn pick_round_t(int m)
 {
-    constexpr int kmax = T <= 256 ? 16 : (T == 512 ? 8 : 4);
+    // K rows per thread stay in registers between the dot products and the
+    // rotation; K = 0 streams the columns twice (taller than K_max * T).
+    constexpr int kmax = T <= 128 ? 16 : (T == 256 ? 32 : (T == 512 ? 8 : 4));
     if (m <= 1 * T) return plain_round_kernel<T, 1, kOnce>;
     if (m <= 2 * T) return plain_round_kernel<T, 2, kOnce>;
     if (m <= 4 * T) return plain_round_kernel<T, 4, kOnce>;
     if (kmax >= 8 && m <= 8 * T) return plain_round_kernel<T, (kmax >= 8 ? 8 : 4), kOnce>;
     if (kmax >= 16 && m <= 16 * T) return plain_round_kernel<T, (kmax >= 16 ? 16 : 4), kOnce>;
+    if (kmax >= 32 && m <= 32 * T) return plain_round_kernel<T, (kmax >= 32 ? 32 : 4), kOnce>;
     return plain_round_kernel<T, 0, kOnce>;
 }
 
