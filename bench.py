@@ -315,7 +315,8 @@ def run_ours(args, rank: int, world: int, device):
     phases = None
     if path == "precond" and cst.solves:
         phases = {"qr_ms": cst.qr_ms / cst.solves, "jacobi_ms": cst.jacobi_ms / cst.solves,
-                  "u_ms": cst.u_ms / cst.solves, "fallbacks": int(cst.fallbacks)}
+                  "u_ms": cst.u_ms / cst.solves, "fallbacks": int(cst.fallbacks),
+                  "gram_checks": pst.gram_checks / cst.solves}
     if bst.solves:
         phases = dict(phases or {}, blocked_sweeps=bst.sweeps / bst.solves,
                       blocked_sweep_ms=bst.sweep_ms / max(1, bst.sweeps),

@@ -130,6 +130,7 @@ typedef struct jsvd_plain_stats {
     unsigned long long other_launches; /* layout, identity, sigma, U and V kernels */
     double round_ms;
     double vpass_ms;
+    unsigned long long gram_checks; /* Gram convergence tests (QR-preconditioned path) */
 } jsvd_plain_stats;
 
 void jsvd_plain_stats_get(jsvd_plain_stats *out);
@@ -218,6 +219,15 @@ void jsvd_blockpair_stats_reset(void);
  * where it applies, else plain; 1 = the plain sweep (default, faster on B200
  * for the shapes measured).  Process-wide. */
 void jsvd_precond_set_inner(int engine);
+
+/* 1 (default): inside jsvd_precond_svd*, when epsilon >= 1e-12 and a sweep
+ * of the plain Jacobi stage rotates fewer than 1/8 of its pairs, every pair is
+ * tested on the Gram matrix of the columns (one DSYRK); when none would
+ * rotate, the final sweep (which would rotate nothing) is not run but is
+ * still counted in `sweeps`.  Below 1e-12 the GEMM's own rounding of the
+ * off-diagonal entries is too close to epsilon for the test to succeed.
+ * 0: always run that sweep.  Process-wide. */
+void jsvd_precond_set_gram_stop(int enable);
 
 /* Cumulative counters of the batched solver on the calling thread. */
 typedef struct jsvd_batch_stats {

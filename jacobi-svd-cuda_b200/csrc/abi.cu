@@ -150,7 +150,7 @@ int validate_plain_request(const void *input, size_t rows, size_t columns, const
 namespace {
 
 int plain_device_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config *cfg, double *d_u,
-                      double *d_sigma, double *d_v, int *sweeps, cudaStream_t stream)
+                      double *d_sigma, double *d_v, int *sweeps, cudaStream_t stream, bool gram_stop = false)
 {
     jsvd_config def;
     jsvd_config_default(&def);
@@ -177,13 +177,21 @@ int plain_device_impl(const double *d_a, size_t rows, size_t cols, const jsvd_co
     PlainPlan *plan = nullptr;
     rc = acquire_plain_plan(rows, cols, reduction_lanes(c.threads_per_block), c.epsilon, stream, &plan);
     if (rc != JSVD_OK) return rc;
-    rc = plan->run(d_a, d_u, d_sigma, d_v, c.max_sweeps, sweeps, stream);
+    rc = plan->run(d_a, d_u, d_sigma, d_v, c.max_sweeps, sweeps, stream, gram_stop);
     if (rc != JSVD_OK) return rc;
     JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
     return JSVD_OK;
 }
 
 }  // namespace
+
+int plain_device_solve(const double *d_a, size_t rows, size_t cols, const jsvd_config *cfg, double *d_u,
+                       double *d_sigma, double *d_v, int *sweeps, cudaStream_t stream, bool gram_stop)
+{
+    set_last_error(JSVD_OK, "");
+    return plain_device_impl(d_a, rows, cols, cfg, d_u, d_sigma, d_v, sweeps, stream, gram_stop);
+}
+
 }  // namespace jsvd
 
 using namespace jsvd;
@@ -335,6 +343,7 @@ void jsvd_plain_stats_get(jsvd_plain_stats *out)
     out->other_launches = s.other_launches;
     out->round_ms = s.round_ms;
     out->vpass_ms = s.vpass_ms;
+    out->gram_checks = s.gram_checks;
 }
 
 void jsvd_plain_stats_reset(void) { plain_stats() = PlainStats{}; }

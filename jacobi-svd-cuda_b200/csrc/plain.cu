@@ -203,6 +203,24 @@ __global__ void __launch_bounds__(T) plain_round_kernel(double *__restrict__ a, 
     }
 }
 
+// Counts the pairs p > q of the lower triangle of G (column-major, ld n) that
+// pass the reference's rotation test (src/kernels.cu:503-505):
+// |g_pq| > eps sqrt(max(g_pp, 0) max(g_qq, 0)) and |g_pq| > 1e-300.
+__global__ void gram_offdiag_count(const double *__restrict__ G, int n, double eps, unsigned *__restrict__ count)
+{
+    unsigned local = 0;
+    const size_t total = (size_t)n * n;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int q = (int)(e / n), p = (int)(e - (size_t)q * n);
+        if (p <= q) continue;
+        const double g = G[e];
+        const double rhs = eps * sqrt(fmax(G[(size_t)p * n + p], 0.0) * fmax(G[(size_t)q * n + q], 0.0));
+        if (fabs(g) > rhs && fabs(g) > 1.0e-300) ++local;
+    }
+    for (int off = 16; off > 0; off >>= 1) local += __shfl_down_sync(0xffffffffu, local, off);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
 // Pair k of round r of the fixed-head circle schedule in closed form (the
 // same sequence build_schedule tabulates): positions 1..ne-1 rotate by one per
 // round, so position i >= 1 holds 1 + ((i - 1 - r) mod (ne - 1)); for odd n
@@ -601,9 +619,11 @@ PlainPlan::~PlainPlan()
         for (cudaEvent_t e : {ev_rounds_done[p], ev_vpass_done[p], ev_v0[p], ev_v1[p]})
             if (e) cudaEventDestroy(e);
     for (void *p : {(void *)a_w, (void *)v_w, (void *)pairs, (void *)cs, (void *)cs2, (void *)counter, (void *)flags,
-                    (void *)d_in,
-                    (void *)d_u, (void *)d_sigma, (void *)d_v, (void *)sigma_w})
+                    (void *)d_in, (void *)d_u, (void *)d_sigma, (void *)d_v, (void *)sigma_w, (void *)gram,
+                    (void *)gram_count})
         if (p) cudaFreeAsync(p, stream);
+    if (h_gram_count) cudaFreeHost(h_gram_count);
+    if (cublas) cublasDestroy(cublas);
     if (prev >= 0) cudaSetDevice(prev);
 }
 
@@ -775,8 +795,40 @@ int PlainPlan::ensure_host_staging()
     return JSVD_OK;
 }
 
+int PlainPlan::gram_converged(cudaStream_t st, bool &converged)
+{
+    if (gram == nullptr) {
+        JSVD_CUDA_TRY(cudaMallocAsync((void **)&gram, sizeof(double) * n * n, stream));
+        JSVD_CUDA_TRY(cudaMallocAsync((void **)&gram_count, sizeof(unsigned), stream));
+        JSVD_CUDA_TRY(cudaMallocHost((void **)&h_gram_count, sizeof(unsigned)));
+        JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
+    }
+    if (cublas == nullptr) {
+        const cublasStatus_t cs0 = cublasCreate(&cublas);
+        if (cs0 != CUBLAS_STATUS_SUCCESS) {
+            cublas = nullptr;
+            set_last_error(JSVD_ERR_CUDA, "cublasCreate failed (status " + std::to_string((int)cs0) + ").");
+            return JSVD_ERR_CUDA;
+        }
+    }
+    const double one = 1.0, zero = 0.0;
+    if (cublasSetStream(cublas, st) != CUBLAS_STATUS_SUCCESS ||
+        cublasDsyrk(cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)n, (int)m, &one, a_w, (int)lda, &zero, gram,
+                    (int)n) != CUBLAS_STATUS_SUCCESS) {
+        set_last_error(JSVD_ERR_CUDA, "cublasDsyrk failed in the Gram convergence test.");
+        return JSVD_ERR_CUDA;
+    }
+    JSVD_CUDA_TRY(cudaMemsetAsync(gram_count, 0, sizeof(unsigned), st));
+    gram_offdiag_count<<<std::min<size_t>(1184, (n * n + 255) / 256), 256, 0, st>>>(gram, (int)n, eps, gram_count);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    JSVD_CUDA_TRY(cudaMemcpyAsync(h_gram_count, gram_count, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+    converged = *h_gram_count == 0;
+    return JSVD_OK;
+}
+
 int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *out_v, int max_sweeps, int *sweeps,
-                   cudaStream_t stream)
+                   cudaStream_t stream, bool gram_stop)
 {
     const int im = (int)m, in = (int)n;
     {
@@ -864,6 +916,21 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             st.round_launches += (unsigned long long)rounds;
             st.vpass_launches += 1;
             if (rotated == 0) break;
+            // Few rotations: the next sweep may rotate nothing; test every pair
+            // on the Gram matrix instead of running it.
+            // Only for eps >= 1e-12: the GEMM's rounding of an off-diagonal
+            // entry (about sqrt(m) u relative) must stay well below eps, or
+            // the test never confirms convergence (measured at eps = 1e-14).
+            if (gram_stop && eps >= 1e-12 && s + 1 < max_sweeps && (size_t)rotated * 8 <= (size_t)rounds * npairs) {
+                bool conv = false;
+                const int rc = gram_converged(stream, conv);
+                if (rc != JSVD_OK) return rc;
+                st.gram_checks += 1;
+                if (conv) {
+                    executed = s + 2;  // the sweep that would have found no rotation
+                    break;
+                }
+            }
         }
         for (int p = 0; p < 2; ++p) {
             if (vpending[p]) JSVD_CUDA_TRY(cudaStreamWaitEvent(stream, ev_vpass_done[p], 0));

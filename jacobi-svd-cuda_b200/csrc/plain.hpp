@@ -4,10 +4,13 @@
 // graph instantiation once.
 #pragma once
 
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
 #include <memory>
+
+#include "jsvd.h"
 
 namespace jsvd {
 
@@ -39,6 +42,11 @@ struct PlainPlan {
     bool sweep_exec_capturing = false;
     // staging for host-buffer calls
     double *d_in = nullptr, *d_u = nullptr, *d_sigma = nullptr, *d_v = nullptr;
+    // convergence test on the Gram matrix (run option gram_stop), made on first use
+    double *gram = nullptr;            // n x n, lower triangle
+    unsigned *gram_count = nullptr;    // pairs that would rotate
+    unsigned *h_gram_count = nullptr;  // pinned
+    cublasHandle_t cublas = nullptr;
 
     cudaGraphExec_t sweep_exec = nullptr;   // rounds of even sweeps
     cudaGraphExec_t sweep_exec2 = nullptr;  // rounds of odd sweeps
@@ -60,14 +68,23 @@ struct PlainPlan {
     int enqueue_vpass(cudaStream_t st, int parity);
     int enqueue_persistent(cudaStream_t st, int parity, int g0);
     int capture_rounds(cudaStream_t st, int parity);
-    // Runs the whole solve on device buffers; outputs may be null.
+    // Runs the whole solve on device buffers; outputs may be null.  With
+    // gram_stop and eps >= 1e-12, a sweep that rotated few pairs is followed
+    // by a test of every pair on G = A^T A (one DSYRK): when no pair would
+    // rotate, the next sweep would change nothing and is not run (it is
+    // counted in `sweeps`).  The
+    // dot products then come from the GEMM, not the reference's reduction
+    // tree, so results equal the default's only to working accuracy; the
+    // bit-exact drop-in never sets it.
     int run(const double *d_a, double *out_u, double *out_sigma, double *out_v, int max_sweeps, int *sweeps,
-            cudaStream_t stream);
+            cudaStream_t stream, bool gram_stop = false);
+    int gram_converged(cudaStream_t stream, bool &converged);
 };
 
 // Cumulative per-thread counters of the plain path (jsvd_plain_stats).
 struct PlainStats {
     unsigned long long solves = 0, sweeps = 0, round_launches = 0, vpass_launches = 0, other_launches = 0;
+    unsigned long long gram_checks = 0;  // Gram convergence tests (run option gram_stop)
     double round_ms = 0.0, vpass_ms = 0.0;
 };
 PlainStats &plain_stats();
@@ -80,6 +97,11 @@ PlainStats &plain_stats();
 // record the mode they were created with.
 int sweep_mode();
 void set_sweep_mode(int mode);
+
+// The plain device-buffer solve (jsvd_plain_svd_device) with the run option
+// gram_stop (see PlainPlan::run); for paths held to a tolerance.
+int plain_device_solve(const double *d_a, size_t rows, size_t cols, const jsvd_config *cfg, double *d_u,
+                       double *d_sigma, double *d_v, int *sweeps, cudaStream_t stream, bool gram_stop);
 
 // Per-thread plan cache and stream.
 int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t stream, PlainPlan **plan);

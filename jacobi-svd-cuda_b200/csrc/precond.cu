@@ -256,6 +256,7 @@ int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Q, double *Qout, in
 }
 
 std::atomic<int> g_inner{1};
+std::atomic<int> g_gram_stop{1};
 
 // The Jacobi stage on X (row-major cols x cols): the plain sweep (default) or,
 // when selected, the block-pair engine where it applies.  The plain sweep
@@ -267,7 +268,9 @@ int inner_jacobi(const double *x, size_t cols, const jsvd_config &c, double *u, 
 {
     if (g_inner.load() == 0 && bp_supported(cols, cols))
         return bp_solve(x, cols, cols, c.epsilon, c.max_sweeps, u, sigma, v, sweeps, st);
-    return jsvd_plain_svd_device(x, cols, cols, &c, u, sigma, v, sweeps, st);
+    // The last, rotation-free sweep is replaced by a test of every pair on the
+    // Gram matrix (this path is held to a tolerance, not to the bits).
+    return plain_device_solve(x, cols, cols, &c, u, sigma, v, sweeps, st, g_gram_stop.load() != 0);
 }
 
 struct PrecondStats {
@@ -468,6 +471,8 @@ extern "C" int jsvd_precond_svd(const double *a, size_t rows, size_t columns, co
 }
 
 extern "C" void jsvd_precond_set_inner(int engine) { g_inner.store(engine == 0 ? 0 : 1); }
+
+extern "C" void jsvd_precond_set_gram_stop(int enable) { g_gram_stop.store(enable ? 1 : 0); }
 
 extern "C" void jsvd_precond_stats_get(jsvd_precond_stats *out)
 {

@@ -59,6 +59,7 @@ class PlainStats(ctypes.Structure):
         ("other_launches", ctypes.c_ulonglong),
         ("round_ms", ctypes.c_double),
         ("vpass_ms", ctypes.c_double),
+        ("gram_checks", ctypes.c_ulonglong),
     ]
 
 
@@ -152,6 +153,7 @@ def exported_symbols() -> list[str]:
         "jsvd_blocked_svd", "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset", "jsvd_plain_set_sweep_mode",
         "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
+        "jsvd_precond_set_gram_stop",
     ]
 
 
@@ -226,6 +228,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_blockpair_stats_reset.restype = None
         L.jsvd_precond_set_inner.argtypes = [I]
         L.jsvd_precond_set_inner.restype = None
+        L.jsvd_precond_set_gram_stop.argtypes = [I]
+        L.jsvd_precond_set_gram_stop.restype = None
         _LIB = L
     return _LIB
 
@@ -357,6 +361,12 @@ def blockpair_stats_reset() -> None:
 def precond_set_inner(engine: int) -> None:
     """0 = block-pair Jacobi stage where it applies, 1 = plain sweep (default)."""
     lib().jsvd_precond_set_inner(engine)
+
+
+def precond_set_gram_stop(enable: bool) -> None:
+    """True (default): the precond path's final, rotation-free sweep is
+    replaced by a test of every pair on the Gram matrix."""
+    lib().jsvd_precond_set_gram_stop(1 if enable else 0)
 
 
 def precond_stats() -> PrecondStats:

@@ -68,3 +68,29 @@ def test_precond_device_entry(cuda_device):
     assert np.array_equal(ds.cpu().numpy(), host[1])
     st = jsvd.precond_stats()
     assert st.solves >= 1 and st.fallbacks == 0 and st.qr_ms > 0 and st.jacobi_ms > 0
+
+
+@pytest.mark.parametrize("name,make,kappa", [CASES[0], CASES[3], CASES[4]], ids=[CASES[0][0], CASES[3][0], CASES[4][0]])
+def test_precond_gram_stop_matches_full_sweeps(cuda_device, name, make, kappa):
+    """At epsilon 1e-10 the final rotation-free sweep is replaced by the Gram
+    test: same sweep count, results within the precond tolerance of the run
+    that executes every sweep."""
+    a = make()
+    n = a.shape[1]
+    cfg = jsvd.default_config(epsilon=1e-10)
+    jsvd.plain_stats_reset()
+    gu, gs, gv, gsw = jsvd.precond_svd(a, cfg)
+    checks = jsvd.plain_stats().gram_checks
+    jsvd.plain_stats_reset()
+    jsvd.precond_set_gram_stop(False)
+    try:
+        fu, fs, fv, fsw = jsvd.precond_svd(a, cfg)
+    finally:
+        jsvd.precond_set_gram_stop(True)
+    assert jsvd.plain_stats().gram_checks == 0
+    if name == CASES[0][0]:
+        assert checks >= 1  # the 2048 x 512 graded case reaches the test before converging
+    assert gsw == fsw
+    assert O.sigma_errors(gs, fs)["normwise"] <= 1e-15 * max(n, 100)
+    r = O.residuals(a, gu, gs, gv)
+    assert r["rho_A"] <= 1e-11 * n and r["rho_V"] <= 1e-12 * n and r["rho_U"] <= 1e-10 * n, r
