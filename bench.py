@@ -39,6 +39,25 @@ FLUSH_BYTES = 256 << 20  # > 126 MB L2
 PLAIN_SWEEPS = {"tall": 30, "square512": 14}
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """Maximum of a per-rank scalar over all ranks (times: the job is as slow
+    as its slowest replica); identity on one rank.  `device` is where the
+    process group's backend reduces (a CUDA device for NCCL, cpu for gloo)."""
+    if world <= 1:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank: float, world: int, max_seconds: float) -> float:
+    """Whole-job throughput of `world` independent replicas: all units that
+    all ranks processed, over the slowest rank's time."""
+    return world * units_per_rank / max_seconds
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -180,10 +199,7 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
     torch.cuda.synchronize(device)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world, device)
     return total_ms, sweeps, (jsvd.plain_stats(), jsvd.precond_stats(), jsvd.blocked_stats(),
                               jsvd.blockpair_stats()), ds.cpu().numpy(), (du, dv)
 
@@ -218,7 +234,7 @@ def run_ours(args, rank: int, world: int, device):
                                                                        args.warmup, flush, world)
     clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms / 1e3)
+    value = replica_rate(args.steps, world, total_ms / 1e3)
     launches = int(pst.round_launches + pst.vpass_launches + pst.other_launches)
     if kst.solves:
         # outer rounds + per solve: layout in, identity, sigma, U and V layout out
@@ -264,11 +280,8 @@ def run_ours(args, rank: int, world: int, device):
         jsvd.check(entry(ha.ctypes.data, m, n, ctypes.byref(cfg), hu.ctypes.data, hs.ctypes.data, hv.ctypes.data,
                          ctypes.byref(sw)))
         e2e_s += time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * e2e_steps / e2e_s if e2e_steps else None
+    e2e_s = max_over_ranks(e2e_s, world, device)
+    e2e_value = replica_rate(e2e_steps, world, e2e_s) if e2e_steps else None
 
     # the plain drop-in on the same input, for the speed-up of the fast path
     plain = None
@@ -429,11 +442,8 @@ def run_batch(args, rank: int, world: int, device):
         total_ms += step_ms[-1]
     clocks = sampler.stop()
     st = jsvd.batch_stats()
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps * b.count / (total_ms / 1e3)
+    total_ms = max_over_ranks(total_ms, world, device)
+    value = replica_rate(args.steps * b.count, world, total_ms / 1e3)
     flops = batch_flops(b.rows, b.cols, b.sweeps)
     kernel_ms = st.kernel_ms / max(1, st.calls)
     achieved = flops / (kernel_ms * 1e-3) / 1e12
@@ -454,10 +464,7 @@ def run_batch(args, rank: int, world: int, device):
         torch.cuda.synchronize(device)
         if i > 0:
             e2e_s += time.perf_counter() - t1
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, world, device)
     line = {
         "metric": "SVDs/s",
         "value": value,
@@ -479,7 +486,8 @@ def run_batch(args, rank: int, world: int, device):
                    "generation_s": gen_s, "step_ms": step_ms,
                    "classes": {"count": [int(x) for x in st.class_count],
                                "ms_per_step": [x / max(1, st.calls) for x in st.class_ms]}},
-        "e2e": {"value": world * args.steps * b.count / e2e_s, "unit": "SVD/s", "h2d_bytes_per_step": b.h2d_bytes,
+        "e2e": {"value": replica_rate(args.steps * b.count, world, e2e_s), "unit": "SVD/s",
+                "h2d_bytes_per_step": b.h2d_bytes,
                 "d2h_bytes_per_step": int((b.sigma.numel() + b.v.numel()) * 8),
                 "timer": "host wall clock around H2D + solve + D2H"},
         "gpu_launches": int(st.launches),

@@ -1,0 +1,51 @@
+"""Multi-rank plumbing of bench.py on the CPU (gloo, world size 2): replicas
+only, so the only cross-rank step is the max over ranks of each timing, and
+the job rate counts every rank's units over the slowest rank's time.  The
+reference arm runs on rank 0 alone; other ranks exit 0 without output."""
+import os
+import subprocess
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+
+def _worker(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        dist.barrier()
+        t = bench.max_over_ranks(10.0 + 5.0 * rank, world, torch.device("cpu"))
+        out[rank] = (t, bench.replica_rate(3, world, t))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_rate_gloo():
+    port = 29500 + (os.getpid() % 2000)
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
+        res = dict(out)
+    # both ranks see the slowest rank's time; 2 replicas x 3 units over 15 s
+    assert res[0] == res[1] == (15.0, 0.4)
+
+
+def test_single_rank_helpers():
+    assert bench.max_over_ranks(7.5, 1, None) == 7.5
+    assert bench.replica_rate(4, 1, 2.0) == 2.0
+
+
+@pytest.mark.timeout(120)
+def test_reference_arm_other_ranks_exit_silently():
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                       capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == ""
