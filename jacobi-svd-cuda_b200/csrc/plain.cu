@@ -854,16 +854,41 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             if (rc == JSVD_OK) rc = capture_rounds(stream, 1);
             if (rc != JSVD_OK) return rc;
         }
-        // The V pass of sweep s runs on vstream while the rounds of sweep s + 1
-        // run on `stream`; the (c, s) tables alternate between sweeps, and the
-        // rounds of sweep s + 2 wait for the V pass of sweep s.
         bool vpending[2] = {false, false};
+        float r_ms_of[2] = {0.f, 0.f};  // rounds time of the sweep whose V pass is pending
+        // V pass width: the pass runs beside the next sweep's rounds and its
+        // CTAs take registers the rounds could use, so it is made as narrow
+        // as it can be while it still ends well inside those rounds: measured
+        // against the rounds of the same sweep, halve the threads (>= 128)
+        // when it took under 0.6 of their time, double them (<= the pair
+        // count, <= 512) when it took over 0.9.  Kept in the plan.  The
+        // result does not depend on the width (the slots of a round are
+        // disjoint).  At 1024 rows: 512 -> 128 threads, rounds 3.98 -> 3.73 us.
+        auto adapt_vpass = [&](float v_ms, float r_ms) {
+            if (r_ms <= 0.f) return;
+            const int cap = std::min(512, std::max(32, (npairs + 31) / 32 * 32));
+            if (v_ms < 0.6f * r_ms && vpass_threads > 128) vpass_threads = std::max(128, vpass_threads / 2);
+            else if (v_ms > 0.9f * r_ms && vpass_threads < cap) vpass_threads = std::min(cap, vpass_threads * 2);
+        };
         auto collect_v = [&](int p) -> int {
             if (!vpending[p]) return JSVD_OK;
             JSVD_CUDA_TRY(cudaEventSynchronize(ev_v1[p]));
             float v_ms = 0.f;
-            if (cudaEventElapsedTime(&v_ms, ev_v0[p], ev_v1[p]) == cudaSuccess) st.vpass_ms += v_ms;
+            if (cudaEventElapsedTime(&v_ms, ev_v0[p], ev_v1[p]) == cudaSuccess) {
+                st.vpass_ms += v_ms;
+                if (!persistent) adapt_vpass(v_ms, r_ms_of[p]);
+            }
             vpending[p] = false;
+            return JSVD_OK;
+        };
+        auto launch_vpass = [&](int p, cudaStream_t vs) -> int {
+            JSVD_CUDA_TRY(cudaEventRecord(ev_v0[p], vs));
+            const int rc = enqueue_vpass(vs, p);
+            if (rc != JSVD_OK) return rc;
+            JSVD_CUDA_TRY(cudaEventRecord(ev_v1[p], vs));
+            JSVD_CUDA_TRY(cudaEventRecord(ev_vpass_done[p], vs));
+            vpending[p] = true;
+            st.vpass_launches += 1;
             return JSVD_OK;
         };
         for (int s = 0; s < max_sweeps; ++s) {
@@ -877,6 +902,10 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             if (persistent) {
                 const int rc = enqueue_persistent(stream, p, s * rounds);
                 if (rc != JSVD_OK) return rc;
+                // All CTAs of a persistent sweep must be resident: its V pass
+                // runs after it on the same stream.
+                const int rc2 = launch_vpass(p, stream);
+                if (rc2 != JSVD_OK) return rc2;
             } else {
                 cudaGraphExec_t g = p ? sweep_exec2 : sweep_exec;
                 if (g != nullptr) {
@@ -885,22 +914,8 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
                     const int rc = enqueue_rounds(stream, p);
                     if (rc != JSVD_OK) return rc;
                 }
-            }
-            // A persistent sweep needs all of its CTAs resident: its V pass runs
-            // after it on the same stream instead of beside the next sweep.
-            cudaStream_t vs = persistent ? stream : vstream;
-            if (!persistent) {
                 JSVD_CUDA_TRY(cudaEventRecord(ev_rounds_done[p], stream));
-                JSVD_CUDA_TRY(cudaStreamWaitEvent(vstream, ev_rounds_done[p], 0));
             }
-            JSVD_CUDA_TRY(cudaEventRecord(ev_v0[p], vs));
-            {
-                const int rc = enqueue_vpass(vs, p);
-                if (rc != JSVD_OK) return rc;
-            }
-            JSVD_CUDA_TRY(cudaEventRecord(ev_v1[p], vs));
-            JSVD_CUDA_TRY(cudaEventRecord(ev_vpass_done[p], vs));
-            vpending[p] = true;
             unsigned cnt[2] = {0, 0};
             JSVD_CUDA_TRY(cudaMemcpyAsync(cnt, counter, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
             JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -914,8 +929,16 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             float r_ms = 0.f;
             if (cudaEventElapsedTime(&r_ms, ev_round_begin, ev_round_end) == cudaSuccess) st.round_ms += r_ms;
             st.round_launches += (unsigned long long)rounds;
-            st.vpass_launches += 1;
-            if (rotated == 0) break;
+            if (rotated == 0) break;  // V unchanged by this sweep: no V pass
+            // The V pass of sweep s runs on vstream while the rounds of sweep
+            // s + 1 run on `stream`; the (c, s) tables alternate between
+            // sweeps, and the rounds of sweep s + 2 wait for this V pass.
+            if (!persistent) {
+                r_ms_of[p] = r_ms;
+                JSVD_CUDA_TRY(cudaStreamWaitEvent(vstream, ev_rounds_done[p], 0));
+                const int rc = launch_vpass(p, vstream);
+                if (rc != JSVD_OK) return rc;
+            }
             // Few rotations: the next sweep may rotate nothing; test every pair
             // on the Gram matrix instead of running it.
             // Only for eps >= 1e-12: the GEMM's rounding of an off-diagonal
