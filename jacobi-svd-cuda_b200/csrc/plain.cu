@@ -855,20 +855,22 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             if (rc != JSVD_OK) return rc;
         }
         bool vpending[2] = {false, false};
-        float r_ms_of[2] = {0.f, 0.f};  // rounds time of the sweep whose V pass is pending
+        float r_ref = 0.f;  // rounds time of this solve's first sweep: no V pass runs beside it
         // V pass width: the pass runs beside the next sweep's rounds and its
         // CTAs take registers the rounds could use, so it is made as narrow
-        // as it can be while it still ends well inside those rounds: measured
-        // against the rounds of the same sweep, halve the threads (>= 128)
-        // when it took under 0.6 of their time, double them (<= the pair
-        // count, <= 512) when it took over 0.9.  Kept in the plan.  The
-        // result does not depend on the width (the slots of a round are
-        // disjoint).  At 1024 rows: 512 -> 128 threads, rounds 3.98 -> 3.73 us.
-        auto adapt_vpass = [&](float v_ms, float r_ms) {
-            if (r_ms <= 0.f) return;
+        // as it can be while it still ends well inside those rounds.  The
+        // yardstick is the first sweep's rounds (uncontended; the rounds that
+        // a V pass overlaps are slowed by it): halve the threads (>= 128) when
+        // the pass took under 0.45 of that time, double them (<= the pair
+        // count, <= 512) when it took over 0.9.  Kept in the plan.  The result
+        // does not depend on the width (the slots of a round are disjoint).
+        // At 1024 rows: 512 -> 128 threads, rounds 3.98 -> 3.73 us; at 8192
+        // rows the pass stays at 512 (0.85 of the rounds' time).
+        auto adapt_vpass = [&](float v_ms) {
+            if (r_ref <= 0.f) return;
             const int cap = std::min(512, std::max(32, (npairs + 31) / 32 * 32));
-            if (v_ms < 0.6f * r_ms && vpass_threads > 128) vpass_threads = std::max(128, vpass_threads / 2);
-            else if (v_ms > 0.9f * r_ms && vpass_threads < cap) vpass_threads = std::min(cap, vpass_threads * 2);
+            if (v_ms < 0.45f * r_ref && vpass_threads > 128) vpass_threads = std::max(128, vpass_threads / 2);
+            else if (v_ms > 0.9f * r_ref && vpass_threads < cap) vpass_threads = std::min(cap, vpass_threads * 2);
         };
         auto collect_v = [&](int p) -> int {
             if (!vpending[p]) return JSVD_OK;
@@ -876,7 +878,7 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             float v_ms = 0.f;
             if (cudaEventElapsedTime(&v_ms, ev_v0[p], ev_v1[p]) == cudaSuccess) {
                 st.vpass_ms += v_ms;
-                if (!persistent) adapt_vpass(v_ms, r_ms_of[p]);
+                if (!persistent) adapt_vpass(v_ms);
             }
             vpending[p] = false;
             return JSVD_OK;
@@ -933,8 +935,8 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
             // The V pass of sweep s runs on vstream while the rounds of sweep
             // s + 1 run on `stream`; the (c, s) tables alternate between
             // sweeps, and the rounds of sweep s + 2 wait for this V pass.
+            if (s == 0) r_ref = r_ms;
             if (!persistent) {
-                r_ms_of[p] = r_ms;
                 JSVD_CUDA_TRY(cudaStreamWaitEvent(vstream, ev_rounds_done[p], 0));
                 const int rc = launch_vpass(p, vstream);
                 if (rc != JSVD_OK) return rc;
