@@ -250,6 +250,8 @@ __device__ __forceinline__ int2 schedule_pair(int n, int r, int k)
 // same bank (which a column-by-column staging with R = 8 would cause).
 // Thread k owns pair slot k of every round; the (c, s) of the next round is
 // loaded while the current one is applied.
+constexpr int kVpassSlots = 8;  // prefetched pair slots per thread and round
+
 template <int R>
 __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v, long ldv, int n,
                                                           const double2 *__restrict__ cs, int rounds, int npairs)
@@ -263,17 +265,52 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
         sv[rr * n + col] = (rr < rows) ? v[(size_t)col * ldv + r0 + rr] : 0.0;
     }
     __syncthreads();
+    // Thread k0 owns pair slots k0, k0 + blockDim.x, ...: the (c, s) of its
+    // first kVpassSlots slots for round r + 1 are loaded while round r is
+    // applied, so a round waits on one L2 round trip, not one per slot (the
+    // loads cannot move past the shared-memory stores of the previous slot).
+    // Slots beyond those (more than kVpassSlots * blockDim.x pairs) are read
+    // when used.
     const int k0 = threadIdx.x;
-    double2 g_next = (k0 < npairs) ? cs[k0] : make_double2(0.0, 0.0);
+    const int nb = blockDim.x;
+    double2 g_next[kVpassSlots];
+#pragma unroll
+    for (int j = 0; j < kVpassSlots; ++j) {
+        const int k = k0 + j * nb;
+        g_next[j] = (k < npairs) ? cs[k] : make_double2(0.0, 0.0);
+    }
     for (int r = 0; r < rounds; ++r) {
-        for (int k = k0; k < npairs; k += blockDim.x) {
-            double2 g;
-            if (k == k0) {
-                g = g_next;
-                if (r + 1 < rounds) g_next = cs[(size_t)(r + 1) * npairs + k0];
-            } else {
-                g = cs[(size_t)r * npairs + k];
+        double2 g_cur[kVpassSlots];
+#pragma unroll
+        for (int j = 0; j < kVpassSlots; ++j) g_cur[j] = g_next[j];
+        if (r + 1 < rounds) {
+#pragma unroll
+            for (int j = 0; j < kVpassSlots; ++j) {
+                const int k = k0 + j * nb;
+                if (k < npairs) g_next[j] = cs[(size_t)(r + 1) * npairs + k];
             }
+        }
+#pragma unroll
+        for (int j = 0; j < kVpassSlots; ++j) {
+            const int k = k0 + j * nb;
+            const double2 g = g_cur[j];
+            if (k < npairs && g.x != 0.0) {
+                const int2 pq = schedule_pair(n, r, k);
+                double x[R], y[R];
+#pragma unroll
+                for (int h = 0; h < R; ++h) {
+                    x[h] = sv[h * n + pq.x];
+                    y[h] = sv[h * n + pq.y];
+                }
+#pragma unroll
+                for (int h = 0; h < R; ++h) {
+                    sv[h * n + pq.x] = rot_p(g.x, g.y, x[h], y[h]);
+                    sv[h * n + pq.y] = rot_q(g.x, g.y, x[h], y[h]);
+                }
+            }
+        }
+        for (int k = k0 + kVpassSlots * nb; k < npairs; k += nb) {
+            const double2 g = cs[(size_t)r * npairs + k];
             if (g.x != 0.0) {
                 const int2 pq = schedule_pair(n, r, k);
                 double x[R], y[R];
@@ -869,7 +906,9 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
         auto adapt_vpass = [&](float v_ms) {
             if (r_ref <= 0.f) return;
             const int cap = std::min(512, std::max(32, (npairs + 31) / 32 * 32));
-            if (v_ms < 0.45f * r_ref && vpass_threads > 128) vpass_threads = std::max(128, vpass_threads / 2);
+            // at most kVpassSlots slots per thread (all prefetched), >= 128 threads
+            const int floor_t = std::min(cap, std::max(128, (npairs + kVpassSlots - 1) / kVpassSlots + 31) / 32 * 32);
+            if (v_ms < 0.45f * r_ref && vpass_threads > floor_t) vpass_threads = std::max(floor_t, vpass_threads / 2);
             else if (v_ms > 0.9f * r_ref && vpass_threads < cap) vpass_threads = std::min(cap, vpass_threads * 2);
         };
         auto collect_v = [&](int p) -> int {
