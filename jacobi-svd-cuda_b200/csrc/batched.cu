@@ -7,7 +7,8 @@
 // depends on the class:
 //   class 0-2: A and V in shared memory (<= 48 KiB, <= 100 KiB, <= ~226 KiB)
 //   class 3  : A in shared memory, V in a per-CTA slice of global memory
-//   class 4  : A and V in global memory (L2-resident per-CTA slices)
+//   class 4  : A and V in global memory (L2-resident per-CTA slices), the
+//              leading columns of A that fit in shared memory kept there
 // Each round runs in three phases separated by __syncthreads:
 //   1. one warp per pair: the three dot products, reduced in the reference's
 //      order (T = 256 virtual lanes; lane l holds virtual lanes l + 32j, then
@@ -143,8 +144,13 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
                                                     int a_is_f32, double eps, int max_sweeps,
                                                     double *__restrict__ sigma_all, double *__restrict__ v_all,
                                                     double *__restrict__ u_all, int *__restrict__ sweeps_all,
-                                                    double *__restrict__ workspace, size_t ws_stride)
+                                                    double *__restrict__ workspace, size_t ws_stride,
+                                                    int smem_doubles)
 {
+    // A and V in global memory: the leading columns of A that fit the shared
+    // memory left over live there instead (a pair reads its columns from
+    // whichever space holds them).
+    constexpr bool kHybrid = !kAShared && !kVShared;
     extern __shared__ double smem[];
     __shared__ int s_idx;
     __shared__ int s_rot;
@@ -165,18 +171,24 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
         double *A = kAShared ? sm_rest : gws;
         double *V = kVShared ? (kAShared ? sm_rest + (size_t)m * n : gws + (size_t)m * n)
                              : (kAShared ? gws : gws + (size_t)m * n);
+        // columns 0 .. ks-1 of A in shared memory, ks .. n-1 in the global slice
+        const int ks = kHybrid ? max(0, min(n, (smem_doubles - (int)round_scratch_doubles(n)) / m)) : 0;
+        auto colA = [&](int c) -> double * {
+            if constexpr (kHybrid) return c < ks ? sm_rest + (size_t)c * m : gws + (size_t)(c - ks) * m;
+            else return A + (size_t)c * m;
+        };
         const size_t mn = (size_t)m * n;
         if (a_is_f32) {
             const float *src = reinterpret_cast<const float *>(a_all) + d.a_off;
             for (size_t e = threadIdx.x; e < mn; e += blockDim.x) {
                 const size_t r = e / n, c = e - r * n;
-                A[c * m + r] = (double)src[e];
+                colA((int)c)[r] = (double)src[e];
             }
         } else {
             const double *src = reinterpret_cast<const double *>(a_all) + d.a_off;
             for (size_t e = threadIdx.x; e < mn; e += blockDim.x) {
                 const size_t r = e / n, c = e - r * n;
-                A[c * m + r] = src[e];
+                colA((int)c)[r] = src[e];
             }
         }
         for (size_t e = threadIdx.x; e < (size_t)n * n; e += blockDim.x) V[e] = (e / n == e % n) ? 1.0 : 0.0;
@@ -193,7 +205,7 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
                     for (int k = warp; k < npairs; k += nwarps) {
                         const int2 pq = batch_pair(n, r, k);
                         double pp, qq, pqv;
-                        warp_pair_stats(A + (size_t)pq.x * m, A + (size_t)pq.y * m, m, lane, pp, qq, pqv);
+                        warp_pair_stats(colA(pq.x), colA(pq.y), m, lane, pp, qq, pqv);
                         if (lane == 0) {
                             st_pp[k] = pp;
                             st_qq[k] = qq;
@@ -213,7 +225,7 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
                         const double2 g = st_cs[k];
                         if (g.x == 0.0) continue;
                         const int2 pq = batch_pair(n, r, k);
-                        warp_rotate(A + (size_t)pq.x * m, A + (size_t)pq.y * m, m, V + (size_t)pq.x * n,
+                        warp_rotate(colA(pq.x), colA(pq.y), m, V + (size_t)pq.x * n,
                                     V + (size_t)pq.y * n, n, lane, g.x, g.y);
                     }
                     __syncthreads();
@@ -228,7 +240,7 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
         // sigma, U (optional), V (row-major)
         double *sg = sigma_all + d.s_off;
         for (int c = warp; c < n; c += nwarps) {
-            const double *x = A + (size_t)c * m;
+            const double *x = colA(c);
             const double sc = sqrt(fmax(warp_norm2(x, m, lane), 0.0));
             if (lane == 0) sg[c] = sc;
             if (u_all != nullptr) {
@@ -249,7 +261,7 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
 }
 
 using BatchFn = void (*)(const BatchDesc *, int, int *, const void *, int, double, int, double *, double *,
-                         double *, int *, double *, size_t);
+                         double *, int *, double *, size_t, int);
 
 // Per-thread timing events: whole call and one pair per size class.
 struct ThreadEvents {
@@ -416,9 +428,12 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         // starved each other (a 512-thread CTA of the global class fills an
         // SM's register file).
         JSVD_CUDA_TRY(cudaEventRecord(ts->c0[c], stream));
-        cl.fn<<<grid_of[c], cl.threads, smem_of[c], stream>>>(d_desc + first[c], cnt, d_next + c, req.a, req.a_is_f32,
-                                                          req.eps, req.max_sweeps, req.sigma, req.v, req.u,
-                                                          d_sweeps + first[c], d_ws + gws_base[c], gws_of[c]);
+        // The global class keeps leading columns of A in the shared memory left over.
+        const size_t dyn = (!cl.a_shared && !cl.v_shared) ? (smem_cap & ~(size_t)7) : smem_of[c];
+        cl.fn<<<grid_of[c], cl.threads, dyn, stream>>>(d_desc + first[c], cnt, d_next + c, req.a, req.a_is_f32,
+                                                       req.eps, req.max_sweeps, req.sigma, req.v, req.u,
+                                                       d_sweeps + first[c], d_ws + gws_base[c], gws_of[c],
+                                                       (int)(dyn / sizeof(double)));
         JSVD_CUDA_TRY(cudaGetLastError());
         JSVD_CUDA_TRY(cudaEventRecord(ts->c1[c], stream));
         ++launches;
