@@ -42,4 +42,6 @@ def main(out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/reference_gpu.json")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/reference_gpu_timing.py OUT.json")
+    main(sys.argv[1])
