@@ -282,6 +282,7 @@ struct BpPlan {
             if (xw) cudaFreeAsync(xw, alloc_stream);
             if (bpairs) cudaFreeAsync(bpairs, alloc_stream);
             cudaStreamSynchronize(alloc_stream);
+            cudaStreamDestroy(alloc_stream);
         }
     }
 
@@ -321,9 +322,17 @@ int create_plan(int dev, size_t m, size_t n, const Variant *var, std::unique_ptr
     plan->m = m;
     plan->n = n;
     plan->var = var;
-    plan->alloc_stream = thread_stream(dev);
-    if (plan->alloc_stream == nullptr)
-        return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+    // The plan owns its allocation stream: plans are cached per thread and may
+    // outlive the library's per-thread streams at thread exit.  Every solve
+    // synchronises before it returns, so no work of a plan is in flight when
+    // it is released.
+    {
+        const cudaError_t e = cudaStreamCreateWithFlags(&plan->alloc_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            plan->alloc_stream = nullptr;
+            return cuda_failure(e, "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+        }
+    }
     const int B = var->B;
     plan->nblocks = (int)((n + B - 1) / B);
     const int nbe = plan->nblocks + (plan->nblocks & 1);
