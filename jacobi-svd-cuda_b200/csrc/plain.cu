@@ -12,14 +12,16 @@
 //     column tiles written back in place.  The reference needs three launches
 //     and three blocking host transfers per round.
 //   * V never sits on the round-to-round critical path.  Each round records
-//     its (c, s); after the sweep one row-parallel pass applies the whole
-//     sweep to V, rows held in shared memory, on a second stream while the
-//     next sweep's rounds run (the angle tables alternate between sweeps).
-//     Per element the sequence of rotations is the reference's, so V is
-//     bit-identical.
-//   * A sweep (n-1 round kernels + the V pass) is launched directly the first
-//     time a plan (device, m, n, T, eps) is used and captured into a CUDA graph
-//     when the plan is reused; the host reads one rotation counter per sweep.
+//     its (c, s); after a sweep that rotated, one row-parallel pass applies the
+//     whole sweep to V, rows held in shared memory, on a second stream while
+//     the next sweep's rounds run (the angle tables alternate between sweeps).
+//     The pass is kept as narrow as it can be while it still ends inside
+//     those rounds, so that it takes few of their registers.  Per element the
+//     sequence of rotations is the reference's, so V is bit-identical.
+//   * The n-1 round kernels of a sweep are launched directly the first time a
+//     plan (device, m, n, T, eps, sweep mode) is used and captured into a CUDA
+//     graph when the plan is reused; the host reads one rotation counter per
+//     sweep.
 //   * Plan workspaces use stream-ordered allocation, so creating or evicting a
 //     plan never synchronises the whole device.
 #include <cuda_runtime.h>
