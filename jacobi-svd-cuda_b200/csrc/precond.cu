@@ -101,78 +101,123 @@ __global__ void __launch_bounds__(256) pc_shift_diagonal(double *__restrict__ G,
 
 // Cholesky of the kb x kb diagonal block at (k0, k0) of the lower triangle of
 // G (column-major, ld = n) into the same block of Lm, and the inverse of that
-// factor into Linv (column-major, ld = kNb).  1024 threads; thread t owns row
-// i = t % 64 and columns 4 (t / 64) .. 4 (t / 64) + 3 of the block, so a warp
-// reads 32 consecutive rows of one column: coalesced in global memory and free
-// of bank conflicts in shared memory (row stride kNb + 1), and the column
-// group is uniform across the warp.
+// factor into Linv (column-major, ld = kNb).  The block is padded to kNb x kNb
+// with the identity.
 //
-// Factorisation and inverse run in one right-looking loop with one barrier
-// per step j: every thread reads the unscaled column j (a[., j], x[j, .]) and
-// scales what it needs by 1/L(j,j) itself, so no value read in step j is
-// written in step j (the scaled column goes straight to Lm and Linv, the
-// updates touch columns > j of a and rows > j of x).  The pivot's square root
-// and reciprocal are computed once, by the thread that finishes the pivot's
-// last update, and published in shared memory before the barrier.  The
-// inverse is forward elimination of [L | I]: row j of L^{-1} is
-// x[j, .] / L(j,j), then x[i, .] -= L(i,j) L^{-1}[j, .] for i > j.
+// Blocked in panels of kPanel columns, so the block synchronises 2 * kNb /
+// kPanel times instead of once per column (a per-column form measured 57 us
+// per block on B200 under ncu, bound by its 64 barriers; the QR stage's event
+// time did not change with this form, its ~500 launches being enqueue-bound):
+//   factorisation: warp 0 factors the panel's columns (right-looking inside
+//     the panel, __syncwarp between columns; each lane owns two rows and reads
+//     the pivot column's panel entries before any of them is rescaled), then
+//     all threads apply the panel's rank-kPanel update to the trailing
+//     triangle, a[i][k] -= sum_j L(i,j) L(k,j);
+//   inverse: block forward substitution of [L | I], kPanel rows at a time:
+//     thread c solves column c through the panel's triangular block (rows in
+//     order, by the stored reciprocal pivots), then all threads subtract the
+//     panel's contribution from the rows below.
 // status <- 1 on a pivot that is not positive and finite.
+constexpr int kPanel = 8;
+constexpr int kDiagThreads = 256;
 constexpr size_t kDiagSmem = sizeof(double) * 2 * kNb * (kNb + 1);
 
-__device__ __forceinline__ void pc_publish_pivot(double d, double *piv, int j, int *status)
-{
-    const bool ok = d > 0.0 && d < INFINITY;
-    const double r = ok ? sqrt(d) : 1.0;
-    if (!ok) atomicExch(status, 1);
-    piv[2 * j] = r;
-    piv[2 * j + 1] = 1.0 / r;
-}
-
-__global__ void __launch_bounds__(1024) pc_chol_inv_diag(const double *__restrict__ G, double *__restrict__ Lm,
-                                                         int n, int k0, int kb, double *__restrict__ Linv,
-                                                         int *__restrict__ status)
+__global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *__restrict__ G,
+                                                                 double *__restrict__ Lm, int n, int k0, int kb,
+                                                                 double *__restrict__ Linv, int *__restrict__ status)
 {
     extern __shared__ double dsm[];
-    __shared__ double piv[2 * kNb];  // (L(j,j), 1 / L(j,j))
+    __shared__ double dinv[kNb];  // 1 / L(i,i)
     double(*a)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);
     double(*x)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm + kNb * (kNb + 1));
-    const int t = threadIdx.x, i = t & (kNb - 1), kq = (t / kNb) * 4;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int k = kq + u;
-        const double g =
-            (i < kb && k < kb) ? (i >= k ? G[(size_t)(k0 + k) * n + k0 + i] : 0.0) : (i == k ? 1.0 : 0.0);
-        a[i][k] = g;
+    const int t = threadIdx.x;
+    for (int e = t; e < kNb * kNb; e += kDiagThreads) {
+        const int i = e % kNb, k = e / kNb;  // consecutive threads read consecutive rows of column k
+        a[i][k] = (i < kb && k < kb) ? (i >= k ? G[(size_t)(k0 + k) * n + k0 + i] : 0.0) : (i == k ? 1.0 : 0.0);
         x[i][k] = (i == k) ? 1.0 : 0.0;
-        if (i == 0 && k == 0) pc_publish_pivot(g, piv, 0, status);
-        // entries of L^{-1} that the loop below does not write
-        if (k > i || i >= kb || k >= kb) Linv[i + (size_t)k * kNb] = 0.0;
     }
     __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        const double r = piv[2 * j], rinv = piv[2 * j + 1];
-        if (i == j) {
-            if (kq <= j && j < kq + 4) Lm[(size_t)(k0 + j) * n + k0 + j] = r;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int c = kq + u;
-                if (c <= j) Linv[j + (size_t)c * kNb] = x[j][c] * rinv;
-            }
-        } else if (i > j && i < kb) {
-            const double lij = a[i][j] * rinv;
-            if (kq <= j && j < kq + 4) Lm[(size_t)(k0 + j) * n + k0 + i] = lij;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int k = kq + u;
-                if (k > j && k <= i) {
-                    const double v = fma(-lij, a[k][j] * rinv, a[i][k]);
-                    a[i][k] = v;
-                    if (k == i && i == j + 1) pc_publish_pivot(v, piv, j + 1, status);
+    // ---- factorisation ----
+    for (int c0 = 0; c0 < kNb; c0 += kPanel) {
+        if (t < 32) {
+            const int lane = t;
+            for (int j = 0; j < kPanel; ++j) {
+                const int cj = c0 + j;
+                const double d = a[cj][cj];
+                const bool ok = d > 0.0 && d < INFINITY;
+                const double r = ok ? sqrt(d) : 1.0;
+                const double rinv = 1.0 / r;
+                if (lane == 0) {
+                    if (!ok) atomicExch(status, 1);
+                    dinv[cj] = rinv;
                 }
-                if (k <= j) x[i][k] = fma(-lij, x[j][k] * rinv, x[i][k]);
+                double colk[kPanel];  // unscaled a[k][cj] of the panel rows below cj
+#pragma unroll
+                for (int kk = 0; kk < kPanel; ++kk) colk[kk] = (kk > j) ? a[c0 + kk][cj] : 0.0;
+                __syncwarp();
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int i = c0 + lane + 32 * h;
+                    if (i >= kNb) continue;
+                    if (i == cj) {
+                        a[i][cj] = r;
+                    } else if (i > cj) {
+                        const double lij = a[i][cj] * rinv;
+                        a[i][cj] = lij;
+#pragma unroll
+                        for (int kk = 0; kk < kPanel; ++kk) {
+                            const int k = c0 + kk;
+                            if (kk > j && k <= i) a[i][k] = fma(-lij, colk[kk] * rinv, a[i][k]);
+                        }
+                    }
+                }
+                __syncwarp();
             }
         }
         __syncthreads();
+        const int base = c0 + kPanel, w = kNb - base;
+        for (int e = t; e < w * w; e += kDiagThreads) {
+            const int i = base + e / w, k = base + e % w;
+            if (k > i) continue;
+            double acc = a[i][k];
+#pragma unroll
+            for (int jj = 0; jj < kPanel; ++jj) acc = fma(-a[i][c0 + jj], a[k][c0 + jj], acc);
+            a[i][k] = acc;
+        }
+        __syncthreads();
+    }
+    // ---- inverse: forward substitution of [L | I] ----
+    for (int r0 = 0; r0 < kNb; r0 += kPanel) {
+        const int cols = r0 + kPanel;  // columns 0 .. cols-1 can be non-zero in these rows
+        if (t < cols) {
+            const int c = t;
+#pragma unroll
+            for (int r = 0; r < kPanel; ++r) {
+                const int i = r0 + r;
+                double val = x[i][c];
+#pragma unroll
+                for (int rr = 0; rr < r; ++rr) val = fma(-a[i][r0 + rr], x[r0 + rr][c], val);
+                x[i][c] = val * dinv[i];
+            }
+        }
+        __syncthreads();
+        const int below = kNb - cols;
+        for (int e = t; e < below * cols; e += kDiagThreads) {
+            const int i = cols + e / cols, c = e % cols;
+            double acc = x[i][c];
+#pragma unroll
+            for (int r = 0; r < kPanel; ++r) acc = fma(-a[i][r0 + r], x[r0 + r][c], acc);
+            x[i][c] = acc;
+        }
+        __syncthreads();
+    }
+    for (int e = t; e < kb * kb; e += kDiagThreads) {
+        const int i = e % kb, k = e / kb;
+        if (i >= k) Lm[(size_t)(k0 + k) * n + k0 + i] = a[i][k];
+    }
+    for (int e = t; e < kNb * kNb; e += kDiagThreads) {
+        const int i = e % kNb, k = e / kNb;
+        Linv[i + (size_t)k * kNb] = (i < kb && k < kb && k <= i) ? x[i][k] : 0.0;
     }
 }
 
@@ -227,7 +272,7 @@ int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Q, double *Qout, in
     for (int k0 = 0, blk = 0; k0 < n; k0 += kNb, ++blk) {
         const int kb = std::min(kNb, n - k0);
         double *li = Linv + (size_t)blk * kNb * kNb;
-        pc_chol_inv_diag<<<1, 1024, kDiagSmem, st>>>(G, Lm, n, k0, kb, li, d_status);
+        pc_chol_inv_diag<<<1, kDiagThreads, kDiagSmem, st>>>(G, Lm, n, k0, kb, li, d_status);
         JSVD_CUDA_TRY(cudaGetLastError());
         const int rest = n - k0 - kb;
         if (rest > 0) {
