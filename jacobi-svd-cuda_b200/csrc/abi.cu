@@ -358,6 +358,7 @@ void jsvd_release_thread_cache(void)
     for (auto &s : cache.streams) cudaStreamSynchronize(s.second);
     cache.plans.clear();
     bp_release_thread_plans();
+    pc_release_thread_plans();
 }
 
 }  // extern "C"

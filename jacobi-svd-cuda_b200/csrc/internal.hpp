@@ -59,6 +59,9 @@ inline int reduction_lanes(int raw_threads)
     return p;
 }
 
+// Drops the calling thread's cached QR-stage plans (precond.cu).
+void pc_release_thread_plans();
+
 }  // namespace jsvd
 
 #define JSVD_CUDA_TRY(EXPR)                                                          \

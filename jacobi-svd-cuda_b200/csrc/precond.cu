@@ -24,9 +24,11 @@
 #include <atomic>
 
 #include <algorithm>
+#include <memory>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "blockpair.hpp"
 #include "internal.hpp"
@@ -330,22 +332,107 @@ PrecondStats &precond_stats()
     return s;
 }
 
+// Per-thread cached resources of the QR stage for one shape: the workspace,
+// a stream for allocation and graph capture, a cuBLAS handle with its own
+// fixed workspace (so the captured GEMMs never allocate and the handle never
+// refers to another plan's memory), and the two shifted CholeskyQR3 stages
+// captured as graphs on the plan's second use.  The stage is ~500 small
+// launches whose enqueueing, not their device time, set its duration.
+struct PcPlan {
+    int device = -1;
+    size_t m = 0, n = 0;
+    double *ws = nullptr;
+    void *blas_ws = nullptr;
+    cudaStream_t own = nullptr;
+    cublasHandle_t blas = nullptr;
+    cudaGraphExec_t qr1 = nullptr, qr2 = nullptr;
+    bool no_graph = false;  // a capture failed: launch directly from then on
+    unsigned long long uses = 0;
+    ~PcPlan()
+    {
+        if (qr1) cudaGraphExecDestroy(qr1);
+        if (qr2) cudaGraphExecDestroy(qr2);
+        if (blas) cublasDestroy(blas);
+        if (own) {
+            if (ws) cudaFreeAsync(ws, own);
+            if (blas_ws) cudaFreeAsync(blas_ws, own);
+            cudaStreamSynchronize(own);
+            cudaStreamDestroy(own);
+        }
+    }
+};
+
+constexpr size_t kPcBlasWorkspace = size_t(32) << 20;
+constexpr size_t kPcMaxPlanBytes = size_t(2) << 30;  // larger shapes allocate per call, no graphs
+constexpr size_t kPcMaxPlans = 2;
+
+std::vector<std::unique_ptr<PcPlan>> &pc_plans()
+{
+    thread_local std::vector<std::unique_ptr<PcPlan>> plans;
+    return plans;
+}
+
+// The cached plan for (device, m, n), created on first use; nullptr (and
+// JSVD_OK) when the shape's workspace is above kPcMaxPlanBytes.
+int acquire_pc_plan(int dev, size_t m, size_t n, size_t ws_doubles, PcPlan **out)
+{
+    *out = nullptr;
+    if (sizeof(double) * ws_doubles > kPcMaxPlanBytes) return JSVD_OK;
+    auto &plans = pc_plans();
+    for (size_t i = 0; i < plans.size(); ++i) {
+        if (plans[i]->device == dev && plans[i]->m == m && plans[i]->n == n) {
+            std::rotate(plans.begin(), plans.begin() + i, plans.begin() + i + 1);
+            *out = plans.front().get();
+            return JSVD_OK;
+        }
+    }
+    auto p = std::make_unique<PcPlan>();
+    p->device = dev;
+    p->m = m;
+    p->n = n;
+    {
+        const cudaError_t e = cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            p->own = nullptr;
+            return cuda_failure(e, "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+        }
+    }
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&p->ws, sizeof(double) * ws_doubles, p->own));
+    JSVD_CUDA_TRY(cudaMallocAsync(&p->blas_ws, kPcBlasWorkspace, p->own));
+    JSVD_CUDA_TRY(cudaStreamSynchronize(p->own));
+    JSVD_CUBLAS_TRY(cublasCreate(&p->blas));
+    JSVD_CUBLAS_TRY(cublasSetWorkspace(p->blas, p->blas_ws, kPcBlasWorkspace));
+    JSVD_CUDA_TRY(cudaFuncSetAttribute(pc_chol_inv_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
+    plans.insert(plans.begin(), std::move(p));
+    while (plans.size() > kPcMaxPlans) plans.pop_back();
+    *out = plans.front().get();
+    return JSVD_OK;
+}
+
 int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config &c, double *d_u, double *d_sigma,
                  double *d_v, int *sweeps, cudaStream_t st)
 {
     const int m = (int)rows, n = (int)cols;
     int dev = 0;
     JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    cublasHandle_t hb = nullptr;
-    int rc = thread_cublas(dev, st, &hb);
-    if (rc != JSVD_OK) return rc;
     const size_t mn = (size_t)m * n, nn = (size_t)n * n;
     // workspace: Qa, Qb (m x n) | G | Lm | R1 | R2 | R3 | T | Vx | Ux | Sa | Sb | P1 (n x n)
     //            | Linv (blocks x 64 x 64) | sigma | status
     const int nblk = (n + kNb - 1) / kNb;
-    double *ws = nullptr;
     const size_t ws_doubles = 2 * mn + 11 * nn + (size_t)nblk * kNb * kNb + n + 1;
-    JSVD_CUDA_TRY(cudaMallocAsync((void **)&ws, sizeof(double) * ws_doubles, st));
+    PcPlan *plan = nullptr;
+    int rc = acquire_pc_plan(dev, rows, cols, ws_doubles, &plan);
+    if (rc != JSVD_OK) return rc;
+    cublasHandle_t hb = nullptr;
+    if (plan) {
+        hb = plan->blas;
+        JSVD_CUBLAS_TRY(cublasSetStream(hb, st));
+    } else {
+        rc = thread_cublas(dev, st, &hb);
+        if (rc != JSVD_OK) return rc;
+    }
+    double *ws = plan ? plan->ws : nullptr;
+    if (!plan) JSVD_CUDA_TRY(cudaMallocAsync((void **)&ws, sizeof(double) * ws_doubles, st));
     double *Qa = ws, *Qb = Qa + mn, *G = Qb + mn, *Lm = G + nn, *R1 = Lm + nn, *R2 = R1 + nn, *R3 = R2 + nn,
            *Tm = R3 + nn, *Vx = Tm + nn, *Ux = Vx + nn, *Sa = Ux + nn, *Sb = Sa + nn, *P1 = Sb + nn,
            *Linv = P1 + nn, *sg = Linv + (size_t)nblk * kNb * kNb;
@@ -358,7 +445,7 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     cudaEventCreate(&e2);
     cudaEventCreate(&e3);
     auto cleanup = [&]() {
-        cudaFreeAsync(ws, st);
+        if (!plan) cudaFreeAsync(ws, st);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaEventDestroy(e2);
@@ -368,14 +455,43 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     // Shifted CholeskyQR3 of Xa (rows x n, column-major, overwritten): the
     // orthonormal factor ends in Xb, R = R3 R2 R1 in Ra (upper, column-major);
     // Rb, Rc are scratch.
-    auto scqr3 = [&](double *Xa, double *Xb, int rows, double *Ra, double *Rb, double *Rc) -> int {
-        int r = chol_qr_pass(hb, st, Xa, Xb, rows, n, G, Lm, Linv, Ra, true, d_status);
-        if (r == JSVD_OK) r = chol_qr_pass(hb, st, Xb, Xa, rows, n, G, Lm, Linv, Rb, false, d_status);
-        if (r == JSVD_OK) r = chol_qr_pass(hb, st, Xa, Xb, rows, n, G, Lm, Linv, Rc, false, d_status);
+    auto scqr3 = [&](cudaStream_t s2, double *Xa, double *Xb, int rows, double *Ra, double *Rb, double *Rc) -> int {
+        int r = chol_qr_pass(hb, s2, Xa, Xb, rows, n, G, Lm, Linv, Ra, true, d_status);
+        if (r == JSVD_OK) r = chol_qr_pass(hb, s2, Xb, Xa, rows, n, G, Lm, Linv, Rb, false, d_status);
+        if (r == JSVD_OK) r = chol_qr_pass(hb, s2, Xa, Xb, rows, n, G, Lm, Linv, Rc, false, d_status);
         if (r != JSVD_OK) return r;
         JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Rb, n, Ra, n, &zero, Tm, n));
         JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Rc, n, Tm, n, &zero, Ra, n));
         return JSVD_OK;
+    };
+    // Runs a QR stage: directly, or (a plan on its second use onwards) as a
+    // graph captured once on the plan's own stream and replayed on st.
+    auto run_stage = [&](cudaGraphExec_t *exec, auto &&enqueue) -> int {
+        if (plan && !plan->no_graph && *exec == nullptr && plan->uses >= 1) {
+            JSVD_CUBLAS_TRY(cublasSetStream(hb, plan->own));
+            cudaGraph_t graph = nullptr;
+            int r = JSVD_OK;
+            cudaError_t ce = cudaStreamBeginCapture(plan->own, cudaStreamCaptureModeThreadLocal);
+            if (ce == cudaSuccess) {
+                r = enqueue(plan->own);
+                ce = cudaStreamEndCapture(plan->own, &graph);
+            }
+            if (r == JSVD_OK && ce == cudaSuccess && graph != nullptr) {
+                if (cudaGraphInstantiate(exec, graph, 0) != cudaSuccess) *exec = nullptr;
+            }
+            if (graph) cudaGraphDestroy(graph);
+            if (*exec == nullptr) {
+                plan->no_graph = true;  // launch directly from now on
+                cudaGetLastError();
+                set_last_error(JSVD_OK, "");
+            }
+            JSVD_CUBLAS_TRY(cublasSetStream(hb, st));
+        }
+        if (plan && *exec != nullptr) {
+            JSVD_CUDA_TRY(cudaGraphLaunch(*exec, st));
+            return JSVD_OK;
+        }
+        return enqueue(st);
     };
     auto read_status = [&](int *out) -> int {
         JSVD_CUDA_TRY(cudaMemcpyAsync(out, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -388,7 +504,8 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
         d_a, m, n, Qa);
     JSVD_CUDA_TRY(cudaGetLastError());
     // A = Q R
-    rc = scqr3(Qa, Qb, m, R1, R2, R3);
+    rc = run_stage(plan ? &plan->qr1 : nullptr,
+                   [&](cudaStream_t s2) { return scqr3(s2, Qa, Qb, m, R1, R2, R3); });
     int status = 0;
     if (rc == JSVD_OK) rc = read_status(&status);
     if (rc != JSVD_OK) {
@@ -404,10 +521,12 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
         return jsvd_plain_svd_device(d_a, rows, cols, &c, d_u, d_sigma, d_v, sweeps, st);
     }
     // R^T = Q1 P (P upper): R1's column-major buffer read as row-major is R^T.
-    pc_to_colmajor<<<dim3((n + kTile - 1) / kTile, (n + kTile - 1) / kTile), dim3(kTile, kTileRows), 0, st>>>(
-        R1, n, n, Sa);
-    JSVD_CUDA_TRY(cudaGetLastError());
-    rc = scqr3(Sa, Sb, n, P1, R2, R3);
+    rc = run_stage(plan ? &plan->qr2 : nullptr, [&](cudaStream_t s2) -> int {
+        pc_to_colmajor<<<dim3((n + kTile - 1) / kTile, (n + kTile - 1) / kTile), dim3(kTile, kTileRows), 0, s2>>>(
+            R1, n, n, Sa);
+        JSVD_CUDA_TRY(cudaGetLastError());
+        return scqr3(s2, Sa, Sb, n, P1, R2, R3);
+    });
     int status2 = 0;
     if (rc == JSVD_OK) rc = read_status(&status2);
     if (rc != JSVD_OK) {
@@ -456,6 +575,7 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     ps.jacobi_ms += b;
     ps.u_ms += d;
     ps.last_sweeps = sweeps ? *sweeps : 0;
+    if (plan) plan->uses += 1;
     cleanup();
     return JSVD_OK;
 }
@@ -514,6 +634,10 @@ extern "C" int jsvd_precond_svd(const double *a, size_t rows, size_t columns, co
     JSVD_CUDA_TRY(cudaStreamSynchronize(st));
     return rc;
 }
+
+namespace jsvd {
+void pc_release_thread_plans() { pc_plans().clear(); }
+}  // namespace jsvd
 
 extern "C" void jsvd_precond_set_inner(int engine) { g_inner.store(engine == 0 ? 0 : 1); }
 

@@ -94,3 +94,15 @@ def test_precond_gram_stop_matches_full_sweeps(cuda_device, name, make, kappa):
     assert O.sigma_errors(gs, fs)["normwise"] <= 1e-15 * max(n, 100)
     r = O.residuals(a, gu, gs, gv)
     assert r["rho_A"] <= 1e-11 * n and r["rho_V"] <= 1e-12 * n and r["rho_U"] <= 1e-10 * n, r
+
+
+def test_precond_graph_replay_identical(cuda_device):
+    """The QR stage runs directly on a shape's first solve and from captured
+    graphs afterwards: the results are the same bytes."""
+    a = W.spectrum_matrix(1500, 400, W.geometric_sigma(400, 1e-6), 77)
+    cfg = jsvd.default_config(epsilon=1e-14)
+    runs = [jsvd.precond_svd(a, cfg) for _ in range(3)]
+    for r in runs[1:]:
+        assert r[3] == runs[0][3]
+        for x, y in zip(r[:3], runs[0][:3]):
+            assert np.array_equal(x, y)
