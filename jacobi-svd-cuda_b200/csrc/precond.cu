@@ -106,10 +106,11 @@ __global__ void __launch_bounds__(256) pc_shift_diagonal(double *__restrict__ G,
 // factor into Linv (column-major, ld = kNb).  The block is padded to kNb x kNb
 // with the identity.
 //
-// Blocked in panels of kPanel columns, so the block synchronises 2 * kNb /
-// kPanel times instead of once per column (a per-column form measured 57 us
-// per block on B200 under ncu, bound by its 64 barriers; the QR stage's event
-// time did not change with this form, its ~500 launches being enqueue-bound):
+// Blocked in panels of kPanel columns: the block synchronises 2 * kNb /
+// kPanel times and executes a quarter of the instructions of a per-column
+// form with one barrier per column; both measured about 60 us per block on
+// B200 (ncu), set by the serial chain of 64 pivots (square root and
+// reciprocal in FP64) that warp 0 walks while the other warps wait:
 //   factorisation: warp 0 factors the panel's columns (right-looking inside
 //     the panel, __syncwarp between columns; each lane owns two rows and reads
 //     the pivot column's panel entries before any of them is rescaled), then
