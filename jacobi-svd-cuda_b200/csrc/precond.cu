@@ -106,20 +106,20 @@ __global__ void __launch_bounds__(256) pc_shift_diagonal(double *__restrict__ G,
 // factor into Linv (column-major, ld = kNb).  The block is padded to kNb x kNb
 // with the identity.
 //
-// Blocked in panels of kPanel columns: the block synchronises 2 * kNb /
-// kPanel times and executes a quarter of the instructions of a per-column
-// form with one barrier per column; both measured about 60 us per block on
-// B200 (ncu), set by the serial chain of 64 pivots (square root and
-// reciprocal in FP64) that warp 0 walks while the other warps wait:
+// The factor is computed as G = L D L^T (L unit lower): each column costs one
+// reciprocal of its pivot on the serial chain, and the square roots are taken
+// afterwards, all at once (Cholesky factor L sqrt(D), inverse
+// D^{-1/2} L^{-1}, where L^{-1} needs no division).  Panels of kPanel columns:
 //   factorisation: warp 0 factors the panel's columns (right-looking inside
 //     the panel, __syncwarp between columns; each lane owns two rows and reads
-//     the pivot column's panel entries before any of them is rescaled), then
-//     all threads apply the panel's rank-kPanel update to the trailing
-//     triangle, a[i][k] -= sum_j L(i,j) L(k,j);
-//   inverse: block forward substitution of [L | I], kPanel rows at a time:
-//     thread c solves column c through the panel's triangular block (rows in
-//     order, by the stored reciprocal pivots), then all threads subtract the
-//     panel's contribution from the rows below.
+//     the pivot column's panel entries before they are rescaled), then all
+//     threads apply the panel's update to the trailing triangle,
+//     a[i][k] -= sum_j L(i,j) d_j L(k,j);
+//   inverse of L: block forward substitution of [L | I], kPanel rows at a
+//     time: thread c solves column c through the panel's unit triangle, then
+//     all threads subtract the panel's contribution from the rows below.
+// A form with a square root and a reciprocal per column measured about 60 us
+// per block on B200 (ncu), set by that serial chain of 64 pivots.
 // status <- 1 on a pivot that is not positive and finite.
 constexpr int kPanel = 8;
 constexpr int kDiagThreads = 256;
@@ -130,7 +130,9 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
                                                                  double *__restrict__ Linv, int *__restrict__ status)
 {
     extern __shared__ double dsm[];
-    __shared__ double dinv[kNb];  // 1 / L(i,i)
+    __shared__ double dvec[kNb];  // pivots d_i
+    __shared__ double sq[kNb];    // sqrt(d_i)
+    __shared__ double isq[kNb];   // 1 / sqrt(d_i)
     double(*a)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);
     double(*x)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm + kNb * (kNb + 1));
     const int t = threadIdx.x;
@@ -140,38 +142,34 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
         x[i][k] = (i == k) ? 1.0 : 0.0;
     }
     __syncthreads();
-    // ---- factorisation ----
+    // ---- G = L D L^T ----
     for (int c0 = 0; c0 < kNb; c0 += kPanel) {
         if (t < 32) {
             const int lane = t;
             for (int j = 0; j < kPanel; ++j) {
                 const int cj = c0 + j;
-                const double d = a[cj][cj];
-                const bool ok = d > 0.0 && d < INFINITY;
-                const double r = ok ? sqrt(d) : 1.0;
-                const double rinv = 1.0 / r;
+                const double d0 = a[cj][cj];
+                const bool ok = d0 > 0.0 && d0 < INFINITY;
+                const double d = ok ? d0 : 1.0;
+                const double rd = 1.0 / d;
                 if (lane == 0) {
                     if (!ok) atomicExch(status, 1);
-                    dinv[cj] = rinv;
+                    dvec[cj] = d;
                 }
-                double colk[kPanel];  // unscaled a[k][cj] of the panel rows below cj
+                double colk[kPanel];  // a[k][cj] = L(k,cj) d_cj of the panel rows below cj
 #pragma unroll
                 for (int kk = 0; kk < kPanel; ++kk) colk[kk] = (kk > j) ? a[c0 + kk][cj] : 0.0;
                 __syncwarp();
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const int i = c0 + lane + 32 * h;
-                    if (i >= kNb) continue;
-                    if (i == cj) {
-                        a[i][cj] = r;
-                    } else if (i > cj) {
-                        const double lij = a[i][cj] * rinv;
-                        a[i][cj] = lij;
+                    if (i >= kNb || i <= cj) continue;
+                    const double lij = a[i][cj] * rd;
+                    a[i][cj] = lij;
 #pragma unroll
-                        for (int kk = 0; kk < kPanel; ++kk) {
-                            const int k = c0 + kk;
-                            if (kk > j && k <= i) a[i][k] = fma(-lij, colk[kk] * rinv, a[i][k]);
-                        }
+                    for (int kk = 0; kk < kPanel; ++kk) {
+                        const int k = c0 + kk;
+                        if (kk > j && k <= i) a[i][k] = fma(-lij, colk[kk], a[i][k]);
                     }
                 }
                 __syncwarp();
@@ -184,12 +182,16 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
             if (k > i) continue;
             double acc = a[i][k];
 #pragma unroll
-            for (int jj = 0; jj < kPanel; ++jj) acc = fma(-a[i][c0 + jj], a[k][c0 + jj], acc);
+            for (int jj = 0; jj < kPanel; ++jj) acc = fma(-a[i][c0 + jj], a[k][c0 + jj] * dvec[c0 + jj], acc);
             a[i][k] = acc;
         }
         __syncthreads();
     }
-    // ---- inverse: forward substitution of [L | I] ----
+    if (t < kNb) {
+        sq[t] = sqrt(dvec[t]);
+        isq[t] = 1.0 / sq[t];
+    }
+    // ---- L^{-1}: forward substitution of [L | I] (unit diagonal) ----
     for (int r0 = 0; r0 < kNb; r0 += kPanel) {
         const int cols = r0 + kPanel;  // columns 0 .. cols-1 can be non-zero in these rows
         if (t < cols) {
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
                 double val = x[i][c];
 #pragma unroll
                 for (int rr = 0; rr < r; ++rr) val = fma(-a[i][r0 + rr], x[r0 + rr][c], val);
-                x[i][c] = val * dinv[i];
+                x[i][c] = val;
             }
         }
         __syncthreads();
@@ -214,13 +216,14 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
         }
         __syncthreads();
     }
+    // Cholesky factor L sqrt(D) and its inverse D^{-1/2} L^{-1}
     for (int e = t; e < kb * kb; e += kDiagThreads) {
         const int i = e % kb, k = e / kb;
-        if (i >= k) Lm[(size_t)(k0 + k) * n + k0 + i] = a[i][k];
+        if (i >= k) Lm[(size_t)(k0 + k) * n + k0 + i] = (i == k) ? sq[i] : a[i][k] * sq[k];
     }
     for (int e = t; e < kNb * kNb; e += kDiagThreads) {
         const int i = e % kNb, k = e / kNb;
-        Linv[i + (size_t)k * kNb] = (i < kb && k < kb && k <= i) ? x[i][k] : 0.0;
+        Linv[i + (size_t)k * kNb] = (i < kb && k < kb && k <= i) ? x[i][k] * isq[i] : 0.0;
     }
 }
 
