@@ -484,6 +484,7 @@ def run_batch(args, rank: int, world: int, device):
                    "epsilon": 1e-14, "mean_sweeps": float(np.mean(b.sweeps)),
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                    "generation_s": gen_s, "step_ms": step_ms,
+                   "launch_shapes": jsvd.batch_builtin_tuning(),
                    "classes": {"count": [int(x) for x in st.class_count],
                                "ms_per_step": [x / max(1, st.calls) for x in st.class_ms]}},
         "e2e": {"value": replica_rate(args.steps * b.count, world, e2e_s), "unit": "SVD/s",

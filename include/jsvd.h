@@ -157,12 +157,18 @@ void jsvd_plain_stats_reset(void);
  * the plain path's (T = 256 reduction order), so each result is bit-identical
  * to jsvd_plain_svd on the FP64-promoted input. */
 
-/* Launch shape of one size class: 0 keeps the built-in choice. */
+/* Launch shape of one size class.  An entry of three zeros keeps the
+ * built-in shape of its class; otherwise threads or ctas_per_sm 0 keeps that
+ * built-in value and max_ctas 0 means no cap. */
 typedef struct jsvd_batch_tuning {
     int threads;     /* threads per CTA (multiple of 32, <= 512) */
     int ctas_per_sm; /* persistent CTAs per SM */
     int max_ctas;    /* upper bound on the class's grid (bounds the L2 working set of the global classes) */
 } jsvd_batch_tuning;
+
+/* The built-in shapes (5 entries), compiled in from the table that
+ * jsvd_batch_autotune's generator writes.  No CUDA call. */
+void jsvd_batch_builtin_tuning(jsvd_batch_tuning *out);
 
 /*
  * count matrices; matrix i is rows[i] x cols[i] (rows >= cols >= 1), row-major
@@ -180,6 +186,34 @@ typedef struct jsvd_batch_tuning {
 int jsvd_batch_svd_device(int count, const int *rows, const int *cols, const long long *a_offsets, const void *d_a,
                           int a_is_f32, const jsvd_config *cfg, double *d_sigma, double *d_v, double *d_u,
                           int *sweeps, const jsvd_batch_tuning *tuning, void *stream);
+
+/* Result of jsvd_batch_autotune, per size class. */
+typedef struct jsvd_batch_autotune_report {
+    jsvd_batch_tuning best[5];    /* chosen shape (the built-in one unless another is > 2% faster) */
+    jsvd_batch_tuning builtin[5]; /* the built-in shape */
+    double best_ms[5];            /* device ms of the class's sample under best (min over reps) */
+    double builtin_ms[5];         /* the same under the built-in shape */
+    int members[5];               /* matrices of the batch in the class */
+    int sampled[5];               /* matrices timed */
+    int candidates[5];            /* shapes timed, the built-in one included */
+} jsvd_batch_autotune_report;
+
+/*
+ * Launch-shape autotuner of the batched solver.  Takes the same batch
+ * description as jsvd_batch_svd_device (the outputs go to buffers of its own)
+ * and, for every size class with members, times the built-in shape and each
+ * candidate shape (threads 128/256/512 x CTAs per SM as shared memory allows;
+ * for the classes that take a whole SM, threads x grid cap none/0.75/0.5 of the
+ * SMs) on up to `sample` of the class's matrices (0 = all; evenly spaced over
+ * the work order), L2 flushed before each of `reps` runs (0 = 2), minimum kept.
+ * Every shape must give the same sigma bytes and sweep counts as the built-in
+ * one, else JSVD_ERR_RUNTIME.  want_u / want_v: compute U / V as the timed
+ * workload does.  Synchronous on `stream` (NULL = library stream).  The
+ * batch statistics are left as they were.
+ */
+int jsvd_batch_autotune(int count, const int *rows, const int *cols, const long long *a_offsets, const void *d_a,
+                        int a_is_f32, const jsvd_config *cfg, int sample, int reps, int want_u, int want_v,
+                        jsvd_batch_autotune_report *report, void *stream);
 
 /*
  * One-sided block-pair Jacobi on device buffers (same arguments and outputs as

@@ -25,6 +25,7 @@
 #include <numeric>
 #include <vector>
 
+#include "batch_tuning_table.h"
 #include "batched.hpp"
 #include "common.cuh"
 #include "internal.hpp"
@@ -296,6 +297,55 @@ int thread_events(int dev, ThreadEvents **out)
     return JSVD_OK;
 }
 
+constexpr jsvd_batch_tuning kBuiltinTuning[kClasses] = JSVD_BATCH_TUNING_TABLE;
+
+// Where each class keeps its working copies (see the file comment).
+constexpr bool class_a_shared(int c) { return c <= 3; }
+constexpr bool class_v_shared(int c) { return c <= 2; }
+
+// Largest dynamic shared memory a batch CTA asks for: the opt-in limit less
+// 1 KiB for the static variables.
+int batch_smem_cap(int dev, size_t *cap)
+{
+    int smem_optin = 0;
+    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    *cap = (size_t)std::min(smem_optin, 227 * 1024) - 1024;
+    return JSVD_OK;
+}
+
+// Size class of an m x n member and the shared-memory bytes it needs there.
+int member_class(int m, int n, size_t smem_cap, size_t *smem_need)
+{
+    const size_t scratch = sizeof(double) * round_scratch_doubles(n);
+    const size_t a_bytes = sizeof(double) * (size_t)m * n, v_bytes = sizeof(double) * (size_t)n * n;
+    int c;
+    if (scratch + a_bytes + v_bytes <= 48 * 1024) c = 0;
+    else if (scratch + a_bytes + v_bytes <= 100 * 1024) c = 1;
+    else if (scratch + a_bytes + v_bytes <= smem_cap) c = 2;
+    else if (scratch + a_bytes <= smem_cap) c = 3;
+    else c = 4;
+    if (smem_need)
+        *smem_need = scratch + (class_a_shared(c) ? a_bytes : 0) + (class_v_shared(c) ? v_bytes : 0);
+    return c;
+}
+
+// Work of one member per sweep, ~ n^2 (m + n): the queue order inside a class.
+double member_work(int m, int n) { return (double)n * n * (m + n); }
+
+// Argument checks shared by the solver and the autotuner.
+int check_batch_args(int count, const int *rows, const int *cols, const long long *a_offsets, const void *d_a,
+                     bool sigma_missing, const jsvd_config &c)
+{
+    if (count < 0) return invalid_argument("count must be non-negative.");
+    if (count > 0 && (rows == nullptr || cols == nullptr || a_offsets == nullptr || d_a == nullptr || sigma_missing))
+        return invalid_argument("Batch buffers must not be null.");
+    if (!(c.epsilon > 0.0)) return invalid_argument("epsilon must be positive.");
+    if (c.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
+    if (reduction_lanes(c.threads_per_block) != 256)
+        return invalid_argument("The batched solver reduces with threads_per_block = 256.");
+    return JSVD_OK;
+}
+
 }  // namespace
 
 BatchStats &batch_stats()
@@ -310,29 +360,31 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     if (count <= 0) return JSVD_OK;
     int dev = 0;
     JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    int sms = 0, smem_optin = 0;
+    int sms = 0;
     JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const size_t smem_cap = (size_t)std::min(smem_optin, 227 * 1024) - 1024;
+    size_t smem_cap = 0;
+    int rc = batch_smem_cap(dev, &smem_cap);
+    if (rc != JSVD_OK) return rc;
     ThreadEvents *ts = nullptr;
-    int rc = thread_events(dev, &ts);
+    rc = thread_events(dev, &ts);
     if (rc != JSVD_OK) return rc;
 
     struct Class {
-        size_t limit;  // max shared-memory bytes of a member
         int threads;
         int ctas_per_sm;
         bool a_shared, v_shared;
         BatchFn fn;
     };
-    Class classes[kClasses] = {
-        {48 * 1024, 256, 4, true, true, batch_kernel<true, true>},
-        {100 * 1024, 256, 2, true, true, batch_kernel<true, true>},
-        {smem_cap, 512, 1, true, true, batch_kernel<true, true>},
-        {smem_cap, 512, 1, true, false, batch_kernel<true, false>},
-        {(size_t)-1, 512, 1, false, false, batch_kernel<false, false>},
-    };
+    Class classes[kClasses];
     int max_ctas[kClasses] = {};
+    for (int c = 0; c < kClasses; ++c) {
+        classes[c].threads = kBuiltinTuning[c].threads;
+        classes[c].ctas_per_sm = kBuiltinTuning[c].ctas_per_sm;
+        classes[c].a_shared = class_a_shared(c);
+        classes[c].v_shared = class_v_shared(c);
+        classes[c].fn = c <= 2 ? batch_kernel<true, true> : (c == 3 ? batch_kernel<true, false> : batch_kernel<false, false>);
+        max_ctas[c] = kBuiltinTuning[c].max_ctas;
+    }
     if (req.tuning != nullptr) {
         for (int c = 0; c < kClasses; ++c) {
             const jsvd_batch_tuning &t = req.tuning[c];
@@ -340,7 +392,7 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
                 return invalid_argument("Batch tuning: threads must be a multiple of 32 up to 512, counts >= 0.");
             if (t.threads > 0) classes[c].threads = t.threads;
             if (t.ctas_per_sm > 0) classes[c].ctas_per_sm = t.ctas_per_sm;
-            max_ctas[c] = t.max_ctas;
+            if (t.threads > 0 || t.ctas_per_sm > 0 || t.max_ctas > 0) max_ctas[c] = t.max_ctas;
         }
     }
     std::vector<std::vector<int>> members(kClasses);
@@ -361,20 +413,10 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         v_off += (size_t)d.n * d.n;
         u_off += (size_t)d.m * d.n;
         all[i] = d;
-        const size_t scratch = sizeof(double) * round_scratch_doubles(d.n);
-        const size_t a_bytes = sizeof(double) * (size_t)d.m * d.n, v_bytes = sizeof(double) * (size_t)d.n * d.n;
-        int c;
-        if (scratch + a_bytes + v_bytes <= classes[0].limit) c = 0;
-        else if (scratch + a_bytes + v_bytes <= classes[1].limit) c = 1;
-        else if (scratch + a_bytes + v_bytes <= classes[2].limit) c = 2;
-        else if (scratch + a_bytes <= classes[3].limit) c = 3;
-        else c = 4;
-        need_smem[i] = scratch + (classes[c].a_shared ? a_bytes : 0) + (classes[c].v_shared ? v_bytes : 0);
-        members[c].push_back(i);
+        members[member_class(d.m, d.n, smem_cap, &need_smem[i])].push_back(i);
     }
-    // Largest work first inside each class (tail balance of the work queue):
-    // work ~ n^2 (m + n) per sweep.
-    auto work = [&](int i) { return (double)all[i].n * all[i].n * (all[i].m + all[i].n); };
+    // Largest work first inside each class (tail balance of the work queue).
+    auto work = [&](int i) { return member_work(all[i].m, all[i].n); };
     std::vector<BatchDesc> ordered;
     ordered.reserve(count);
     std::vector<int> first(kClasses + 1, 0), order_index;
@@ -481,14 +523,8 @@ extern "C" int jsvd_batch_svd_device(int count, const int *rows, const int *cols
     jsvd_config def;
     jsvd_config_default(&def);
     const jsvd_config &c = cfg ? *cfg : def;
-    if (count < 0) return invalid_argument("count must be non-negative.");
-    if (count > 0 && (rows == nullptr || cols == nullptr || a_offsets == nullptr || d_a == nullptr ||
-                      d_sigma == nullptr))
-        return invalid_argument("Batch buffers must not be null.");
-    if (!(c.epsilon > 0.0)) return invalid_argument("epsilon must be positive.");
-    if (c.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
-    if (reduction_lanes(c.threads_per_block) != 256)
-        return invalid_argument("The batched solver reduces with threads_per_block = 256.");
+    const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, d_sigma == nullptr, c);
+    if (bad != JSVD_OK) return bad;
     int dev = 0;
     JSVD_CUDA_TRY(cudaGetDevice(&dev));
     cudaStream_t st = (cudaStream_t)stream;
@@ -530,3 +566,201 @@ extern "C" void jsvd_batch_stats_get(jsvd_batch_stats *out)
 }
 
 extern "C" void jsvd_batch_stats_reset(void) { batch_stats() = BatchStats{}; }
+
+extern "C" void jsvd_batch_builtin_tuning(jsvd_batch_tuning *out)
+{
+    if (!out) return;
+    for (int c = 0; c < kClasses; ++c) out[c] = kBuiltinTuning[c];
+}
+
+namespace jsvd {
+namespace {
+
+// Candidate launch shapes of class c whose largest sampled member needs
+// smem_need bytes of shared memory.  Classes 0-2: threads x persistent CTAs
+// per SM, as many CTAs as the SM's shared memory and 2048 threads allow.
+// Classes 3-4 take a whole SM's shared memory per CTA: threads x grid cap
+// (the cap bounds the per-CTA global-memory slices that compete for L2).
+std::vector<jsvd_batch_tuning> batch_candidates(int c, size_t smem_need, int sms, size_t smem_per_sm)
+{
+    std::vector<jsvd_batch_tuning> out;
+    for (int t : {128, 256, 512}) {
+        if (c <= 2) {
+            for (int k : {1, 2, 4, 8})
+                if (t * k <= 2048 && (size_t)k * (smem_need + 1024) <= smem_per_sm) out.push_back({t, k, 0});
+        } else {
+            for (int cap : {0, (3 * sms) / 4, sms / 2}) out.push_back({t, 1, cap});
+        }
+    }
+    return out;
+}
+
+bool same_shape(const jsvd_batch_tuning &x, const jsvd_batch_tuning &y)
+{
+    return x.threads == y.threads && x.ctas_per_sm == y.ctas_per_sm && x.max_ctas == y.max_ctas;
+}
+
+}  // namespace
+}  // namespace jsvd
+
+extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, const long long *a_offsets,
+                                   const void *d_a, int a_is_f32, const jsvd_config *cfg, int sample, int reps,
+                                   int want_u, int want_v, jsvd_batch_autotune_report *report, void *stream)
+{
+    set_last_error(JSVD_OK, "");
+    jsvd_config def;
+    jsvd_config_default(&def);
+    const jsvd_config &c = cfg ? *cfg : def;
+    if (report == nullptr) return invalid_argument("Autotune report must not be null.");
+    const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, false, c);
+    if (bad != JSVD_OK) return bad;
+    *report = jsvd_batch_autotune_report{};
+    for (int k = 0; k < kClasses; ++k) report->builtin[k] = kBuiltinTuning[k];
+    if (count == 0) return JSVD_OK;
+    if (reps <= 0) reps = 2;
+    int dev = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    cudaStream_t st = (cudaStream_t)stream;
+    if (st == nullptr) {
+        st = thread_stream(dev);
+        if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+        JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+    }
+    int sms = 0, smem_per_sm = 0;
+    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    size_t smem_cap = 0;
+    int rc = batch_smem_cap(dev, &smem_cap);
+    if (rc != JSVD_OK) return rc;
+
+    std::vector<std::vector<int>> members(kClasses);
+    for (int i = 0; i < count; ++i) {
+        if (rows[i] <= 0 || cols[i] <= 0 || rows[i] < cols[i])
+            return invalid_argument("Batch matrix shape must satisfy rows >= columns > 0.");
+        members[member_class(rows[i], cols[i], smem_cap, nullptr)].push_back(i);
+    }
+
+    // Flush buffer (larger than L2) and output buffers sized for the largest sample.
+    const size_t flush_bytes = (size_t)256 << 20;
+    std::vector<std::vector<int>> picked(kClasses);
+    size_t max_s = 0, max_v = 0, max_u = 0;
+    for (int k = 0; k < kClasses; ++k) {
+        auto &mem = members[k];
+        std::sort(mem.begin(), mem.end(),
+                  [&](int x, int y) { return member_work(rows[x], cols[x]) > member_work(rows[y], cols[y]); });
+        const size_t cnt = mem.size();
+        const size_t s = (sample > 0 && (size_t)sample < cnt) ? (size_t)sample : cnt;
+        size_t ns = 0, nv = 0, nu = 0;
+        for (size_t j = 0; j < s; ++j) {  // evenly spaced over the work order
+            const int i = mem[j * cnt / s];
+            picked[k].push_back(i);
+            ns += (size_t)cols[i];
+            nv += (size_t)cols[i] * cols[i];
+            nu += (size_t)rows[i] * cols[i];
+        }
+        max_s = std::max(max_s, ns);
+        max_v = std::max(max_v, nv);
+        max_u = std::max(max_u, nu);
+        report->members[k] = (int)cnt;
+        report->sampled[k] = (int)s;
+    }
+    void *d_flush = nullptr;
+    double *d_sigma = nullptr, *d_v = nullptr, *d_u = nullptr;
+    auto release = [&]() {
+        if (d_flush) cudaFreeAsync(d_flush, st);
+        if (d_sigma) cudaFreeAsync(d_sigma, st);
+        if (d_v) cudaFreeAsync(d_v, st);
+        if (d_u) cudaFreeAsync(d_u, st);
+        cudaStreamSynchronize(st);
+    };
+    // The autotuner's own solves are not counted in the batch statistics.
+    const BatchStats saved = batch_stats();
+    auto finish = [&](int code) {
+        release();
+        batch_stats() = saved;
+        return code;
+    };
+    if (cudaMallocAsync(&d_flush, flush_bytes, st) != cudaSuccess ||
+        cudaMallocAsync((void **)&d_sigma, sizeof(double) * std::max<size_t>(max_s, 1), st) != cudaSuccess ||
+        (want_v && cudaMallocAsync((void **)&d_v, sizeof(double) * std::max<size_t>(max_v, 1), st) != cudaSuccess) ||
+        (want_u && cudaMallocAsync((void **)&d_u, sizeof(double) * std::max<size_t>(max_u, 1), st) != cudaSuccess))
+        return finish(cuda_failure(cudaGetLastError(), "cudaMallocAsync", __FILE__, __LINE__));
+
+    for (int k = 0; k < kClasses; ++k) {
+        const auto &pk = picked[k];
+        if (pk.empty()) continue;
+        const int s = (int)pk.size();
+        std::vector<int> r_s(s), c_s(s), sw(s), sw_ref(s);
+        std::vector<long long> off_s(s);
+        size_t need = 0, nsig = 0;
+        for (int j = 0; j < s; ++j) {
+            r_s[j] = rows[pk[j]];
+            c_s[j] = cols[pk[j]];
+            off_s[j] = a_offsets[pk[j]];
+            size_t nj = 0;
+            member_class(r_s[j], c_s[j], smem_cap, &nj);
+            need = std::max(need, nj);
+            nsig += (size_t)c_s[j];
+        }
+        std::vector<double> sig(nsig), sig_ref(nsig);
+        // the built-in shape first: it is the yardstick and the bitwise reference
+        std::vector<jsvd_batch_tuning> cands{kBuiltinTuning[k]};
+        for (const auto &t : batch_candidates(k, need, sms, (size_t)smem_per_sm))
+            if (!same_shape(t, kBuiltinTuning[k])) cands.push_back(t);
+        report->candidates[k] = (int)cands.size();
+        double best_ms = -1.0;
+        jsvd_batch_tuning best = kBuiltinTuning[k];
+        for (size_t ci = 0; ci < cands.size(); ++ci) {
+            jsvd_batch_tuning tun[kClasses] = {};
+            tun[k] = cands[ci];
+            BatchRequest req;
+            req.count = s;
+            req.rows = r_s.data();
+            req.cols = c_s.data();
+            req.a_offsets = off_s.data();
+            req.a = d_a;
+            req.a_is_f32 = a_is_f32;
+            req.eps = c.epsilon;
+            req.max_sweeps = c.max_sweeps;
+            req.sigma = d_sigma;
+            req.v = d_v;
+            req.u = d_u;
+            req.sweeps = sw.data();
+            req.tuning = tun;
+            double ms = -1.0;
+            for (int r = 0; r < reps; ++r) {
+                if (cudaMemsetAsync(d_flush, r & 0xff, flush_bytes, st) != cudaSuccess)
+                    return finish(cuda_failure(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
+                const double before = batch_stats().class_ms[k];
+                rc = batch_solve(req, st);
+                if (rc != JSVD_OK) return finish(rc);
+                const double t = batch_stats().class_ms[k] - before;
+                ms = ms < 0.0 ? t : std::min(ms, t);
+            }
+            if (cudaMemcpyAsync(sig.data(), d_sigma, sizeof(double) * nsig, cudaMemcpyDeviceToHost, st) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                return finish(cuda_failure(cudaGetLastError(), "cudaMemcpyAsync", __FILE__, __LINE__));
+            if (ci == 0) {
+                sig_ref = sig;
+                sw_ref = sw;
+                report->builtin_ms[k] = ms;
+            } else if (std::memcmp(sig.data(), sig_ref.data(), sizeof(double) * nsig) != 0 || sw != sw_ref) {
+                set_last_error(JSVD_ERR_RUNTIME, "Batch launch shapes disagree on sigma or sweep counts.");
+                return finish(JSVD_ERR_RUNTIME);
+            }
+            if (best_ms < 0.0 || ms < best_ms) {
+                best_ms = ms;
+                best = cands[ci];
+            }
+        }
+        // a shape replaces the built-in one only when it is more than 2% faster
+        if (best_ms > 0.98 * report->builtin_ms[k]) {
+            best = kBuiltinTuning[k];
+            best_ms = report->builtin_ms[k];
+        }
+        report->best[k] = best;
+        report->best_ms[k] = best_ms;
+    }
+    return finish(JSVD_OK);
+}

@@ -76,6 +76,18 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("max_ctas", ctypes.c_int)]
 
 
+class BatchAutotuneReport(ctypes.Structure):
+    _fields_ = [
+        ("best", BatchTuning * 5),
+        ("builtin", BatchTuning * 5),
+        ("best_ms", ctypes.c_double * 5),
+        ("builtin_ms", ctypes.c_double * 5),
+        ("members", ctypes.c_int * 5),
+        ("sampled", ctypes.c_int * 5),
+        ("candidates", ctypes.c_int * 5),
+    ]
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [
         ("calls", ctypes.c_ulonglong),
@@ -153,7 +165,7 @@ def exported_symbols() -> list[str]:
         "jsvd_blocked_svd", "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset", "jsvd_plain_set_sweep_mode",
         "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
-        "jsvd_precond_set_gram_stop",
+        "jsvd_precond_set_gram_stop", "jsvd_batch_builtin_tuning", "jsvd_batch_autotune",
     ]
 
 
@@ -183,6 +195,11 @@ def lib() -> ctypes.CDLL:
         L.jsvd_batch_svd_device.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), P, P, P, P,
                                             ctypes.POINTER(BatchTuning), P]
         L.jsvd_batch_svd_device.restype = I
+        L.jsvd_batch_builtin_tuning.argtypes = [ctypes.POINTER(BatchTuning)]
+        L.jsvd_batch_builtin_tuning.restype = None
+        L.jsvd_batch_autotune.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), I, I, I, I,
+                                          ctypes.POINTER(BatchAutotuneReport), P]
+        L.jsvd_batch_autotune.restype = I
         L.jsvd_batch_stats_get.argtypes = [ctypes.POINTER(BatchStats)]
         L.jsvd_batch_stats_get.restype = None
         L.jsvd_batch_stats_reset.restype = None
@@ -446,6 +463,19 @@ class DeviceBatch:
             self.u.data_ptr() if self.u is not None else None, self.sweeps.ctypes.data, tun, stream or None)
         check(rc)
 
+    def autotune(self, cfg: Config | None = None, sample: int = 0, reps: int = 2,
+                 stream: int = 0) -> BatchAutotuneReport:
+        """jsvd_batch_autotune on this batch (computing U and V as this batch
+        was set up to)."""
+        cfg = cfg or default_config()
+        rep = BatchAutotuneReport()
+        rc = lib().jsvd_batch_autotune(
+            self.count, self.rows.ctypes.data, self.cols.ctypes.data, self.a_off.ctypes.data, self.a.data_ptr(),
+            1 if self.f32 else 0, ctypes.byref(cfg), sample, reps, 1 if self.u is not None else 0,
+            1 if self.v is not None else 0, ctypes.byref(rep), stream or None)
+        check(rc)
+        return rep
+
     def results(self):
         s = self.sigma.cpu().numpy()
         v = self.v.cpu().numpy() if self.v is not None else None
@@ -458,6 +488,14 @@ class DeviceBatch:
             uk = u[self.a_off[k]: self.a_off[k] + m * n].reshape(m, n) if u is not None else None
             out.append((uk, sk, vk, int(self.sweeps[k])))
         return out
+
+
+def batch_builtin_tuning() -> list[tuple[int, int, int]]:
+    """The batched solver's compiled-in launch shapes, (threads, ctas_per_sm,
+    max_ctas) per size class."""
+    out = (BatchTuning * 5)()
+    lib().jsvd_batch_builtin_tuning(out)
+    return [(t.threads, t.ctas_per_sm, t.max_ctas) for t in out]
 
 
 def probe_fp64_tflops() -> float:

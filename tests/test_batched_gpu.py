@@ -67,3 +67,40 @@ def test_batch_tuning_and_empty(cuda_device):
     empty = jsvd.DeviceBatch([np.zeros((3, 2))], cuda_device)
     empty.count = 0
     empty.solve()
+
+
+# two matrices per shape; the shapes fall in all five size classes
+AUTOTUNE_SHAPES = [(16, 8), (40, 33), (31, 1), (64, 63), (60, 50), (100, 90), (120, 100), (160, 120),
+                   (170, 110), (256, 200), (200, 150)]
+
+
+def test_batch_autotune(cuda_device):
+    """The autotuner times every class, leaves the batch statistics alone,
+    and its chosen shapes give the same bytes as the built-in ones."""
+    rng = np.random.default_rng(21)
+    mats = [rng.standard_normal(s) for s in AUTOTUNE_SHAPES for _ in range(2)]
+    b = jsvd.DeviceBatch(mats, cuda_device, want_u=True)
+    cfg = jsvd.default_config(epsilon=1e-13)
+    b.solve(cfg)
+    ref = b.results()
+    before = jsvd.batch_stats()
+    rep = b.autotune(cfg, sample=0, reps=1)
+    after = jsvd.batch_stats()
+    assert after.calls == before.calls and after.kernel_ms == before.kernel_ms
+    assert sum(rep.members) == len(mats) and all(x > 0 for x in rep.members)
+    builtin = jsvd.batch_builtin_tuning()
+    for c in range(5):
+        assert rep.sampled[c] == rep.members[c]
+        assert rep.candidates[c] >= 2
+        assert (rep.builtin[c].threads, rep.builtin[c].ctas_per_sm, rep.builtin[c].max_ctas) == builtin[c]
+        assert 0.0 < rep.best_ms[c] <= rep.builtin_ms[c]
+        t = rep.best[c]
+        assert t.threads in (128, 256, 512) and t.ctas_per_sm >= 1 and t.max_ctas >= 0
+    best = [(t.threads, t.ctas_per_sm, t.max_ctas) for t in rep.best]
+    b.solve(cfg, tuning=best)
+    for x, y in zip(b.results(), ref):
+        assert x[3] == y[3]
+        for p, q in zip(x[:3], y[:3]):
+            assert np.array_equal(p, q)
+    one = b.autotune(cfg, sample=1, reps=1)
+    assert list(one.sampled) == [1] * 5
