@@ -1,12 +1,18 @@
 /* Built-in launch shapes of the batched solver, one entry per size class:
  * {threads per CTA, persistent CTAs per SM, grid cap (0 = none)}.
- * Classes: A and V in <= 48 KiB / <= 100 KiB / <= ~226 KiB of shared memory;
- * A alone in shared memory; A and V in global memory.
  *
- * Source: hand-picked from launch-shape sweeps of the 20,000-matrix mixed
- * batch (m ~ U{16..256}, n ~ U{8..m}, FP32-stored, seed 3) on one B200.
- * jacobi-svd-cuda_b200/batch_autotune.py regenerates this file from
- * jsvd_batch_autotune on the device it runs on. */
+ * Generated by jacobi-svd-cuda_b200/batch_autotune.py on NVIDIA B200
+ * (148 SMs), 2026-12-03, from jsvd_batch_autotune over 4000 FP32-stored matrices m ~ U{16..256}, n ~ U{8..m} (seed 3);
+ * 2 runs per shape, L2 flushed before each, minimum kept.  A shape
+ * replaces the previous built-in one only when it is more than 2% faster.
+ *
+ * class: members timed / in batch, shapes tried, ms previous -> chosen
+ *   0 (A and V in <= 48 KiB of shared memory): 1535 / 1535, 9 shapes, 6.40 -> 6.40
+ *   1 (A and V in <= 100 KiB of shared memory): 630 / 630, 6 shapes, 12.43 -> 12.43
+ *   2 (A and V in <= ~226 KiB of shared memory): 844 / 844, 3 shapes, 46.86 -> 46.86
+ *   3 (A in shared memory, V in global memory): 485 / 485, 9 shapes, 76.49 -> 76.49
+ *   4 (A and V in global memory): 506 / 506, 9 shapes, 240.89 -> 240.89
+ */
 #pragma once
 
 #define JSVD_BATCH_TUNING_TABLE \
