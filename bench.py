@@ -204,6 +204,18 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
                               jsvd.blockpair_stats()), ds.cpu().numpy(), (du, dv)
 
 
+def nominal_rate(m: int, n: int, plain_sweeps: int | None, svd_per_s: float | None) -> dict | None:
+    """Nominal FP64 rate of a path: F_nom = S_plain * P * (12 m + 6 n) flops
+    per SVD, P = n(n-1)/2 and S_plain the plain path's sweep count on the same
+    input, times the path's SVDs/s, so that paths with fewer or cheaper sweeps
+    are compared on the plain path's work."""
+    if not plain_sweeps or svd_per_s is None:
+        return None
+    f_nom = float(plain_sweeps) * n * (n - 1) / 2.0 * (12.0 * m + 6.0 * n)
+    return {"gflop_per_svd": f_nom / 1e9, "gflops": f_nom * svd_per_s / 1e9, "plain_sweeps": int(plain_sweeps),
+            "model": "S_plain * n(n-1)/2 * (12m + 6n) per SVD"}
+
+
 def blocked_sweep_flops(rows: int, n: int, b: int = 32) -> float:
     """FP64 flops of one blocked sweep: for every block pair, the panel Gram
     (2 rows w^2) and the panel update of X and V (2 (rows + n) w^2), w = 2b."""
@@ -358,6 +370,8 @@ def run_ours(args, rank: int, world: int, device):
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
                    "phases_ms": phases},
         "plain_path": plain,
+        "nominal": nominal_rate(m, n, plain["sweeps_per_svd"] if plain else (
+            sweeps[0] if path == "plain" and sweeps else PLAIN_SWEEPS.get(wl["name"])), value),
         "e2e": {"value": e2e_value, "unit": "SVD/s", "h2d_bytes_per_step": a.nbytes,
                 "d2h_bytes_per_step": (m * n + n + n * n) * 8, "timer": "host wall clock around the synchronous call"},
         "gpu_launches": launches,

@@ -71,3 +71,19 @@ def test_reference_arm_json_line():
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "SVD/s"
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_nominal_rate_model():
+    """F_nom = S_plain * n(n-1)/2 * (12m + 6n) per SVD; the batch's nominal
+    flops use the same per-matrix model."""
+    import numpy as np
+
+    r = bench.nominal_rate(512, 512, 14, 50.0)
+    f = 14 * 512 * 511 / 2 * (12 * 512 + 6 * 512)
+    assert r["gflop_per_svd"] == pytest.approx(f / 1e9)
+    assert r["gflops"] == pytest.approx(50.0 * f / 1e9)
+    assert r["plain_sweeps"] == 14
+    assert bench.nominal_rate(512, 512, None, 50.0) is None
+    assert bench.nominal_rate(512, 512, 14, None) is None
+    one = bench.batch_flops(np.array([512]), np.array([512]), np.array([14]))
+    assert one == pytest.approx(f)
