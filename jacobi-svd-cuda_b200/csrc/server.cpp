@@ -68,6 +68,7 @@ struct Request {
     size_t footprint = 0;
     Clock::time_point t_submit, t_done;
     bool done = false;
+    bool claimed = false;  // a wait() has taken this ticket
 };
 
 // Pinned host staging that grows and is reused by one worker.
@@ -149,9 +150,14 @@ public:
         {
             std::unique_lock<std::mutex> lk(mu_);
             auto it = requests_.find(ticket);
-            if (it == requests_.end()) return invalid_argument("Unknown or already collected ticket.");
+            if (it == requests_.end() || it->second->claimed)
+                return invalid_argument("Unknown or already collected ticket.");
             Request *raw = it->second.get();
+            raw->claimed = true;
+            // The wait releases the lock: a submit() may rehash the map, so the
+            // iterator is looked up again afterwards (the element itself stays put).
             cv_done_.wait(lk, [&] { return raw->done; });
+            it = requests_.find(ticket);
             r = std::move(it->second);
             requests_.erase(it);
         }

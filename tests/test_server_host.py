@@ -1,0 +1,127 @@
+"""Serving-core bookkeeping on the host: tickets, waits, budget admission and
+counters (jsvd_server_*).
+
+These run with or without a GPU.  Without one every request ends with a CUDA
+error status; with one they succeed.  Either way each ticket is collected
+exactly once, a second wait on it is rejected, and submitted = completed +
+failed.  Submitters and waiters run in separate threads (ctypes releases the
+GIL for the call), so waits overlap submits that grow the ticket table.
+"""
+import ctypes
+import threading
+
+import numpy as np
+import pytest
+
+import jsvd
+
+
+def _server(**kw):
+    opt = jsvd.ServerOptions()
+    jsvd.lib().jsvd_server_options_default(ctypes.byref(opt))
+    for k, v in kw.items():
+        setattr(opt, k, v)
+    h = ctypes.c_void_p()
+    jsvd.check(jsvd.lib().jsvd_server_create(ctypes.byref(opt), ctypes.byref(h)))
+    return h
+
+
+def _submit(h, a):
+    t = ctypes.c_uint64(0)
+    rc = jsvd.lib().jsvd_server_submit(h, a.ctypes.data, a.shape[0], a.shape[1], 0, ctypes.byref(t))
+    return rc, t.value
+
+
+def _wait(h, ticket, n):
+    s = np.empty(n)
+    v = np.empty((n, n))
+    sw = ctypes.c_int(0)
+    lat = ctypes.c_double(0.0)
+    return jsvd.lib().jsvd_server_wait(h, ticket, None, s.ctypes.data, v.ctypes.data, ctypes.byref(sw),
+                                       ctypes.byref(lat))
+
+
+def _stats(h):
+    st = jsvd.ServerStats()
+    jsvd.check(jsvd.lib().jsvd_server_get_stats(h, ctypes.byref(st)))
+    return st
+
+
+def test_request_over_budget_is_rejected_at_submit():
+    h = _server(device_budget_bytes=64 * 1024)
+    try:
+        rc, _ = _submit(h, np.ones((80, 64)))  # needs 107,008 bytes
+        assert rc == jsvd.JSVD_ERR_BUDGET
+        assert "more than the serving budget of 65536" in jsvd.last_error()[1]
+        rc, _ = _submit(h, np.ones((3, 4)))
+        assert rc == jsvd.JSVD_ERR_INVALID_ARGUMENT
+        assert _stats(h).submitted == 0
+    finally:
+        jsvd.lib().jsvd_server_destroy(h)
+
+
+@pytest.mark.timeout(300)
+def test_tickets_collected_once_under_concurrent_submit_and_wait():
+    h = _server(small_workers=2, large_workers=2, max_batch=16)
+    shapes = [(8, 4), (300, 260), (33, 17), (2, 2), (70, 64), (257, 200)] * 40
+    rng = np.random.default_rng(5)
+    mats = [rng.standard_normal(s) for s in shapes]
+    tickets = [None] * len(mats)
+    ready = [threading.Event() for _ in mats]
+    results = [None] * len(mats)
+
+    def submitter(lo, step):
+        for i in range(lo, len(mats), step):
+            rc, t = _submit(h, mats[i])
+            assert rc == jsvd.JSVD_OK
+            tickets[i] = t
+            ready[i].set()
+
+    def waiter(lo, step):
+        for i in range(lo, len(mats), step):
+            ready[i].wait()
+            results[i] = _wait(h, tickets[i], mats[i].shape[1])
+
+    try:
+        ths = [threading.Thread(target=submitter, args=(k, 2)) for k in range(2)]
+        ths += [threading.Thread(target=waiter, args=(k, 4)) for k in range(4)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        assert all(rc in (jsvd.JSVD_OK, jsvd.JSVD_ERR_CUDA) for rc in results), set(results)
+        assert len(set(tickets)) == len(mats)
+        st = _stats(h)
+        assert st.submitted == len(mats)
+        assert st.completed + st.failed == len(mats)
+        assert st.completed == sum(rc == jsvd.JSVD_OK for rc in results)
+        assert st.device_bytes_in_use == 0
+        # a collected ticket cannot be waited on again; an unknown one neither
+        for t in (tickets[0], max(tickets) + 1):
+            assert _wait(h, t, 4) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+            assert jsvd.last_error()[1] == "Unknown or already collected ticket."
+    finally:
+        jsvd.lib().jsvd_server_destroy(h)
+
+
+@pytest.mark.timeout(120)
+def test_two_concurrent_waits_on_one_ticket():
+    """Whatever the timing, exactly one of two threads waiting on the same
+    ticket collects it; the other is rejected (ticket claimed or collected)."""
+    h = _server(small_workers=1, large_workers=1)
+    try:
+        rng = np.random.default_rng(1)
+        for shape in [(40, 30), (300, 260)] * 10:
+            a = rng.standard_normal(shape)
+            rc, t = _submit(h, a)
+            assert rc == jsvd.JSVD_OK
+            out = [None, None]
+            ths = [threading.Thread(target=lambda k=k: out.__setitem__(k, _wait(h, t, shape[1]))) for k in range(2)]
+            for th in ths:
+                th.start()
+            for th in ths:
+                th.join()
+            assert sorted(out) in ([jsvd.JSVD_OK, jsvd.JSVD_ERR_INVALID_ARGUMENT],
+                                   [jsvd.JSVD_ERR_INVALID_ARGUMENT, jsvd.JSVD_ERR_CUDA]), out
+    finally:
+        jsvd.lib().jsvd_server_destroy(h)
