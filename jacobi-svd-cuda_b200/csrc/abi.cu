@@ -60,6 +60,17 @@ void set_last_error(int code, const std::string &message)
 
 const std::string &last_error_message() { return error_state().message; }
 
+void note_exception(const char *what) noexcept
+{
+    ErrorState &e = error_state();
+    e.code = JSVD_ERR_RUNTIME;
+    try {
+        e.message = what;
+    } catch (...) {
+        e.message.clear();
+    }
+}
+
 cudaStream_t thread_stream(int device)
 {
     auto &cache = thread_cache();
@@ -139,8 +150,7 @@ int validate_plain_request(const void *input, size_t rows, size_t columns, const
         return invalid_argument("layout_transpose_benchmark_sweeps must be positive.");
     if (cfg.layout_transpose_mode < JSVD_LAYOUT_AUTO || cfg.layout_transpose_mode > JSVD_LAYOUT_FORCE_DISABLE)
         return invalid_argument("layout_transpose_mode is not a valid LayoutTransposeMode.");
-    // The working copy indexes rows and columns with 32-bit integers.
-    if (rows > (size_t)0x7fffffff || columns > (size_t)0x7fffffff || rows * columns / rows != columns) {
+    if (dims_out_of_range(rows, columns)) {
         set_last_error(JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range.");
         return JSVD_ERR_OVERFLOW;
     }
@@ -231,105 +241,111 @@ int jsvd_plain_arith_variant(void) { return kRotVariant; }
 int jsvd_plain_svd_device(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,
                           double *d_sigma, double *d_v, int *sweeps, void *stream)
 {
-    set_last_error(JSVD_OK, "");
-    return plain_device_impl(d_a, rows, columns, cfg, d_u, d_sigma, d_v, sweeps, (cudaStream_t)stream);
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        return plain_device_impl(d_a, rows, columns, cfg, d_u, d_sigma, d_v, sweeps, (cudaStream_t)stream);
+    });
 }
 
 int jsvd_plain_svd(const double *a, size_t rows, size_t columns, const jsvd_config *cfg, double *u, double *sigma,
                    double *v, int *sweeps)
 {
-    set_last_error(JSVD_OK, "");
-    jsvd_config def;
-    jsvd_config_default(&def);
-    const jsvd_config &c = cfg ? *cfg : def;
-    int rc = validate_plain_request(a, rows, columns, c);
-    if (rc != JSVD_OK) return rc;
-    int dev = 0;
-    JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    cudaStream_t stream = thread_stream(dev);
-    if (stream == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-    PlainPlan *plan = nullptr;
-    rc = acquire_plain_plan(rows, columns, reduction_lanes(c.threads_per_block), c.epsilon, stream, &plan);
-    if (rc != JSVD_OK) return rc;
-    rc = plan->ensure_host_staging();
-    if (rc != JSVD_OK) return rc;
-    JSVD_CUDA_TRY(cudaMemcpyAsync(plan->d_in, a, sizeof(double) * rows * columns, cudaMemcpyHostToDevice, stream));
-    rc = plan->run(plan->d_in, u ? plan->d_u : nullptr, plan->d_sigma, v ? plan->d_v : nullptr, c.max_sweeps,
-                   sweeps, stream);
-    if (rc != JSVD_OK) return rc;
-    if (u)
-        JSVD_CUDA_TRY(cudaMemcpyAsync(u, plan->d_u, sizeof(double) * rows * columns, cudaMemcpyDeviceToHost, stream));
-    if (sigma)
-        JSVD_CUDA_TRY(cudaMemcpyAsync(sigma, plan->d_sigma, sizeof(double) * columns, cudaMemcpyDeviceToHost, stream));
-    if (v)
-        JSVD_CUDA_TRY(
-            cudaMemcpyAsync(v, plan->d_v, sizeof(double) * columns * columns, cudaMemcpyDeviceToHost, stream));
-    JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
-    return JSVD_OK;
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        jsvd_config def;
+        jsvd_config_default(&def);
+        const jsvd_config &c = cfg ? *cfg : def;
+        int rc = validate_plain_request(a, rows, columns, c);
+        if (rc != JSVD_OK) return rc;
+        int dev = 0;
+        JSVD_CUDA_TRY(cudaGetDevice(&dev));
+        cudaStream_t stream = thread_stream(dev);
+        if (stream == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+        PlainPlan *plan = nullptr;
+        rc = acquire_plain_plan(rows, columns, reduction_lanes(c.threads_per_block), c.epsilon, stream, &plan);
+        if (rc != JSVD_OK) return rc;
+        rc = plan->ensure_host_staging();
+        if (rc != JSVD_OK) return rc;
+        JSVD_CUDA_TRY(cudaMemcpyAsync(plan->d_in, a, sizeof(double) * rows * columns, cudaMemcpyHostToDevice, stream));
+        rc = plan->run(plan->d_in, u ? plan->d_u : nullptr, plan->d_sigma, v ? plan->d_v : nullptr, c.max_sweeps,
+                       sweeps, stream);
+        if (rc != JSVD_OK) return rc;
+        if (u)
+            JSVD_CUDA_TRY(cudaMemcpyAsync(u, plan->d_u, sizeof(double) * rows * columns, cudaMemcpyDeviceToHost, stream));
+        if (sigma)
+            JSVD_CUDA_TRY(cudaMemcpyAsync(sigma, plan->d_sigma, sizeof(double) * columns, cudaMemcpyDeviceToHost, stream));
+        if (v)
+            JSVD_CUDA_TRY(
+                cudaMemcpyAsync(v, plan->d_v, sizeof(double) * columns * columns, cudaMemcpyDeviceToHost, stream));
+        JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
+        return JSVD_OK;
+    });
 }
 
 int jsvd_auto_tune_layout(const jsvd_config *cfg, jsvd_autotune_report *report)
 {
-    set_last_error(JSVD_OK, "");
-    jsvd_config def;
-    jsvd_config_default(&def);
-    const jsvd_config &c = cfg ? *cfg : def;
-    if (!report) return invalid_argument("report must not be null.");
-    // Validation order of src/kernels.cu:1078-1086.
-    if (c.layout_transpose_min_columns <= 0)
-        return invalid_argument("layout_transpose_min_columns must be positive.");
-    if (c.layout_transpose_min_elements == 0)
-        return invalid_argument("layout_transpose_min_elements must be positive.");
-    if (c.layout_transpose_benchmark_repetitions <= 0)
-        return invalid_argument("layout_transpose_benchmark_repetitions must be positive.");
-    if (c.layout_transpose_benchmark_sweeps <= 0)
-        return invalid_argument("layout_transpose_benchmark_sweeps must be positive.");
-    if (c.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        jsvd_config def;
+        jsvd_config_default(&def);
+        const jsvd_config &c = cfg ? *cfg : def;
+        if (!report) return invalid_argument("report must not be null.");
+        // Validation order of src/kernels.cu:1078-1086.
+        if (c.layout_transpose_min_columns <= 0)
+            return invalid_argument("layout_transpose_min_columns must be positive.");
+        if (c.layout_transpose_min_elements == 0)
+            return invalid_argument("layout_transpose_min_elements must be positive.");
+        if (c.layout_transpose_benchmark_repetitions <= 0)
+            return invalid_argument("layout_transpose_benchmark_repetitions must be positive.");
+        if (c.layout_transpose_benchmark_sweeps <= 0)
+            return invalid_argument("layout_transpose_benchmark_sweeps must be positive.");
+        if (c.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
 
-    jsvd_config bench = c;
-    bench.layout_transpose_auto_tune = 0;
-    bench.max_sweeps = std::min(c.max_sweeps, std::max(1, c.layout_transpose_benchmark_sweeps));
-    const std::array<int, 8> widths = {8, 12, 16, 24, 32, 48, 64, 96};
-    report->executed = 1;
-    report->recommended_min_columns = c.layout_transpose_min_columns;
-    report->recommended_min_elements = c.layout_transpose_min_elements;
-    report->estimated_best_speedup = 1.0;
-    report->sample_count = widths.size();
-    bool selected = false;
-    for (int cols : widths) {
-        const size_t rows = (size_t)cols * 2;
-        // Deterministic benchmark matrix of src/kernels.cu:1012-1025.
-        std::vector<double> a(rows * cols);
-        for (size_t r = 0; r < rows; ++r)
-            for (size_t k = 0; k < (size_t)cols; ++k)
-                a[r * cols + k] = std::sin(0.013 * (double)((r + 1) * (k + 1))) +
-                                  std::cos(0.017 * (double)((r + 3) * (k + 5)));
-        std::vector<double> u(rows * cols), s(cols), v((size_t)cols * cols);
-        double ms[2] = {0.0, 0.0};
-        for (int mode = 0; mode < 2; ++mode) {
-            bench.layout_transpose_mode = mode == 0 ? JSVD_LAYOUT_FORCE_DISABLE : JSVD_LAYOUT_FORCE_ENABLE;
-            int sw = 0;
-            int rc = jsvd_plain_svd(a.data(), rows, cols, &bench, u.data(), s.data(), v.data(), &sw);
-            if (rc != JSVD_OK) return rc;
-            double acc = 0.0;
-            for (int rep = 0; rep < c.layout_transpose_benchmark_repetitions; ++rep) {
-                auto t0 = std::chrono::steady_clock::now();
-                rc = jsvd_plain_svd(a.data(), rows, cols, &bench, u.data(), s.data(), v.data(), &sw);
-                auto t1 = std::chrono::steady_clock::now();
+        jsvd_config bench = c;
+        bench.layout_transpose_auto_tune = 0;
+        bench.max_sweeps = std::min(c.max_sweeps, std::max(1, c.layout_transpose_benchmark_sweeps));
+        const std::array<int, 8> widths = {8, 12, 16, 24, 32, 48, 64, 96};
+        report->executed = 1;
+        report->recommended_min_columns = c.layout_transpose_min_columns;
+        report->recommended_min_elements = c.layout_transpose_min_elements;
+        report->estimated_best_speedup = 1.0;
+        report->sample_count = widths.size();
+        bool selected = false;
+        for (int cols : widths) {
+            const size_t rows = (size_t)cols * 2;
+            // Deterministic benchmark matrix of src/kernels.cu:1012-1025.
+            std::vector<double> a(rows * cols);
+            for (size_t r = 0; r < rows; ++r)
+                for (size_t k = 0; k < (size_t)cols; ++k)
+                    a[r * cols + k] = std::sin(0.013 * (double)((r + 1) * (k + 1))) +
+                                      std::cos(0.017 * (double)((r + 3) * (k + 5)));
+            std::vector<double> u(rows * cols), s(cols), v((size_t)cols * cols);
+            double ms[2] = {0.0, 0.0};
+            for (int mode = 0; mode < 2; ++mode) {
+                bench.layout_transpose_mode = mode == 0 ? JSVD_LAYOUT_FORCE_DISABLE : JSVD_LAYOUT_FORCE_ENABLE;
+                int sw = 0;
+                int rc = jsvd_plain_svd(a.data(), rows, cols, &bench, u.data(), s.data(), v.data(), &sw);
                 if (rc != JSVD_OK) return rc;
-                acc += std::chrono::duration<double, std::milli>(t1 - t0).count();
+                double acc = 0.0;
+                for (int rep = 0; rep < c.layout_transpose_benchmark_repetitions; ++rep) {
+                    auto t0 = std::chrono::steady_clock::now();
+                    rc = jsvd_plain_svd(a.data(), rows, cols, &bench, u.data(), s.data(), v.data(), &sw);
+                    auto t1 = std::chrono::steady_clock::now();
+                    if (rc != JSVD_OK) return rc;
+                    acc += std::chrono::duration<double, std::milli>(t1 - t0).count();
+                }
+                ms[mode] = acc / c.layout_transpose_benchmark_repetitions;
             }
-            ms[mode] = acc / c.layout_transpose_benchmark_repetitions;
+            const double speedup = ms[0] / std::max(ms[1], 1e-300);
+            report->estimated_best_speedup = std::max(report->estimated_best_speedup, speedup);
+            if (!selected && ms[1] < ms[0]) {
+                report->recommended_min_columns = cols;
+                report->recommended_min_elements = rows * (size_t)cols;
+                selected = true;
+            }
         }
-        const double speedup = ms[0] / std::max(ms[1], 1e-300);
-        report->estimated_best_speedup = std::max(report->estimated_best_speedup, speedup);
-        if (!selected && ms[1] < ms[0]) {
-            report->recommended_min_columns = cols;
-            report->recommended_min_elements = rows * (size_t)cols;
-            selected = true;
-        }
-    }
-    return JSVD_OK;
+        return JSVD_OK;
+    });
 }
 
 void jsvd_plain_stats_get(jsvd_plain_stats *out)

@@ -519,35 +519,37 @@ extern "C" int jsvd_batch_svd_device(int count, const int *rows, const int *cols
                                      double *d_v, double *d_u, int *sweeps, const jsvd_batch_tuning *tuning,
                                      void *stream)
 {
-    set_last_error(JSVD_OK, "");
-    jsvd_config def;
-    jsvd_config_default(&def);
-    const jsvd_config &c = cfg ? *cfg : def;
-    const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, d_sigma == nullptr, c);
-    if (bad != JSVD_OK) return bad;
-    int dev = 0;
-    JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    cudaStream_t st = (cudaStream_t)stream;
-    if (st == nullptr) {
-        st = thread_stream(dev);
-        if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-        JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
-    }
-    BatchRequest req;
-    req.count = count;
-    req.rows = rows;
-    req.cols = cols;
-    req.a_offsets = a_offsets;
-    req.a = d_a;
-    req.a_is_f32 = a_is_f32;
-    req.eps = c.epsilon;
-    req.max_sweeps = c.max_sweeps;
-    req.sigma = d_sigma;
-    req.v = d_v;
-    req.u = d_u;
-    req.sweeps = sweeps;
-    req.tuning = tuning;
-    return batch_solve(req, st);
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        jsvd_config def;
+        jsvd_config_default(&def);
+        const jsvd_config &c = cfg ? *cfg : def;
+        const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, d_sigma == nullptr, c);
+        if (bad != JSVD_OK) return bad;
+        int dev = 0;
+        JSVD_CUDA_TRY(cudaGetDevice(&dev));
+        cudaStream_t st = (cudaStream_t)stream;
+        if (st == nullptr) {
+            st = thread_stream(dev);
+            if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+            JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+        }
+        BatchRequest req;
+        req.count = count;
+        req.rows = rows;
+        req.cols = cols;
+        req.a_offsets = a_offsets;
+        req.a = d_a;
+        req.a_is_f32 = a_is_f32;
+        req.eps = c.epsilon;
+        req.max_sweeps = c.max_sweeps;
+        req.sigma = d_sigma;
+        req.v = d_v;
+        req.u = d_u;
+        req.sweeps = sweeps;
+        req.tuning = tuning;
+        return batch_solve(req, st);
+    });
 }
 
 extern "C" void jsvd_batch_stats_get(jsvd_batch_stats *out)
@@ -607,160 +609,162 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
                                    const void *d_a, int a_is_f32, const jsvd_config *cfg, int sample, int reps,
                                    int want_u, int want_v, jsvd_batch_autotune_report *report, void *stream)
 {
-    set_last_error(JSVD_OK, "");
-    jsvd_config def;
-    jsvd_config_default(&def);
-    const jsvd_config &c = cfg ? *cfg : def;
-    if (report == nullptr) return invalid_argument("Autotune report must not be null.");
-    const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, false, c);
-    if (bad != JSVD_OK) return bad;
-    *report = jsvd_batch_autotune_report{};
-    for (int k = 0; k < kClasses; ++k) report->builtin[k] = kBuiltinTuning[k];
-    if (count == 0) return JSVD_OK;
-    if (reps <= 0) reps = 2;
-    int dev = 0;
-    JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    cudaStream_t st = (cudaStream_t)stream;
-    if (st == nullptr) {
-        st = thread_stream(dev);
-        if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-        JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
-    }
-    int sms = 0, smem_per_sm = 0;
-    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-    size_t smem_cap = 0;
-    int rc = batch_smem_cap(dev, &smem_cap);
-    if (rc != JSVD_OK) return rc;
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        jsvd_config def;
+        jsvd_config_default(&def);
+        const jsvd_config &c = cfg ? *cfg : def;
+        if (report == nullptr) return invalid_argument("Autotune report must not be null.");
+        const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, false, c);
+        if (bad != JSVD_OK) return bad;
+        *report = jsvd_batch_autotune_report{};
+        for (int k = 0; k < kClasses; ++k) report->builtin[k] = kBuiltinTuning[k];
+        if (count == 0) return JSVD_OK;
+        if (reps <= 0) reps = 2;
+        int dev = 0;
+        JSVD_CUDA_TRY(cudaGetDevice(&dev));
+        cudaStream_t st = (cudaStream_t)stream;
+        if (st == nullptr) {
+            st = thread_stream(dev);
+            if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+            JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
+        }
+        int sms = 0, smem_per_sm = 0;
+        JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        size_t smem_cap = 0;
+        int rc = batch_smem_cap(dev, &smem_cap);
+        if (rc != JSVD_OK) return rc;
 
-    std::vector<std::vector<int>> members(kClasses);
-    for (int i = 0; i < count; ++i) {
-        if (rows[i] <= 0 || cols[i] <= 0 || rows[i] < cols[i])
-            return invalid_argument("Batch matrix shape must satisfy rows >= columns > 0.");
-        members[member_class(rows[i], cols[i], smem_cap, nullptr)].push_back(i);
-    }
+        std::vector<std::vector<int>> members(kClasses);
+        for (int i = 0; i < count; ++i) {
+            if (rows[i] <= 0 || cols[i] <= 0 || rows[i] < cols[i])
+                return invalid_argument("Batch matrix shape must satisfy rows >= columns > 0.");
+            members[member_class(rows[i], cols[i], smem_cap, nullptr)].push_back(i);
+        }
 
-    // Flush buffer (larger than L2) and output buffers sized for the largest sample.
-    const size_t flush_bytes = (size_t)256 << 20;
-    std::vector<std::vector<int>> picked(kClasses);
-    size_t max_s = 0, max_v = 0, max_u = 0;
-    for (int k = 0; k < kClasses; ++k) {
-        auto &mem = members[k];
-        std::sort(mem.begin(), mem.end(),
-                  [&](int x, int y) { return member_work(rows[x], cols[x]) > member_work(rows[y], cols[y]); });
-        const size_t cnt = mem.size();
-        const size_t s = (sample > 0 && (size_t)sample < cnt) ? (size_t)sample : cnt;
-        size_t ns = 0, nv = 0, nu = 0;
-        for (size_t j = 0; j < s; ++j) {  // evenly spaced over the work order
-            const int i = mem[j * cnt / s];
-            picked[k].push_back(i);
-            ns += (size_t)cols[i];
-            nv += (size_t)cols[i] * cols[i];
-            nu += (size_t)rows[i] * cols[i];
+        // Flush buffer (larger than L2) and output buffers sized for the largest sample.
+        const size_t flush_bytes = (size_t)256 << 20;
+        std::vector<std::vector<int>> picked(kClasses);
+        size_t max_s = 0, max_v = 0, max_u = 0;
+        for (int k = 0; k < kClasses; ++k) {
+            auto &mem = members[k];
+            std::sort(mem.begin(), mem.end(),
+                      [&](int x, int y) { return member_work(rows[x], cols[x]) > member_work(rows[y], cols[y]); });
+            const size_t cnt = mem.size();
+            const size_t s = (sample > 0 && (size_t)sample < cnt) ? (size_t)sample : cnt;
+            size_t ns = 0, nv = 0, nu = 0;
+            for (size_t j = 0; j < s; ++j) {  // evenly spaced over the work order
+                const int i = mem[j * cnt / s];
+                picked[k].push_back(i);
+                ns += (size_t)cols[i];
+                nv += (size_t)cols[i] * cols[i];
+                nu += (size_t)rows[i] * cols[i];
+            }
+            max_s = std::max(max_s, ns);
+            max_v = std::max(max_v, nv);
+            max_u = std::max(max_u, nu);
+            report->members[k] = (int)cnt;
+            report->sampled[k] = (int)s;
         }
-        max_s = std::max(max_s, ns);
-        max_v = std::max(max_v, nv);
-        max_u = std::max(max_u, nu);
-        report->members[k] = (int)cnt;
-        report->sampled[k] = (int)s;
-    }
-    void *d_flush = nullptr;
-    double *d_sigma = nullptr, *d_v = nullptr, *d_u = nullptr;
-    auto release = [&]() {
-        if (d_flush) cudaFreeAsync(d_flush, st);
-        if (d_sigma) cudaFreeAsync(d_sigma, st);
-        if (d_v) cudaFreeAsync(d_v, st);
-        if (d_u) cudaFreeAsync(d_u, st);
-        cudaStreamSynchronize(st);
-    };
-    // The autotuner's own solves are not counted in the batch statistics.
-    const BatchStats saved = batch_stats();
-    auto finish = [&](int code) {
-        release();
-        batch_stats() = saved;
-        return code;
-    };
-    if (cudaMallocAsync(&d_flush, flush_bytes, st) != cudaSuccess ||
-        cudaMallocAsync((void **)&d_sigma, sizeof(double) * std::max<size_t>(max_s, 1), st) != cudaSuccess ||
-        (want_v && cudaMallocAsync((void **)&d_v, sizeof(double) * std::max<size_t>(max_v, 1), st) != cudaSuccess) ||
-        (want_u && cudaMallocAsync((void **)&d_u, sizeof(double) * std::max<size_t>(max_u, 1), st) != cudaSuccess))
-        return finish(cuda_failure(cudaGetLastError(), "cudaMallocAsync", __FILE__, __LINE__));
+        void *d_flush = nullptr;
+        double *d_sigma = nullptr, *d_v = nullptr, *d_u = nullptr;
+        auto release = [&]() {
+            if (d_flush) cudaFreeAsync(d_flush, st);
+            if (d_sigma) cudaFreeAsync(d_sigma, st);
+            if (d_v) cudaFreeAsync(d_v, st);
+            if (d_u) cudaFreeAsync(d_u, st);
+            cudaStreamSynchronize(st);
+        };
+        // The autotuner's own solves are not counted in the batch statistics.
+        const BatchStats saved = batch_stats();
+        auto finish = [&](int code) {
+            release();
+            batch_stats() = saved;
+            return code;
+        };
+        if (cudaMallocAsync(&d_flush, flush_bytes, st) != cudaSuccess ||
+            cudaMallocAsync((void **)&d_sigma, sizeof(double) * std::max<size_t>(max_s, 1), st) != cudaSuccess ||
+            (want_v && cudaMallocAsync((void **)&d_v, sizeof(double) * std::max<size_t>(max_v, 1), st) != cudaSuccess) ||
+            (want_u && cudaMallocAsync((void **)&d_u, sizeof(double) * std::max<size_t>(max_u, 1), st) != cudaSuccess))
+            return finish(cuda_failure(cudaGetLastError(), "cudaMallocAsync", __FILE__, __LINE__));
 
-    for (int k = 0; k < kClasses; ++k) {
-        const auto &pk = picked[k];
-        if (pk.empty()) continue;
-        const int s = (int)pk.size();
-        std::vector<int> r_s(s), c_s(s), sw(s), sw_ref(s);
-        std::vector<long long> off_s(s);
-        size_t need = 0, nsig = 0;
-        for (int j = 0; j < s; ++j) {
-            r_s[j] = rows[pk[j]];
-            c_s[j] = cols[pk[j]];
-            off_s[j] = a_offsets[pk[j]];
-            size_t nj = 0;
-            member_class(r_s[j], c_s[j], smem_cap, &nj);
-            need = std::max(need, nj);
-            nsig += (size_t)c_s[j];
-        }
-        std::vector<double> sig(nsig), sig_ref(nsig);
-        // the built-in shape first: it is the yardstick and the bitwise reference
-        std::vector<jsvd_batch_tuning> cands{kBuiltinTuning[k]};
-        for (const auto &t : batch_candidates(k, need, sms, (size_t)smem_per_sm))
-            if (!same_shape(t, kBuiltinTuning[k])) cands.push_back(t);
-        report->candidates[k] = (int)cands.size();
-        double best_ms = -1.0;
-        jsvd_batch_tuning best = kBuiltinTuning[k];
-        for (size_t ci = 0; ci < cands.size(); ++ci) {
-            jsvd_batch_tuning tun[kClasses] = {};
-            tun[k] = cands[ci];
-            BatchRequest req;
-            req.count = s;
-            req.rows = r_s.data();
-            req.cols = c_s.data();
-            req.a_offsets = off_s.data();
-            req.a = d_a;
-            req.a_is_f32 = a_is_f32;
-            req.eps = c.epsilon;
-            req.max_sweeps = c.max_sweeps;
-            req.sigma = d_sigma;
-            req.v = d_v;
-            req.u = d_u;
-            req.sweeps = sw.data();
-            req.tuning = tun;
-            double ms = -1.0;
-            for (int r = 0; r < reps; ++r) {
-                if (cudaMemsetAsync(d_flush, r & 0xff, flush_bytes, st) != cudaSuccess)
-                    return finish(cuda_failure(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
-                const double before = batch_stats().class_ms[k];
-                rc = batch_solve(req, st);
-                if (rc != JSVD_OK) return finish(rc);
-                const double t = batch_stats().class_ms[k] - before;
-                ms = ms < 0.0 ? t : std::min(ms, t);
+        for (int k = 0; k < kClasses; ++k) {
+            const auto &pk = picked[k];
+            if (pk.empty()) continue;
+            const int s = (int)pk.size();
+            std::vector<int> r_s(s), c_s(s), sw(s), sw_ref(s);
+            std::vector<long long> off_s(s);
+            size_t need = 0, nsig = 0;
+            for (int j = 0; j < s; ++j) {
+                r_s[j] = rows[pk[j]];
+                c_s[j] = cols[pk[j]];
+                off_s[j] = a_offsets[pk[j]];
+                size_t nj = 0;
+                member_class(r_s[j], c_s[j], smem_cap, &nj);
+                need = std::max(need, nj);
+                nsig += (size_t)c_s[j];
             }
-            if (cudaMemcpyAsync(sig.data(), d_sigma, sizeof(double) * nsig, cudaMemcpyDeviceToHost, st) !=
-                    cudaSuccess ||
-                cudaStreamSynchronize(st) != cudaSuccess)
-                return finish(cuda_failure(cudaGetLastError(), "cudaMemcpyAsync", __FILE__, __LINE__));
-            if (ci == 0) {
-                sig_ref = sig;
-                sw_ref = sw;
-                report->builtin_ms[k] = ms;
-            } else if (std::memcmp(sig.data(), sig_ref.data(), sizeof(double) * nsig) != 0 || sw != sw_ref) {
-                set_last_error(JSVD_ERR_RUNTIME, "Batch launch shapes disagree on sigma or sweep counts.");
-                return finish(JSVD_ERR_RUNTIME);
+            std::vector<double> sig(nsig), sig_ref(nsig);
+            // the built-in shape first: it is the yardstick and the bitwise reference
+            std::vector<jsvd_batch_tuning> cands{kBuiltinTuning[k]};
+            for (const auto &t : batch_candidates(k, need, sms, (size_t)smem_per_sm))
+                if (!same_shape(t, kBuiltinTuning[k])) cands.push_back(t);
+            report->candidates[k] = (int)cands.size();
+            double best_ms = -1.0;
+            jsvd_batch_tuning best = kBuiltinTuning[k];
+            for (size_t ci = 0; ci < cands.size(); ++ci) {
+                jsvd_batch_tuning tun[kClasses] = {};
+                tun[k] = cands[ci];
+                BatchRequest req;
+                req.count = s;
+                req.rows = r_s.data();
+                req.cols = c_s.data();
+                req.a_offsets = off_s.data();
+                req.a = d_a;
+                req.a_is_f32 = a_is_f32;
+                req.eps = c.epsilon;
+                req.max_sweeps = c.max_sweeps;
+                req.sigma = d_sigma;
+                req.v = d_v;
+                req.u = d_u;
+                req.sweeps = sw.data();
+                req.tuning = tun;
+                double ms = -1.0;
+                for (int r = 0; r < reps; ++r) {
+                    if (cudaMemsetAsync(d_flush, r & 0xff, flush_bytes, st) != cudaSuccess)
+                        return finish(cuda_failure(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
+                    const double before = batch_stats().class_ms[k];
+                    rc = batch_solve(req, st);
+                    if (rc != JSVD_OK) return finish(rc);
+                    const double t = batch_stats().class_ms[k] - before;
+                    ms = ms < 0.0 ? t : std::min(ms, t);
+                }
+                if (cudaMemcpyAsync(sig.data(), d_sigma, sizeof(double) * nsig, cudaMemcpyDeviceToHost, st) !=
+                        cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess)
+                    return finish(cuda_failure(cudaGetLastError(), "cudaMemcpyAsync", __FILE__, __LINE__));
+                if (ci == 0) {
+                    sig_ref = sig;
+                    sw_ref = sw;
+                    report->builtin_ms[k] = ms;
+                } else if (std::memcmp(sig.data(), sig_ref.data(), sizeof(double) * nsig) != 0 || sw != sw_ref) {
+                    set_last_error(JSVD_ERR_RUNTIME, "Batch launch shapes disagree on sigma or sweep counts.");
+                    return finish(JSVD_ERR_RUNTIME);
+                }
+                if (best_ms < 0.0 || ms < best_ms) {
+                    best_ms = ms;
+                    best = cands[ci];
+                }
             }
-            if (best_ms < 0.0 || ms < best_ms) {
-                best_ms = ms;
-                best = cands[ci];
+            // a shape replaces the built-in one only when it is more than 2% faster
+            if (best_ms > 0.98 * report->builtin_ms[k]) {
+                best = kBuiltinTuning[k];
+                best_ms = report->builtin_ms[k];
             }
+            report->best[k] = best;
+            report->best_ms[k] = best_ms;
         }
-        // a shape replaces the built-in one only when it is more than 2% faster
-        if (best_ms > 0.98 * report->builtin_ms[k]) {
-            best = kBuiltinTuning[k];
-            best_ms = report->builtin_ms[k];
-        }
-        report->best[k] = best;
-        report->best_ms[k] = best_ms;
-    }
-    return finish(JSVD_OK);
+        return finish(JSVD_OK);
+    });
 }

@@ -8,6 +8,8 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <exception>
+#include <new>
 #include <sstream>
 #include <string>
 
@@ -17,6 +19,28 @@ namespace jsvd {
 
 void set_last_error(int code, const std::string &message);
 const std::string &last_error_message();
+
+// Records a C++ exception caught at a C entry point as JSVD_ERR_RUNTIME (the
+// message is dropped if even that cannot be allocated).
+void note_exception(const char *what) noexcept;
+
+// Runs the body of a C entry point: a C++ exception (host allocation, thread
+// creation, ...) becomes JSVD_ERR_RUNTIME and the last-error text instead of
+// unwinding into a C caller.
+template <class Body>
+int c_entry(Body &&body) noexcept
+{
+    try {
+        return body();
+    } catch (const std::bad_alloc &) {
+        note_exception("Host memory allocation failed.");
+    } catch (const std::exception &e) {
+        note_exception(e.what());
+    } catch (...) {
+        note_exception("Unknown C++ exception.");
+    }
+    return JSVD_ERR_RUNTIME;
+}
 
 // Formats a CUDA failure like the reference's JACOBI_CUDA_CHECK:
 // "CUDA call failed: <expr> @ <file>:<line>, code=<n>, message=<text>".
@@ -33,6 +57,15 @@ inline int invalid_argument(const char *message)
 {
     set_last_error(JSVD_ERR_INVALID_ARGUMENT, message);
     return JSVD_ERR_INVALID_ARGUMENT;
+}
+
+// True when a rows x columns request is outside the supported range: the
+// working copies index rows and columns with 32-bit integers, and byte
+// counts of several m x n buffers must not overflow size_t.
+inline bool dims_out_of_range(std::size_t rows, std::size_t columns)
+{
+    if (rows > (std::size_t)0x7fffffff || columns > (std::size_t)0x7fffffff) return true;
+    return rows * columns > SIZE_MAX / 64;  // both factors < 2^31: the product itself fits
 }
 
 // Validates a plain-path request exactly as the reference does, in the same

@@ -283,30 +283,32 @@ using namespace jsvd;
 extern "C" int jsvd_plain_svd_noalloc(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg,
                                       double *d_u, double *d_sigma, double *d_v, int *sweeps, void *stream)
 {
-    set_last_error(JSVD_OK, "");
-    jsvd_config def;
-    jsvd_config_default(&def);
-    const jsvd_config &c = cfg ? *cfg : def;
-    int rc = validate_plain_request(d_a, rows, columns, c);
-    if (rc != JSVD_OK) return rc;
-    const size_t need = rows * columns + columns * columns + columns + 1;
-    if (rows > kNoAllocScratchDoubles || need > kNoAllocScratchDoubles)
-        return invalid_argument(
-            "jsvd_plain_svd_noalloc: rows*columns + columns*columns + columns + 1 exceeds the fixed scratch of "
-            "2097152 doubles (16 MiB).");
-    int dev = 0;
-    JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    double *scratch = nullptr;
-    rc = noalloc_scratch(dev, &scratch);
-    if (rc != JSVD_OK) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
-    const int m = (int)rows, n = (int)columns;
-    switch (reduction_lanes(c.threads_per_block)) {
-    case 32: return na_solve<32>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
-    case 64: return na_solve<64>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
-    case 128: return na_solve<128>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
-    case 256: return na_solve<256>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
-    case 512: return na_solve<512>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
-    default: return na_solve<1024>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
-    }
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        jsvd_config def;
+        jsvd_config_default(&def);
+        const jsvd_config &c = cfg ? *cfg : def;
+        int rc = validate_plain_request(d_a, rows, columns, c);
+        if (rc != JSVD_OK) return rc;
+        const size_t need = rows * columns + columns * columns + columns + 1;
+        if (rows > kNoAllocScratchDoubles || need > kNoAllocScratchDoubles)
+            return invalid_argument(
+                "jsvd_plain_svd_noalloc: rows*columns + columns*columns + columns + 1 exceeds the fixed scratch of "
+                "2097152 doubles (16 MiB).");
+        int dev = 0;
+        JSVD_CUDA_TRY(cudaGetDevice(&dev));
+        double *scratch = nullptr;
+        rc = noalloc_scratch(dev, &scratch);
+        if (rc != JSVD_OK) return rc;
+        cudaStream_t st = (cudaStream_t)stream;
+        const int m = (int)rows, n = (int)columns;
+        switch (reduction_lanes(c.threads_per_block)) {
+        case 32: return na_solve<32>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
+        case 64: return na_solve<64>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
+        case 128: return na_solve<128>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
+        case 256: return na_solve<256>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
+        case 512: return na_solve<512>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
+        default: return na_solve<1024>(d_a, m, n, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st, scratch);
+        }
+    });
 }

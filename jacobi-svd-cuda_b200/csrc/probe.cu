@@ -35,32 +35,34 @@ using namespace jsvd;
 
 extern "C" int jsvd_probe_fp64_tflops(double *tflops)
 {
-    set_last_error(JSVD_OK, "");
-    if (!tflops) return invalid_argument("tflops must not be null.");
-    int dev = 0, sms = 0;
-    JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int grid = sms * 8, block = 256, iters = 4096;
-    cudaStream_t st = nullptr;
-    JSVD_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    cudaEvent_t e0, e1;
-    JSVD_CUDA_TRY(cudaEventCreate(&e0));
-    JSVD_CUDA_TRY(cudaEventCreate(&e1));
-    fp64_fma_probe<<<grid, block, 0, st>>>(nullptr, iters, 0.999999, 1e-7, 0);  // warm-up
-    float best = 1e30f;
-    for (int rep = 0; rep < 5; ++rep) {
-        JSVD_CUDA_TRY(cudaEventRecord(e0, st));
-        fp64_fma_probe<<<grid, block, 0, st>>>(nullptr, iters, 0.999999, 1e-7, 0);
-        JSVD_CUDA_TRY(cudaEventRecord(e1, st));
-        JSVD_CUDA_TRY(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        JSVD_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) best = ms;
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaStreamDestroy(st);
-    const double flops = 2.0 * kChains * (double)iters * grid * block;
-    *tflops = flops / (best * 1e-3) / 1e12;
-    return JSVD_OK;
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (!tflops) return invalid_argument("tflops must not be null.");
+        int dev = 0, sms = 0;
+        JSVD_CUDA_TRY(cudaGetDevice(&dev));
+        JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int grid = sms * 8, block = 256, iters = 4096;
+        cudaStream_t st = nullptr;
+        JSVD_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        cudaEvent_t e0, e1;
+        JSVD_CUDA_TRY(cudaEventCreate(&e0));
+        JSVD_CUDA_TRY(cudaEventCreate(&e1));
+        fp64_fma_probe<<<grid, block, 0, st>>>(nullptr, iters, 0.999999, 1e-7, 0);  // warm-up
+        float best = 1e30f;
+        for (int rep = 0; rep < 5; ++rep) {
+            JSVD_CUDA_TRY(cudaEventRecord(e0, st));
+            fp64_fma_probe<<<grid, block, 0, st>>>(nullptr, iters, 0.999999, 1e-7, 0);
+            JSVD_CUDA_TRY(cudaEventRecord(e1, st));
+            JSVD_CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            JSVD_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) best = ms;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(st);
+        const double flops = 2.0 * kChains * (double)iters * grid * block;
+        *tflops = flops / (best * 1e-3) / 1e12;
+        return JSVD_OK;
+    });
 }

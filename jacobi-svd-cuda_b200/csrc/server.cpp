@@ -98,26 +98,26 @@ public:
     explicit Server(const jsvd_server_options &o) : opt_(o)
     {
         cudaGetDevice(&device_);
-        for (int i = 0; i < opt_.small_workers; ++i) threads_.emplace_back([this] { small_loop(); });
-        for (int i = 0; i < opt_.large_workers; ++i) threads_.emplace_back([this] { large_loop(); });
+        try {
+            for (int i = 0; i < opt_.small_workers; ++i) threads_.emplace_back([this] { small_loop(); });
+            for (int i = 0; i < opt_.large_workers; ++i) threads_.emplace_back([this] { large_loop(); });
+        } catch (...) {
+            stop();  // the workers already started must be joined before the vector goes away
+            throw;
+        }
     }
 
-    ~Server()
-    {
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            stopping_ = true;
-        }
-        cv_work_.notify_all();
-        cv_budget_.notify_all();
-        for (auto &t : threads_) t.join();
-    }
+    ~Server() { stop(); }
 
     int submit(const double *a, size_t m, size_t n, int want_u, uint64_t *ticket)
     {
         if (a == nullptr || ticket == nullptr) return invalid_argument("Request buffers must not be null.");
         if (m == 0 || n == 0) return invalid_argument("Input matrix shape must be non-zero.");
         if (m < n) return invalid_argument("One-sided Jacobi SVD requires rows >= columns in this implementation.");
+        if (dims_out_of_range(m, n)) {
+            set_last_error(JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range.");
+            return JSVD_ERR_OVERFLOW;
+        }
         auto r = std::make_unique<Request>();
         r->m = m;
         r->n = n;
@@ -198,6 +198,18 @@ public:
     }
 
 private:
+    void stop()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stopping_ = true;
+        }
+        cv_work_.notify_all();
+        cv_budget_.notify_all();
+        for (auto &t : threads_)
+            if (t.joinable()) t.join();
+    }
+
     // Takes requests from q while their footprints fit the budget; blocks while
     // the first one does not fit.  Returns an empty list when stopping.
     std::vector<Request *> admit(std::deque<Request *> &q, size_t max_count)
@@ -415,43 +427,51 @@ void jsvd_server_options_default(jsvd_server_options *o)
 
 int jsvd_server_create(const jsvd_server_options *opt, jsvd_server **out)
 {
-    set_last_error(JSVD_OK, "");
-    if (!out) return invalid_argument("out must not be null.");
-    jsvd_server_options o;
-    jsvd_server_options_default(&o);
-    if (opt) o = *opt;
-    if (o.device_budget_bytes == 0) o.device_budget_bytes = size_t(40) << 30;
-    if (o.small_workers <= 0) o.small_workers = 2;
-    if (o.large_workers <= 0) o.large_workers = 4;
-    if (o.max_batch <= 0) o.max_batch = 4096;
-    if (!(o.cfg.epsilon > 0.0)) return invalid_argument("epsilon must be positive.");
-    if (o.cfg.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
-    auto *s = new jsvd_server;
-    s->impl = std::make_unique<Server>(o);
-    *out = s;
-    return JSVD_OK;
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (!out) return invalid_argument("out must not be null.");
+        jsvd_server_options o;
+        jsvd_server_options_default(&o);
+        if (opt) o = *opt;
+        if (o.device_budget_bytes == 0) o.device_budget_bytes = size_t(40) << 30;
+        if (o.small_workers <= 0) o.small_workers = 2;
+        if (o.large_workers <= 0) o.large_workers = 4;
+        if (o.max_batch <= 0) o.max_batch = 4096;
+        if (!(o.cfg.epsilon > 0.0)) return invalid_argument("epsilon must be positive.");
+        if (o.cfg.max_sweeps <= 0) return invalid_argument("max_sweeps must be positive.");
+        auto s = std::make_unique<jsvd_server>();
+        s->impl = std::make_unique<Server>(o);
+        *out = s.release();
+        return JSVD_OK;
+    });
 }
 
 int jsvd_server_submit(jsvd_server *s, const double *a, size_t rows, size_t columns, int want_u, uint64_t *ticket)
 {
-    set_last_error(JSVD_OK, "");
-    if (!s) return invalid_argument("server must not be null.");
-    return s->impl->submit(a, rows, columns, want_u, ticket);
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (!s) return invalid_argument("server must not be null.");
+        return s->impl->submit(a, rows, columns, want_u, ticket);
+    });
 }
 
 int jsvd_server_wait(jsvd_server *s, uint64_t ticket, double *u, double *sigma, double *v, int *sweeps,
                      double *latency_ms)
 {
-    set_last_error(JSVD_OK, "");
-    if (!s) return invalid_argument("server must not be null.");
-    return s->impl->wait(ticket, u, sigma, v, sweeps, latency_ms);
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (!s) return invalid_argument("server must not be null.");
+        return s->impl->wait(ticket, u, sigma, v, sweeps, latency_ms);
+    });
 }
 
 int jsvd_server_get_stats(jsvd_server *s, jsvd_server_stats *out)
 {
-    if (!s || !out) return invalid_argument("server and out must not be null.");
-    s->impl->stats(out);
-    return JSVD_OK;
+    return c_entry([&]() -> int {
+        if (!s || !out) return invalid_argument("server and out must not be null.");
+        s->impl->stats(out);
+        return JSVD_OK;
+    });
 }
 
 void jsvd_server_destroy(jsvd_server *s) { delete s; }

@@ -80,3 +80,14 @@ def test_null_input_is_rejected():
 def test_python_wrapper_raises_invalid_argument():
     with pytest.raises(jsvd.InvalidArgument, match="rows >= columns"):
         jsvd.plain_svd(np.zeros((2, 5)))
+
+
+@pytest.mark.parametrize("rows,cols", [(1 << 31, 1), (1 << 30, 1 << 30), (1 << 31, 1 << 31)])
+def test_oversized_dimensions_are_rejected_before_any_access(rows, cols):
+    """Shapes whose byte counts would overflow are refused with
+    JSVD_ERR_OVERFLOW before the (dummy) buffer is touched."""
+    cfg = jsvd.default_config()
+    dummy = ctypes.c_void_p(16)
+    rc = jsvd.lib().jsvd_plain_svd(dummy, rows, cols, ctypes.byref(cfg), None, None, None, None)
+    assert rc == jsvd.JSVD_ERR_OVERFLOW
+    assert jsvd.last_error() == (jsvd.JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range.")

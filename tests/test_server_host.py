@@ -125,3 +125,15 @@ def test_two_concurrent_waits_on_one_ticket():
                                    [jsvd.JSVD_ERR_INVALID_ARGUMENT, jsvd.JSVD_ERR_CUDA]), out
     finally:
         jsvd.lib().jsvd_server_destroy(h)
+
+
+def test_oversized_request_is_rejected_before_copy():
+    h = _server()
+    try:
+        t = ctypes.c_uint64(0)
+        rc = jsvd.lib().jsvd_server_submit(h, ctypes.c_void_p(16), 1 << 31, 1, 0, ctypes.byref(t))
+        assert rc == jsvd.JSVD_ERR_OVERFLOW
+        assert jsvd.last_error()[1] == "Matrix dimensions exceed the supported range."
+        assert _stats(h).submitted == 0
+    finally:
+        jsvd.lib().jsvd_server_destroy(h)
