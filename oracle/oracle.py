@@ -130,7 +130,11 @@ def partial_sweep(a: np.ndarray, eps: float, lanes: int = 256, variant: int = VA
 # ---- metrics -----------------------------------------------------------------
 
 def residuals(a: np.ndarray, u: np.ndarray | None, s: np.ndarray, v: np.ndarray) -> dict:
-    """rho_A, rho_U, rho_V of the reference's validation contract."""
+    """rho_A = ||A - U S V^T||_F / max(1, ||A||_F), rho_U = ||U^T U - I||_F,
+    rho_V = ||V^T V - I||_F, the reference's validation metrics
+    (tex/sections/03-gpu-parallel-reduction.tex:30-40).  rho_U runs over the
+    columns with sigma > 0: the reference writes zero U columns where
+    sigma <= eps (src/kernels.cu:599-627), which carry no orthogonality."""
     out = {}
     n = s.shape[0]
     if u is not None:
