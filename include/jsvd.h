@@ -149,6 +149,22 @@ void jsvd_plain_set_sweep_mode(int mode);
 int jsvd_plain_get_sweep_mode(void);
 void jsvd_plain_stats_reset(void);
 
+/* ---- validation -------------------------------------------------------------
+ * The reference's validation metrics of one result
+ * (tex/sections/03-gpu-parallel-reduction.tex:30-40), computed on the host. */
+typedef struct jsvd_residual_report {
+    double rho_a;     /* ||A - U S V^T||_F / max(1, ||A||_F); -1 when a or u is NULL */
+    double rho_u;     /* ||U^T U - I||_F over the columns with sigma > 0; -1 when u is NULL */
+    double rho_v;     /* ||V^T V - I||_F */
+    double sigma_max; /* largest sigma */
+} jsvd_residual_report;
+
+/* a (optional) rows x columns, u (optional) rows x columns, v columns x
+ * columns, all row-major host buffers as jsvd_plain_svd returns them; sigma
+ * the columns singular values.  Uses the host's threads; no CUDA call. */
+int jsvd_residuals(const double *a, const double *u, const double *sigma, const double *v, size_t rows,
+                   size_t columns, jsvd_residual_report *out);
+
 /* ---- batched solver ---------------------------------------------------------
  * Many independent matrices in one persistent launch per size class.  The
  * reference solves them one call at a time from a host thread pool

@@ -47,6 +47,7 @@ namespace
         bool force = false, dry_run = false, print_config = false, json = false, quiet = false;
         bool help = false, version = false;
         bool precond = false;
+        std::filesystem::path residual_report;  // empty: off
     };
 
     struct Flag
@@ -80,6 +81,8 @@ namespace
         {"json-report", '\0', false, "", "Print execution report in JSON."},
         {"quiet", 'q', false, "", "Suppress text report."},
         {"solver", '\0', true, "NAME", "Large-testcase solver: plain (bit-identical, default) | precond."},
+        {"residual-report", '\0', true, "PATH",
+         "Write each testcase's rows, columns, epsilon, sweeps, rho_A, rho_U, rho_V as a JSON line."},
         {"help", 'h', false, "", "Show this help message."},
         {"version", 'v', false, "", "Show version information."},
     };
@@ -185,6 +188,7 @@ namespace
                 throw ArgError("Invalid value for --solver: expected plain|precond.");
             o.precond = l == "precond";
         }
+        else if (n == "residual-report") o.residual_report = std::string(v);
         else if (n == "help") o.help = true;
         else if (n == "version") o.version = true;
     }
@@ -262,6 +266,9 @@ namespace
             throw ArgError("Output path points to a directory: " + o.output.string());
         if (comparable(o.input) == comparable(o.output))
             throw ArgError("Input and output paths must be different files.");
+        if (!o.residual_report.empty() && (comparable(o.residual_report) == comparable(o.input) ||
+                                           comparable(o.residual_report) == comparable(o.output)))
+            throw ArgError("--residual-report must name a file other than the input and output.");
         if (std::filesystem::exists(o.output) && !o.force)
             throw ArgError("Output file already exists. Use --force to overwrite: " + o.output.string());
     }
@@ -370,7 +377,9 @@ namespace
                   << "layout-bench-swp: " << o.layout_bench_sweeps << '\n'
                   << "queue-capacity  : " << o.queue_capacity << '\n'
                   << "force-overwrite : " << (o.force ? "true" : "false") << '\n'
-                  << "solver          : " << (o.precond ? "precond" : "plain") << '\n';
+                  << "solver          : " << (o.precond ? "precond" : "plain") << '\n'
+                  << "residual-report : " << (o.residual_report.empty() ? "off" : o.residual_report.string())
+                  << '\n';
     }
 } // namespace
 
@@ -403,6 +412,7 @@ int main(int argc, char **argv)
             print_config(o);
             std::cout << '\n';
         }
+        jacobi::svd::pipeline::set_residual_report(o.residual_report);
         jacobi::svd::pipeline::set_large_solver(o.precond ? jacobi::svd::pipeline::LargeSolver::precond
                                                           : jacobi::svd::pipeline::LargeSolver::plain);
         jacobi::svd::pipeline::PipelineConfig cfg;

@@ -13,16 +13,23 @@
 #include <algorithm>
 #include <atomic>
 #include <cctype>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <exception>
+#include <fstream>
+#include <iomanip>
 #include <limits>
+#include <locale>
+#include <memory>
 #include <mutex>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <thread>
 #include <utility>
+#include <vector>
 
 #include "io.hpp"
 #include "jsvd.h"
@@ -135,6 +142,7 @@ namespace jacobi::svd::pipeline
         {
             std::uint64_t ticket;
             std::size_t rows, columns, bytes;
+            std::shared_ptr<const std::vector<double>> input; ///< kept only for the residual report
         };
 
         struct ServerHandle
@@ -151,6 +159,46 @@ namespace jacobi::svd::pipeline
     namespace
     {
         std::atomic<int> g_large_solver{0};
+        std::mutex g_report_mu;
+        std::filesystem::path g_report_path;
+
+        void json_number(std::ostream &os, double x)
+        {
+            if (std::isfinite(x))
+                os << x;
+            else
+                os << "null";
+        }
+    } // namespace
+
+    void set_residual_report(const std::filesystem::path &path)
+    {
+        std::lock_guard<std::mutex> lk(g_report_mu);
+        g_report_path = path;
+    }
+
+    std::filesystem::path residual_report()
+    {
+        std::lock_guard<std::mutex> lk(g_report_mu);
+        return g_report_path;
+    }
+
+    std::string residual_record_json(const ResidualRecord &r)
+    {
+        std::ostringstream os;
+        os.imbue(std::locale::classic());
+        os << std::setprecision(std::numeric_limits<double>::max_digits10);
+        os << "{\"index\": " << r.index << ", \"rows\": " << r.rows << ", \"columns\": " << r.columns
+           << ", \"epsilon\": ";
+        json_number(os, r.epsilon);
+        os << ", \"max_sweeps\": " << r.max_sweeps << ", \"sweeps\": " << r.sweeps << ", \"rho_A\": ";
+        json_number(os, r.rho_a);
+        os << ", \"rho_U\": ";
+        json_number(os, r.rho_u);
+        os << ", \"rho_V\": ";
+        json_number(os, r.rho_v);
+        os << '}';
+        return os.str();
     }
 
     void set_large_solver(LargeSolver solver) noexcept { g_large_solver.store(solver == LargeSolver::precond ? 1 : 0); }
@@ -197,6 +245,15 @@ namespace jacobi::svd::pipeline
             rethrow_status(rc);
 
         OrderedSink sink(config_.output_path, out_fmt);
+        const std::filesystem::path report_path = residual_report();
+        const bool reporting = !report_path.empty();
+        std::ofstream report_out;
+        if (reporting)
+        {
+            report_out.open(report_path, std::ios::out | std::ios::trunc);
+            if (!report_out)
+                throw std::runtime_error("Cannot open residual report file: " + report_path.string());
+        }
         std::mutex mu;
         std::condition_variable cv;
         std::deque<Pending> queue;
@@ -209,7 +266,7 @@ namespace jacobi::svd::pipeline
         std::thread writer([&] {
             try
             {
-                for (;;)
+                for (std::size_t index = 0;; ++index)
                 {
                     Pending p;
                     {
@@ -231,6 +288,25 @@ namespace jacobi::svd::pipeline
                     sink.write(s);
                     sink.write(v);
                     total_sweeps.fetch_add(static_cast<std::size_t>(sweeps));
+                    if (reporting)
+                    {
+                        jsvd_residual_report rr{};
+                        if (const int rrc = jsvd_residuals(p.input->data(), u.values.data(), s.values.data(),
+                                                           v.values.data(), p.rows, p.columns, &rr);
+                            rrc != JSVD_OK)
+                            rethrow_status(rrc);
+                        ResidualRecord rec;
+                        rec.index = index;
+                        rec.rows = p.rows;
+                        rec.columns = p.columns;
+                        rec.epsilon = kernel.epsilon;
+                        rec.max_sweeps = kernel.max_sweeps;
+                        rec.sweeps = sweeps;
+                        rec.rho_a = rr.rho_a;
+                        rec.rho_u = rr.rho_u;
+                        rec.rho_v = rr.rho_v;
+                        report_out << residual_record_json(rec) << '\n';
+                    }
                     {
                         std::lock_guard<std::mutex> lk(mu);
                         queue.pop_front();
@@ -252,7 +328,8 @@ namespace jacobi::svd::pipeline
         std::exception_ptr reader_error;
         auto submit = [&](const io::Matrix &m) {
             validate_testcase(m, submitted);
-            const std::size_t bytes = sizeof(double) * m.values.size();
+            // the residual report keeps a copy of the input until its result is written
+            const std::size_t bytes = sizeof(double) * m.values.size() * (reporting ? 2 : 1);
             {
                 std::unique_lock<std::mutex> lk(mu);
                 cv.wait(lk, [&] {
@@ -266,9 +343,12 @@ namespace jacobi::svd::pipeline
             if (const int rc = jsvd_server_submit(server.s, m.values.data(), m.rows, m.columns, 1, &ticket);
                 rc != JSVD_OK)
                 rethrow_status(rc);
+            std::shared_ptr<const std::vector<double>> input;
+            if (reporting)
+                input = std::make_shared<const std::vector<double>>(m.values);
             {
                 std::lock_guard<std::mutex> lk(mu);
-                queue.push_back({ticket, m.rows, m.columns, bytes});
+                queue.push_back({ticket, m.rows, m.columns, bytes, std::move(input)});
                 queued_bytes += bytes;
             }
             cv.notify_all();
@@ -309,6 +389,12 @@ namespace jacobi::svd::pipeline
         if (writer_error)
             std::rethrow_exception(writer_error);
         sink.flush();
+        if (reporting)
+        {
+            report_out.flush();
+            if (!report_out)
+                throw std::runtime_error("Failed to write residual report file: " + report_path.string());
+        }
 
         PipelineReport report;
         report.testcase_count = submitted;

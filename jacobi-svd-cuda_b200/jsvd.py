@@ -76,6 +76,11 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("max_ctas", ctypes.c_int)]
 
 
+class ResidualReport(ctypes.Structure):
+    _fields_ = [("rho_a", ctypes.c_double), ("rho_u", ctypes.c_double), ("rho_v", ctypes.c_double),
+                ("sigma_max", ctypes.c_double)]
+
+
 class BatchAutotuneReport(ctypes.Structure):
     _fields_ = [
         ("best", BatchTuning * 5),
@@ -165,7 +170,7 @@ def exported_symbols() -> list[str]:
         "jsvd_blocked_svd", "jsvd_blocked_stats_get", "jsvd_blocked_stats_reset", "jsvd_plain_set_sweep_mode",
         "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
-        "jsvd_precond_set_gram_stop", "jsvd_batch_builtin_tuning", "jsvd_batch_autotune",
+        "jsvd_precond_set_gram_stop", "jsvd_batch_builtin_tuning", "jsvd_batch_autotune", "jsvd_residuals",
     ]
 
 
@@ -195,6 +200,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_batch_svd_device.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), P, P, P, P,
                                             ctypes.POINTER(BatchTuning), P]
         L.jsvd_batch_svd_device.restype = I
+        L.jsvd_residuals.argtypes = [P, P, P, P, S, S, ctypes.POINTER(ResidualReport)]
+        L.jsvd_residuals.restype = I
         L.jsvd_batch_builtin_tuning.argtypes = [ctypes.POINTER(BatchTuning)]
         L.jsvd_batch_builtin_tuning.restype = None
         L.jsvd_batch_autotune.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), I, I, I, I,
@@ -488,6 +495,21 @@ class DeviceBatch:
             uk = u[self.a_off[k]: self.a_off[k] + m * n].reshape(m, n) if u is not None else None
             out.append((uk, sk, vk, int(self.sweeps[k])))
         return out
+
+
+def residuals(a, u, s, v) -> dict:
+    """rho_A, rho_U, rho_V and sigma_max of one result (jsvd_residuals, host
+    threads); a and u may be None (their metrics are then -1)."""
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    n = s.shape[0]
+    m = u.shape[0] if u is not None else (a.shape[0] if a is not None else n)
+    a = np.ascontiguousarray(a, dtype=np.float64) if a is not None else None
+    u = np.ascontiguousarray(u, dtype=np.float64) if u is not None else None
+    rep = ResidualReport()
+    check(lib().jsvd_residuals(a.ctypes.data if a is not None else None, u.ctypes.data if u is not None else None,
+                               s.ctypes.data, v.ctypes.data, m, n, ctypes.byref(rep)))
+    return {"rho_A": rep.rho_a, "rho_U": rep.rho_u, "rho_V": rep.rho_v, "sigma_max": rep.sigma_max}
 
 
 def batch_builtin_tuning() -> list[tuple[int, int, int]]:

@@ -6,6 +6,7 @@ whether it ran alone or in a mix of small (batched) and large (per-stream)
 requests.  The CLI pipeline's *.mat output is compared byte for byte with the
 reference CLI's output on the same input (tests/golden/pipeline_*).
 """
+import json
 import os
 import subprocess
 
@@ -14,6 +15,7 @@ import pytest
 
 import jsvd
 import matfile
+import oracle as O
 import workloads as W
 from conftest import GOLDEN, PKG
 
@@ -100,6 +102,32 @@ def test_cli_pipeline_matches_reference_cli_bytes(cuda_device, tmp_path):
     assert r.returncode == 0, r.stderr
     assert out.read_bytes() == open(ref_out, "rb").read()
     assert '"testcase_count": ' in r.stdout
+
+
+def test_cli_residual_report(cuda_device, tmp_path):
+    """--residual-report leaves the output bytes unchanged and writes one
+    record per testcase, in input order, whose sweeps match the oracle and whose
+    rho_A, rho_U, rho_V match the oracle's metrics on the written factors."""
+    inp, ref_out = _golden_pipeline()
+    assert inp is not None, "pipeline golden fixture missing"
+    out = tmp_path / "out.mat"
+    rep = tmp_path / "res.jsonl"
+    r = subprocess.run([CLI, inp, str(out), "-e", "1e-12", "-q", "--residual-report", str(rep)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert out.read_bytes() == open(ref_out, "rb").read()
+    mats = matfile.read(inp)
+    res = matfile.read(str(out))
+    recs = [json.loads(line) for line in rep.read_text().splitlines()]
+    assert len(recs) == len(mats)
+    for k, (a, rec) in enumerate(zip(mats, recs)):
+        u, s, v = res[3 * k], res[3 * k + 1].ravel(), res[3 * k + 2]
+        assert rec["index"] == k and (rec["rows"], rec["columns"]) == a.shape
+        assert rec["epsilon"] == 1e-12 and rec["max_sweeps"] == 128
+        assert rec["sweeps"] == O.plain_svd(a, eps=1e-12, variant=jsvd.arith_variant())[3]
+        ref = O.residuals(a, u, s, v)
+        for key in ("rho_A", "rho_U", "rho_V"):
+            assert abs(rec[key] - ref[key]) <= 1e-14 + 1e-10 * abs(ref[key]), (k, key, rec[key], ref[key])
 
 
 def test_cli_pipeline_txt_roundtrip(cuda_device, tmp_path):
