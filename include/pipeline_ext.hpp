@@ -42,4 +42,18 @@ namespace jacobi::svd::pipeline
     /// run.  Empty (the default) turns this off.  Process-wide setting.
     void set_residual_report(const std::filesystem::path &path);
     [[nodiscard]] std::filesystem::path residual_report();
+
+    /// Serving-core figures of the last pipeline run that completed in this
+    /// process (zeros before the first).
+    struct RunServiceStats
+    {
+        std::size_t batches = 0;           ///< batched launches of small testcases
+        std::size_t batched_testcases = 0; ///< testcases solved in those launches
+        std::size_t large_solves = 0;      ///< testcases solved one per stream
+        double latency_p50_ms = 0.0;       ///< submission to completion
+        double latency_p99_ms = 0.0;
+        double latency_mean_ms = 0.0;
+        std::size_t peak_device_bytes = 0; ///< admitted footprint high-water mark
+    };
+    [[nodiscard]] RunServiceStats last_run_service_stats();
 } // namespace jacobi::svd::pipeline

@@ -460,7 +460,17 @@ int main(int argc, char **argv)
                       << (report.layout_transpose_auto_tuned ? "true" : "false")
                       << ",\n  \"layout_transpose_estimated_best_speedup\": " << std::fixed << std::setprecision(3)
                       << report.layout_transpose_estimated_best_speedup << ",\n  \"elapsed_ms\": " << std::fixed
-                      << std::setprecision(3) << ms << "\n}\n";
+                      << std::setprecision(3) << ms;
+            // serving-core figures of this run (no counterpart in the reference's report)
+            const auto svc = jacobi::svd::pipeline::last_run_service_stats();
+            const double rate = ms > 0.0 ? 1e3 * (double)report.testcase_count / ms : 0.0;
+            std::cout << ",\n  \"testcases_per_s\": " << std::setprecision(3) << rate
+                      << ",\n  \"latency_p50_ms\": " << svc.latency_p50_ms
+                      << ",\n  \"latency_p99_ms\": " << svc.latency_p99_ms
+                      << ",\n  \"latency_mean_ms\": " << svc.latency_mean_ms
+                      << ",\n  \"batches\": " << svc.batches << ",\n  \"batched_testcases\": "
+                      << svc.batched_testcases << ",\n  \"large_solves\": " << svc.large_solves
+                      << ",\n  \"peak_device_bytes\": " << svc.peak_device_bytes << "\n}\n";
         }
         return 0;
     }

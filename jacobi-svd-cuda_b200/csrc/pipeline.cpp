@@ -161,6 +161,7 @@ namespace jacobi::svd::pipeline
         std::atomic<int> g_large_solver{0};
         std::mutex g_report_mu;
         std::filesystem::path g_report_path;
+        RunServiceStats g_last_run; // guarded by g_report_mu
 
         void json_number(std::ostream &os, double x)
         {
@@ -181,6 +182,12 @@ namespace jacobi::svd::pipeline
     {
         std::lock_guard<std::mutex> lk(g_report_mu);
         return g_report_path;
+    }
+
+    RunServiceStats last_run_service_stats()
+    {
+        std::lock_guard<std::mutex> lk(g_report_mu);
+        return g_last_run;
     }
 
     std::string residual_record_json(const ResidualRecord &r)
@@ -394,6 +401,20 @@ namespace jacobi::svd::pipeline
             report_out.flush();
             if (!report_out)
                 throw std::runtime_error("Failed to write residual report file: " + report_path.string());
+        }
+        jsvd_server_stats st{};
+        if (jsvd_server_get_stats(server.s, &st) == JSVD_OK)
+        {
+            RunServiceStats run;
+            run.batches = st.batches;
+            run.batched_testcases = st.batched_requests;
+            run.large_solves = st.large_solves;
+            run.latency_p50_ms = st.p50_ms;
+            run.latency_p99_ms = st.p99_ms;
+            run.latency_mean_ms = st.mean_ms;
+            run.peak_device_bytes = st.peak_device_bytes;
+            std::lock_guard<std::mutex> lk(g_report_mu);
+            g_last_run = run;
         }
 
         PipelineReport report;

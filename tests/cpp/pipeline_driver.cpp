@@ -4,6 +4,7 @@
 //                 with a NaN residual, one per line
 //   report-path P sets the residual report path to P, prints what it reads
 //                 back, clears it and prints the cleared value in brackets
+//   last-run      prints the fields of last_run_service_stats (no run yet)
 #include <cmath>
 #include <iostream>
 #include <limits>
@@ -42,6 +43,13 @@ int main(int argc, char **argv)
         std::cout << residual_report().string() << '\n';
         set_residual_report({});
         std::cout << '[' << residual_report().string() << "]\n";
+        return 0;
+    }
+    if (cmd == "last-run")
+    {
+        const RunServiceStats r = last_run_service_stats();
+        std::cout << r.batches << ' ' << r.batched_testcases << ' ' << r.large_solves << ' ' << r.latency_p50_ms << ' '
+                  << r.latency_p99_ms << ' ' << r.latency_mean_ms << ' ' << r.peak_device_bytes << '\n';
         return 0;
     }
     return 64;

@@ -59,3 +59,8 @@ def test_cli_residual_report_flag(tmp_path):
         assert r.returncode == 2 and "--residual-report must name a file other than" in r.stderr
     r = _cli("-h")
     assert "--residual-report PATH" in r.stdout
+
+
+def test_last_run_stats_are_zero_before_a_run(driver):
+    out = subprocess.run([driver, "last-run"], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["0"] * 7

@@ -101,7 +101,10 @@ def test_cli_pipeline_matches_reference_cli_bytes(cuda_device, tmp_path):
     r = subprocess.run([CLI, inp, str(out), "-e", "1e-12", "--json-report"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert out.read_bytes() == open(ref_out, "rb").read()
-    assert '"testcase_count": ' in r.stdout
+    js = json.loads(r.stdout[r.stdout.index("{"):])  # the text report comes first
+    assert js["testcase_count"] == 12 and js["emitted_matrix_count"] == 36
+    assert js["batched_testcases"] + js["large_solves"] == 12 and js["batches"] >= 1
+    assert js["testcases_per_s"] > 0 and 0 <= js["latency_p50_ms"] <= js["latency_p99_ms"]
 
 
 def test_cli_residual_report(cuda_device, tmp_path):
