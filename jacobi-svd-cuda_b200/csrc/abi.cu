@@ -71,6 +71,34 @@ void note_exception(const char *what) noexcept
     }
 }
 
+int host_buffer_solve(DeviceSolveFn device_fn, const double *a, size_t rows, size_t columns, const jsvd_config *cfg,
+                      double *u, double *sigma, double *v, int *sweeps)
+{
+    set_last_error(JSVD_OK, "");
+    jsvd_config def;
+    jsvd_config_default(&def);
+    const jsvd_config &c = cfg ? *cfg : def;
+    int rc = validate_plain_request(a, rows, columns, c);
+    if (rc != JSVD_OK) return rc;
+    int dev = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    cudaStream_t st = thread_stream(dev);
+    if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+    const size_t mn = rows * columns, nn = columns * columns;
+    double *d = nullptr;
+    JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * (2 * mn + nn + columns), st));
+    ScopeExit free_d([&] { cudaFreeAsync(d, st); });
+    double *da = d, *du = d + mn, *dv = du + mn, *ds = dv + nn;
+    JSVD_CUDA_TRY(cudaMemcpyAsync(da, a, sizeof(double) * mn, cudaMemcpyHostToDevice, st));
+    rc = device_fn(da, rows, columns, &c, u ? du : nullptr, ds, v ? dv : nullptr, sweeps, st);
+    if (rc != JSVD_OK) return rc;
+    if (u) JSVD_CUDA_TRY(cudaMemcpyAsync(u, du, sizeof(double) * mn, cudaMemcpyDeviceToHost, st));
+    if (sigma) JSVD_CUDA_TRY(cudaMemcpyAsync(sigma, ds, sizeof(double) * columns, cudaMemcpyDeviceToHost, st));
+    if (v) JSVD_CUDA_TRY(cudaMemcpyAsync(v, dv, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+    return JSVD_OK;
+}
+
 cudaStream_t thread_stream(int device)
 {
     auto &cache = thread_cache();

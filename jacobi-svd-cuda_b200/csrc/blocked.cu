@@ -351,6 +351,7 @@ int blocked_solve(const double *d_a, int rows, int n, double eps, int max_sweeps
     double *ws = nullptr;
     const size_t doubles = mn + nn + n + part + wbytes;
     JSVD_CUDA_TRY(cudaMallocAsync((void **)&ws, sizeof(double) * doubles + sizeof(int) * (npairs + 2), st));
+    ScopeExit free_ws([&] { cudaFreeAsync(ws, st); });
     double *X = ws, *V = X + mn, *sg = V + nn, *partial = sg + n, *W = partial + part;
     int *flags = reinterpret_cast<int *>(W + wbytes);
     unsigned *counter = reinterpret_cast<unsigned *>(flags + npairs + 1);
@@ -360,9 +361,13 @@ int blocked_solve(const double *d_a, int rows, int n, double eps, int max_sweeps
     JSVD_CUDA_TRY(cudaGetLastError());
     BlockedStats &bs = blocked_stats();
     int executed = 1;
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    ScopeExit destroy_events([&] {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    });
     cudaEventRecord(e0, st);
     if (rounds > 0) {
         for (int s = 0; s < max_sweeps; ++s) {
@@ -395,13 +400,10 @@ int blocked_solve(const double *d_a, int rows, int n, double eps, int max_sweeps
     JSVD_CUDA_TRY(cudaStreamSynchronize(st));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     bs.solves += 1;
     bs.sweeps += (unsigned long long)executed;
     bs.sweep_ms += ms;
     if (sweeps) *sweeps = executed;
-    JSVD_CUDA_TRY(cudaFreeAsync(ws, st));
     return JSVD_OK;
 }
 
@@ -438,30 +440,7 @@ extern "C" int jsvd_blocked_svd(const double *a, size_t rows, size_t columns, co
                                 double *sigma, double *v, int *sweeps)
 {
     return c_entry([&]() -> int {
-        set_last_error(JSVD_OK, "");
-        jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
-        int rc = validate_plain_request(a, rows, columns, c);
-        if (rc != JSVD_OK) return rc;
-        int dev = 0;
-        JSVD_CUDA_TRY(cudaGetDevice(&dev));
-        cudaStream_t st = thread_stream(dev);
-        if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-        const size_t mn = rows * columns, nn = columns * columns;
-        double *d = nullptr;
-        JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * (2 * mn + nn + columns), st));
-        double *da = d, *du = d + mn, *dv = du + mn, *ds = dv + nn;
-        JSVD_CUDA_TRY(cudaMemcpyAsync(da, a, sizeof(double) * mn, cudaMemcpyHostToDevice, st));
-        rc = jsvd_blocked_svd_device(da, rows, columns, &c, u ? du : nullptr, ds, v ? dv : nullptr, sweeps, st);
-        if (rc == JSVD_OK) {
-            if (u) JSVD_CUDA_TRY(cudaMemcpyAsync(u, du, sizeof(double) * mn, cudaMemcpyDeviceToHost, st));
-            if (sigma) JSVD_CUDA_TRY(cudaMemcpyAsync(sigma, ds, sizeof(double) * columns, cudaMemcpyDeviceToHost, st));
-            if (v) JSVD_CUDA_TRY(cudaMemcpyAsync(v, dv, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
-        }
-        cudaFreeAsync(d, st);
-        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
-        return rc;
+        return host_buffer_solve(jsvd_blocked_svd_device, a, rows, columns, cfg, u, sigma, v, sweeps);
     });
 }
 

@@ -12,6 +12,7 @@
 #include <new>
 #include <sstream>
 #include <string>
+#include <utility>
 
 #include "jsvd.h"
 
@@ -19,6 +20,29 @@ namespace jsvd {
 
 void set_last_error(int code, const std::string &message);
 const std::string &last_error_message();
+
+// Calls `release` when the enclosing scope ends, on every return path.
+template <class F>
+class ScopeExit {
+public:
+    explicit ScopeExit(F release) : release_(std::move(release)) {}
+    ScopeExit(const ScopeExit &) = delete;
+    ScopeExit &operator=(const ScopeExit &) = delete;
+    ~ScopeExit() { release_(); }
+
+private:
+    F release_;
+};
+
+// A device-buffer entry point (jsvd_*_svd_device).
+using DeviceSolveFn = int (*)(const double *, size_t, size_t, const jsvd_config *, double *, double *, double *,
+                              int *, void *);
+
+// Host-buffer form of a device-buffer entry point: validates like the plain
+// path, copies A in and the requested outputs back on the calling thread's
+// library stream, synchronously.
+int host_buffer_solve(DeviceSolveFn device_fn, const double *a, size_t rows, size_t columns, const jsvd_config *cfg,
+                      double *u, double *sigma, double *v, int *sweeps);
 
 // Records a C++ exception caught at a C entry point as JSVD_ERR_RUNTIME (the
 // message is dropped if even that cannot be allocated).

@@ -448,13 +448,18 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     cudaEventCreate(&e1);
     cudaEventCreate(&e2);
     cudaEventCreate(&e3);
+    bool cleaned = false;
     auto cleanup = [&]() {
+        if (cleaned) return;
+        cleaned = true;
         if (!plan) cudaFreeAsync(ws, st);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaEventDestroy(e2);
         cudaEventDestroy(e3);
     };
+    // every return below, the early ones of the status macros included, releases them
+    ScopeExit guard([&] { cleanup(); });
     const double one = 1.0, zero = 0.0;
     // Shifted CholeskyQR3 of Xa (rows x n, column-major, overwritten): the
     // orthonormal factor ends in Xb, R = R3 R2 R1 in Ra (upper, column-major);
@@ -616,30 +621,7 @@ extern "C" int jsvd_precond_svd(const double *a, size_t rows, size_t columns, co
                                 double *sigma, double *v, int *sweeps)
 {
     return c_entry([&]() -> int {
-        set_last_error(JSVD_OK, "");
-        jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
-        int rc = validate_plain_request(a, rows, columns, c);
-        if (rc != JSVD_OK) return rc;
-        int dev = 0;
-        JSVD_CUDA_TRY(cudaGetDevice(&dev));
-        cudaStream_t st = thread_stream(dev);
-        if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-        const size_t mn = rows * columns, nn = columns * columns;
-        double *d = nullptr;
-        JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * (2 * mn + nn + columns), st));
-        double *da = d, *du = d + mn, *dv = du + mn, *ds = dv + nn;
-        JSVD_CUDA_TRY(cudaMemcpyAsync(da, a, sizeof(double) * mn, cudaMemcpyHostToDevice, st));
-        rc = jsvd_precond_svd_device(da, rows, columns, &c, u ? du : nullptr, ds, v ? dv : nullptr, sweeps, st);
-        if (rc == JSVD_OK) {
-            if (u) JSVD_CUDA_TRY(cudaMemcpyAsync(u, du, sizeof(double) * mn, cudaMemcpyDeviceToHost, st));
-            if (sigma) JSVD_CUDA_TRY(cudaMemcpyAsync(sigma, ds, sizeof(double) * columns, cudaMemcpyDeviceToHost, st));
-            if (v) JSVD_CUDA_TRY(cudaMemcpyAsync(v, dv, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
-        }
-        cudaFreeAsync(d, st);
-        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
-        return rc;
+        return host_buffer_solve(jsvd_precond_svd_device, a, rows, columns, cfg, u, sigma, v, sweeps);
     });
 }
 
