@@ -449,6 +449,12 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     BatchDesc *d_desc = nullptr;
     int *d_next = nullptr, *d_sweeps = nullptr;
     double *d_ws = nullptr;
+    ScopeExit free_buffers([&] {  // stream-ordered, on every return path
+        if (d_desc) cudaFreeAsync(d_desc, stream);
+        if (d_next) cudaFreeAsync(d_next, stream);
+        if (d_sweeps) cudaFreeAsync(d_sweeps, stream);
+        if (d_ws) cudaFreeAsync(d_ws, stream);
+    });
     JSVD_CUDA_TRY(cudaMallocAsync(&d_desc, sizeof(BatchDesc) * ordered.size(), stream));
     JSVD_CUDA_TRY(cudaMallocAsync(&d_next, sizeof(int) * kClasses, stream));
     JSVD_CUDA_TRY(cudaMallocAsync(&d_sweeps, sizeof(int) * (size_t)count, stream));
@@ -483,10 +489,6 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     JSVD_CUDA_TRY(cudaEventRecord(ts->t1, stream));
     std::vector<int> h_sweeps(count);
     JSVD_CUDA_TRY(cudaMemcpyAsync(h_sweeps.data(), d_sweeps, sizeof(int) * count, cudaMemcpyDeviceToHost, stream));
-    JSVD_CUDA_TRY(cudaFreeAsync(d_desc, stream));
-    JSVD_CUDA_TRY(cudaFreeAsync(d_next, stream));
-    JSVD_CUDA_TRY(cudaFreeAsync(d_sweeps, stream));
-    if (d_ws) JSVD_CUDA_TRY(cudaFreeAsync(d_ws, stream));
     JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ts->t0, ts->t1);
