@@ -149,6 +149,17 @@ void jsvd_plain_set_sweep_mode(int mode);
 int jsvd_plain_get_sweep_mode(void);
 void jsvd_plain_stats_reset(void);
 
+/*
+ * The round-robin pair schedule the kernels follow (reference
+ * src/kernels.cu:637-678): for n columns, rounds = n_e - 1 (n_e = n rounded
+ * up to even; no rounds for n = 1) of n/2 pairs each, written round-major as
+ * (p, q) int pairs.  form 0: the table the plain path uploads; form 1: the
+ * closed form that the kernels deriving their own pairs evaluate.  *needed
+ * (optional) receives 2 * rounds * (n/2); out may be NULL to query it.
+ * 1 <= n <= 65536.  No CUDA call.
+ */
+int jsvd_round_robin_schedule(int n, int form, int *out, size_t capacity, size_t *needed);
+
 /* ---- validation -------------------------------------------------------------
  * The reference's validation metrics of one result
  * (tex/sections/03-gpu-parallel-reduction.tex:30-40), computed on the host. */

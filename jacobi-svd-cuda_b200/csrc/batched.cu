@@ -38,24 +38,6 @@ constexpr int kLanes = 256;      // reduction width T (reference default)
 constexpr int kW = kLanes / 32;  // virtual lanes per physical lane
 constexpr int kClasses = 5;
 
-// Closed-form pair k of round r (fixed-head circle, reference
-// src/kernels.cu:637-678).
-__device__ __forceinline__ int2 batch_pair(int n, int r, int k)
-{
-    const int ne = n + (n & 1);
-    const int L = ne - 1;
-    int i = k;
-    if (n & 1) {
-        const int j = 1 + ((n - 1 + r) % L);
-        const int slot = j < ne / 2 ? j : ne - 1 - j;
-        if (i >= slot) i += 1;
-    }
-    const int i2 = ne - 1 - i;
-    const int p = i == 0 ? 0 : 1 + ((i - 1 - r) % L + L) % L;
-    const int q = 1 + ((i2 - 1 - r) % L + L) % L;
-    return make_int2(p, q);
-}
-
 // Reference-order dot products of columns x, y (length m) by one warp; the
 // totals are valid in lane 0.
 __device__ __forceinline__ void warp_pair_stats(const double *x, const double *y, int m, int lane, double &pp,
@@ -204,7 +186,7 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
                 for (int r = 0; r < rounds; ++r) {
                     // phase 1: dot products, one warp per pair
                     for (int k = warp; k < npairs; k += nwarps) {
-                        const int2 pq = batch_pair(n, r, k);
+                        const int2 pq = round_robin_pair(n, r, k);
                         double pp, qq, pqv;
                         warp_pair_stats(colA(pq.x), colA(pq.y), m, lane, pp, qq, pqv);
                         if (lane == 0) {
@@ -225,7 +207,7 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
                     for (int k = warp; k < npairs; k += nwarps) {
                         const double2 g = st_cs[k];
                         if (g.x == 0.0) continue;
-                        const int2 pq = batch_pair(n, r, k);
+                        const int2 pq = round_robin_pair(n, r, k);
                         warp_rotate(colA(pq.x), colA(pq.y), m, V + (size_t)pq.x * n,
                                     V + (size_t)pq.y * n, n, lane, g.x, g.y);
                     }

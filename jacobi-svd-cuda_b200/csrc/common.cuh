@@ -58,6 +58,30 @@ __host__ __device__ __forceinline__ double rot_q(double c, double s, double x, d
 #endif
 }
 
+// Pair k (0 <= k < n/2) of round r (0 <= r < rounds) of the reference's
+// round-robin schedule (src/kernels.cu:637-678: fixed head, a dummy column for
+// odd n, pair i = (circle[i], circle[ne-1-i])) in closed form: positions
+// 1..ne-1 rotate by one per round, so position i >= 1 holds
+// 1 + ((i - 1 - r) mod (ne - 1)); for odd n the value n is the dummy column
+// and its slot is skipped.  The one definition used by every kernel that
+// derives its pairs instead of reading a table, and by the host-side check
+// (jsvd_round_robin_schedule).
+__host__ __device__ __forceinline__ int2 round_robin_pair(int n, int r, int k)
+{
+    const int ne = n + (n & 1);
+    const int L = ne - 1;
+    int i = k;
+    if (n & 1) {
+        const int j = 1 + ((n - 1 + r) % L);
+        const int slot = j < ne / 2 ? j : ne - 1 - j;
+        if (i >= slot) i += 1;
+    }
+    const int i2 = ne - 1 - i;
+    const int p = i == 0 ? 0 : 1 + ((i - 1 - r) % L + L) % L;
+    const int q = 1 + ((i2 - 1 - r) % L + L) % L;
+    return make_int2(p, q);
+}
+
 // Rutishauser rotation for the 2x2 Gram [pp pq; pq qq]; returns true when the
 // pair rotates.  A pair that does not rotate reports c = 0, s = 0 (a real
 // rotation always has c >= 1/sqrt(2)), which is how the deferred V update

@@ -62,24 +62,6 @@ int noalloc_scratch(int dev, double **out)
     return JSVD_OK;
 }
 
-// Pair k of round r of the fixed-head circle schedule (reference
-// src/kernels.cu:637-678) in closed form: positions 1..ne-1 rotate by one
-// per round, so position i >= 1 holds 1 + ((i - 1 - r) mod (ne - 1)); for odd
-// n the value n is the dummy column and its slot is skipped.
-__device__ __forceinline__ int2 na_pair(int n, int r, int k)
-{
-    const int ne = n + (n & 1);
-    const int L = ne - 1;
-    auto at = [&](int i) -> int { return i == 0 ? 0 : 1 + ((i - 1 - r) % L + L) % L; };
-    int i = k;
-    if (n & 1) {
-        const int j = 1 + ((n - 1 + r) % L);              // position of the dummy
-        const int slot = j < ne / 2 ? j : ne - 1 - j;     // its pair slot
-        if (i >= slot) i += 1;
-    }
-    return make_int2(at(i), at(ne - 1 - i));
-}
-
 constexpr int kTile = 32, kTileRows = 8;
 
 __global__ void __launch_bounds__(kTile *kTileRows)
@@ -169,7 +151,7 @@ __global__ void __launch_bounds__(T) na_round_kernel(double *__restrict__ a, int
     __shared__ double red[T == 32 ? 1 : 3 * T];
     __shared__ double2 rot;
     const int t = threadIdx.x;
-    const int2 pq_idx = na_pair(n, round, blockIdx.x);
+    const int2 pq_idx = round_robin_pair(n, round, blockIdx.x);
     double *__restrict__ ap = a + (size_t)pq_idx.x * m;
     double *__restrict__ aq = a + (size_t)pq_idx.y * m;
     double spp = 0.0, sqq = 0.0, spq = 0.0;

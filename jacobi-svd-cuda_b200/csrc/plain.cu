@@ -223,26 +223,6 @@ __global__ void gram_offdiag_count(const double *__restrict__ G, int n, double e
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
 }
 
-// Pair k of round r of the fixed-head circle schedule in closed form (the
-// same sequence build_schedule tabulates): positions 1..ne-1 rotate by one per
-// round, so position i >= 1 holds 1 + ((i - 1 - r) mod (ne - 1)); for odd n
-// the value n is the dummy column and its slot is skipped.
-__device__ __forceinline__ int2 schedule_pair(int n, int r, int k)
-{
-    const int ne = n + (n & 1);
-    const int L = ne - 1;
-    int i = k;
-    if (n & 1) {
-        const int j = 1 + ((n - 1 + r) % L);
-        const int slot = j < ne / 2 ? j : ne - 1 - j;
-        if (i >= slot) i += 1;
-    }
-    const int i2 = ne - 1 - i;
-    const int p = i == 0 ? 0 : 1 + ((i - 1 - r) % L + L) % L;
-    const int q = 1 + ((i2 - 1 - r) % L + L) % L;
-    return make_int2(p, q);
-}
-
 // Deferred V update: applies every rotation of one sweep to R rows of V
 // (R in {1, 2, 4, 8}, a template parameter so the row loop unrolls).
 // V is column-major (element (row, col) at col*ldv + row); the CTA stages its
@@ -297,7 +277,7 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
             const int k = k0 + j * nb;
             const double2 g = g_cur[j];
             if (k < npairs && g.x != 0.0) {
-                const int2 pq = schedule_pair(n, r, k);
+                const int2 pq = round_robin_pair(n, r, k);
                 double x[R], y[R];
 #pragma unroll
                 for (int h = 0; h < R; ++h) {
@@ -314,7 +294,7 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
         for (int k = k0 + kVpassSlots * nb; k < npairs; k += nb) {
             const double2 g = cs[(size_t)r * npairs + k];
             if (g.x != 0.0) {
-                const int2 pq = schedule_pair(n, r, k);
+                const int2 pq = round_robin_pair(n, r, k);
                 double x[R], y[R];
 #pragma unroll
                 for (int h = 0; h < R; ++h) {
@@ -1027,3 +1007,38 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
 }
 
 }  // namespace jsvd
+
+using namespace jsvd;
+
+extern "C" int jsvd_round_robin_schedule(int n, int form, int *out, size_t capacity, size_t *needed)
+{
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (n < 1 || n > (1 << 16)) return invalid_argument("n must be in [1, 65536].");
+        if (form != 0 && form != 1) return invalid_argument("form must be 0 (table) or 1 (closed form).");
+        const int ne = n + (n & 1);
+        const int rounds = n >= 2 ? ne - 1 : 0, npairs = n / 2;
+        const size_t ints = 2 * (size_t)rounds * (size_t)npairs;
+        if (needed) *needed = ints;
+        if (out == nullptr) return JSVD_OK;
+        if (capacity < ints) return invalid_argument("Schedule buffer too small.");
+        if (form == 0) {
+            std::vector<int2> pairs;
+            int r_out = 0, p_out = 0;
+            build_schedule(n, pairs, r_out, p_out);
+            for (size_t i = 0; i < pairs.size(); ++i) {
+                out[2 * i] = pairs[i].x;
+                out[2 * i + 1] = pairs[i].y;
+            }
+        } else {
+            size_t i = 0;
+            for (int r = 0; r < rounds; ++r)
+                for (int k = 0; k < npairs; ++k, ++i) {
+                    const int2 pq = round_robin_pair(n, r, k);
+                    out[2 * i] = pq.x;
+                    out[2 * i + 1] = pq.y;
+                }
+        }
+        return JSVD_OK;
+    });
+}

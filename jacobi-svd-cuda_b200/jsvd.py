@@ -171,6 +171,7 @@ def exported_symbols() -> list[str]:
         "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
         "jsvd_precond_set_gram_stop", "jsvd_batch_builtin_tuning", "jsvd_batch_autotune", "jsvd_residuals",
+        "jsvd_round_robin_schedule",
     ]
 
 
@@ -200,6 +201,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_batch_svd_device.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), P, P, P, P,
                                             ctypes.POINTER(BatchTuning), P]
         L.jsvd_batch_svd_device.restype = I
+        L.jsvd_round_robin_schedule.argtypes = [I, I, P, S, ctypes.POINTER(S)]
+        L.jsvd_round_robin_schedule.restype = I
         L.jsvd_residuals.argtypes = [P, P, P, P, S, S, ctypes.POINTER(ResidualReport)]
         L.jsvd_residuals.restype = I
         L.jsvd_batch_builtin_tuning.argtypes = [ctypes.POINTER(BatchTuning)]
@@ -510,6 +513,19 @@ def residuals(a, u, s, v) -> dict:
     check(lib().jsvd_residuals(a.ctypes.data if a is not None else None, u.ctypes.data if u is not None else None,
                                s.ctypes.data, v.ctypes.data, m, n, ctypes.byref(rep)))
     return {"rho_A": rep.rho_a, "rho_U": rep.rho_u, "rho_V": rep.rho_v, "sigma_max": rep.sigma_max}
+
+
+def round_robin_schedule(n: int, form: int = 1) -> np.ndarray:
+    """The library's pair schedule for n columns as an array (rounds, n/2, 2):
+    form 0 = the plain path's uploaded table, 1 = the kernels' closed form."""
+    need = ctypes.c_size_t(0)
+    check(lib().jsvd_round_robin_schedule(n, form, None, 0, ctypes.byref(need)))
+    out = np.empty(need.value, dtype=np.int32)
+    check(lib().jsvd_round_robin_schedule(n, form, out.ctypes.data if out.size else None, out.size,
+                                          ctypes.byref(need)))
+    half = n // 2
+    rounds = need.value // (2 * half) if half else 0
+    return out.reshape(rounds, half, 2)
 
 
 def batch_builtin_tuning() -> list[tuple[int, int, int]]:
