@@ -6,6 +6,8 @@
 
 #include <cuda_runtime.h>
 
+#include "kernels_ext.hpp"
+
 #include <new>
 #include <sstream>
 #include <string>
@@ -135,6 +137,15 @@ namespace jacobi::svd
                                          std::size_t columns,
                                          const JacobiSvdConfig &config)
     {
+        return jacobi_svd(host_input, rows, columns, config, SvdSolver::plain);
+    }
+
+    JacobiSvdResult jacobi_svd(std::span<const double> host_input,
+                               std::size_t rows,
+                               std::size_t columns,
+                               const JacobiSvdConfig &config,
+                               SvdSolver solver)
+    {
         // Shape checks in the reference's order; the buffer-size check can only
         // be made here, where the span's length is known.
         if (rows == 0 || columns == 0)
@@ -150,11 +161,49 @@ namespace jacobi::svd
         result.u.resize(rows * columns);
         result.sigma.resize(columns);
         result.v.resize(columns * columns);
-        const int rc = jsvd_plain_svd(host_input.data(), rows, columns, &c, result.u.data(), result.sigma.data(),
-                                      result.v.data(), &result.sweeps);
+        using HostEntry = int (*)(const double *, std::size_t, std::size_t, const jsvd_config *, double *, double *,
+                                  double *, int *);
+        HostEntry entry = jsvd_plain_svd;
+        switch (solver)
+        {
+        case SvdSolver::plain:
+            entry = jsvd_plain_svd;
+            break;
+        case SvdSolver::precond:
+            entry = jsvd_precond_svd;
+            break;
+        case SvdSolver::blockpair:
+            entry = jsvd_blockpair_svd;
+            break;
+        case SvdSolver::blocked:
+            entry = jsvd_blocked_svd;
+            break;
+        default:
+            throw std::invalid_argument("Unknown SvdSolver.");
+        }
+        const int rc = entry(host_input.data(), rows, columns, &c, result.u.data(), result.sigma.data(),
+                             result.v.data(), &result.sweeps);
         if (rc != JSVD_OK)
             rethrow_status(rc);
         return result;
+    }
+
+    SvdResiduals residuals(std::span<const double> host_input, const JacobiSvdResult &result)
+    {
+        const std::size_t m = result.rows, n = result.columns;
+        if (m == 0 || n == 0)
+            throw std::invalid_argument("Input matrix shape must be non-zero.");
+        if (m < n)
+            throw std::invalid_argument("One-sided Jacobi SVD requires rows >= columns in this implementation.");
+        if (host_input.size() != m * n || result.u.size() != m * n || result.sigma.size() != n ||
+            result.v.size() != n * n)
+            throw std::invalid_argument("Result buffers do not match rows and columns.");
+        jsvd_residual_report r{};
+        const int rc = jsvd_residuals(host_input.data(), result.u.data(), result.sigma.data(), result.v.data(), m, n,
+                                      &r);
+        if (rc != JSVD_OK)
+            rethrow_status(rc);
+        return SvdResiduals{r.rho_a, r.rho_u, r.rho_v};
     }
 
     LayoutTransposeAutoTuneReport auto_tune_layout_transpose_threshold(const JacobiSvdConfig &config)

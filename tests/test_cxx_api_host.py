@@ -1,0 +1,57 @@
+"""The jacobi::svd C++ extensions (include/kernels_ext.hpp) on the host (no
+GPU): every solver validates like one_sided_jacobi_svd and throws the
+reference's exception types before any CUDA call, and residuals() agrees with
+the oracle's restatement of the reference's validation metrics."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import PKG, ROOT
+
+DRIVER = os.path.join(ROOT, "tests", "cpp", "api_driver.cpp")
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    out = tmp_path_factory.mktemp("api") / "api_driver"
+    subprocess.check_call(["g++", "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include"),
+                           "-I/usr/local/cuda/include", DRIVER, "-o", str(out), "-L", PKG, "-ljsvd",
+                           f"-Wl,-rpath,{PKG}"])
+    return str(out)
+
+
+def test_every_solver_validates_like_the_reference(driver):
+    out = subprocess.run([driver, "validate"], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert len(out) == 12
+    for k, solver in enumerate(["plain", "precond", "blockpair", "blocked"]):
+        assert out[3 * k] == f"{solver} invalid_argument " \
+                             "One-sided Jacobi SVD requires rows >= columns in this implementation."
+        assert out[3 * k + 1] == f"{solver} invalid_argument Input buffer size mismatch."
+        assert out[3 * k + 2] == f"{solver} invalid_argument epsilon must be positive."
+
+
+@pytest.mark.parametrize("m,n", [(3, 2), (30, 17), (64, 64)])
+def test_residuals_match_oracle(driver, tmp_path, m, n):
+    rng = np.random.default_rng(m * 100 + n)
+    a = rng.standard_normal((m, n))
+    uu, s, vt = np.linalg.svd(a, full_matrices=False)
+    u = uu + 1e-9 * rng.standard_normal(uu.shape)
+    v = vt.T + 1e-8 * rng.standard_normal((n, n))
+    f = tmp_path / "case.txt"
+    with open(f, "w") as fh:
+        fh.write(f"{m} {n}\n")
+        for arr in (a, u, s, v):
+            fh.write(" ".join(repr(float(x)) for x in np.ravel(arr)) + "\n")
+    got = [float(x) for x in subprocess.run([driver, "residuals", str(f)], capture_output=True, text=True,
+                                            check=True).stdout.split()]
+    ref = O.residuals(a, u, s, v)
+    for g, key in zip(got, ("rho_A", "rho_U", "rho_V")):
+        assert abs(g - ref[key]) <= 1e-14 + 1e-10 * ref[key], (key, g, ref[key])
+
+
+def test_residuals_reject_mismatched_result(driver):
+    out = subprocess.run([driver, "bad-result"], capture_output=True, text=True, check=True).stdout.strip()
+    assert out == "Result buffers do not match rows and columns."
