@@ -195,6 +195,8 @@ int plain_device_impl(const double *d_a, size_t rows, size_t cols, const jsvd_co
     const jsvd_config &c = cfg ? *cfg : def;
     int rc = validate_plain_request(d_a, rows, cols, c);
     if (rc != JSVD_OK) return rc;
+    rc = check_plain_columns(cols);
+    if (rc != JSVD_OK) return rc;
     int dev = 0;
     JSVD_CUDA_TRY(cudaGetDevice(&dev));
     if (stream == nullptr) {
@@ -284,6 +286,8 @@ int jsvd_plain_svd(const double *a, size_t rows, size_t columns, const jsvd_conf
         jsvd_config_default(&def);
         const jsvd_config &c = cfg ? *cfg : def;
         int rc = validate_plain_request(a, rows, columns, c);
+        if (rc != JSVD_OK) return rc;
+        rc = check_plain_columns(columns);
         if (rc != JSVD_OK) return rc;
         int dev = 0;
         JSVD_CUDA_TRY(cudaGetDevice(&dev));

@@ -682,7 +682,7 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
         JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
         // V pass geometry: R rows of V per CTA (R in {1,2,4,8}), about n/128 so
         // the grid covers the SMs, capped by 200 KB of shared memory.
-        const size_t smem_cap = 200 * 1024;
+        const size_t smem_cap = kVpassSmemCap;
         const int rmax = (int)std::max<size_t>(1, smem_cap / (sizeof(double) * n_));
         int R = 1;
         while (R * 2 <= 8 && R * 2 <= rmax && (size_t)(R * 2) * 128 <= n_) R *= 2;
@@ -1006,6 +1006,16 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
     return JSVD_OK;
 }
 
+}  // namespace jsvd
+
+namespace jsvd {
+int check_plain_columns(size_t columns)
+{
+    if (columns <= kPlainMaxColumns) return JSVD_OK;
+    set_last_error(JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range: the plain sweep takes at most " +
+                                          std::to_string(kPlainMaxColumns) + " columns.");
+    return JSVD_ERR_OVERFLOW;
+}
 }  // namespace jsvd
 
 using namespace jsvd;

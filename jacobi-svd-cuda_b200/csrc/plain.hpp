@@ -14,6 +14,16 @@
 
 namespace jsvd {
 
+// The deferred V pass keeps R >= 1 whole rows of V in one CTA's shared memory,
+// at most this many bytes: the plain sweep takes at most
+// kVpassSmemCap / 8 = 25600 columns.
+constexpr size_t kVpassSmemCap = 200 * 1024;
+constexpr size_t kPlainMaxColumns = kVpassSmemCap / sizeof(double);
+
+// JSVD_OK, or JSVD_ERR_OVERFLOW with a message when `columns` is above
+// kPlainMaxColumns (checked before any CUDA call).
+int check_plain_columns(size_t columns);
+
 struct PlainPlan {
     int device = -1;
     cudaStream_t stream = nullptr;  // allocation / release stream (the creating thread's)
