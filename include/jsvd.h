@@ -147,6 +147,13 @@ void jsvd_plain_stats_get(jsvd_plain_stats *out);
  * 2.6 us, mode 3 2.9 us, mode 2 3.9 us, mode 1 6.9 us. */
 void jsvd_plain_set_sweep_mode(int mode);
 int jsvd_plain_get_sweep_mode(void);
+
+/* Forces (1) or releases (0) the in-place global-memory form of the plain
+ * path's deferred V pass for plans created afterwards.  That form is used by
+ * itself for more than 25600 columns, where a row of V does not fit a CTA's
+ * shared memory; results are the same bytes either way.  Process-wide; for
+ * tests. */
+void jsvd_plain_set_vpass_in_global(int enable);
 void jsvd_plain_stats_reset(void);
 
 /*

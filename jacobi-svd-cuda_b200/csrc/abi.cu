@@ -130,7 +130,8 @@ int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t strea
     auto &plans = thread_cache().plans;
     for (size_t i = 0; i < plans.size(); ++i) {
         PlainPlan *p = plans[i].get();
-        if (p->device == dev && p->m == m && p->n == n && p->T == T && p->eps == eps && p->mode == sweep_mode()) {
+        if (p->device == dev && p->m == m && p->n == n && p->T == T && p->eps == eps && p->mode == sweep_mode() &&
+            p->vpass_global_forced == vpass_global_forced()) {
             std::rotate(plans.begin() + i, plans.begin() + i + 1, plans.end());
             *out = plans.back().get();
             return JSVD_OK;
@@ -194,8 +195,6 @@ int plain_device_impl(const double *d_a, size_t rows, size_t cols, const jsvd_co
     jsvd_config_default(&def);
     const jsvd_config &c = cfg ? *cfg : def;
     int rc = validate_plain_request(d_a, rows, cols, c);
-    if (rc != JSVD_OK) return rc;
-    rc = check_plain_columns(cols);
     if (rc != JSVD_OK) return rc;
     int dev = 0;
     JSVD_CUDA_TRY(cudaGetDevice(&dev));
@@ -286,8 +285,6 @@ int jsvd_plain_svd(const double *a, size_t rows, size_t columns, const jsvd_conf
         jsvd_config_default(&def);
         const jsvd_config &c = cfg ? *cfg : def;
         int rc = validate_plain_request(a, rows, columns, c);
-        if (rc != JSVD_OK) return rc;
-        rc = check_plain_columns(columns);
         if (rc != JSVD_OK) return rc;
         int dev = 0;
         JSVD_CUDA_TRY(cudaGetDevice(&dev));
@@ -399,6 +396,8 @@ void jsvd_plain_stats_reset(void) { plain_stats() = PlainStats{}; }
 void jsvd_plain_set_sweep_mode(int mode) { set_sweep_mode(mode); }
 
 int jsvd_plain_get_sweep_mode(void) { return sweep_mode(); }
+
+void jsvd_plain_set_vpass_in_global(int enable) { set_vpass_global_forced(enable != 0); }
 
 void jsvd_release_thread_cache(void)
 {

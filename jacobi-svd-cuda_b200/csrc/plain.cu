@@ -232,9 +232,14 @@ __global__ void gram_offdiag_count(const double *__restrict__ G, int n, double e
 // same bank (which a column-by-column staging with R = 8 would cause).
 // Thread k owns pair slot k of every round; the (c, s) of the next round is
 // loaded while the current one is applied.
+// kStaged = false (R = 1) is the form for V rows too long for shared memory:
+// the CTA rotates its row of V in place in global memory; the pairs of a
+// round are disjoint and the barrier between rounds makes each round's global
+// stores visible to the block, so the sequence of rotations per element, and
+// so the result, is the same.
 constexpr int kVpassSlots = 8;  // prefetched pair slots per thread and round
 
-template <int R>
+template <int R, bool kStaged>
 __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v, long ldv, int n,
                                                           const double2 *__restrict__ cs, int rounds, int npairs)
 {
@@ -242,11 +247,18 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
     const int r0 = blockIdx.x * R;
     const int rows = min(R, n - r0);
     const int total = n * R;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx / R, rr = idx - col * R;
-        sv[rr * n + col] = (rr < rows) ? v[(size_t)col * ldv + r0 + rr] : 0.0;
+    // element (h, col) of this CTA's rows of V
+    auto elem = [&](int h, int col) -> double & {
+        if constexpr (kStaged) return sv[h * n + col];
+        else return v[(size_t)col * ldv + r0 + h];
+    };
+    if constexpr (kStaged) {
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            const int col = idx / R, rr = idx - col * R;
+            sv[rr * n + col] = (rr < rows) ? v[(size_t)col * ldv + r0 + rr] : 0.0;
+        }
+        __syncthreads();
     }
-    __syncthreads();
     // Thread k0 owns pair slots k0, k0 + blockDim.x, ...: the (c, s) of its
     // first kVpassSlots slots for round r + 1 are loaded while round r is
     // applied, so a round waits on one L2 round trip, not one per slot (the
@@ -281,13 +293,13 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
                 double x[R], y[R];
 #pragma unroll
                 for (int h = 0; h < R; ++h) {
-                    x[h] = sv[h * n + pq.x];
-                    y[h] = sv[h * n + pq.y];
+                    x[h] = elem(h, pq.x);
+                    y[h] = elem(h, pq.y);
                 }
 #pragma unroll
                 for (int h = 0; h < R; ++h) {
-                    sv[h * n + pq.x] = rot_p(g.x, g.y, x[h], y[h]);
-                    sv[h * n + pq.y] = rot_q(g.x, g.y, x[h], y[h]);
+                    elem(h, pq.x) = rot_p(g.x, g.y, x[h], y[h]);
+                    elem(h, pq.y) = rot_q(g.x, g.y, x[h], y[h]);
                 }
             }
         }
@@ -298,21 +310,23 @@ __global__ void __launch_bounds__(512) plain_vpass_kernel(double *__restrict__ v
                 double x[R], y[R];
 #pragma unroll
                 for (int h = 0; h < R; ++h) {
-                    x[h] = sv[h * n + pq.x];
-                    y[h] = sv[h * n + pq.y];
+                    x[h] = elem(h, pq.x);
+                    y[h] = elem(h, pq.y);
                 }
 #pragma unroll
                 for (int h = 0; h < R; ++h) {
-                    sv[h * n + pq.x] = rot_p(g.x, g.y, x[h], y[h]);
-                    sv[h * n + pq.y] = rot_q(g.x, g.y, x[h], y[h]);
+                    elem(h, pq.x) = rot_p(g.x, g.y, x[h], y[h]);
+                    elem(h, pq.y) = rot_q(g.x, g.y, x[h], y[h]);
                 }
             }
         }
         __syncthreads();
     }
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx / R, rr = idx - col * R;
-        if (rr < rows) v[(size_t)col * ldv + r0 + rr] = sv[rr * n + col];
+    if constexpr (kStaged) {
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            const int col = idx / R, rr = idx - col * R;
+            if (rr < rows) v[(size_t)col * ldv + r0 + rr] = sv[rr * n + col];
+        }
     }
 }
 
@@ -523,13 +537,14 @@ using RoundFn = void (*)(double *, long, int, const int2 *, double2 *, double, u
 using SigmaFn = void (*)(const double *, long, int, double *);
 using VpassFn = void (*)(double *, long, int, const double2 *, int, int);
 
-VpassFn pick_vpass(int R)
+VpassFn pick_vpass(int R, bool staged)
 {
+    if (!staged) return plain_vpass_kernel<1, false>;
     switch (R) {
-    case 1: return plain_vpass_kernel<1>;
-    case 2: return plain_vpass_kernel<2>;
-    case 4: return plain_vpass_kernel<4>;
-    default: return plain_vpass_kernel<8>;
+    case 1: return plain_vpass_kernel<1, true>;
+    case 2: return plain_vpass_kernel<2, true>;
+    case 4: return plain_vpass_kernel<4, true>;
+    default: return plain_vpass_kernel<8, true>;
     }
 }
 
@@ -607,7 +622,11 @@ void build_schedule(int n, std::vector<int2> &pairs, int &rounds, int &npairs)
 
 namespace {
 std::atomic<int> g_sweep_mode{0};
-}
+std::atomic<int> g_vpass_global{0};
+}  // namespace
+
+bool vpass_global_forced() { return g_vpass_global.load() != 0; }
+void set_vpass_global_forced(bool on) { g_vpass_global.store(on ? 1 : 0); }
 
 int sweep_mode() { return g_sweep_mode.load(); }
 void set_sweep_mode(int mode) { g_sweep_mode.store(mode >= 0 && mode <= 3 ? mode : 0); }
@@ -682,18 +701,23 @@ int PlainPlan::create(int dev, size_t m_, size_t n_, int T_, double eps_, cudaSt
         JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
         // V pass geometry: R rows of V per CTA (R in {1,2,4,8}), about n/128 so
         // the grid covers the SMs, capped by 200 KB of shared memory.
+        // Rows of more than kVpassSmemCap bytes (n > 25600), or the forced
+        // global form: one row per CTA, rotated in place in global memory.
         const size_t smem_cap = kVpassSmemCap;
+        plan->vpass_global_forced = jsvd::vpass_global_forced();
+        plan->vpass_staged = !plan->vpass_global_forced && sizeof(double) * n_ <= smem_cap;
         const int rmax = (int)std::max<size_t>(1, smem_cap / (sizeof(double) * n_));
         int R = 1;
-        while (R * 2 <= 8 && R * 2 <= rmax && (size_t)(R * 2) * 128 <= n_) R *= 2;
+        while (plan->vpass_staged && R * 2 <= 8 && R * 2 <= rmax && (size_t)(R * 2) * 128 <= n_) R *= 2;
         plan->vpass_rows = R;
-        plan->vpass_smem = (int)(sizeof(double) * n_ * R);
+        plan->vpass_smem = plan->vpass_staged ? (int)(sizeof(double) * n_ * R) : 0;
         plan->vpass_threads = std::min(512, std::max(32, (plan->npairs + 31) / 32 * 32));
         // The attribute is per function and process-wide: always raise it to the
         // fixed cap, never to this plan's size, or a plan created concurrently
         // on another thread could lower it under a larger plan's launch.
-        JSVD_CUDA_TRY(
-            cudaFuncSetAttribute(pick_vpass(R), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+        if (plan->vpass_staged)
+            JSVD_CUDA_TRY(cudaFuncSetAttribute(pick_vpass(R, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem_cap));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_begin));
         JSVD_CUDA_TRY(cudaEventCreate(&plan->ev_round_end));
         // Persistent sweep when the whole grid can be co-resident.
@@ -753,8 +777,8 @@ int PlainPlan::enqueue_rounds(cudaStream_t st, int parity)
 int PlainPlan::enqueue_vpass(cudaStream_t st, int parity)
 {
     const int vgrid = (int)((n + vpass_rows - 1) / vpass_rows);
-    pick_vpass(vpass_rows)<<<vgrid, vpass_threads, vpass_smem, st>>>(v_w, ldv, (int)n, parity ? cs2 : cs, rounds,
-                                                                      npairs);
+    pick_vpass(vpass_rows, vpass_staged)<<<vgrid, vpass_threads, vpass_smem, st>>>(v_w, ldv, (int)n,
+                                                                                    parity ? cs2 : cs, rounds, npairs);
     JSVD_CUDA_TRY(cudaGetLastError());
     return JSVD_OK;
 }
@@ -1006,16 +1030,6 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
     return JSVD_OK;
 }
 
-}  // namespace jsvd
-
-namespace jsvd {
-int check_plain_columns(size_t columns)
-{
-    if (columns <= kPlainMaxColumns) return JSVD_OK;
-    set_last_error(JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range: the plain sweep takes at most " +
-                                          std::to_string(kPlainMaxColumns) + " columns.");
-    return JSVD_ERR_OVERFLOW;
-}
 }  // namespace jsvd
 
 using namespace jsvd;

@@ -15,14 +15,14 @@
 namespace jsvd {
 
 // The deferred V pass keeps R >= 1 whole rows of V in one CTA's shared memory,
-// at most this many bytes: the plain sweep takes at most
-// kVpassSmemCap / 8 = 25600 columns.
+// at most this many bytes; longer rows (more than 25600 columns) are rotated
+// in place in global memory, one row per CTA.
 constexpr size_t kVpassSmemCap = 200 * 1024;
-constexpr size_t kPlainMaxColumns = kVpassSmemCap / sizeof(double);
 
-// JSVD_OK, or JSVD_ERR_OVERFLOW with a message when `columns` is above
-// kPlainMaxColumns (checked before any CUDA call).
-int check_plain_columns(size_t columns);
+// Forces the in-place global-memory form of the V pass for plans created
+// afterwards (process-wide; part of the plan cache key).  For tests.
+bool vpass_global_forced();
+void set_vpass_global_forced(bool on);
 
 struct PlainPlan {
     int device = -1;
@@ -33,6 +33,8 @@ struct PlainPlan {
     long lda = 0, ldv = 0;
     int rounds = 0, npairs = 0;
     int vpass_rows = 1, vpass_smem = 0, vpass_threads = 256;
+    bool vpass_staged = true;          // rows of V staged in shared memory (else rotated in global memory)
+    bool vpass_global_forced = false;  // created under set_vpass_global_forced(true)
     size_t bytes = 0;
 
     double *a_w = nullptr;      // column-major working copy of A (m x n)

@@ -604,8 +604,6 @@ extern "C" int jsvd_precond_svd_device(const double *d_a, size_t rows, size_t co
         const jsvd_config &c = cfg ? *cfg : def;
         int rc = validate_plain_request(d_a, rows, columns, c);
         if (rc != JSVD_OK) return rc;
-        rc = check_plain_columns(columns);  // the Jacobi stage runs the plain sweep on an n x n factor
-        if (rc != JSVD_OK) return rc;
         int dev = 0;
         JSVD_CUDA_TRY(cudaGetDevice(&dev));
         cudaStream_t st = (cudaStream_t)stream;
@@ -623,8 +621,6 @@ extern "C" int jsvd_precond_svd(const double *a, size_t rows, size_t columns, co
                                 double *sigma, double *v, int *sweeps)
 {
     return c_entry([&]() -> int {
-        const int rc = check_plain_columns(columns);
-        if (rc != JSVD_OK) return rc;
         return host_buffer_solve(jsvd_precond_svd_device, a, rows, columns, cfg, u, sigma, v, sweeps);
     });
 }

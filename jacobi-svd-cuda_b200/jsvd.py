@@ -171,7 +171,7 @@ def exported_symbols() -> list[str]:
         "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
         "jsvd_precond_set_gram_stop", "jsvd_batch_builtin_tuning", "jsvd_batch_autotune", "jsvd_residuals",
-        "jsvd_round_robin_schedule",
+        "jsvd_round_robin_schedule", "jsvd_plain_set_vpass_in_global",
     ]
 
 
@@ -201,6 +201,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_batch_svd_device.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), P, P, P, P,
                                             ctypes.POINTER(BatchTuning), P]
         L.jsvd_batch_svd_device.restype = I
+        L.jsvd_plain_set_vpass_in_global.argtypes = [I]
+        L.jsvd_plain_set_vpass_in_global.restype = None
         L.jsvd_round_robin_schedule.argtypes = [I, I, P, S, ctypes.POINTER(S)]
         L.jsvd_round_robin_schedule.restype = I
         L.jsvd_residuals.argtypes = [P, P, P, P, S, S, ctypes.POINTER(ResidualReport)]
@@ -414,6 +416,13 @@ def plain_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None 
                                      stream or None)
     check(rc)
     return sw.value
+
+
+def set_vpass_in_global(enable: bool) -> None:
+    """Forces the plain path's deferred V pass to rotate V in place in global
+    memory (the form used by itself above 25600 columns) for plans created
+    afterwards; same bytes either way."""
+    lib().jsvd_plain_set_vpass_in_global(1 if enable else 0)
 
 
 def set_sweep_mode(mode: int) -> None:

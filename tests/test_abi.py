@@ -91,20 +91,3 @@ def test_oversized_dimensions_are_rejected_before_any_access(rows, cols):
     rc = jsvd.lib().jsvd_plain_svd(dummy, rows, cols, ctypes.byref(cfg), None, None, None, None)
     assert rc == jsvd.JSVD_ERR_OVERFLOW
     assert jsvd.last_error() == (jsvd.JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range.")
-
-
-@pytest.mark.parametrize("entry", ["jsvd_plain_svd", "jsvd_plain_svd_device", "jsvd_precond_svd",
-                                   "jsvd_precond_svd_device"])
-def test_columns_above_the_plain_limit_are_refused_before_cuda(entry):
-    """The plain sweep's V pass keeps a row of V in 200 KiB of shared memory:
-    more than 25600 columns are refused up front with JSVD_ERR_OVERFLOW (no
-    CUDA call, the dummy buffer is never touched)."""
-    cfg = jsvd.default_config()
-    fn = getattr(jsvd.lib(), entry)
-    dummy = ctypes.c_void_p(16)
-    args = [dummy, 25601, 25601, ctypes.byref(cfg), None, None, None, None]
-    if entry.endswith("_device"):
-        args.append(None)
-    assert fn(*args) == jsvd.JSVD_ERR_OVERFLOW
-    assert jsvd.last_error() == (jsvd.JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range: the plain "
-                                                         "sweep takes at most 25600 columns.")

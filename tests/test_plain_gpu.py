@@ -153,6 +153,41 @@ def test_plain_persistent_sweep_bitwise(cuda_device, m, n):
     _assert_bitwise(got, _oracle(a, eps))
 
 
+@pytest.mark.parametrize("m,n", [(17, 9), (300, 257), (600, 600), (1100, 64)])
+def test_plain_vpass_in_global_memory_bitwise(cuda_device, m, n):
+    """The V pass that rotates V in place in global memory (used by itself
+    above 25600 columns, where a row of V does not fit shared memory; forced
+    here) gives the same bytes, on the first call (direct launches) and the
+    second (captured sweep graph)."""
+    a = W.gaussian_splitmix(m, n, seed=5151 + m + 7 * n)
+    cfg = jsvd.default_config(epsilon=1e-13)
+    jsvd.set_vpass_in_global(True)
+    try:
+        first = jsvd.plain_svd(a, cfg)
+        second = jsvd.plain_svd(a, cfg)
+    finally:
+        jsvd.set_vpass_in_global(False)
+    exp = _oracle(a, 1e-13)
+    _assert_bitwise(first, exp)
+    _assert_bitwise(second, exp)
+
+
+def test_precond_with_vpass_in_global_memory_identical(cuda_device):
+    """The preconditioned path's Jacobi stage through the global-memory V pass
+    gives the same bytes as through the staged one."""
+    a = W.gaussian_splitmix(700, 300, seed=6262)
+    cfg = jsvd.default_config(epsilon=1e-13)
+    ref = jsvd.precond_svd(a, cfg)
+    jsvd.set_vpass_in_global(True)
+    try:
+        got = jsvd.precond_svd(a, cfg)
+    finally:
+        jsvd.set_vpass_in_global(False)
+    assert got[3] == ref[3]
+    for x, y in zip(got[:3], ref[:3]):
+        assert np.array_equal(x, y)
+
+
 def test_plain_rounds_with_pdl_bitwise(cuda_device):
     """Sweep mode 2 (programmatic dependent launch between rounds) gives the
     same bytes."""
