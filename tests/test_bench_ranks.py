@@ -87,3 +87,35 @@ def test_nominal_rate_model():
     assert bench.nominal_rate(512, 512, 14, None) is None
     one = bench.batch_flops(np.array([512]), np.array([512]), np.array([14]))
     assert one == pytest.approx(f)
+
+
+def test_cpu_baseline_contract_fields():
+    """The cpu_baseline object of the bench line: the oracle on a bounded
+    sample of rounds, extrapolated; kind "port", the threads used as cores."""
+    import numpy as np
+
+    rng = np.random.default_rng(1)
+    wl = {"name": "t", "a": rng.standard_normal((300, 101)), "eps": 1e-14}
+    cb = bench.cpu_baseline(wl, sweeps=10, budget_s=0.2, threads=2)
+    assert cb["unit"] == "SVD/s" and cb["kind"] == "port" and cb["cores"] == 2
+    assert cb["value"] > 0 and "rounds of one sweep of the same 300x101 input" in cb["sample"]
+    assert "x 10 sweeps" in cb["sample"]
+
+
+def test_rounds_per_sweep_used_for_extrapolation():
+    """cpu_baseline extrapolates over n - 1 rounds (even n) or n rounds (odd
+    n): the schedule's round count."""
+    import oracle as O
+
+    for n in (2, 3, 10, 11, 64, 65):
+        assert len(O.schedule(n)) == (n - 1 if n % 2 == 0 else n)
+
+
+def test_batch_cpu_baseline_contract_fields():
+    import numpy as np
+
+    rng = np.random.default_rng(2)
+    mats = [rng.standard_normal((20 + k, 8 + k % 5)).astype(np.float32) for k in range(40)]
+    cb = bench.batch_cpu_baseline(mats, budget_s=0.05, threads=2)
+    assert cb["unit"] == "SVD/s" and cb["kind"] == "port" and cb["cores"] == 2 and cb["value"] > 0
+    assert cb["sample"].startswith("first ") and "of 40 matrices" in cb["sample"]
