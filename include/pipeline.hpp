@@ -28,7 +28,11 @@ namespace jacobi::svd::pipeline
         std::filesystem::path output_path;
         MatrixFileFormat input_format = MatrixFileFormat::auto_detect;
         MatrixFileFormat output_format = MatrixFileFormat::auto_detect;
-        /// Bound on testcases in flight between reader and ordered writer.
+        /// Accepted for source compatibility (the reference's in-flight bound).
+        /// Here the serving core sets the window: at most 8192 testcases and
+        /// 4 GiB of inputs in flight, because small testcases are batched
+        /// into one launch and a window of a few would leave them unbatched.
+        /// Output order is the input order either way.
         std::size_t max_queued_results = 4;
         JacobiSvdConfig kernel_config{};
     };
