@@ -2,9 +2,9 @@
 
 Every matrix of a batch uses the plain path's arithmetic, so each result must
 be bit-identical to the oracle on the same FP64 (or FP32-promoted) input:
-same sigma, U and V bytes and sweep count.  The batch spans all four size
-classes (<= 48 KiB, <= 100 KiB, <= 227 KiB of shared memory, and the global
-memory class) and odd/even n.
+same sigma, U and V bytes and sweep count.  The batches span the five size
+classes (A and V in <= 48 KiB, <= 100 KiB, <= ~226 KiB of shared memory; A
+alone in shared memory; A and V in global memory) and odd/even n.
 """
 import numpy as np
 import pytest
