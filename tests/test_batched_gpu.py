@@ -16,7 +16,7 @@ import workloads as W
 pytestmark = pytest.mark.gpu
 
 SHAPES = [(16, 8), (17, 17), (40, 33), (60, 50), (31, 1), (2, 2), (100, 90), (120, 100), (129, 64),
-          (256, 200), (256, 256), (250, 131), (8, 8), (64, 63), (200, 9)]
+          (256, 200), (256, 256), (250, 131), (8, 8), (64, 63), (200, 9), (160, 120), (161, 117)]
 
 
 def _mats(seed, f32):
