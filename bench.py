@@ -732,11 +732,12 @@ def run_reference(args):
                 vals.append(cb["value"])
         value = statistics.mean(vals)
         cb["value"] = value
-        return {"impl": "reference", "metric": "SVDs/s", "value": value, "unit": "SVD/s", "n_gpus": 0,
+        return {"impl": "reference", "metric": "SVDs/s", "value": value, "unit": "SVD/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                 "config": {"workload": "batch (FP32-stored, m~U{16..256}, n~U{8..m}), sample of the same "
-                                       "distribution", "path": "FP64 host oracle"},
+                                       "distribution", "path": "FP64 host oracle",
+                           "devices": "host cores only (rank 0); no GPU is used by this arm"},
                 "cpu_baseline": cb,
                 "e2e": {"value": value, "unit": "SVD/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     wl = make_workload(args.workload)
@@ -754,7 +755,7 @@ def run_reference(args):
         "metric": "SVDs/s",
         "value": value,
         "unit": "SVD/s",
-        "n_gpus": 0,
+        "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": 1e3 / value,
@@ -764,7 +765,8 @@ def run_reference(args):
         "dtype": "f64",
         "data": "synthetic (seeded)",
         "config": {"workload": wl["desc"], "path": "FP64 host oracle (reference arithmetic; the reference has "
-                                                   "no CPU path)", "epsilon": wl["eps"]},
+                                                   "no CPU path)", "epsilon": wl["eps"],
+                   "devices": "host cores only (rank 0); no GPU is used by this arm"},
         "cpu_baseline": cb,
         "e2e": {"value": value, "unit": "SVD/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -68,7 +68,7 @@ def test_reference_arm_json_line():
     for key in ("impl", "metric", "value", "unit", "steps", "warmup", "higher_is_better", "config", "cpu_baseline",
                 "e2e"):
         assert key in d, key
-    assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "SVD/s"
+    assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "SVD/s" and d["n_gpus"] == 1
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
 
