@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstddef>
 
 namespace jsvd {
@@ -32,6 +33,26 @@ __global__ void __launch_bounds__(kTile *kTileRows)
         const int c = c0 + k, r = r0 + threadIdx.x;
         if (r < rows && c < cols) dst[(size_t)c * ldd + r] = tile[threadIdx.x][k];
     }
+}
+
+// rowmajor_to_colmajor_kernel over all rows: row tiles run along grid.y
+// (at most 65535 blocks), so taller inputs take one launch per 65535 * 32 rows,
+// each on the sub-matrix starting at that row (src advanced by whole rows, dst
+// by the same number of rows within each column).  One launch, with exactly
+// the plain arguments, up to 2,097,120 rows.
+inline cudaError_t launch_rowmajor_to_colmajor(const double *src, int rows, int cols, double *dst, long ldd,
+                                               cudaStream_t stream)
+{
+    constexpr int kMaxRows = 65535 * kTile;
+    const dim3 block(kTile, kTileRows);
+    for (long long r0 = 0; r0 < rows; r0 += kMaxRows) {
+        const int rr = (int)std::min<long long>(kMaxRows, rows - r0);
+        const dim3 grid((cols + kTile - 1) / kTile, (rr + kTile - 1) / kTile);
+        rowmajor_to_colmajor_kernel<<<grid, block, 0, stream>>>(src + (size_t)r0 * cols, rr, cols, dst + r0, ldd);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // column-major src (rows x cols, leading dimension lds) -> row-major dst.

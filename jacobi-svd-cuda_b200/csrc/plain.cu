@@ -874,12 +874,7 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
                    cudaStream_t stream, bool gram_stop)
 {
     const int im = (int)m, in = (int)n;
-    {
-        dim3 block(kTile, kTileRows);
-        dim3 grid((in + kTile - 1) / kTile, (im + kTile - 1) / kTile);
-        rowmajor_to_colmajor_kernel<<<grid, block, 0, stream>>>(d_a, im, in, a_w, lda);
-        JSVD_CUDA_TRY(cudaGetLastError());
-    }
+    JSVD_CUDA_TRY(launch_rowmajor_to_colmajor(d_a, im, in, a_w, lda, stream));
     identity_colmajor_kernel<<<std::min<size_t>(1184, (n * n + 255) / 256), 256, 0, stream>>>(v_w, in, ldv);
     JSVD_CUDA_TRY(cudaGetLastError());
 

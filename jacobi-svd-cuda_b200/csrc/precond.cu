@@ -33,6 +33,7 @@
 #include "blockpair.hpp"
 #include "internal.hpp"
 #include "jsvd.h"
+#include "layout.cuh"
 #include "plain.hpp"
 
 namespace jsvd {
@@ -65,9 +66,8 @@ int cublas_failure(cublasStatus_t s, const char *expr, const char *file, int lin
         if (st_ != CUBLAS_STATUS_SUCCESS) return cublas_failure(st_, #EXPR, __FILE__, __LINE__); \
     } while (0)
 
-constexpr int kTile = 32, kTileRows = 8;
-
-// row-major (rows x cols) -> column-major (ld = rows)
+// row-major (rows x cols) -> column-major (ld = rows), one launch (the n x n
+// factor; the m x n input goes through launch_rowmajor_to_colmajor)
 __global__ void __launch_bounds__(kTile *kTileRows)
     pc_to_colmajor(const double *__restrict__ src, int rows, int cols, double *__restrict__ dst)
 {
@@ -509,9 +509,7 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     };
     cudaEventRecord(e0, st);
     JSVD_CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
-    pc_to_colmajor<<<dim3((n + kTile - 1) / kTile, (m + kTile - 1) / kTile), dim3(kTile, kTileRows), 0, st>>>(
-        d_a, m, n, Qa);
-    JSVD_CUDA_TRY(cudaGetLastError());
+    JSVD_CUDA_TRY(launch_rowmajor_to_colmajor(d_a, m, n, Qa, m, st));
     // A = Q R
     rc = run_stage(plan ? &plan->qr1 : nullptr,
                    [&](cudaStream_t s2) { return scqr3(s2, Qa, Qb, m, R1, R2, R3); });

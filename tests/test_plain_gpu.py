@@ -172,6 +172,20 @@ def test_plain_vpass_in_global_memory_bitwise(cuda_device, m, n):
     _assert_bitwise(second, exp)
 
 
+def test_plain_rows_beyond_one_transpose_grid(cuda_device):
+    """More than 65535 * 32 = 2,097,120 rows: the input transpose takes one
+    launch per 2,097,120-row chunk (the grid's y limit); bit-identical to the
+    oracle, and the QR-preconditioned path agrees with LAPACK."""
+    a = W.gaussian_splitmix(2_100_000, 3, seed=818)
+    cfg = jsvd.default_config(epsilon=1e-13)
+    got = jsvd.plain_svd(a, cfg)
+    _assert_bitwise(got, _oracle(a, 1e-13))
+    ref = np.linalg.svd(a, compute_uv=False)
+    pc = jsvd.precond_svd(a, cfg)
+    assert O.sigma_errors(pc[1], ref)["normwise"] <= 1e-13
+    assert O.residuals(a, pc[0], pc[1], pc[2])["rho_A"] <= 1e-12
+
+
 def test_precond_with_vpass_in_global_memory_identical(cuda_device):
     """The preconditioned path's Jacobi stage through the global-memory V pass
     gives the same bytes as through the staged one."""
