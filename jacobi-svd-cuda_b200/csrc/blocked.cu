@@ -430,8 +430,10 @@ extern "C" int jsvd_blocked_svd_device(const double *d_a, size_t rows, size_t co
             JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
         }
         // Fewer than two blocks: there is no block pair to rotate; the plain sweep
-        // handles it.
-        if (columns < 2 * (size_t)kB) return jsvd_plain_svd_device(d_a, rows, columns, &c, d_u, d_sigma, d_v, sweeps, st);
+        // handles it.  So does it for inputs taller than this engine's grids
+        // allow (row tiles of 32 along grid.y, at most 65535 blocks).
+        if (columns < 2 * (size_t)kB || rows > (size_t)65535 * 32)
+            return jsvd_plain_svd_device(d_a, rows, columns, &c, d_u, d_sigma, d_v, sweeps, st);
         return blocked_solve(d_a, (int)rows, (int)columns, c.epsilon, c.max_sweeps, d_u, d_sigma, d_v, sweeps, st);
     });
 }
