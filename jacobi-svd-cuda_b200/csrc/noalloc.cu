@@ -277,6 +277,9 @@ extern "C" int jsvd_plain_svd_noalloc(const double *d_a, size_t rows, size_t col
             return invalid_argument(
                 "jsvd_plain_svd_noalloc: rows*columns + columns*columns + columns + 1 exceeds the fixed scratch of "
                 "2097152 doubles (16 MiB).");
+        // its input transpose runs one launch with row tiles of 32 along grid.y
+        if (rows > (size_t)65535 * 32)
+            return invalid_argument("jsvd_plain_svd_noalloc: at most 2097120 rows.");
         int dev = 0;
         JSVD_CUDA_TRY(cudaGetDevice(&dev));
         double *scratch = nullptr;

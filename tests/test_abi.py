@@ -91,3 +91,16 @@ def test_oversized_dimensions_are_rejected_before_any_access(rows, cols):
     rc = jsvd.lib().jsvd_plain_svd(dummy, rows, cols, ctypes.byref(cfg), None, None, None, None)
     assert rc == jsvd.JSVD_ERR_OVERFLOW
     assert jsvd.last_error() == (jsvd.JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range.")
+
+
+def test_noalloc_refuses_rows_beyond_its_transpose_grid_before_cuda():
+    """jsvd_plain_svd_noalloc transposes in one launch (row tiles of 32 along
+    grid.y): a 2097130 x 1 request fits its scratch but not that grid, and is
+    refused before any CUDA call (the dummy buffer is never touched)."""
+    fn = jsvd.lib().jsvd_plain_svd_noalloc
+    P, S = ctypes.c_void_p, ctypes.c_size_t
+    fn.argtypes = [P, S, S, ctypes.POINTER(jsvd.Config), P, P, P, P, P]
+    fn.restype = ctypes.c_int
+    rc = fn(ctypes.c_void_p(16), 2097130, 1, ctypes.byref(jsvd.default_config()), None, None, None, None, None)
+    assert rc == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == "jsvd_plain_svd_noalloc: at most 2097120 rows."
