@@ -104,3 +104,11 @@ def test_noalloc_refuses_rows_beyond_its_transpose_grid_before_cuda():
     rc = fn(ctypes.c_void_p(16), 2097130, 1, ctypes.byref(jsvd.default_config()), None, None, None, None, None)
     assert rc == jsvd.JSVD_ERR_INVALID_ARGUMENT
     assert jsvd.last_error()[1] == "jsvd_plain_svd_noalloc: at most 2097120 rows."
+
+
+def test_integration_guide_names_every_entry_point():
+    """Every C entry point declared in include/jsvd.h is described in the
+    integration guide a reference-side caller reads."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [n for n in _declared_functions() if f"`{n}`" not in text]
+    assert not missing, missing
