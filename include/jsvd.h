@@ -390,6 +390,10 @@ int jsvd_server_submit(jsvd_server *s, const double *a, size_t rows, size_t colu
  * requested at submit, sigma, row-major V); each ticket can be collected once. */
 int jsvd_server_wait(jsvd_server *s, uint64_t ticket, double *u, double *sigma, double *v, int *sweeps,
                      double *latency_ms);
+/* Non-blocking: *done = 1 when the request has finished (a following
+ * jsvd_server_wait returns without blocking), else 0.  JSVD_ERR_INVALID_ARGUMENT
+ * for an unknown or already collected ticket. */
+int jsvd_server_poll(jsvd_server *s, uint64_t ticket, int *done);
 int jsvd_server_get_stats(jsvd_server *s, jsvd_server_stats *out);
 /* Stops the workers; requests still queued are dropped. */
 void jsvd_server_destroy(jsvd_server *s);

@@ -173,6 +173,17 @@ public:
         return JSVD_OK;
     }
 
+    int poll(uint64_t ticket, int *done)
+    {
+        if (done == nullptr) return invalid_argument("done must not be null.");
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = requests_.find(ticket);
+        if (it == requests_.end() || it->second->claimed)
+            return invalid_argument("Unknown or already collected ticket.");
+        *done = it->second->done ? 1 : 0;
+        return JSVD_OK;
+    }
+
     void stats(jsvd_server_stats *s)
     {
         std::lock_guard<std::mutex> lk(mu_);
@@ -462,6 +473,15 @@ int jsvd_server_wait(jsvd_server *s, uint64_t ticket, double *u, double *sigma, 
         set_last_error(JSVD_OK, "");
         if (!s) return invalid_argument("server must not be null.");
         return s->impl->wait(ticket, u, sigma, v, sweeps, latency_ms);
+    });
+}
+
+int jsvd_server_poll(jsvd_server *s, uint64_t ticket, int *done)
+{
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (!s) return invalid_argument("server must not be null.");
+        return s->impl->poll(ticket, done);
     });
 }
 

@@ -171,7 +171,7 @@ def exported_symbols() -> list[str]:
         "jsvd_plain_get_sweep_mode", "jsvd_blockpair_svd_device", "jsvd_blockpair_svd", "jsvd_blockpair_set_variant",
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
         "jsvd_precond_set_gram_stop", "jsvd_batch_builtin_tuning", "jsvd_batch_autotune", "jsvd_residuals",
-        "jsvd_round_robin_schedule", "jsvd_plain_set_vpass_in_global",
+        "jsvd_round_robin_schedule", "jsvd_plain_set_vpass_in_global", "jsvd_server_poll",
     ]
 
 
@@ -225,6 +225,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_server_submit.restype = I
         L.jsvd_server_wait.argtypes = [P, ctypes.c_uint64, P, P, P, ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double)]
         L.jsvd_server_wait.restype = I
+        L.jsvd_server_poll.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(I)]
+        L.jsvd_server_poll.restype = I
         L.jsvd_server_get_stats.argtypes = [P, ctypes.POINTER(ServerStats)]
         L.jsvd_server_get_stats.restype = I
         L.jsvd_server_destroy.argtypes = [P]
@@ -591,6 +593,12 @@ class Server:
         check(lib().jsvd_server_wait(self.h, ticket, u.ctypes.data if u is not None else None, s.ctypes.data,
                                      v.ctypes.data, ctypes.byref(sw), ctypes.byref(lat)))
         return u, s, v, sw.value, lat.value
+
+    def poll(self, ticket: int) -> bool:
+        """True when the request has finished (wait() will not block)."""
+        done = ctypes.c_int(0)
+        check(lib().jsvd_server_poll(self.h, ticket, ctypes.byref(done)))
+        return bool(done.value)
 
     def stats(self) -> ServerStats:
         st = ServerStats()

@@ -137,3 +137,31 @@ def test_oversized_request_is_rejected_before_copy():
         assert _stats(h).submitted == 0
     finally:
         jsvd.lib().jsvd_server_destroy(h)
+
+
+@pytest.mark.timeout(120)
+def test_poll_reports_completion_without_blocking():
+    import time
+
+    h = _server(small_workers=1, large_workers=1)
+    try:
+        a = np.random.default_rng(4).standard_normal((30, 20))
+        rc, t = _submit(h, a)
+        assert rc == jsvd.JSVD_OK
+        done = ctypes.c_int(-1)
+        deadline = time.monotonic() + 60.0
+        while True:
+            assert jsvd.lib().jsvd_server_poll(h, t, ctypes.byref(done)) == jsvd.JSVD_OK
+            if done.value == 1 or time.monotonic() > deadline:
+                break
+            time.sleep(0.01)
+        assert done.value == 1
+        assert _wait(h, t, 20) in (jsvd.JSVD_OK, jsvd.JSVD_ERR_CUDA)
+        for ticket in (t, t + 1000):
+            assert jsvd.lib().jsvd_server_poll(h, ticket, ctypes.byref(done)) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+            assert jsvd.last_error()[1] == "Unknown or already collected ticket."
+        rc, t2 = _submit(h, a)
+        assert jsvd.lib().jsvd_server_poll(h, t2, None) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+        _wait(h, t2, 20)
+    finally:
+        jsvd.lib().jsvd_server_destroy(h)
