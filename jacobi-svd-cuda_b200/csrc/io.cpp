@@ -179,19 +179,35 @@ namespace jacobi::svd::io
                     throw std::system_error(errno, std::system_category(), "msync failed");
             }
 
+            // Releases the mapping and the descriptor on every path; the first
+            // failure (msync, ftruncate, close) is reported after that.
             void close()
             {
                 if (fd_ < 0)
                     return;
-                flush();
+                int err = 0;
+                const char *what = nullptr;
+                if (data_ != nullptr && size_ > 0 && ::msync(data_, size_, MS_SYNC) != 0)
+                {
+                    err = errno;
+                    what = "msync failed";
+                }
                 if (data_ != nullptr)
                     ::munmap(data_, capacity_);
                 data_ = nullptr;
-                const int rc = ::ftruncate(fd_, static_cast<off_t>(size_));
-                ::close(fd_);
+                if (::ftruncate(fd_, static_cast<off_t>(size_)) != 0 && what == nullptr)
+                {
+                    err = errno;
+                    what = "ftruncate failed";
+                }
+                if (::close(fd_) != 0 && what == nullptr)
+                {
+                    err = errno;
+                    what = "close failed";
+                }
                 fd_ = -1;
-                if (rc != 0)
-                    throw std::system_error(errno, std::system_category(), "ftruncate failed");
+                if (what != nullptr)
+                    throw std::system_error(err, std::system_category(), what);
             }
 
         private:
