@@ -334,6 +334,18 @@ namespace jacobi::svd::io
         if (rows > std::numeric_limits<std::size_t>::max() || cols > std::numeric_limits<std::size_t>::max())
             throw std::overflow_error("Matrix dimensions exceed platform size_t range.");
         const std::size_t payload = mul_checked(mul_checked(rows, cols), kElementBytes);
+        // A header claiming more payload than the file holds is reported as
+        // truncated before any pinned memory is reserved for it (seekable
+        // files; a stream that cannot tell its position is read as it comes).
+        const std::streamoff here = input_.tellg();
+        if (here >= 0)
+        {
+            input_.seekg(0, std::ios::end);
+            const std::streamoff end = input_.tellg();
+            input_.seekg(here);
+            if (end >= here && static_cast<std::uint64_t>(end - here) < payload)
+                throw std::runtime_error("Truncated *.mat payload while dispatch reading.");
+        }
         task.buffer.reserve(payload, workspace_bytes);
         if (payload > 0)
         {

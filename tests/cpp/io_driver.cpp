@@ -6,6 +6,9 @@
 //   stream-copy IN OUT     MatInputStream >> / MatOutputStream << record by record
 //   dispatch IN OUT        MatDispatchReader + decode_dispatch_task_matrix -> *.mat
 //                          (needs pinned memory: exits 3 when CUDA is unavailable)
+//   dispatch-count IN X    MatDispatchReader over IN, printing the record count
+//                          (no device check: for inputs it must refuse before
+//                          reserving pinned memory)
 // Prints "error: <what>" and exits 1 on an exception.
 #include <cuda_runtime.h>
 
@@ -74,6 +77,15 @@ int main(int argc, char **argv)
                 out.push_back(decode_dispatch_task_matrix(task));
             }
             write_mat_file(argv[3], out);
+        }
+        else if (cmd == "dispatch-count")
+        {
+            MatDispatchReader reader(argv[2]);
+            MatDispatchTask task;
+            std::size_t k = 0;
+            while (reader.read_next(task, 0))
+                ++k;
+            std::cout << "records " << k << '\n';
         }
         else
         {

@@ -73,6 +73,17 @@ def test_truncated_mat(driver, tmp_path, cut, msg):
     assert r.returncode == 1 and msg in r.stdout
 
 
+def test_dispatch_refuses_oversized_claim_before_reserving(driver, tmp_path):
+    """A record header that claims more payload than the file holds (here 1e12
+    x 8 doubles) is refused as truncated before pinned memory is reserved."""
+    import struct
+
+    bad = tmp_path / "bad.mat"
+    bad.write_bytes(struct.pack(">QQ", 10**12, 8) + b"\0" * 64)
+    r = run(driver, "dispatch-count", bad, tmp_path / "unused")
+    assert r.returncode == 1 and r.stdout.strip() == "error: Truncated *.mat payload while dispatch reading."
+
+
 def test_txt_errors(driver, tmp_path):
     bad = tmp_path / "bad.txt"
     bad.write_text("1 2\n3\n")
