@@ -84,11 +84,14 @@ inline int invalid_argument(const char *message)
 }
 
 // True when a rows x columns request is outside the supported range: the
-// working copies index rows and columns with 32-bit integers, and byte
-// counts of several m x n buffers must not overflow size_t.
+// kernels index rows and columns with 32-bit integers and step them by up to
+// 1024 (+ 31 in the tile kernels) past the last one, so each dimension stays
+// 2048 below 2^31; byte counts of several m x n buffers must not overflow
+// size_t.
 inline bool dims_out_of_range(std::size_t rows, std::size_t columns)
 {
-    if (rows > (std::size_t)0x7fffffff || columns > (std::size_t)0x7fffffff) return true;
+    constexpr std::size_t kMaxDim = (std::size_t)0x7fffffff - 2047;
+    if (rows > kMaxDim || columns > kMaxDim) return true;
     return rows * columns > SIZE_MAX / 64;  // both factors < 2^31: the product itself fits
 }
 

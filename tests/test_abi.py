@@ -82,7 +82,7 @@ def test_python_wrapper_raises_invalid_argument():
         jsvd.plain_svd(np.zeros((2, 5)))
 
 
-@pytest.mark.parametrize("rows,cols", [(1 << 31, 1), (1 << 30, 1 << 30), (1 << 31, 1 << 31)])
+@pytest.mark.parametrize("rows,cols", [(1 << 31, 1), (2147481601, 1), (1 << 30, 1 << 30), (1 << 31, 1 << 31)])
 def test_oversized_dimensions_are_rejected_before_any_access(rows, cols):
     """Shapes whose byte counts would overflow are refused with
     JSVD_ERR_OVERFLOW before the (dummy) buffer is touched."""
