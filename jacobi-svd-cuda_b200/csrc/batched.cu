@@ -387,6 +387,10 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         d.n = req.cols[i];
         if (d.m <= 0 || d.n <= 0 || d.m < d.n)
             return invalid_argument("Batch matrix shape must satisfy rows >= columns > 0.");
+        if (dims_out_of_range((size_t)d.m, (size_t)d.n)) {
+            set_last_error(JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range.");
+            return JSVD_ERR_OVERFLOW;
+        }
         d.a_off = req.a_offsets[i];
         d.s_off = (long long)s_off;
         d.v_off = (long long)v_off;
@@ -624,6 +628,10 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
         for (int i = 0; i < count; ++i) {
             if (rows[i] <= 0 || cols[i] <= 0 || rows[i] < cols[i])
                 return invalid_argument("Batch matrix shape must satisfy rows >= columns > 0.");
+            if (dims_out_of_range((size_t)rows[i], (size_t)cols[i])) {
+                set_last_error(JSVD_ERR_OVERFLOW, "Matrix dimensions exceed the supported range.");
+                return JSVD_ERR_OVERFLOW;
+            }
             members[member_class(rows[i], cols[i], smem_cap, nullptr)].push_back(i);
         }
 
