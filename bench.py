@@ -13,7 +13,13 @@ torchrun every rank solves its own replica (no collective on the data path):
 `--impl reference` times the reference's CPU arithmetic - the FP64 host
 oracle, a restatement of the reference's kernels (the reference has no CPU
 path of its own) - on the host cores, on a bounded sample of the same
-workload, extrapolated to SVDs/s.
+workload, extrapolated to SVDs/s.  Its line carries the launched N as n_gpus;
+the arm itself uses no GPU.
+
+Single-matrix lines also carry `nominal`: the rate in the nominal FP64 count
+S_plain * n(n-1)/2 * (12m + 6n) per SVD, S_plain being the plain path's sweep
+count on the same input, so that paths with fewer sweeps are compared on the
+plain path's work.
 """
 from __future__ import annotations
 
