@@ -395,7 +395,9 @@ int jsvd_server_wait(jsvd_server *s, uint64_t ticket, double *u, double *sigma, 
  * for an unknown or already collected ticket. */
 int jsvd_server_poll(jsvd_server *s, uint64_t ticket, int *done);
 int jsvd_server_get_stats(jsvd_server *s, jsvd_server_stats *out);
-/* Stops the workers; requests still queued are dropped. */
+/* Stops the workers (requests being solved finish first).  Requests still
+ * queued fail with JSVD_ERR_RUNTIME, which wakes threads waiting on them;
+ * returns once no thread is inside jsvd_server_wait.  No call on s after. */
 void jsvd_server_destroy(jsvd_server *s);
 
 /* Measured FP64 FMA throughput of the current device in TFLOP/s (eight

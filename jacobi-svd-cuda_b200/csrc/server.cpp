@@ -107,7 +107,14 @@ public:
         }
     }
 
-    ~Server() { stop(); }
+    // Fails the requests still queued (their waiters wake with an error) and
+    // returns once no thread is inside wait().
+    ~Server()
+    {
+        stop();
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_done_.wait(lk, [&] { return waiters_ == 0; });
+    }
 
     int submit(const double *a, size_t m, size_t n, int want_u, uint64_t *ticket)
     {
@@ -154,12 +161,18 @@ public:
                 return invalid_argument("Unknown or already collected ticket.");
             Request *raw = it->second.get();
             raw->claimed = true;
+            ++waiters_;
             // The wait releases the lock: a submit() may rehash the map, so the
             // iterator is looked up again afterwards (the element itself stays put).
             cv_done_.wait(lk, [&] { return raw->done; });
             it = requests_.find(ticket);
             r = std::move(it->second);
             requests_.erase(it);
+            --waiters_;
+            // Under the lock: a destructor waiting for the last waiter cannot
+            // proceed before this scope ends, and after it this thread only
+            // touches its own request.
+            cv_done_.notify_all();
         }
         if (r->status != JSVD_OK) {
             set_last_error(r->status, r->error);
@@ -219,6 +232,19 @@ private:
         cv_budget_.notify_all();
         for (auto &t : threads_)
             if (t.joinable()) t.join();
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (auto *q : {&small_q_, &large_q_}) {
+                for (Request *r : *q) {
+                    r->status = JSVD_ERR_RUNTIME;
+                    r->error = "The server was destroyed before the request ran.";
+                    r->done = true;
+                    ++failed_;
+                }
+                q->clear();
+            }
+        }
+        cv_done_.notify_all();
     }
 
     // Takes requests from q while their footprints fit the budget; blocks while
@@ -408,6 +434,7 @@ private:
     std::unordered_map<uint64_t, std::unique_ptr<Request>> requests_;
     std::vector<std::thread> threads_;
     bool stopping_ = false;
+    int waiters_ = 0;  // threads inside wait()
     uint64_t next_id_ = 1;
     size_t in_use_ = 0, peak_bytes_ = 0;
     unsigned long long submitted_ = 0, completed_ = 0, failed_ = 0, batches_ = 0, batched_requests_ = 0,

@@ -165,3 +165,28 @@ def test_poll_reports_completion_without_blocking():
         _wait(h, t2, 20)
     finally:
         jsvd.lib().jsvd_server_destroy(h)
+
+
+@pytest.mark.timeout(120)
+def test_destroy_fails_queued_requests_and_releases_their_waiter():
+    """Destroying the server with requests still queued fails them and wakes
+    a thread waiting on one; destroy returns once that thread has left the
+    wait.  The waiter is known to be inside the wait (or past it) before
+    destroy starts: a claimed ticket polls as invalid."""
+    import time
+
+    h = _server(small_workers=1, large_workers=1)
+    a = np.random.default_rng(3).standard_normal((40, 30))
+    tickets = [_submit(h, a)[1] for _ in range(300)]
+    out = {}
+    th = threading.Thread(target=lambda: out.__setitem__("rc", _wait(h, tickets[-1], 30)))
+    th.start()
+    done = ctypes.c_int(0)
+    deadline = time.monotonic() + 60.0
+    while jsvd.lib().jsvd_server_poll(h, tickets[-1], ctypes.byref(done)) == jsvd.JSVD_OK:
+        assert time.monotonic() < deadline
+        time.sleep(0.001)
+    jsvd.lib().jsvd_server_destroy(h)
+    th.join(timeout=60)
+    assert not th.is_alive()
+    assert out["rc"] in (jsvd.JSVD_OK, jsvd.JSVD_ERR_CUDA, jsvd.JSVD_ERR_RUNTIME)
