@@ -392,7 +392,7 @@ int jsvd_server_wait(jsvd_server *s, uint64_t ticket, double *u, double *sigma, 
                      double *latency_ms);
 /* Non-blocking: *done = 1 when the request has finished (a following
  * jsvd_server_wait returns without blocking), else 0.  JSVD_ERR_INVALID_ARGUMENT
- * for an unknown or already collected ticket. */
+ * for a ticket that is unknown, already collected, or being waited on. */
 int jsvd_server_poll(jsvd_server *s, uint64_t ticket, int *done);
 int jsvd_server_get_stats(jsvd_server *s, jsvd_server_stats *out);
 /* Stops the workers (requests being solved finish first).  Requests still
