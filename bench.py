@@ -828,18 +828,19 @@ def main():
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    try:
-        if args.workload == "batch":
-            line = run_batch(args, rank, world, device)
-        elif args.workload == "serve":
-            line = run_serve(args, rank, world, device)
-        elif args.workload == "large":
-            line = run_large(args, rank, world, device)
-        else:
-            line = run_ours(args, rank, world, device)
-    finally:
-        if world > 1:
-            torch.distributed.barrier()
+    # A rank that fails raises at once, without a further collective (the
+    # others end in theirs: the launcher stops them, or the process group's
+    # timeout does); ranks that succeed meet at the barrier.
+    if args.workload == "batch":
+        line = run_batch(args, rank, world, device)
+    elif args.workload == "serve":
+        line = run_serve(args, rank, world, device)
+    elif args.workload == "large":
+        line = run_large(args, rank, world, device)
+    else:
+        line = run_ours(args, rank, world, device)
+    if world > 1:
+        torch.distributed.barrier()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
