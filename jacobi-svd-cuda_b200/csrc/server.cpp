@@ -141,6 +141,10 @@ public:
         r->a.assign(a, a + m * n);
         r->t_submit = Clock::now();
         std::lock_guard<std::mutex> lk(mu_);
+        if (stopping_) {
+            set_last_error(JSVD_ERR_RUNTIME, "The server is being destroyed.");
+            return JSVD_ERR_RUNTIME;
+        }
         r->id = next_id_++;
         *ticket = r->id;
         Request *raw = r.get();
