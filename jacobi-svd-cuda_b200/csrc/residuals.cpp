@@ -67,11 +67,15 @@ double row_gram_minus_identity_sq(const double *x, size_t count, size_t len, siz
     });
 }
 
-int host_threads(size_t work_rows)
+// Threads for a phase of `flops` multiply-adds split over `items` rows or
+// column pairs: about 2M per thread (a thread start costs tens of
+// microseconds), at most the host's threads and 64.
+int host_threads(double flops, size_t items)
 {
     const unsigned hc = std::thread::hardware_concurrency();
-    const size_t t = std::min<size_t>(hc == 0 ? 1 : hc, 64);
-    return (int)std::max<size_t>(1, std::min(t, work_rows));
+    const size_t cap = std::min<size_t>(hc == 0 ? 1 : hc, 64);
+    const size_t by_work = (size_t)std::max(1.0, flops / (double)(1 << 21));
+    return (int)std::max<size_t>(1, std::min({cap, by_work, items}));
 }
 
 }  // namespace
@@ -97,10 +101,10 @@ extern "C" int jsvd_residuals(const double *a, const double *u, const double *si
         *out = jsvd_residual_report{};
         out->rho_a = -1.0;
         out->rho_u = -1.0;
-        const int threads = host_threads(m);
+        const double dm = (double)m, dn = (double)n;
 
         // rho_V: rows of V are contiguous
-        out->rho_v = std::sqrt(row_gram_minus_identity_sq(v, n, n, n, std::min(threads, (int)n)));
+        out->rho_v = std::sqrt(row_gram_minus_identity_sq(v, n, n, n, host_threads(dn * dn * dn / 2, n)));
 
         if (u != nullptr) {
             // rho_U: U^T U over the columns with sigma > 0, from a transposed copy
@@ -110,13 +114,14 @@ extern "C" int jsvd_residuals(const double *a, const double *u, const double *si
             std::vector<double> ut(keep.size() * m);
             for (size_t i = 0; i < m; ++i)
                 for (size_t c = 0; c < keep.size(); ++c) ut[c * m + i] = u[i * n + keep[c]];
-            out->rho_u = std::sqrt(
-                row_gram_minus_identity_sq(ut.data(), keep.size(), m, m, std::min(threads, (int)keep.size() + 1)));
+            const double kept = (double)keep.size();
+            out->rho_u = std::sqrt(row_gram_minus_identity_sq(ut.data(), keep.size(), m, m,
+                                                              host_threads(kept * kept * dm / 2, keep.size())));
 
             if (a != nullptr) {
                 // rho_A: row i of U S V^T is (u_i .* sigma) . v_j over j
                 double norm_a = 0.0;
-                const double err = parallel_sum(threads, [&](int k, int t) {
+                const double err = parallel_sum(host_threads(dm * dn * dn, m), [&](int k, int t) {
                     std::vector<double> w(n);
                     double local = 0.0;
                     for (size_t i = (size_t)k; i < m; i += (size_t)t) {
