@@ -112,3 +112,30 @@ def test_integration_guide_names_every_entry_point():
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     missing = [n for n in _declared_functions() if f"`{n}`" not in text]
     assert not missing, missing
+
+
+@pytest.mark.parametrize(
+    "overrides,message",
+    [
+        ({"layout_transpose_min_columns": 0}, "layout_transpose_min_columns must be positive."),
+        ({"layout_transpose_min_elements": 0}, "layout_transpose_min_elements must be positive."),
+        ({"layout_transpose_benchmark_repetitions": 0}, "layout_transpose_benchmark_repetitions must be positive."),
+        ({"layout_transpose_benchmark_sweeps": 0}, "layout_transpose_benchmark_sweeps must be positive."),
+        ({"max_sweeps": 0}, "max_sweeps must be positive."),
+        # the layout settings are checked first, as in the reference
+        ({"max_sweeps": 0, "layout_transpose_min_columns": 0}, "layout_transpose_min_columns must be positive."),
+    ],
+)
+def test_auto_tune_layout_validates_before_any_solve(overrides, message):
+    """jsvd_auto_tune_layout checks its settings in the reference's order
+    (src/kernels.cu:1078-1086) before running any benchmark solve."""
+    cfg = jsvd.default_config(**overrides)
+    rep = jsvd.AutoTuneReport()
+    assert jsvd.lib().jsvd_auto_tune_layout(ctypes.byref(cfg), ctypes.byref(rep)) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == message
+
+
+def test_auto_tune_layout_needs_a_report():
+    cfg = jsvd.default_config()
+    assert jsvd.lib().jsvd_auto_tune_layout(ctypes.byref(cfg), None) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == "report must not be null."
