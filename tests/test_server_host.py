@@ -190,3 +190,35 @@ def test_destroy_fails_queued_requests_and_releases_their_waiter():
     th.join(timeout=60)
     assert not th.is_alive()
     assert out["rc"] in (jsvd.JSVD_OK, jsvd.JSVD_ERR_CUDA, jsvd.JSVD_ERR_RUNTIME)
+
+
+@pytest.mark.parametrize("field,value,message", [
+    ("epsilon", 0.0, "epsilon must be positive."),
+    ("epsilon", -1.0, "epsilon must be positive."),
+    ("max_sweeps", 0, "max_sweeps must be positive."),
+])
+def test_create_rejects_bad_settings(field, value, message):
+    opt = jsvd.ServerOptions()
+    jsvd.lib().jsvd_server_options_default(ctypes.byref(opt))
+    setattr(opt.cfg, field, value)
+    h = ctypes.c_void_p()
+    assert jsvd.lib().jsvd_server_create(ctypes.byref(opt), ctypes.byref(h)) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == message and not h.value
+
+
+def test_options_defaults_and_null_handles():
+    opt = jsvd.ServerOptions()
+    jsvd.lib().jsvd_server_options_default(ctypes.byref(opt))
+    assert opt.device_budget_bytes == 40 << 30 and opt.small_workers == 2 and opt.large_workers == 4
+    assert opt.max_batch == 4096 and opt.large_path == 0 and opt.cfg.epsilon == 1e-9
+    L = jsvd.lib()
+    assert L.jsvd_server_create(ctypes.byref(opt), None) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    t = ctypes.c_uint64(0)
+    a = np.ones((2, 2))
+    assert L.jsvd_server_submit(None, a.ctypes.data, 2, 2, 0, ctypes.byref(t)) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert L.jsvd_server_wait(None, 1, None, None, None, None, None) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    done = ctypes.c_int(0)
+    assert L.jsvd_server_poll(None, 1, ctypes.byref(done)) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    st = jsvd.ServerStats()
+    assert L.jsvd_server_get_stats(None, ctypes.byref(st)) == jsvd.JSVD_ERR_INVALID_ARGUMENT
+    L.jsvd_server_destroy(None)  # no-op
