@@ -514,6 +514,7 @@ extern "C" int jsvd_batch_svd_device(int count, const int *rows, const int *cols
         const jsvd_config &c = cfg ? *cfg : def;
         const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, d_sigma == nullptr, c);
         if (bad != JSVD_OK) return bad;
+        if (count == 0) return JSVD_OK;  // nothing to solve, no CUDA call
         int dev = 0;
         JSVD_CUDA_TRY(cudaGetDevice(&dev));
         cudaStream_t st = (cudaStream_t)stream;

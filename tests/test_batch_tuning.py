@@ -85,3 +85,33 @@ def test_autotune_rejects_bad_arguments_before_cuda():
                                0, 2, 0, 1, ctypes.byref(rep), None)
     assert rc == jsvd.JSVD_ERR_INVALID_ARGUMENT
     assert jsvd.last_error()[1] == "The batched solver reduces with threads_per_block = 256."
+
+
+def test_batch_solver_rejects_bad_arguments_before_cuda():
+    cfg = jsvd.default_config()
+    rows = np.array([4], dtype=np.int32)
+    cols = np.array([3], dtype=np.int32)
+    off = np.array([0], dtype=np.int64)
+    L = jsvd.lib()
+    P = ctypes.c_void_p
+
+    def call(count, r, c, o, a, sigma, c_cfg):
+        return L.jsvd_batch_svd_device(count, r, c, o, a, 0, ctypes.byref(c_cfg), sigma, None, None, None, None,
+                                       None)
+
+    assert call(-1, rows.ctypes.data, cols.ctypes.data, off.ctypes.data, P(8), P(8), cfg) == \
+        jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == "count must be non-negative."
+    assert call(1, rows.ctypes.data, cols.ctypes.data, off.ctypes.data, P(8), None, cfg) == \
+        jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == "Batch buffers must not be null."
+    bad = jsvd.default_config(epsilon=0.0)
+    assert call(1, rows.ctypes.data, cols.ctypes.data, off.ctypes.data, P(8), P(8), bad) == \
+        jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == "epsilon must be positive."
+    bad = jsvd.default_config(threads_per_block=512)
+    assert call(1, rows.ctypes.data, cols.ctypes.data, off.ctypes.data, P(8), P(8), bad) == \
+        jsvd.JSVD_ERR_INVALID_ARGUMENT
+    assert jsvd.last_error()[1] == "The batched solver reduces with threads_per_block = 256."
+    # an empty batch is a no-op
+    assert call(0, None, None, None, None, None, cfg) == jsvd.JSVD_OK
