@@ -790,8 +790,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     ap.add_argument("--no-plain-compare", action="store_true")
-    ap.add_argument("--rates", default="50,200,1000")
-    ap.add_argument("--serve-count", type=int, default=300)
+    ap.add_argument("--rates", default="50,200,500,1000,2000",
+                    help="Poisson arrival rates (req/s) of the serve workload")
+    ap.add_argument("--serve-count", type=int, default=2000, help="requests per rate of the serve workload")
     ap.add_argument("--serve-plain-sample", type=int, default=40)
     ap.add_argument("--serve-large-workers", type=int, default=0, help="0 = the serving core's default")
     ap.add_argument("--large-m", type=int, default=16384)
