@@ -13,8 +13,10 @@
 //     and three blocking host transfers per round.
 //   * V never sits on the round-to-round critical path.  Each round records
 //     its (c, s); after a sweep that rotated, one row-parallel pass applies the
-//     whole sweep to V, rows held in shared memory, on a second stream while
-//     the next sweep's rounds run (the angle tables alternate between sweeps).
+//     whole sweep to V, rows held in shared memory (rotated in place in global
+//     memory when a row is longer than the shared-memory cap), on a second
+//     stream while the next sweep's rounds run (the angle tables alternate
+//     between sweeps).
 //     The pass is kept as narrow as it can be while it still ends inside
 //     those rounds, so that it takes few of their registers.  Per element the
 //     sequence of rotations is the reference's, so V is bit-identical.
