@@ -9,6 +9,9 @@
 //   class 3  : A in shared memory, V in a per-CTA slice of global memory
 //   class 4  : A and V in global memory (L2-resident per-CTA slices), the
 //              leading columns of A that fit in shared memory kept there
+// Launch shapes per class (threads, CTAs per SM, grid cap) come from the
+// compiled-in table batch_tuning_table.h, which batch_autotune.py writes from
+// jsvd_batch_autotune (defined at the end of this file).
 // Each round runs in three phases separated by __syncthreads:
 //   1. one warp per pair: the three dot products, reduced in the reference's
 //      order (T = 256 virtual lanes; lane l holds virtual lanes l + 32j, then
