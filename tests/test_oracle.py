@@ -120,3 +120,30 @@ def test_oracle_reproduces_reference_outputs(path):
         import hashlib
         assert hashlib.sha256(u.tobytes()).hexdigest() == rec["u_sha256"]
         assert hashlib.sha256(v.tobytes()).hexdigest() == rec["v_sha256"]
+
+
+def test_golden_comparison_rejects_planted_mistakes():
+    """The bitwise golden comparison can fail: with any other FMA placement,
+    or with a wrong reduction width, the oracle no longer reproduces some of
+    the reference's outputs.  (Mistakes are planted in the oracle, on the CPU.)"""
+    summ = _summary()
+    small = [p for p in _golden_cases() if os.path.basename(p)[:-4] in ("g8x8", "g17x9", "g33x16", "g64x48")]
+    assert small, "small golden cases missing"
+
+    def reproduces(path, variant, lanes=None):
+        g = np.load(path)
+        name = os.path.basename(path)[:-4]
+        a = golden_input(name, g)
+        T = int(g["T"]) if lanes is None else lanes
+        u, s, v, sw = O.plain_svd(a, eps=float(g["eps"]), lanes=T, variant=variant, threads=2)
+        return sw == int(g["sweeps"]) and np.array_equal(s, g["sigma"]) and np.array_equal(u, g["u"])
+
+    pinned = O.VARIANTS[summ["pinned_variant"]]
+    assert all(reproduces(p, pinned) for p in small)
+    for name, code in O.VARIANTS.items():
+        if code != pinned:
+            assert not all(reproduces(p, code) for p in small), name
+    # T = 32 instead of 256 changes the summation order once a column has
+    # more than 32 rows (up to 128 rows, T = 128 and T = 256 reduce alike:
+    # the upper lanes hold zeros)
+    assert not all(reproduces(p, pinned, lanes=32) for p in small), "reduction width"
