@@ -147,3 +147,25 @@ def test_golden_comparison_rejects_planted_mistakes():
     # more than 32 rows (up to 128 rows, T = 128 and T = 256 reduce alike:
     # the upper lanes hold zeros)
     assert not all(reproduces(p, pinned, lanes=32) for p in small), "reduction width"
+
+
+def test_recorded_variant_votes_are_reproduced():
+    """summary.json records, per golden case and FMA variant, whether that
+    variant reproduces the reference bit for bit; the oracle reproduces each
+    recorded vote (cases that store full U and V)."""
+    summ = _summary()
+    checked = 0
+    for path in _golden_cases():
+        name = os.path.basename(path)[:-4]
+        g = np.load(path)
+        if "u" not in g:
+            continue
+        a = golden_input(name, g)
+        for vname, vote in summ["cases"][name]["match"].items():
+            u, s, v, sw = O.plain_svd(a, eps=float(g["eps"]), lanes=int(g["T"]), variant=O.VARIANTS[vname],
+                                      threads=2)
+            bitwise = (sw == int(g["sweeps"]) and np.array_equal(s, g["sigma"]) and np.array_equal(u, g["u"])
+                       and np.array_equal(v, g["v"]))
+            assert bitwise == vote["bitwise"], (name, vname)
+            checked += 1
+    assert checked >= 5 * 10
