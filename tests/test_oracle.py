@@ -169,3 +169,20 @@ def test_recorded_variant_votes_are_reproduced():
             assert bitwise == vote["bitwise"], (name, vname)
             checked += 1
     assert checked >= 5 * 10
+
+
+def test_oracle_reproduces_reference_cli_output():
+    """tests/golden/pipeline_ref_out.mat is the reference CLI's output for
+    pipeline_in.mat at epsilon 1e-12: per testcase U, Sigma (1 x n) and V.
+    The oracle under the pinned variant reproduces every record bit for bit."""
+    import matfile
+
+    summ = _summary()
+    mats = matfile.read(os.path.join(GOLDEN, "pipeline_in.mat"))
+    out = matfile.read(os.path.join(GOLDEN, "pipeline_ref_out.mat"))
+    assert len(out) == 3 * len(mats)
+    for k, a in enumerate(mats):
+        u, s, v, _ = O.plain_svd(a, eps=1e-12, variant=O.VARIANTS[summ["pinned_variant"]], threads=2)
+        ru, rs, rv = out[3 * k], out[3 * k + 1], out[3 * k + 2]
+        assert rs.shape == (1, a.shape[1]) and np.array_equal(s, rs.ravel()), k
+        assert np.array_equal(u, ru) and np.array_equal(v, rv), k
