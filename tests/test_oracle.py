@@ -179,10 +179,16 @@ def test_oracle_reproduces_reference_cli_output():
 
     summ = _summary()
     mats = matfile.read(os.path.join(GOLDEN, "pipeline_in.mat"))
-    out = matfile.read(os.path.join(GOLDEN, "pipeline_ref_out.mat"))
+    with open(os.path.join(GOLDEN, "pipeline_ref_out.mat"), "rb") as f:
+        ref_bytes = f.read()
+    out = matfile.decode(ref_bytes)
     assert len(out) == 3 * len(mats)
+    records = []
     for k, a in enumerate(mats):
         u, s, v, _ = O.plain_svd(a, eps=1e-12, variant=O.VARIANTS[summ["pinned_variant"]], threads=2)
         ru, rs, rv = out[3 * k], out[3 * k + 1], out[3 * k + 2]
         assert rs.shape == (1, a.shape[1]) and np.array_equal(s, rs.ravel()), k
         assert np.array_equal(u, ru) and np.array_equal(v, rv), k
+        records += [u, s.reshape(1, -1), v]
+    # and the records, encoded as *.mat, are the reference CLI's file byte for byte
+    assert matfile.encode(records) == ref_bytes
