@@ -101,8 +101,8 @@ int jsvd_plain_svd_device(const double *d_a, size_t rows, size_t columns, const 
  * V (U, sigma, V may be NULL), work runs on `stream` as given (NULL = the
  * legacy default stream), and the working copies live in one fixed 16 MiB
  * device array inside the library, so rows*columns + columns*columns +
- * columns + 1 must not exceed 2097152 (larger requests fail with
- * JSVD_ERR_INVALID_ARGUMENT).  That array is held by every GPU that loads the
+ * columns + 1 must not exceed 2097152 and rows 2097120 (larger requests fail
+ * with JSVD_ERR_INVALID_ARGUMENT).  That array is held by every GPU that loads the
  * library until exit and is shared by all calls: calls that overlap on the GPU
  * race and must be serialised by the caller.  The first call on a device looks
  * up the array's device address; make it before any stream capture begins.
