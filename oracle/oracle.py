@@ -158,6 +158,33 @@ def sigma_errors(s_test: np.ndarray, s_ref: np.ndarray) -> dict:
     return {"max_rel": float(rel.max()) if rel.size else 0.0, "normwise": float(d.max() / smax) if d.size else 0.0}
 
 
+def cluster_subspace_sines(v_test, s_test, v_ref, s_ref, rel_gap: float = 1e-6, floor: float = 0.0) -> dict:
+    """Singular-subspace agreement where singular values cluster (single
+    vectors are not defined inside a cluster): both results are sorted by
+    sigma, consecutive reference values closer than rel_gap (relative) form
+    one cluster, and for every cluster with sigma >= floor * sigma_max the
+    largest principal-angle sine between span(V_test[:, cluster]) and
+    span(V_ref[:, cluster]) is ||T - R (R^T T)||_2 (accurate for tiny angles,
+    R orthonormal).  Returns the largest sine, the clusters compared and the
+    largest cluster size."""
+    it = np.argsort(-np.asarray(s_test), kind="stable")
+    ir = np.argsort(-np.asarray(s_ref), kind="stable")
+    sr = np.asarray(s_ref)[ir]
+    vt, vr = np.asarray(v_test)[:, it], np.asarray(v_ref)[:, ir]
+    n = sr.shape[0]
+    worst, used, largest, start = 0.0, 0, 0, 0
+    for i in range(1, n + 1):
+        if i < n and abs(sr[i - 1] - sr[i]) <= rel_gap * abs(sr[i - 1]):
+            continue
+        if sr[start] >= floor * sr[0]:
+            t, r = vt[:, start:i], vr[:, start:i]
+            worst = max(worst, float(np.linalg.norm(t - r @ (r.T @ t), 2)))
+            used += 1
+            largest = max(largest, i - start)
+        start = i
+    return {"max_sine": worst, "clusters": used, "largest_cluster": largest}
+
+
 def columns_match_up_to_sign(x: np.ndarray, y: np.ndarray, tol: float) -> float:
     """Max over columns of min(||x_j - y_j||, ||x_j + y_j||); returns that maximum."""
     dp = np.linalg.norm(x - y, axis=0)

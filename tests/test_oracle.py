@@ -192,3 +192,25 @@ def test_oracle_reproduces_reference_cli_output():
         records += [u, s.reshape(1, -1), v]
     # and the records, encoded as *.mat, are the reference CLI's file byte for byte
     assert matfile.encode(records) == ref_bytes
+
+
+def test_cluster_subspaces_agree_with_lapack():
+    """Clustered spectrum (graded 1 .. 1e-10 with runs of 8 values 1e-10
+    apart, as in the 16384 x 8192 workload): single vectors are not defined
+    inside a cluster, so the oracle's V is compared with LAPACK's cluster by
+    cluster through principal angles.  Clusters with sigma >= 1e-3 sigma_max
+    agree to sin(theta) <= 1e-10; below that the comparison is limited by
+    LAPACK's own absolute-gap accuracy."""
+    n, m = 160, 300
+    s = W.graded_clustered_sigma(n, clusters=4, size=8, gap=1e-10)
+    a = W.spectrum_matrix(m, n, s, 77)
+    _, so, v, _ = O.plain_svd(a, eps=1e-14, threads=os.cpu_count() or 1)
+    _, sl, vt = np.linalg.svd(a, full_matrices=False)
+    r = O.cluster_subspace_sines(v, so, vt.T, sl, floor=1e-3)
+    assert r["largest_cluster"] == 8 and r["clusters"] >= 30
+    assert r["max_sine"] <= 1e-10, r
+    # a planted mistake is seen: swapping two columns across a cluster boundary
+    bad = v.copy()
+    order = np.argsort(-so)
+    bad[:, [order[0], order[1]]] = bad[:, [order[1], order[0]]]
+    assert O.cluster_subspace_sines(bad, so, vt.T, sl, floor=1e-3)["max_sine"] > 0.5

@@ -106,3 +106,17 @@ def test_precond_graph_replay_identical(cuda_device):
         assert r[3] == runs[0][3]
         for x, y in zip(r[:3], runs[0][:3]):
             assert np.array_equal(x, y)
+
+
+def test_precond_cluster_subspaces_agree_with_lapack(cuda_device):
+    """Graded spectrum 1 .. 1e-10 with runs of 8 singular values 1e-10 apart
+    (the 16384 x 8192 workload's shape of spectrum, at 300 x 160): cluster
+    subspaces of V with sigma >= 1e-3 sigma_max agree with LAPACK's to
+    sin(theta) <= 1e-10 (single vectors are not defined inside a cluster)."""
+    n, m = 160, 300
+    s = W.graded_clustered_sigma(n, clusters=4, size=8, gap=1e-10)
+    a = W.spectrum_matrix(m, n, s, 77)
+    _, sp, vp, _ = jsvd.precond_svd(a, jsvd.default_config(epsilon=1e-14))
+    _, sl, vt = np.linalg.svd(a, full_matrices=False)
+    r = O.cluster_subspace_sines(vp, sp, vt.T, sl, floor=1e-3)
+    assert r["largest_cluster"] == 8 and r["max_sine"] <= 1e-10, r
