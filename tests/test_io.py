@@ -227,3 +227,20 @@ def test_txt_codec_round_trip_property(driver, tmp_path_factory, mats):
     for blk, a in zip(blocks, mats):
         got = np.array([[float(t) for t in ln.split()] for ln in blk.strip().splitlines()])
         assert got.shape == a.shape and np.array_equal(got.view(np.uint64), a.view(np.uint64))
+
+
+def test_cli_reports_solver_failure_with_exit_1(tmp_path):
+    """A solve that fails (here: no CUDA device) reaches the CLI through the
+    serving core, the writer thread and the pipeline's exception path: exit
+    code 1 and the reference's "Execution failed:" message
+    (src/main.cpp:1289-1298)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("checks the failure path of a machine without a GPU")
+    src = tmp_path / "in.mat"
+    matfile.write(src, _mats())
+    r = subprocess.run([CLI, str(src), str(tmp_path / "out.mat"), "-q"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 1, (r.returncode, r.stderr)
+    assert r.stderr.startswith("Execution failed: ") and "CUDA" in r.stderr
