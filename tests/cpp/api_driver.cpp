@@ -5,6 +5,9 @@
 //   residuals FILE   reads rows, columns, then A, U, sigma, V (whitespace-
 //                    separated doubles) from FILE and prints rho_a rho_u rho_v
 //   bad-result       prints the message of residuals() on mismatched buffers
+//   cuda-error       solves a valid 4 x 3 matrix with every solver and prints
+//                    the exception type and message of each (for a machine
+//                    without a GPU, where the first CUDA call fails)
 #include <fstream>
 #include <iomanip>
 #include <iostream>
@@ -90,6 +93,27 @@ int main(int argc, char **argv)
         const SvdResiduals res = residuals(a, r);
         std::cout << std::setprecision(std::numeric_limits<double>::max_digits10) << res.rho_a << ' ' << res.rho_u
                   << ' ' << res.rho_v << '\n';
+        return 0;
+    }
+    if (cmd == "cuda-error")
+    {
+        const std::vector<double> a = {4, 1, 0, 1, 3, 1, 0, 1, 2, 1, 1, 1};
+        for (SvdSolver s : {SvdSolver::plain, SvdSolver::precond, SvdSolver::blockpair, SvdSolver::blocked})
+        {
+            try
+            {
+                (void)jacobi_svd(a, 4, 3, {}, s);
+                std::cout << name(s) << " ok\n";
+            }
+            catch (const CudaError &e)
+            {
+                std::cout << name(s) << " CudaError " << e.what() << '\n';
+            }
+            catch (const std::exception &e)
+            {
+                std::cout << name(s) << " other " << e.what() << '\n';
+            }
+        }
         return 0;
     }
     if (cmd == "bad-result")

@@ -55,3 +55,19 @@ def test_residuals_match_oracle(driver, tmp_path, m, n):
 def test_residuals_reject_mismatched_result(driver):
     out = subprocess.run([driver, "bad-result"], capture_output=True, text=True, check=True).stdout.strip()
     assert out == "Result buffers do not match rows and columns."
+
+
+def test_cuda_failures_surface_as_cuda_error(driver):
+    """Without a GPU the first CUDA call of every solver fails: the C++ API
+    throws jacobi::svd::CudaError with the reference's message format
+    ("CUDA call failed: <expr> @ <file>:<line>, code=<n>, message=<text>")."""
+    import re
+
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("checks the failure path of a machine without a GPU")
+    out = subprocess.run([driver, "cuda-error"], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert len(out) == 4
+    for line, solver in zip(out, ["plain", "precond", "blockpair", "blocked"]):
+        assert re.match(rf"{solver} CudaError CUDA call failed: .+ @ .+:\d+, code=\d+, message=.+", line), line
