@@ -5,6 +5,8 @@
 //   residuals FILE   reads rows, columns, then A, U, sigma, V (whitespace-
 //                    separated doubles) from FILE and prints rho_a rho_u rho_v
 //   bad-result       prints the message of residuals() on mismatched buffers
+//   device-matrix    prints the messages of DeviceMatrix's argument checks
+//                    (zero dimensions; a default-constructed matrix given data)
 //   cuda-error       solves a valid 4 x 3 matrix with every solver and prints
 //                    the exception type and message of each (for a machine
 //                    without a GPU, where the first CUDA call fails)
@@ -93,6 +95,33 @@ int main(int argc, char **argv)
         const SvdResiduals res = residuals(a, r);
         std::cout << std::setprecision(std::numeric_limits<double>::max_digits10) << res.rho_a << ' ' << res.rho_u
                   << ' ' << res.rho_v << '\n';
+        return 0;
+    }
+    if (cmd == "device-matrix")
+    {
+        for (auto [r, c] : {std::pair<std::size_t, std::size_t>{0, 3}, {3, 0}})
+        {
+            try
+            {
+                DeviceMatrix d(r, c);
+                std::cout << "constructed\n";
+            }
+            catch (const std::invalid_argument &e)
+            {
+                std::cout << e.what() << '\n';
+            }
+        }
+        try
+        {
+            DeviceMatrix d;  // 0 x 0, no allocation
+            const std::vector<double> host(6, 1.0);
+            d.copy_from_host(host);
+            std::cout << "copied\n";
+        }
+        catch (const std::invalid_argument &e)
+        {
+            std::cout << e.what() << '\n';
+        }
         return 0;
     }
     if (cmd == "cuda-error")

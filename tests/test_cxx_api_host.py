@@ -71,3 +71,12 @@ def test_cuda_failures_surface_as_cuda_error(driver):
     assert len(out) == 4
     for line, solver in zip(out, ["plain", "precond", "blockpair", "blocked"]):
         assert re.match(rf"{solver} CudaError CUDA call failed: .+ @ .+:\d+, code=\d+, message=.+", line), line
+
+
+def test_device_matrix_argument_checks(driver):
+    """DeviceMatrix (reference include/kernels.hpp:130-244) rejects zero
+    dimensions and mismatched host data with the reference's messages,
+    before any device allocation or copy."""
+    out = subprocess.run([driver, "device-matrix"], capture_output=True, text=True, check=True).stdout.splitlines()
+    assert out == ["DeviceMatrix dimensions must be positive."] * 2 + \
+        ["Host data size does not match device matrix shape."]
