@@ -244,3 +244,16 @@ def test_cli_reports_solver_failure_with_exit_1(tmp_path):
                        timeout=120)
     assert r.returncode == 1, (r.returncode, r.stderr)
     assert r.stderr.startswith("Execution failed: ") and "CUDA" in r.stderr
+
+
+def test_policy_concepts_accept_user_policies(tmp_path):
+    """io.hpp's MatrixInputPolicy / MatrixOutputPolicy concepts (reference
+    include/io.hpp:630-661): the file policies satisfy them, a policy without
+    flush does not (static_asserts), and a user-defined in-memory policy runs
+    through the stream templates."""
+    exe = tmp_path / "policy_driver"
+    subprocess.check_call(["g++", "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include"),
+                           "-I/usr/local/cuda/include", os.path.join(ROOT, "tests", "cpp", "policy_driver.cpp"),
+                           "-o", str(exe)])
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["3", "3", "1", "3", "5", "7"]
