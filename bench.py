@@ -1,7 +1,8 @@
 """Benchmark of the one-sided Jacobi SVD on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tall|square512|batch|serve|large] [--path auto|plain|precond|blocked]
+                    [--workload tall|square512|batch|serve|large]
+                    [--path auto|plain|precond|blocked|blockpair]
 
 One step = one pass of the hot path over one batch of synthetic input (for the
 single-matrix workloads: one full SVD).  `value` is whole-job SVDs/s with the
