@@ -38,6 +38,10 @@ def golden_input(name, fixture):
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+    # temporary files of the tests stay inside the repository's ignored
+    # working folder
+    if not config.option.basetemp:
+        config.option.basetemp = os.path.join(ROOT, "_work", "pytest-tmp")
 
 
 @pytest.fixture(scope="session")

@@ -3,12 +3,15 @@
 // Runs where no GPU is present: every request fails fast with a CUDA error,
 // which still exercises queues, admission, completion, polls, waits and
 // destroy from many threads.  Prints one summary line per scenario.
+// Usage: server_stress DIR (DIR receives the pipeline scenario's files).
 #include <atomic>
 #include <cstdio>
 #include <thread>
 #include <vector>
 
+#include "io.hpp"
 #include "jsvd.h"
+#include "pipeline.hpp"
 
 namespace
 {
@@ -97,6 +100,44 @@ namespace
         std::printf("destroy 10\n");
         return 0;
     }
+    // the pipeline's reader and writer threads on its failure path: the
+    // first collected result fails, the writer records it, the reader stops
+    // and run_pipeline rethrows
+    int pipeline_failure(const std::filesystem::path &dir)
+    {
+        using namespace jacobi::svd;
+        const std::filesystem::path in = dir / "stress_in.mat";
+        const std::filesystem::path out = dir / "stress_out.mat";
+        std::vector<io::Matrix> mats;
+        for (int i = 0; i < 60; ++i)
+            mats.push_back(io::Matrix{20, 10, std::vector<double>(200, 1.0 + i)});
+        io::write_mat_file(in, mats);
+        int failures = 0;
+        for (int trial = 0; trial < 20; ++trial)
+        {
+            pipeline::PipelineConfig cfg;
+            cfg.input_path = in;
+            cfg.output_path = out;
+            try
+            {
+                (void)pipeline::run_pipeline(cfg);
+            }
+            catch (const std::exception &)
+            {
+                ++failures;
+            }
+        }
+        std::filesystem::remove(in);
+        std::filesystem::remove(out);
+        std::printf("pipeline %d\n", failures);
+        return 0;
+    }
 } // namespace
 
-int main() { return mixed() | destroy_with_waiter(); }
+// argv[1]: a directory for the pipeline scenario's files
+int main(int argc, char **argv)
+{
+    if (argc != 2)
+        return 64;
+    return mixed() | destroy_with_waiter() | pipeline_failure(argv[1]);
+}

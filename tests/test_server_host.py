@@ -253,13 +253,17 @@ def tsan_stress(tmp_path_factory):
     exe = str(d / "server_stress")
     subprocess.check_call(["g++", "-fsanitize=thread", *objs, "-o", exe, "-L/usr/local/cuda/lib64", "-lcublas",
                            "-lcudart", "-lpthread"])
-    return exe
+    for obj in objs:
+        os.remove(obj)
+    yield exe
+    os.remove(exe)  # the build is tens of MB
 
 
 @pytest.mark.timeout(900)
-def test_serving_core_has_no_data_races(tsan_stress):
-    """Many submit / poll / wait / stats threads and destroy with a waiter,
-    under ThreadSanitizer: no race reported, every request accounted for.
+def test_serving_core_has_no_data_races(tsan_stress, tmp_path):
+    """Many submit / poll / wait / stats threads, destroy with a waiter, and
+    the pipeline's reader and writer threads on its failure path, under
+    ThreadSanitizer: no race reported, every request accounted for.
     (Without a GPU each request fails fast; the locking is exercised all the
     same.)"""
     import os
@@ -270,7 +274,8 @@ def test_serving_core_has_no_data_races(tsan_stress):
     if torch.cuda.is_available():
         pytest.skip("the stress relies on requests failing fast without a GPU")
     env = dict(os.environ, TSAN_OPTIONS="halt_on_error=1 exitcode=66")
-    r = subprocess.run([tsan_stress], capture_output=True, text=True, timeout=600, env=env)
+    r = subprocess.run([tsan_stress, str(tmp_path)], capture_output=True, text=True, timeout=600, env=env)
     assert "ThreadSanitizer" not in r.stderr, r.stderr[-3000:]
     assert r.returncode == 0, (r.returncode, r.stderr[-2000:])
     assert r.stdout.split("\n")[0] == "mixed 800 800 800" and "destroy 10" in r.stdout
+    assert "pipeline 20" in r.stdout  # every run failed cleanly (no device)
