@@ -41,6 +41,7 @@ def pytest_configure(config):
     # temporary files of the tests stay inside the repository's ignored
     # working folder
     if not config.option.basetemp:
+        os.makedirs(os.path.join(ROOT, "_work"), exist_ok=True)  # pytest creates only the last level
         config.option.basetemp = os.path.join(ROOT, "_work", "pytest-tmp")
 
 
