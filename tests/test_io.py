@@ -182,7 +182,8 @@ def _records(draw):
     return out
 
 
-@settings(derandomize=True, max_examples=40, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+@settings(derandomize=True, max_examples=40, deadline=None,
+          suppress_health_check=[HealthCheck.function_scoped_fixture])
 @given(mats=_records())
 def test_mat_codec_round_trip_property(driver, tmp_path_factory, mats):
     d = tmp_path_factory.mktemp("prop")
@@ -210,7 +211,8 @@ def _finite_records(draw):
     return out
 
 
-@settings(derandomize=True, max_examples=30, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+@settings(derandomize=True, max_examples=30, deadline=None,
+          suppress_health_check=[HealthCheck.function_scoped_fixture])
 @given(mats=_finite_records())
 def test_txt_codec_round_trip_property(driver, tmp_path_factory, mats):
     """*.txt with finite values (subnormals and -0.0 included): the C++ reader
@@ -293,7 +295,8 @@ def test_codec_clean_under_sanitizers(asan_driver, tmp_path):
     assert (tmp_path / "out.bin").exists()
 
 
-@settings(derandomize=True, max_examples=25, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+@settings(derandomize=True, max_examples=25, deadline=None,
+          suppress_health_check=[HealthCheck.function_scoped_fixture])
 @given(mats=_records())
 def test_mat_round_trip_under_sanitizers(asan_driver, tmp_path_factory, mats):
     d = tmp_path_factory.mktemp("asanprop")
