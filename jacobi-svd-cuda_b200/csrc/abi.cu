@@ -300,9 +300,11 @@ int jsvd_plain_svd(const double *a, size_t rows, size_t columns, const jsvd_conf
                        sweeps, stream);
         if (rc != JSVD_OK) return rc;
         if (u)
-            JSVD_CUDA_TRY(cudaMemcpyAsync(u, plan->d_u, sizeof(double) * rows * columns, cudaMemcpyDeviceToHost, stream));
+            JSVD_CUDA_TRY(
+                cudaMemcpyAsync(u, plan->d_u, sizeof(double) * rows * columns, cudaMemcpyDeviceToHost, stream));
         if (sigma)
-            JSVD_CUDA_TRY(cudaMemcpyAsync(sigma, plan->d_sigma, sizeof(double) * columns, cudaMemcpyDeviceToHost, stream));
+            JSVD_CUDA_TRY(
+                cudaMemcpyAsync(sigma, plan->d_sigma, sizeof(double) * columns, cudaMemcpyDeviceToHost, stream));
         if (v)
             JSVD_CUDA_TRY(
                 cudaMemcpyAsync(v, plan->d_v, sizeof(double) * columns * columns, cudaMemcpyDeviceToHost, stream));

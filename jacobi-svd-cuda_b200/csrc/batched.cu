@@ -367,7 +367,8 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         classes[c].ctas_per_sm = kBuiltinTuning[c].ctas_per_sm;
         classes[c].a_shared = class_a_shared(c);
         classes[c].v_shared = class_v_shared(c);
-        classes[c].fn = c <= 2 ? batch_kernel<true, true> : (c == 3 ? batch_kernel<true, false> : batch_kernel<false, false>);
+        classes[c].fn = c <= 2 ? batch_kernel<true, true>
+                               : (c == 3 ? batch_kernel<true, false> : batch_kernel<false, false>);
         max_ctas[c] = kBuiltinTuning[c].max_ctas;
     }
     if (req.tuning != nullptr) {
@@ -681,7 +682,8 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
         };
         if (cudaMallocAsync(&d_flush, flush_bytes, st) != cudaSuccess ||
             cudaMallocAsync((void **)&d_sigma, sizeof(double) * std::max<size_t>(max_s, 1), st) != cudaSuccess ||
-            (want_v && cudaMallocAsync((void **)&d_v, sizeof(double) * std::max<size_t>(max_v, 1), st) != cudaSuccess) ||
+            (want_v &&
+             cudaMallocAsync((void **)&d_v, sizeof(double) * std::max<size_t>(max_v, 1), st) != cudaSuccess) ||
             (want_u && cudaMallocAsync((void **)&d_u, sizeof(double) * std::max<size_t>(max_u, 1), st) != cudaSuccess))
             return finish(cuda_failure(cudaGetLastError(), "cudaMallocAsync", __FILE__, __LINE__));
 
