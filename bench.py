@@ -729,6 +729,13 @@ def run_large(args, rank: int, world: int, device):
 
 
 def run_reference(args):
+    if args.workload in ("serve", "large"):
+        why = {"serve": "the reference has no serving path (its pipeline solves one matrix per host thread); its "
+                        "CPU arithmetic is timed on the tall, square512 and batch workloads",
+               "large": "the CPU sample extrapolates sampled rounds by the plain path's sweep count, and no "
+                        "plain-path sweep count has been measured on the 16384x8192 input; the reference's CPU "
+                        "arithmetic is timed on the tall, square512 and batch workloads"}
+        return {"impl": "reference", "unavailable": why[args.workload]}
     if args.workload == "batch":
         import workloads as W
         mats = W.batch_workload(min(args.batch_count, 400), seed=3)

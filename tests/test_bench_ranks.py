@@ -119,3 +119,15 @@ def test_batch_cpu_baseline_contract_fields():
     cb = bench.batch_cpu_baseline(mats, budget_s=0.05, threads=2)
     assert cb["unit"] == "SVD/s" and cb["kind"] == "port" and cb["cores"] == 2 and cb["value"] > 0
     assert cb["sample"].startswith("first ") and "of 40 matrices" in cb["sample"]
+
+
+@pytest.mark.parametrize("workload", ["serve", "large"])
+def test_reference_arm_unavailable_lines(workload):
+    import json
+
+    env = dict(os.environ, RANK="0", LOCAL_RANK="0", WORLD_SIZE="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                        workload], capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0, r.stderr[-1000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["impl"] == "reference" and d["unavailable"]
