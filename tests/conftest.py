@@ -38,11 +38,10 @@ def golden_input(name, fixture):
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
-    # temporary files of the tests stay inside the repository's ignored
-    # working folder
+    # temporary files of the tests stay inside the repository, in a folder
+    # that git ignores and each session starts afresh
     if not config.option.basetemp:
-        os.makedirs(os.path.join(ROOT, "_work"), exist_ok=True)  # pytest creates only the last level
-        config.option.basetemp = os.path.join(ROOT, "_work", "pytest-tmp")
+        config.option.basetemp = os.path.join(ROOT, ".pytest_tmp")
 
 
 @pytest.fixture(scope="session")
