@@ -80,3 +80,18 @@ def test_device_matrix_argument_checks(driver):
     out = subprocess.run([driver, "device-matrix"], capture_output=True, text=True, check=True).stdout.splitlines()
     assert out == ["DeviceMatrix dimensions must be positive."] * 2 + \
         ["Host data size does not match device matrix shape."]
+
+
+def test_documented_build_line_builds_a_caller(tmp_path):
+    """The integration guide's build line (g++ -std=c++20 -I include ...
+    -ljsvd) compiles and links a caller of the drop-in headers without the
+    CUDA headers on the include path."""
+    src = tmp_path / "app.cpp"
+    src.write_text(
+        "#include <vector>\n#include \"kernels.hpp\"\n#include \"kernels_ext.hpp\"\n"
+        "#include \"pipeline.hpp\"\n#include \"pipeline_ext.hpp\"\n#include \"io.hpp\"\n"
+        "int main() {\n  std::vector<double> a(12, 1.0);\n  jacobi::svd::JacobiSvdConfig cfg;\n"
+        "  try { (void)jacobi::svd::one_sided_jacobi_svd(a, 4, 3, cfg); } catch (const std::exception &) {}\n"
+        "  jacobi::svd::pipeline::PipelineConfig p;\n  (void)p;\n  return 0;\n}\n")
+    subprocess.check_call(["g++", "-std=c++20", "-I", os.path.join(ROOT, "include"), str(src), "-L", PKG,
+                           "-ljsvd", f"-Wl,-rpath,{PKG}", "-o", str(tmp_path / "app")])
