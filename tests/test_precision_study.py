@@ -81,3 +81,60 @@ def test_split_products_are_exact_in_fp32():
         ha = _round_significand(a.astype(np.float32), bits)
         hb = _round_significand((a[::-1] * 3.7).astype(np.float32), bits)
         assert np.array_equal((ha * hb).astype(np.float64), ha.astype(np.float64) * hb.astype(np.float64))
+
+
+def _jacobi_in(x: np.ndarray, eps: float, dtype, max_sweeps: int = 60):
+    """Cyclic one-sided Jacobi carried out in `dtype` (the reference's
+    schedule, rotation test and Rutishauser angle, one round at a time);
+    returns the rotated columns, V and the sweep count."""
+    import oracle as O
+
+    a = x.astype(dtype).copy()
+    n = a.shape[1]
+    v = np.eye(n, dtype=dtype)
+    rounds = [(np.array([p for p, _ in r]), np.array([q for _, q in r])) for r in O.schedule(n)]
+    for sweep in range(1, max_sweeps + 1):
+        rotated = False
+        for p, q in rounds:
+            ap, aq = a[:, p], a[:, q]
+            app, aqq = np.einsum("ij,ij->j", ap, ap), np.einsum("ij,ij->j", aq, aq)
+            apq = np.einsum("ij,ij->j", ap, aq)
+            rot = (np.abs(apq) > eps * np.sqrt(np.maximum(app, 0) * np.maximum(aqq, 0))) & (np.abs(apq) > 1e-300)
+            if not rot.any():
+                continue
+            rotated = True
+            zeta = (aqq - app) / (2 * np.where(rot, apq, 1))
+            t = np.sign(zeta + (zeta == 0)) / (np.abs(zeta) + np.sqrt(1 + zeta * zeta))
+            c = np.where(rot, 1 / np.sqrt(1 + t * t), 1).astype(dtype)
+            s = np.where(rot, c * t, 0).astype(dtype)
+            a[:, p], a[:, q] = c * ap - s * aq, s * ap + c * aq
+            vp, vq = v[:, p], v[:, q]
+            v[:, p], v[:, q] = c * vp - s * vq, s * vp + c * vq
+        if not rotated:
+            return a, v, sweep
+    return a, v, max_sweeps
+
+
+def test_fp32_phase_does_not_save_fp64_sweeps():
+    """On the triangular factor of the tall case (1024 x 256 version, kappa
+    1e6, after two QR factorisations): FP64 Jacobi alone takes 9 sweeps; an
+    FP32 phase to eps = 1e-6 takes 8 (sigma to 1.4e-5) and FP64 refinement on
+    X V32 (V32 re-orthogonalised in FP64) 3 more - 11 sequential sweeps, each
+    as latency-bound as an FP64 one."""
+    import os
+
+    import oracle as O
+    import workloads as W
+
+    a, s_true = W.tall_case(seed=2, m=1024, n=256, kappa=1e6)
+    _, r = np.linalg.qr(a)
+    _, p = np.linalg.qr(r.T)
+    x = p.T
+    _, s64, _, sw64 = O.plain_svd(x, eps=1e-14, threads=os.cpu_count() or 1)
+    a32, v32, sw32 = _jacobi_in(x, 1e-6, np.float32)
+    s32 = np.linalg.norm(a32.astype(np.float64), axis=0)
+    vq, _ = np.linalg.qr(v32.astype(np.float64))
+    _, sref, _, swref = O.plain_svd(x @ vq, eps=1e-14, threads=os.cpu_count() or 1)
+    assert 1e-6 < O.sigma_errors(s32, s_true)["max_rel"] < 1e-4  # the FP32 phase's level
+    assert O.sigma_errors(sref, s_true)["max_rel"] < 1e-10 and O.sigma_errors(s64, s_true)["max_rel"] < 1e-10
+    assert swref >= 2 and sw32 + swref > sw64, (sw64, sw32, swref)
