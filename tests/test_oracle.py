@@ -214,3 +214,18 @@ def test_cluster_subspaces_agree_with_lapack():
     order = np.argsort(-so)
     bad[:, [order[0], order[1]]] = bad[:, [order[1], order[0]]]
     assert O.cluster_subspace_sines(bad, so, vt.T, sl, floor=1e-3)["max_sine"] > 0.5
+
+
+@pytest.mark.parametrize("kind", ["tall", "clustered"])
+def test_workload_generators_have_their_stated_spectrum(kind):
+    """The bench's accuracy guard compares against the generators' own sigma
+    (A = U diag(sigma) V^T with Haar factors, formed in FP64): LAPACK on the
+    formed matrix agrees with it normwise to 1e-14 (smaller instances of the
+    tall and the graded + clustered workloads)."""
+    if kind == "tall":
+        a, s = W.tall_case(seed=2, m=512, n=128, kappa=1e6)
+    else:
+        s = W.graded_clustered_sigma(128, clusters=2, size=16, gap=1e-10)
+        a = W.spectrum_matrix(300, 128, s, 5)
+    got = np.linalg.svd(a, compute_uv=False)
+    assert O.sigma_errors(got, s)["normwise"] <= 1e-14
