@@ -229,3 +229,18 @@ def test_workload_generators_have_their_stated_spectrum(kind):
         a = W.spectrum_matrix(300, 128, s, 5)
     got = np.linalg.svd(a, compute_uv=False)
     assert O.sigma_errors(got, s)["normwise"] <= 1e-14
+
+
+def test_batch_workload_matches_its_description():
+    """m ~ U{16..256}, n ~ U{8..m}, kappa log-uniform in [1e1, 1e6], sigma in
+    [1/kappa, 1], stored as FP32 - as the bench line describes it."""
+    ms, ns, kappas, _ = W.batch_shapes(20000, seed=3)
+    assert ms.min() == 16 and ms.max() == 256 and np.all(ns >= 8) and np.all(ns <= ms)
+    assert kappas.min() >= 10.0 and kappas.max() <= 1e6
+    lk = np.log10(kappas)
+    assert abs(lk.mean() - 3.5) < 0.05  # log-uniform on [1, 6]
+    mats = W.batch_workload(20, seed=3)
+    assert all(a.dtype == np.float32 and a.shape == (m, n) for a, m, n in zip(mats, ms[:20], ns[:20]))
+    for a in mats[:5]:
+        s = np.linalg.svd(a.astype(np.float64), compute_uv=False)
+        assert s[0] <= 1.0 + 1e-6 and s[-1] > 0.0
