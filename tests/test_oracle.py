@@ -240,7 +240,8 @@ def test_batch_workload_matches_its_description():
     lk = np.log10(kappas)
     assert abs(lk.mean() - 3.5) < 0.05  # log-uniform on [1, 6]
     mats = W.batch_workload(20, seed=3)
-    assert all(a.dtype == np.float32 and a.shape == (m, n) for a, m, n in zip(mats, ms[:20], ns[:20]))
+    ms20, ns20, _, _ = W.batch_shapes(20, seed=3)  # shapes depend on the count (all m drawn first)
+    assert all(a.dtype == np.float32 and a.shape == (m, n) for a, m, n in zip(mats, ms20, ns20))
     for a in mats[:5]:
         s = np.linalg.svd(a.astype(np.float64), compute_uv=False)
         assert s[0] <= 1.0 + 1e-6 and s[-1] > 0.0
