@@ -82,7 +82,7 @@ def report_dict(rep) -> dict:
 
 
 def main(argv=None) -> int:
-    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap = argparse.ArgumentParser(description=" ".join(__doc__.split("\n\n")[0].split()))
     ap.add_argument("--out", required=True, help="path of the table header to write")
     ap.add_argument("--json", help="also write the report as JSON here")
     ap.add_argument("--count", type=int, default=20000, help="matrices in the timed batch")
