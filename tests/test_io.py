@@ -304,3 +304,25 @@ def test_mat_round_trip_under_sanitizers(asan_driver, tmp_path_factory, mats):
     r = run(asan_driver, "stream-copy", d / "in.mat", d / "out.mat")
     assert r.returncode == 0 and "Sanitizer" not in r.stderr and "runtime error" not in r.stderr, r.stderr[-800:]
     assert (d / "out.mat").read_bytes() == (d / "in.mat").read_bytes()
+
+
+def test_cli_option_syntax_like_the_reference(tmp_path):
+    """Option forms the reference's parser accepts (src/main.cpp:925-1100):
+    --name=value, --name value, -xVALUE, -x VALUE, clustered flags (-yq), and
+    `--` ending the options; with the same argument errors (exit code 2)."""
+    src = tmp_path / "c.txt"
+    src.write_text("1 2\n3 4\n")
+    for form in (["--epsilon=1e-12"], ["--epsilon", "1e-12"], ["-e1e-12"], ["-e", "1e-12"]):
+        r = cli(src, *form, "--dry-run")
+        assert r.returncode == 0 and "epsilon         : 1e-12" in r.stdout, (form, r.stderr)
+    r = cli(src, "--max-sweeps=7", "-t64", "-yq", "--dry-run")
+    assert r.returncode == 0 and "max-sweeps      : 7" in r.stdout and "threads-per-blk : 64" in r.stdout
+    assert "force-overwrite : true" in r.stdout
+    for args, msg in ((["--force=1"], "Option --force does not take a value."),
+                      (["-z"], "Unknown short option: -z"),
+                      (["--dry-run", "-e"], "Missing value for --epsilon.")):
+        r = cli(src, *args, "--dry-run") if args[-1] != "-e" else cli(src, *args)
+        assert r.returncode == 2 and msg in r.stderr, (args, r.stderr)
+    # after `--` everything is positional: here the output path
+    r = cli(src, "--dry-run", "--", str(tmp_path / "--out.txt"))
+    assert r.returncode == 0 and f"output          : {tmp_path / '--out.txt'}" in r.stdout
