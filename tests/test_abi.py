@@ -139,3 +139,19 @@ def test_auto_tune_layout_needs_a_report():
     cfg = jsvd.default_config()
     assert jsvd.lib().jsvd_auto_tune_layout(ctypes.byref(cfg), None) == jsvd.JSVD_ERR_INVALID_ARGUMENT
     assert jsvd.last_error()[1] == "report must not be null."
+
+
+def test_integration_guide_ctypes_snippet_runs():
+    """The ctypes binding shown in the integration guide runs as written
+    (library path adjusted to this checkout): it loads the library, builds the
+    config and makes the call; without a GPU the call returns the CUDA status,
+    with one it solves."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    start = text.index("```python\n", text.index("A ctypes binding")) + len("```python\n")
+    code = text[start:text.index("```", start)]
+    code = code.replace('"jacobi-svd-cuda_b200/libjsvd.so"', repr(os.path.join(ROOT, "jacobi-svd-cuda_b200",
+                                                                                "libjsvd.so")))
+    scope = {"A": np.arange(12.0).reshape(4, 3) + np.eye(4, 3)}
+    exec(compile(code, "INTEGRATION.md", "exec"), scope)
+    assert scope["rc"] in (jsvd.JSVD_OK, jsvd.JSVD_ERR_CUDA)
+    assert scope["cfg"].epsilon == 1e-9 and scope["cfg"].max_sweeps == 128
