@@ -9,12 +9,15 @@
 #include <filesystem>
 #include <iomanip>
 #include <iostream>
+#include <limits>
 #include <optional>
 #include <stdexcept>
 #include <string>
 #include <string_view>
 #include <vector>
 
+#include "io.hpp"
+#include "jsvd.h"
 #include "kernels.hpp"
 #include "pipeline.hpp"
 #include "pipeline_ext.hpp"
@@ -48,6 +51,7 @@ namespace
         bool help = false, version = false;
         bool precond = false;
         std::filesystem::path residual_report;  // empty: off
+        std::filesystem::path verify;           // empty: solve; else check this result file
     };
 
     struct Flag
@@ -83,6 +87,9 @@ namespace
         {"solver", '\0', true, "NAME", "Large-testcase solver: plain (bit-identical, default) | precond."},
         {"residual-report", '\0', true, "PATH",
          "Write each testcase's rows, columns, epsilon, sweeps, rho_A, rho_U, rho_V as a JSON line."},
+        {"verify", '\0', true, "PATH",
+         "Check the result file PATH (U, Sigma, V per testcase) against the input: print rho_A, rho_U, rho_V "
+         "per testcase as JSON lines; nothing is solved."},
         {"help", 'h', false, "", "Show this help message."},
         {"version", 'v', false, "", "Show version information."},
     };
@@ -189,6 +196,7 @@ namespace
             o.precond = l == "precond";
         }
         else if (n == "residual-report") o.residual_report = std::string(v);
+        else if (n == "verify") o.verify = std::string(v);
         else if (n == "help") o.help = true;
         else if (n == "version") o.version = true;
     }
@@ -336,12 +344,77 @@ namespace
             o.output = positional[p++];
         if (p < positional.size())
             throw ArgError("Unexpected positional argument: " + positional[p]);
-        if (!o.help && !o.version)
+        if (!o.verify.empty() && !o.help && !o.version)
+        {
+            if (o.input.empty())
+                throw ArgError("Missing input file. Use --input <path>.");
+            for (const auto &f : {o.input, o.verify})
+                if (!std::filesystem::is_regular_file(f))
+                    throw ArgError("Input file does not exist: " + f.string());
+        }
+        else if (!o.help && !o.version)
         {
             normalize(o);
             validate(o);
         }
         return o;
+    }
+
+    void json_number(std::ostream &os, double x)
+    {
+        if (std::isfinite(x))
+            os << x;
+        else
+            os << "null";
+    }
+
+    // --verify: the validation metrics of every testcase of the input against
+    // the result file's U, Sigma (1 x n), V records, without solving.
+    int run_verify(const Options &o)
+    {
+        using namespace jacobi::svd;
+        auto read_file = [](const std::filesystem::path &p, MatrixFileFormat f) {
+            if (f == MatrixFileFormat::auto_detect)
+            {
+                const auto e = ext_format(p);
+                if (!e)
+                    throw ArgError("Cannot infer format from extension: " + p.string() + ".");
+                f = *e;
+            }
+            return f == MatrixFileFormat::txt ? io::read_txt_file(p) : io::read_mat_file(p);
+        };
+        const std::vector<io::Matrix> in = read_file(o.input, o.input_format);
+        const std::vector<io::Matrix> res = read_file(o.verify, o.output_format);
+        if (res.size() != 3 * in.size())
+            throw std::runtime_error("Result file holds " + std::to_string(res.size()) +
+                                     " matrices; expected 3 (U, Sigma, V) for each of the " +
+                                     std::to_string(in.size()) + " testcases.");
+        std::cout << std::setprecision(std::numeric_limits<double>::max_digits10);
+        for (std::size_t k = 0; k < in.size(); ++k)
+        {
+            const io::Matrix &a = in[k], &u = res[3 * k], &sg = res[3 * k + 1], &v = res[3 * k + 2];
+            const std::size_t m = a.rows, n = a.columns;
+            if (u.rows != m || u.columns != n || sg.rows != 1 || sg.columns != n || v.rows != n || v.columns != n)
+                throw std::runtime_error("Testcase[" + std::to_string(k) + "] result shapes do not match the input.");
+            jsvd_residual_report r{};
+            if (jsvd_residuals(a.values.data(), u.values.data(), sg.values.data(), v.values.data(), m, n, &r) !=
+                JSVD_OK)
+            {
+                char buf[512];
+                jsvd_last_error(buf, sizeof(buf));
+                throw std::runtime_error("Testcase[" + std::to_string(k) + "]: " + buf);
+            }
+            std::cout << "{\"index\": " << k << ", \"rows\": " << m << ", \"columns\": " << n << ", \"rho_A\": ";
+            json_number(std::cout, r.rho_a);
+            std::cout << ", \"rho_U\": ";
+            json_number(std::cout, r.rho_u);
+            std::cout << ", \"rho_V\": ";
+            json_number(std::cout, r.rho_v);
+            std::cout << ", \"sigma_max\": ";
+            json_number(std::cout, r.sigma_max);
+            std::cout << "}\n";
+        }
+        return 0;
     }
 
     void print_help(const std::string &exe)
@@ -400,6 +473,8 @@ int main(int argc, char **argv)
             std::cout << "jacobi-svd-b200 CLI v0.1.0 (sm_100a)\n";
             return 0;
         }
+        if (!o.verify.empty())
+            return run_verify(o);
         if (o.dry_run)
         {
             std::cout << "Dry run: pipeline was not executed.\n";

@@ -326,3 +326,42 @@ def test_cli_option_syntax_like_the_reference(tmp_path):
     # after `--` everything is positional: here the output path
     r = cli(src, "--dry-run", "--", str(tmp_path / "--out.txt"))
     assert r.returncode == 0 and f"output          : {tmp_path / '--out.txt'}" in r.stdout
+
+
+def test_cli_verify_checks_a_result_file(tmp_path):
+    """--verify IN RESULT prints each testcase's rho_A, rho_U, rho_V (the
+    reference design's validation metrics) for a result file made by any
+    implementation - here the reference CLI's own output - without solving."""
+    import json
+
+    import oracle as O
+
+    inp = os.path.join(ROOT, "tests", "golden", "pipeline_in.mat")
+    ref_out = os.path.join(ROOT, "tests", "golden", "pipeline_ref_out.mat")
+    r = subprocess.run([CLI, inp, "--verify", ref_out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    recs = [json.loads(line) for line in r.stdout.splitlines()]
+    mats, res = matfile.read(inp), matfile.read(ref_out)
+    assert [d["index"] for d in recs] == list(range(len(mats)))
+    for d, a in zip(recs, mats):
+        k = d["index"]
+        exp = O.residuals(a, res[3 * k], res[3 * k + 1].ravel(), res[3 * k + 2])
+        assert (d["rows"], d["columns"]) == a.shape and d["rho_A"] < 1e-13
+        for key in ("rho_A", "rho_U", "rho_V"):
+            assert abs(d[key] - exp[key]) <= 1e-14 + 1e-10 * exp[key]
+    # a tampered U value shows in that testcase's rho_A
+    bad = [x.copy() for x in res]
+    bad[3 * 6][2, 1] += 1e-3
+    matfile.write(tmp_path / "bad.mat", bad)
+    recs = [json.loads(line) for line in subprocess.run([CLI, inp, "--verify", tmp_path / "bad.mat"],
+                                                          capture_output=True, text=True, check=True).stdout.splitlines()]
+    assert recs[6]["rho_A"] > 1e-5 and all(d["rho_A"] < 1e-13 for d in recs if d["index"] != 6)
+    # a record missing, and records in the wrong order
+    matfile.write(tmp_path / "short.mat", res[:-1])
+    r = subprocess.run([CLI, inp, "--verify", tmp_path / "short.mat"], capture_output=True, text=True)
+    assert r.returncode == 1 and "expected 3 (U, Sigma, V) for each of the 12 testcases" in r.stderr
+    matfile.write(tmp_path / "swapped.mat", [res[1], res[0]] + res[2:])
+    r = subprocess.run([CLI, inp, "--verify", tmp_path / "swapped.mat"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Testcase[0] result shapes do not match the input." in r.stderr
+    r = subprocess.run([CLI, inp, "--verify", tmp_path / "missing.mat"], capture_output=True, text=True)
+    assert r.returncode == 2 and "Input file does not exist" in r.stderr
