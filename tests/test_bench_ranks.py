@@ -131,3 +131,27 @@ def test_reference_arm_unavailable_lines(workload):
     assert r.returncode == 0, r.stderr[-1000:]
     d = json.loads(r.stdout.strip().splitlines()[-1])
     assert d["impl"] == "reference" and d["unavailable"]
+
+
+def test_profile_commands_use_committed_files_and_current_flags():
+    """Every ncu summary under profiles/ gives the command that made it: the
+    script it runs exists, each bench flag it passes is one bench.py still
+    accepts, and every ncu command keeps --clock-control none."""
+    import glob
+    import re
+
+    help_text = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True,
+                               text=True, check=True).stdout
+    files = [p for p in glob.glob(os.path.join(ROOT, "profiles", "*.md")) if not p.endswith("README.md")]
+    assert files
+    for path in files:
+        text = open(path).read()
+        cmds = re.findall(r'"(python \S+[^"]*)"', text)
+        assert cmds, path
+        for cmd in cmds:
+            script = cmd.split()[1]
+            assert os.path.exists(os.path.join(ROOT, script)), (path, script)
+            for flag in re.findall(r"(--[a-z][a-z0-9-]*)", cmd):
+                assert flag in help_text, (path, flag)
+        for line in re.findall(r"^\s*ncu .*$", text, flags=re.M):
+            assert "--clock-control none" in line, (path, line)
