@@ -8,6 +8,7 @@ from __future__ import annotations
 import ctypes
 import os
 import subprocess
+from typing import NamedTuple
 
 import numpy as np
 
@@ -321,6 +322,41 @@ def precond_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, w
     check(lib().jsvd_precond_svd(a.ctypes.data, m, n, ctypes.byref(cfg), u.ctypes.data if u is not None else None,
                                  s.ctypes.data, v.ctypes.data if v is not None else None, ctypes.byref(sw)))
     return u, s, v, sw.value
+
+
+class SvdResult(NamedTuple):
+    u: np.ndarray | None
+    sigma: np.ndarray
+    v: np.ndarray | None
+    sweeps: int
+
+
+_HOST_ENTRIES = {"plain": "jsvd_plain_svd", "precond": "jsvd_precond_svd", "blockpair": "jsvd_blockpair_svd",
+                 "blocked": "jsvd_blocked_svd"}
+
+
+def svd(a: np.ndarray, solver: str = "plain", cfg: Config | None = None, want_u: bool = True,
+        want_v: bool = True) -> SvdResult:
+    """One-sided Jacobi SVD of a row-major host matrix (rows >= columns)
+    through the chosen solver's host-buffer entry point.  "plain" is the
+    reference's arithmetic bit for bit; "precond", "blockpair" and "blocked"
+    are accurate to working precision.  sigma is unsorted, as the reference
+    returns it; U and V are row-major."""
+    if solver not in _HOST_ENTRIES:
+        raise ValueError(f"solver must be one of {sorted(_HOST_ENTRIES)}")
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError("expected a 2-D matrix")
+    m, n = a.shape
+    cfg = cfg or default_config()
+    u = np.empty((m, n)) if want_u else None
+    s = np.empty(n)
+    v = np.empty((n, n)) if want_v else None
+    sw = ctypes.c_int(0)
+    fn = getattr(lib(), _HOST_ENTRIES[solver])
+    check(fn(a.ctypes.data if a.size else None, m, n, ctypes.byref(cfg), u.ctypes.data if u is not None else None,
+             s.ctypes.data, v.ctypes.data if v is not None else None, ctypes.byref(sw)))
+    return SvdResult(u, s, v, sw.value)
 
 
 def precond_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:

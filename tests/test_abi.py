@@ -155,3 +155,12 @@ def test_integration_guide_ctypes_snippet_runs():
     exec(compile(code, "INTEGRATION.md", "exec"), scope)
     assert scope["rc"] in (jsvd.JSVD_OK, jsvd.JSVD_ERR_CUDA)
     assert scope["cfg"].epsilon == 1e-9 and scope["cfg"].max_sweeps == 128
+
+
+def test_svd_entry_validates_before_cuda():
+    with pytest.raises(ValueError):
+        jsvd.svd(np.ones((4, 3)), solver="lapack")
+    for solver in ("plain", "precond", "blockpair", "blocked"):
+        with pytest.raises(jsvd.InvalidArgument) as e:
+            jsvd.svd(np.ones((3, 4)), solver=solver)
+        assert "rows >= columns" in str(e.value)

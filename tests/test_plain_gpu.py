@@ -225,3 +225,16 @@ def test_plain_angle_every_warp_bitwise(cuda_device, T):
     finally:
         jsvd.set_sweep_mode(0)
     _assert_bitwise(got, _oracle(a, 1e-13, T))
+
+
+def test_svd_entry_matches_the_solver_entries(cuda_device):
+    """jsvd.svd(a, solver) is the solver's host entry: plain bit for bit,
+    the others within the working-precision tolerance."""
+    a = W.gaussian_splitmix(200, 60, seed=31)
+    cfg = jsvd.default_config(epsilon=1e-13)
+    r = jsvd.svd(a, "plain", cfg)
+    _assert_bitwise((r.u, r.sigma, r.v, r.sweeps), jsvd.plain_svd(a, cfg))
+    ref = np.linalg.svd(a, compute_uv=False)
+    for solver in ("precond", "blockpair", "blocked"):
+        r = jsvd.svd(a, solver, cfg)
+        assert O.sigma_errors(r.sigma, ref)["normwise"] <= 1e-13, solver
