@@ -40,10 +40,18 @@ __global__ void __launch_bounds__(kTile *kTileRows)
 // each on the sub-matrix starting at that row (src advanced by whole rows, dst
 // by the same number of rows within each column).  One launch, with exactly
 // the plain arguments, up to 2,097,120 rows.
+constexpr int kTransposeMaxRows = 65535 * kTile;  // rows one launch covers
+
+// Launches launch_rowmajor_to_colmajor makes for `rows` rows.
+inline int rowmajor_to_colmajor_launches(int rows)
+{
+    return rows <= 0 ? 0 : 1 + (rows - 1) / kTransposeMaxRows;
+}
+
 inline cudaError_t launch_rowmajor_to_colmajor(const double *src, int rows, int cols, double *dst, long ldd,
                                                cudaStream_t stream)
 {
-    constexpr int kMaxRows = 65535 * kTile;
+    constexpr int kMaxRows = kTransposeMaxRows;
     const dim3 block(kTile, kTileRows);
     for (long long r0 = 0; r0 < rows; r0 += kMaxRows) {
         const int rr = (int)std::min<long long>(kMaxRows, rows - r0);

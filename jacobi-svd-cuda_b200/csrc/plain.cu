@@ -1008,7 +1008,7 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
     uses += 1;
     st.solves += 1;
     st.sweeps += (unsigned long long)executed;
-    st.other_launches += 3 + (out_u ? 1 : 0) + (out_v ? 1 : 0);
+    st.other_launches += 2 + rowmajor_to_colmajor_launches(im) + (out_u ? 1 : 0) + (out_v ? 1 : 0);
     double *sig = out_sigma ? out_sigma : sigma_w;
     pick_sigma(T)<<<in, T, 0, stream>>>(a_w, lda, im, sig);
     JSVD_CUDA_TRY(cudaGetLastError());

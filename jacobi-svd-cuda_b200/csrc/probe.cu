@@ -43,8 +43,13 @@ extern "C" int jsvd_probe_fp64_tflops(double *tflops)
         JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         const int grid = sms * 8, block = 256, iters = 4096;
         cudaStream_t st = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ScopeExit release([&] {  // on every return path
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            if (st) cudaStreamDestroy(st);
+        });
         JSVD_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-        cudaEvent_t e0, e1;
         JSVD_CUDA_TRY(cudaEventCreate(&e0));
         JSVD_CUDA_TRY(cudaEventCreate(&e1));
         fp64_fma_probe<<<grid, block, 0, st>>>(nullptr, iters, 0.999999, 1e-7, 0);  // warm-up
@@ -58,9 +63,6 @@ extern "C" int jsvd_probe_fp64_tflops(double *tflops)
             JSVD_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
             if (ms < best) best = ms;
         }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        cudaStreamDestroy(st);
         const double flops = 2.0 * kChains * (double)iters * grid * block;
         *tflops = flops / (best * 1e-3) / 1e12;
         return JSVD_OK;
