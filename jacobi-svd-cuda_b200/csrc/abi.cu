@@ -31,13 +31,24 @@ ErrorState &error_state()
     return state;
 }
 
+// The calling thread's library stream on one device, and the event that
+// orders it after the legacy default stream (created on first use).
+struct DeviceStream {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t legacy_done = nullptr;
+};
+
 struct ThreadCache {
     std::vector<std::unique_ptr<PlainPlan>> plans;  // most recently used last
-    std::vector<std::pair<int, cudaStream_t>> streams;
+    std::vector<DeviceStream> streams;
     ~ThreadCache()
     {
         plans.clear();
-        for (auto &s : streams) cudaStreamDestroy(s.second);
+        for (auto &s : streams) {
+            if (s.legacy_done) cudaEventDestroy(s.legacy_done);
+            cudaStreamDestroy(s.stream);
+        }
     }
 };
 
@@ -76,8 +87,7 @@ int host_buffer_solve(DeviceSolveFn device_fn, const double *a, size_t rows, siz
 {
     set_last_error(JSVD_OK, "");
     jsvd_config def;
-    jsvd_config_default(&def);
-    const jsvd_config &c = cfg ? *cfg : def;
+    const jsvd_config &c = config_or_default(cfg, def);
     int rc = validate_plain_request(a, rows, columns, c);
     if (rc != JSVD_OK) return rc;
     int dev = 0;
@@ -99,14 +109,20 @@ int host_buffer_solve(DeviceSolveFn device_fn, const double *a, size_t rows, siz
     return JSVD_OK;
 }
 
-cudaStream_t thread_stream(int device)
+namespace {
+// The calling thread's stream record for `device`, created on first use;
+// nullptr when the stream cannot be created.
+DeviceStream *device_stream(int device)
 {
     auto &cache = thread_cache();
     for (auto &s : cache.streams)
-        if (s.first == device) return s.second;
+        if (s.device == device) return &s;
     cudaStream_t st = nullptr;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
-    cache.streams.emplace_back(device, st);
+    DeviceStream rec;
+    rec.device = device;
+    rec.stream = st;
+    cache.streams.push_back(rec);
     // The library's workspaces come from the device's default stream-ordered
     // pool.  With the pool's default release threshold (0) every synchronise
     // hands freed memory back to the driver and the next call maps it again
@@ -120,7 +136,32 @@ cudaStream_t thread_stream(int device)
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
-    return st;
+    return &cache.streams.back();
+}
+}  // namespace
+
+cudaStream_t thread_stream(int device)
+{
+    DeviceStream *s = device_stream(device);
+    return s ? s->stream : nullptr;
+}
+
+int entry_stream(void *caller_stream, cudaStream_t *out)
+{
+    if (caller_stream != nullptr) {
+        *out = static_cast<cudaStream_t>(caller_stream);
+        return JSVD_OK;
+    }
+    int dev = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    DeviceStream *s = device_stream(dev);
+    if (s == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
+    if (s->legacy_done == nullptr)
+        JSVD_CUDA_TRY(cudaEventCreateWithFlags(&s->legacy_done, cudaEventDisableTiming));
+    JSVD_CUDA_TRY(cudaEventRecord(s->legacy_done, cudaStreamLegacy));
+    JSVD_CUDA_TRY(cudaStreamWaitEvent(s->stream, s->legacy_done, 0));
+    *out = s->stream;
+    return JSVD_OK;
 }
 
 int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t stream, PlainPlan **out)
@@ -192,27 +233,11 @@ int plain_device_impl(const double *d_a, size_t rows, size_t cols, const jsvd_co
                       double *d_sigma, double *d_v, int *sweeps, cudaStream_t stream, bool gram_stop = false)
 {
     jsvd_config def;
-    jsvd_config_default(&def);
-    const jsvd_config &c = cfg ? *cfg : def;
+    const jsvd_config &c = config_or_default(cfg, def);
     int rc = validate_plain_request(d_a, rows, cols, c);
     if (rc != JSVD_OK) return rc;
-    int dev = 0;
-    JSVD_CUDA_TRY(cudaGetDevice(&dev));
-    if (stream == nullptr) {
-        // The caller's buffers were produced on the legacy default stream:
-        // order the library's stream after everything queued there so far.
-        stream = thread_stream(dev);
-        if (stream == nullptr)
-            return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-        thread_local cudaEvent_t legacy_done = nullptr;
-        thread_local int legacy_dev = -1;
-        if (legacy_done == nullptr || legacy_dev != dev) {
-            JSVD_CUDA_TRY(cudaEventCreateWithFlags(&legacy_done, cudaEventDisableTiming));
-            legacy_dev = dev;
-        }
-        JSVD_CUDA_TRY(cudaEventRecord(legacy_done, cudaStreamLegacy));
-        JSVD_CUDA_TRY(cudaStreamWaitEvent(stream, legacy_done, 0));
-    }
+    rc = entry_stream(stream, &stream);
+    if (rc != JSVD_OK) return rc;
     PlainPlan *plan = nullptr;
     rc = acquire_plain_plan(rows, cols, reduction_lanes(c.threads_per_block), c.epsilon, stream, &plan);
     if (rc != JSVD_OK) return rc;
@@ -282,8 +307,7 @@ int jsvd_plain_svd(const double *a, size_t rows, size_t columns, const jsvd_conf
     return c_entry([&]() -> int {
         set_last_error(JSVD_OK, "");
         jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
+        const jsvd_config &c = config_or_default(cfg, def);
         int rc = validate_plain_request(a, rows, columns, c);
         if (rc != JSVD_OK) return rc;
         int dev = 0;
@@ -318,8 +342,7 @@ int jsvd_auto_tune_layout(const jsvd_config *cfg, jsvd_autotune_report *report)
     return c_entry([&]() -> int {
         set_last_error(JSVD_OK, "");
         jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
+        const jsvd_config &c = config_or_default(cfg, def);
         if (!report) return invalid_argument("report must not be null.");
         // Validation order of src/kernels.cu:1078-1086.
         if (c.layout_transpose_min_columns <= 0)
@@ -404,7 +427,7 @@ void jsvd_plain_set_vpass_in_global(int enable) { set_vpass_global_forced(enable
 void jsvd_release_thread_cache(void)
 {
     auto &cache = thread_cache();
-    for (auto &s : cache.streams) cudaStreamSynchronize(s.second);
+    for (auto &s : cache.streams) cudaStreamSynchronize(s.stream);
     cache.plans.clear();
     bp_release_thread_plans();
     pc_release_thread_plans();

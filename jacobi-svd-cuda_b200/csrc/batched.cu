@@ -514,19 +514,12 @@ extern "C" int jsvd_batch_svd_device(int count, const int *rows, const int *cols
     return c_entry([&]() -> int {
         set_last_error(JSVD_OK, "");
         jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
+        const jsvd_config &c = config_or_default(cfg, def);
         const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, d_sigma == nullptr, c);
         if (bad != JSVD_OK) return bad;
         if (count == 0) return JSVD_OK;  // nothing to solve, no CUDA call
-        int dev = 0;
-        JSVD_CUDA_TRY(cudaGetDevice(&dev));
-        cudaStream_t st = (cudaStream_t)stream;
-        if (st == nullptr) {
-            st = thread_stream(dev);
-            if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-            JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
-        }
+        cudaStream_t st = nullptr;
+        if (const int e = entry_stream(stream, &st); e != JSVD_OK) return e;
         BatchRequest req;
         req.count = count;
         req.rows = rows;
@@ -605,8 +598,7 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
     return c_entry([&]() -> int {
         set_last_error(JSVD_OK, "");
         jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
+        const jsvd_config &c = config_or_default(cfg, def);
         if (report == nullptr) return invalid_argument("Autotune report must not be null.");
         const int bad = check_batch_args(count, rows, cols, a_offsets, d_a, false, c);
         if (bad != JSVD_OK) return bad;
@@ -614,14 +606,10 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
         for (int k = 0; k < kClasses; ++k) report->builtin[k] = kBuiltinTuning[k];
         if (count == 0) return JSVD_OK;
         if (reps <= 0) reps = 2;
+        cudaStream_t st = nullptr;
+        if (const int e = entry_stream(stream, &st); e != JSVD_OK) return e;
         int dev = 0;
         JSVD_CUDA_TRY(cudaGetDevice(&dev));
-        cudaStream_t st = (cudaStream_t)stream;
-        if (st == nullptr) {
-            st = thread_stream(dev);
-            if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-            JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
-        }
         int sms = 0, smem_per_sm = 0;
         JSVD_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         JSVD_CUDA_TRY(cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));

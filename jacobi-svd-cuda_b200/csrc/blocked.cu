@@ -417,18 +417,11 @@ extern "C" int jsvd_blocked_svd_device(const double *d_a, size_t rows, size_t co
     return c_entry([&]() -> int {
         set_last_error(JSVD_OK, "");
         jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
+        const jsvd_config &c = config_or_default(cfg, def);
         int rc = validate_plain_request(d_a, rows, columns, c);
         if (rc != JSVD_OK) return rc;
-        int dev = 0;
-        JSVD_CUDA_TRY(cudaGetDevice(&dev));
-        cudaStream_t st = (cudaStream_t)stream;
-        if (st == nullptr) {
-            st = thread_stream(dev);
-            if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-            JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
-        }
+        cudaStream_t st = nullptr;
+        if (const int e = entry_stream(stream, &st); e != JSVD_OK) return e;
         // Fewer than two blocks: there is no block pair to rotate; the plain sweep
         // handles it.  So does it for inputs taller than this engine's grids
         // allow (row tiles of 32 along grid.y, at most 65535 blocks).

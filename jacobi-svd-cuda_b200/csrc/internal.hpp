@@ -34,6 +34,15 @@ private:
     F release_;
 };
 
+// *cfg, or the defaults (jsvd_config_default) written to `storage` when cfg is
+// null.
+inline const jsvd_config &config_or_default(const jsvd_config *cfg, jsvd_config &storage)
+{
+    if (cfg) return *cfg;
+    jsvd_config_default(&storage);
+    return storage;
+}
+
 // A device-buffer entry point (jsvd_*_svd_device).
 using DeviceSolveFn = int (*)(const double *, size_t, size_t, const jsvd_config *, double *, double *, double *,
                               int *, void *);

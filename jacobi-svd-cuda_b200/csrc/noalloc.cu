@@ -268,8 +268,7 @@ extern "C" int jsvd_plain_svd_noalloc(const double *d_a, size_t rows, size_t col
     return c_entry([&]() -> int {
         set_last_error(JSVD_OK, "");
         jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
+        const jsvd_config &c = config_or_default(cfg, def);
         int rc = validate_plain_request(d_a, rows, columns, c);
         if (rc != JSVD_OK) return rc;
         const size_t need = rows * columns + columns * columns + columns + 1;

@@ -119,4 +119,10 @@ int plain_device_solve(const double *d_a, size_t rows, size_t cols, const jsvd_c
 int acquire_plain_plan(size_t m, size_t n, int T, double eps, cudaStream_t stream, PlainPlan **plan);
 cudaStream_t thread_stream(int device);
 
+// The stream a device-buffer entry point runs on: the caller's when it passed
+// one, else the calling thread's library stream on the current device, made to
+// wait (on the device, without blocking the host) for all work queued so far on
+// the legacy default stream, where the caller's buffers were produced.
+int entry_stream(void *caller_stream, cudaStream_t *out);
+
 }  // namespace jsvd

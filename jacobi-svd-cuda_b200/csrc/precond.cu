@@ -598,18 +598,11 @@ extern "C" int jsvd_precond_svd_device(const double *d_a, size_t rows, size_t co
     return c_entry([&]() -> int {
         set_last_error(JSVD_OK, "");
         jsvd_config def;
-        jsvd_config_default(&def);
-        const jsvd_config &c = cfg ? *cfg : def;
+        const jsvd_config &c = config_or_default(cfg, def);
         int rc = validate_plain_request(d_a, rows, columns, c);
         if (rc != JSVD_OK) return rc;
-        int dev = 0;
-        JSVD_CUDA_TRY(cudaGetDevice(&dev));
-        cudaStream_t st = (cudaStream_t)stream;
-        if (st == nullptr) {
-            st = thread_stream(dev);
-            if (st == nullptr) return cuda_failure(cudaGetLastError(), "cudaStreamCreateWithFlags", __FILE__, __LINE__);
-            JSVD_CUDA_TRY(cudaStreamSynchronize(cudaStreamLegacy));
-        }
+        cudaStream_t st = nullptr;
+        if (const int e = entry_stream(stream, &st); e != JSVD_OK) return e;
         if (columns == 1) return jsvd_plain_svd_device(d_a, rows, columns, &c, d_u, d_sigma, d_v, sweeps, st);
         return precond_impl(d_a, rows, columns, c, d_u, d_sigma, d_v, sweeps, st);
     });
