@@ -292,38 +292,6 @@ def arith_variant() -> int:
     return int(lib().jsvd_plain_arith_variant())
 
 
-def plain_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, want_v: bool = True):
-    """Host-buffer plain solve -> (U or None, sigma, V or None, sweeps)."""
-    a = np.ascontiguousarray(a, dtype=np.float64)
-    if a.ndim != 2:
-        raise ValueError("expected a 2-D matrix")
-    m, n = a.shape
-    cfg = cfg or default_config()
-    u = np.empty((m, n)) if want_u else None
-    s = np.empty(n)
-    v = np.empty((n, n)) if want_v else None
-    sw = ctypes.c_int(0)
-    rc = lib().jsvd_plain_svd(a.ctypes.data if a.size else None, m, n, ctypes.byref(cfg),
-                              u.ctypes.data if u is not None else None, s.ctypes.data,
-                              v.ctypes.data if v is not None else None, ctypes.byref(sw))
-    check(rc)
-    return u, s, v, sw.value
-
-
-def precond_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, want_v: bool = True):
-    """Host-buffer QR-preconditioned solve -> (U or None, sigma, V or None, sweeps on R^T)."""
-    a = np.ascontiguousarray(a, dtype=np.float64)
-    m, n = a.shape
-    cfg = cfg or default_config()
-    u = np.empty((m, n)) if want_u else None
-    s = np.empty(n)
-    v = np.empty((n, n)) if want_v else None
-    sw = ctypes.c_int(0)
-    check(lib().jsvd_precond_svd(a.ctypes.data, m, n, ctypes.byref(cfg), u.ctypes.data if u is not None else None,
-                                 s.ctypes.data, v.ctypes.data if v is not None else None, ctypes.byref(sw)))
-    return u, s, v, sw.value
-
-
 class SvdResult(NamedTuple):
     u: np.ndarray | None
     sigma: np.ndarray
@@ -357,6 +325,16 @@ def svd(a: np.ndarray, solver: str = "plain", cfg: Config | None = None, want_u:
     check(fn(a.ctypes.data if a.size else None, m, n, ctypes.byref(cfg), u.ctypes.data if u is not None else None,
              s.ctypes.data, v.ctypes.data if v is not None else None, ctypes.byref(sw)))
     return SvdResult(u, s, v, sw.value)
+
+
+def plain_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, want_v: bool = True) -> SvdResult:
+    """Host-buffer plain solve -> (U or None, sigma, V or None, sweeps)."""
+    return svd(a, "plain", cfg, want_u, want_v)
+
+
+def precond_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, want_v: bool = True) -> SvdResult:
+    """Host-buffer QR-preconditioned solve -> (U or None, sigma, V or None, sweeps on R^T)."""
+    return svd(a, "precond", cfg, want_u, want_v)
 
 
 def precond_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:

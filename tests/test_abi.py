@@ -164,3 +164,18 @@ def test_svd_entry_validates_before_cuda():
         with pytest.raises(jsvd.InvalidArgument) as e:
             jsvd.svd(np.ones((3, 4)), solver=solver)
         assert "rows >= columns" in str(e.value)
+
+
+def test_host_wrappers_reach_the_library_call():
+    """plain_svd / precond_svd / svd marshal their arguments down to the C
+    call; without a GPU that call fails with the CUDA status, not earlier."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("checks the no-GPU failure")
+    a = np.ones((5, 3))
+    for call in (lambda: jsvd.plain_svd(a), lambda: jsvd.precond_svd(a, want_u=False),
+                 lambda: jsvd.svd(a, "blocked", want_v=False), lambda: jsvd.svd(a, "blockpair")):
+        with pytest.raises(jsvd.JsvdError) as e:
+            call()
+        assert e.value.code == jsvd.JSVD_ERR_CUDA

@@ -228,13 +228,26 @@ def test_plain_angle_every_warp_bitwise(cuda_device, T):
 
 
 def test_svd_entry_matches_the_solver_entries(cuda_device):
-    """jsvd.svd(a, solver) is the solver's host entry: plain bit for bit,
-    the others within the working-precision tolerance."""
+    """jsvd.svd(a, solver) through each host entry: plain is the oracle bit
+    for bit; every solver returns its device entry's bytes and is accurate to
+    working precision."""
+    import torch
+
     a = W.gaussian_splitmix(200, 60, seed=31)
+    m, n = a.shape
     cfg = jsvd.default_config(epsilon=1e-13)
     r = jsvd.svd(a, "plain", cfg)
-    _assert_bitwise((r.u, r.sigma, r.v, r.sweeps), jsvd.plain_svd(a, cfg))
+    _assert_bitwise(r, _oracle(a, 1e-13))
     ref = np.linalg.svd(a, compute_uv=False)
-    for solver in ("precond", "blockpair", "blocked"):
+    device_entries = {"plain": jsvd.plain_svd_device, "precond": jsvd.precond_svd_device,
+                      "blockpair": jsvd.blockpair_svd_device, "blocked": jsvd.blocked_svd_device}
+    for solver, entry in device_entries.items():
         r = jsvd.svd(a, solver, cfg)
         assert O.sigma_errors(r.sigma, ref)["normwise"] <= 1e-13, solver
+        da = torch.from_numpy(a).to(cuda_device)
+        du = torch.empty((m, n), dtype=torch.float64, device=cuda_device)
+        ds = torch.empty(n, dtype=torch.float64, device=cuda_device)
+        dv = torch.empty((n, n), dtype=torch.float64, device=cuda_device)
+        torch.cuda.synchronize(cuda_device)
+        sw = entry(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg)
+        _assert_bitwise(r, (du.cpu().numpy(), ds.cpu().numpy(), dv.cpu().numpy(), sw))
