@@ -233,7 +233,7 @@ def test_svd_entry_matches_the_solver_entries(cuda_device):
     working precision."""
     import torch
 
-    a = W.gaussian_splitmix(200, 60, seed=31)
+    a = W.gaussian_splitmix(200, 96, seed=31)  # 96 columns: three blocks for the blocked engine
     m, n = a.shape
     cfg = jsvd.default_config(epsilon=1e-13)
     r = jsvd.svd(a, "plain", cfg)
