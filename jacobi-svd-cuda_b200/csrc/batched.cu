@@ -654,26 +654,24 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
         }
         void *d_flush = nullptr;
         double *d_sigma = nullptr, *d_v = nullptr, *d_u = nullptr;
-        auto release = [&]() {
+        // The autotuner's own solves are not counted in the batch statistics.
+        // Buffers and statistics are restored on every path, a C++ exception's
+        // included.
+        const BatchStats saved = batch_stats();
+        ScopeExit restore([&] {
             if (d_flush) cudaFreeAsync(d_flush, st);
             if (d_sigma) cudaFreeAsync(d_sigma, st);
             if (d_v) cudaFreeAsync(d_v, st);
             if (d_u) cudaFreeAsync(d_u, st);
             cudaStreamSynchronize(st);
-        };
-        // The autotuner's own solves are not counted in the batch statistics.
-        const BatchStats saved = batch_stats();
-        auto finish = [&](int code) {
-            release();
             batch_stats() = saved;
-            return code;
-        };
+        });
         if (cudaMallocAsync(&d_flush, flush_bytes, st) != cudaSuccess ||
             cudaMallocAsync((void **)&d_sigma, sizeof(double) * std::max<size_t>(max_s, 1), st) != cudaSuccess ||
             (want_v &&
              cudaMallocAsync((void **)&d_v, sizeof(double) * std::max<size_t>(max_v, 1), st) != cudaSuccess) ||
             (want_u && cudaMallocAsync((void **)&d_u, sizeof(double) * std::max<size_t>(max_u, 1), st) != cudaSuccess))
-            return finish(cuda_failure(cudaGetLastError(), "cudaMallocAsync", __FILE__, __LINE__));
+            return cuda_failure(cudaGetLastError(), "cudaMallocAsync", __FILE__, __LINE__);
 
         for (int k = 0; k < kClasses; ++k) {
             const auto &pk = picked[k];
@@ -719,24 +717,24 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
                 double ms = -1.0;
                 for (int r = 0; r < reps; ++r) {
                     if (cudaMemsetAsync(d_flush, r & 0xff, flush_bytes, st) != cudaSuccess)
-                        return finish(cuda_failure(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__));
+                        return cuda_failure(cudaGetLastError(), "cudaMemsetAsync", __FILE__, __LINE__);
                     const double before = batch_stats().class_ms[k];
                     rc = batch_solve(req, st);
-                    if (rc != JSVD_OK) return finish(rc);
+                    if (rc != JSVD_OK) return rc;
                     const double t = batch_stats().class_ms[k] - before;
                     ms = ms < 0.0 ? t : std::min(ms, t);
                 }
                 if (cudaMemcpyAsync(sig.data(), d_sigma, sizeof(double) * nsig, cudaMemcpyDeviceToHost, st) !=
                         cudaSuccess ||
                     cudaStreamSynchronize(st) != cudaSuccess)
-                    return finish(cuda_failure(cudaGetLastError(), "cudaMemcpyAsync", __FILE__, __LINE__));
+                    return cuda_failure(cudaGetLastError(), "cudaMemcpyAsync", __FILE__, __LINE__);
                 if (ci == 0) {
                     sig_ref = sig;
                     sw_ref = sw;
                     report->builtin_ms[k] = ms;
                 } else if (std::memcmp(sig.data(), sig_ref.data(), sizeof(double) * nsig) != 0 || sw != sw_ref) {
                     set_last_error(JSVD_ERR_RUNTIME, "Batch launch shapes disagree on sigma or sweep counts.");
-                    return finish(JSVD_ERR_RUNTIME);
+                    return JSVD_ERR_RUNTIME;
                 }
                 if (best_ms < 0.0 || ms < best_ms) {
                     best_ms = ms;
@@ -751,6 +749,6 @@ extern "C" int jsvd_batch_autotune(int count, const int *rows, const int *cols, 
             report->best[k] = best;
             report->best_ms[k] = best_ms;
         }
-        return finish(JSVD_OK);
+        return JSVD_OK;
     });
 }
