@@ -65,3 +65,28 @@ def test_no_committed_file_refers_to_the_scratch_folder():
         if pattern.search(text):
             offenders.append(os.path.relpath(path, ROOT))
     assert offenders == [], offenders
+
+
+def test_sources_name_no_build_notes_or_machine_paths():
+    """Code and comments stand on their own: no source names the build's
+    notes, its benchmark descriptor, the remote-run tool or this machine's
+    paths.  The oracle's Makefile is the one recipe that reads the reference
+    where it lies."""
+    pattern = re.compile(r"SURVEY|DESIGN\.md|BASELINE|VERDICT|ADVICE|north_star|gpurun|/root/|configs\[")
+    skip_suffixes = (".md", ".json", ".gitignore", ".gpurunignore")
+    allowed = {("oracle/Makefile", "/root/")}
+    offenders = []
+    for path in _tracked_files():
+        rel = os.path.relpath(path, ROOT)
+        if rel.endswith(skip_suffixes) or os.path.abspath(path) == os.path.abspath(__file__):
+            continue
+        if not os.path.isfile(path):
+            continue
+        try:
+            text = open(path, encoding="utf-8").read()
+        except UnicodeDecodeError:
+            continue
+        for m in pattern.finditer(text):
+            if (rel, m.group(0)) not in allowed:
+                offenders.append((rel, m.group(0)))
+    assert offenders == [], offenders
