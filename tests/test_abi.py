@@ -179,3 +179,11 @@ def test_host_wrappers_reach_the_library_call():
         with pytest.raises(jsvd.JsvdError) as e:
             call()
         assert e.value.code == jsvd.JSVD_ERR_CUDA
+
+
+def test_integration_guide_covers_every_declared_function():
+    """Every entry point of include/jsvd.h has its line in the integration
+    guide (the reference interface it replaces, or why it has none)."""
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [name for name in _declared_functions() if name not in guide]
+    assert missing == [], missing
