@@ -11,6 +11,8 @@
 // interleaved over host threads.  No CUDA call.
 #include <algorithm>
 #include <cmath>
+#include <exception>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -35,17 +37,35 @@ double dot(const double *x, const double *y, size_t len)
     return (s0 + s1) + (s2 + s3);
 }
 
-// Sum over threads of body(k, t), where thread k of t handles the indices
-// i = k, k + t, k + 2t, ... of the caller's loop.
+// Sum over threads of body(k, t), where part k of t handles the indices
+// i = k, k + t, k + 2t, ... of the caller's loop.  A part whose thread cannot
+// be started runs on the calling thread; an exception thrown by a part is
+// rethrown here once every thread has been joined.
 template <class Body>
 double parallel_sum(int threads, Body body)
 {
     if (threads <= 1) return body(0, 1);
     std::vector<double> part((size_t)threads, 0.0);
+    std::vector<std::exception_ptr> errors((size_t)threads);
+    auto run = [&](int k) {
+        try {
+            part[(size_t)k] = body(k, threads);
+        } catch (...) {
+            errors[(size_t)k] = std::current_exception();
+        }
+    };
     std::vector<std::thread> pool;
     pool.reserve((size_t)threads);
-    for (int k = 0; k < threads; ++k) pool.emplace_back([&, k] { part[(size_t)k] = body(k, threads); });
+    int started = 0;
+    try {
+        for (; started < threads; ++started) pool.emplace_back(run, started);
+    } catch (const std::system_error &) {
+        // no further thread could be started: the remaining parts run below
+    }
+    for (int k = started; k < threads; ++k) run(k);
     for (auto &th : pool) th.join();
+    for (const auto &e : errors)
+        if (e) std::rethrow_exception(e);
     double s = 0.0;
     for (double p : part) s += p;
     return s;

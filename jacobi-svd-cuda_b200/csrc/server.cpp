@@ -324,6 +324,7 @@ private:
             std::memcpy(h + aoff[i], rs[i]->a.data(), sizeof(double) * rs[i]->a.size());
         double *d = nullptr;
         JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * doubles, st));
+        ScopeExit free_d([&] { cudaFreeAsync(d, st); });  // stream-ordered, on every path
         JSVD_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double) * a_total, cudaMemcpyHostToDevice, st));
         BatchRequest req;
         req.count = count;
@@ -340,13 +341,9 @@ private:
         std::vector<int> sweeps(count);
         req.sweeps = sweeps.data();
         rc = batch_solve(req, st);
-        if (rc != JSVD_OK) {
-            cudaFreeAsync(d, st);
-            return rc;
-        }
+        if (rc != JSVD_OK) return rc;
         JSVD_CUDA_TRY(cudaMemcpyAsync(h + a_total, d + a_total, sizeof(double) * (s_total + v_total + u_total),
                                       cudaMemcpyDeviceToHost, st));
-        JSVD_CUDA_TRY(cudaFreeAsync(d, st));
         JSVD_CUDA_TRY(cudaStreamSynchronize(st));
         size_t so = 0, vo = 0;
         for (int i = 0; i < count; ++i) {
@@ -373,7 +370,8 @@ private:
         for (;;) {
             std::vector<Request *> rs = admit(small_q_, (size_t)opt_.max_batch);
             if (rs.empty()) break;
-            const int rc = run_batch(rs, st, stage);
+            // a C++ exception (a host allocation) fails these requests, not the process
+            const int rc = c_entry([&] { return run_batch(rs, st, stage); });
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 ++batches_;
@@ -396,16 +394,13 @@ private:
         std::memcpy(h, r->a.data(), sizeof(double) * m * n);
         double *d = nullptr;
         JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * doubles, st));
+        ScopeExit free_d([&] { cudaFreeAsync(d, st); });  // stream-ordered, on every path
         JSVD_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double) * m * n, cudaMemcpyHostToDevice, st));
         double *ds = d + m * n, *dv = ds + n, *du = r->want_u ? dv + n * n : nullptr;
         rc = opt_.large_path == 1 ? jsvd_precond_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st)
                                   : jsvd_plain_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st);
-        if (rc != JSVD_OK) {
-            cudaFreeAsync(d, st);
-            return rc;
-        }
+        if (rc != JSVD_OK) return rc;
         JSVD_CUDA_TRY(cudaMemcpyAsync(h + m * n, ds, sizeof(double) * (doubles - m * n), cudaMemcpyDeviceToHost, st));
-        JSVD_CUDA_TRY(cudaFreeAsync(d, st));
         JSVD_CUDA_TRY(cudaStreamSynchronize(st));
         r->sigma.assign(h + m * n, h + m * n + n);
         r->v.assign(h + m * n + n, h + m * n + n + n * n);
@@ -420,7 +415,7 @@ private:
         for (;;) {
             std::vector<Request *> rs = admit(large_q_, 1);
             if (rs.empty()) break;
-            const int rc = run_large(rs[0], stage);
+            const int rc = c_entry([&] { return run_large(rs[0], stage); });
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 ++large_solves_;
