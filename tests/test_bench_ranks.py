@@ -146,6 +146,10 @@ def test_profile_commands_use_committed_files_and_current_flags():
     assert files
     for path in files:
         text = open(path).read()
+        if "-Xptxas -v" in text:  # a compiler resource summary: its nvcc command on committed sources
+            assert re.search(r"^nvcc .*-gencode arch=compute_100a,code=sm_100a", text, flags=re.M), path
+            assert os.path.isdir(os.path.join(ROOT, "jacobi-svd-cuda_b200", "csrc")), path
+            continue
         cmds = re.findall(r'"(python \S+[^"]*)"', text)
         assert cmds, path
         for cmd in cmds:
