@@ -290,7 +290,7 @@ void jsvd_precond_set_inner(int engine);
 
 /* 1 (default): inside jsvd_precond_svd*, when epsilon >= 1e-12 and a sweep
  * of the plain Jacobi stage rotates fewer than 1/8 of its pairs, every pair is
- * tested on the Gram matrix of the columns (one DSYRK); when none would
+ * tested on the Gram matrix of the columns (one lower-triangle GEMM); when none would
  * rotate, the final sweep (which would rotate nothing) is not run but is
  * still counted in `sweeps`.  Below 1e-12 the GEMM's own rounding of the
  * off-diagonal entries is too close to epsilon for the test to succeed.
@@ -353,6 +353,73 @@ typedef struct jsvd_precond_stats {
 
 void jsvd_precond_stats_get(jsvd_precond_stats *out);
 void jsvd_precond_stats_reset(void);
+
+/* ---- blocked mixed-precision path -------------------------------------------
+ * No counterpart in the reference, whose only sweep is the scalar column-pair
+ * loop of src/kernels.cu:889-981.  A is first QR-preconditioned as in
+ * jsvd_precond_svd (A = Q R, R^T = Q1 P, X = P^T).  X's columns are grouped in
+ * blocks of 32 and the blocks paired in the round-robin order.  For each block
+ * pair, the 64 x 64 Gram G = [X_i X_j]^T [X_i X_j] is eigen-solved in FP64
+ * (cyclic two-sided Jacobi, G = W L W^T) and the pair is rotated,
+ * [X_i X_j] <- [X_i X_j] W, likewise V.
+ *   1. Tensor-core phase: Grams and rotations are tcgen05 GEMMs in 3xTF32
+ *      (each FP32 operand split into a TF32 head and tail) with FP32
+ *      accumulation, operands brought in by TMA; X and V are held as TF32
+ *      head/tail pairs.
+ *   2. V of phase 1 is made orthogonal in FP64 (Newton-Schulz polar
+ *      iteration), X' = X V' (FP64).
+ *   3. FP64 refinement: the same blocked sweeps in FP64 (DMMA GEMMs) on X'
+ *      until no pair rotates (threshold max(epsilon, 4 sqrt(m) 2^-53)).
+ * Same arguments, outputs and validation as jsvd_precond_svd; sigma unsorted;
+ * *sweeps = phase-1 sweeps + refinement sweeps.  Inputs with fewer than 128
+ * columns run the QR-preconditioned plain path.  Accurate to working
+ * precision (normwise), not bit-identical to the plain path. */
+typedef struct jsvd_mixed_options {
+    int precondition;   /* 1 (default): blocked sweeps on X = P^T after the two QRs; 0: on A   */
+    int tc_max_sweeps;  /* tensor-core sweeps at most (default 10); 0 = FP64 blocked sweeps only */
+    double tc_tol;      /* phase 1 ends when no pair's |g_pq| / sqrt(g_pp g_qq) exceeds this    */
+    int inner_sweeps;   /* two-sided sweeps per 64 x 64 block eigen-solve (default 2)           */
+    int refine;         /* refinement: 0 = blocked FP64 sweeps (default), 1 = plain scalar sweep */
+    int f64_max_sweeps; /* cap on refinement sweeps; 0 = the config's max_sweeps                  */
+    int gram_splits;    /* row splits of each block-pair Gram; 0 = automatic                      */
+} jsvd_mixed_options;
+
+void jsvd_mixed_options_default(jsvd_mixed_options *o);
+/* Options of later jsvd_mixed_svd* calls on the calling thread (NULL: defaults). */
+void jsvd_mixed_set_options(const jsvd_mixed_options *o);
+
+int jsvd_mixed_svd(const double *a, size_t rows, size_t columns, const jsvd_config *cfg, double *u, double *sigma,
+                   double *v, int *sweeps);
+int jsvd_mixed_svd_device(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,
+                          double *d_sigma, double *d_v, int *sweeps, void *stream);
+
+/* Cumulative counters of the mixed path on the calling thread. */
+typedef struct jsvd_mixed_stats {
+    unsigned long long solves, tc_sweeps, f64_sweeps, block_rounds, fallbacks;
+    double qr_ms, tc_ms, orth_ms, refine_ms, out_ms; /* device time per phase (events)           */
+    double last_tc_offdiag;   /* largest scaled off-diagonal Gram entry, last phase-1 sweep      */
+    double last_f64_offdiag;  /* the same for the last refinement sweep                           */
+    int last_tc_sweeps, last_f64_sweeps;
+    unsigned long long tc_gram_launches, tc_rot_launches, f64_gram_launches, f64_rot_launches, evd_launches;
+    unsigned long long tc_discarded; /* solves whose phase-1 V did not orthogonalise (FP64 sweeps from X) */
+} jsvd_mixed_stats;
+
+void jsvd_mixed_stats_get(jsvd_mixed_stats *out);
+void jsvd_mixed_stats_reset(void);
+
+/* Kernel-level test hook of the mixed path: one block round (`round`) of its
+ * kernels on X (rows x cols, column-major FP64, device, both multiples of
+ * 128).  kind 0: tensor-core Gram of each block pair -> gw (pairs x 64 x 64,
+ * column-major FP64); 1: FP64 Gram -> gw; 2: tensor-core rotation
+ * X_pair <- X_pair W_pair with W read from gw, in place; 3: FP64 rotation. */
+int jsvd_mixed_test_round(int kind, double *d_x, int rows, int cols, int round, double *d_gw);
+
+/* FP64 GEMM of the library (DMMA tensor cores), for tests and tools:
+ * C = alpha op(A) op(B) + beta C, column-major device buffers, op 'N' or 'T';
+ * lower != 0 writes only C's lower triangle.  Synchronous on the calling
+ * thread's library stream. */
+int jsvd_dgemm_device(char op_a, char op_b, int m, int n, int k, double alpha, const double *a, long lda,
+                      const double *b, long ldb, double beta, double *c, long ldc, int lower);
 
 /* ---- serving loop -----------------------------------------------------------
  * Continuous batching of SVD requests on the current device.  Replaces the

@@ -1,0 +1,1259 @@
+// Blocked mixed-precision one-sided Jacobi SVD on sm_100a.
+//
+// The reference's sweep (src/kernels.cu:889-981) rotates one column pair at a
+// time: every pair reads and writes two full columns, so a sweep of an m x n
+// matrix moves about n^2/2 (6m + 4n) 8-byte words
+// (tex/sections/03-gpu-parallel-reduction.tex:66-90).  Here the columns are
+// grouped into blocks of kB = 32; a sweep pairs the blocks with the same
+// fixed-head circle (round_robin_pair over blocks) and, for each block pair
+// P = [X_i X_j] (m x 64):
+//   1. Gram     G = P^T P (64 x 64), split over row ranges;
+//   2. solve    G = W L W^T by cyclic two-sided Jacobi in FP64 (one CTA,
+//               rounds of 32 disjoint index pairs; Rutishauser angles and the
+//               reference's threshold |g_pq| <= tau sqrt(g_pp g_qq));
+//   3. rotate   P <- P W, [V_i V_j] <- [V_i V_j] W, in place.
+// A block round moves each column once instead of once per column round.
+//
+// Phase 1 (tensor cores).  X and V are held as pairs of FP32 arrays, a TF32
+// head (low 13 mantissa bits zero) and its FP32 tail.  Grams and rotations run
+// on tcgen05.mma kind::tf32 with FP32 accumulation in TMEM, operands fetched by
+// TMA (no multicast):
+//   Gram:   A operand = [h_i h_j l_i l_j]^T (M = 128, K-major, 128-byte
+//           swizzle), B = [h_i h_j] then [l_i l_j] (N = 64): D[0:64] =
+//           h^T (h+l), D[64:128] = l^T (h+l), G = D[0:64] + D[64:128].
+//   Rotate: A operand = the 128-row tile of h (then l), MN-major (X is column
+//           major; MN-major TF32 needs the 128-byte swizzle with 32-byte
+//           atoms), B = [W_h | W_l] (N = 128, K-major): D[:, 0:64] =
+//           (h+l) W_h, D[:, 64:128] = (h+l) W_l, out = their sum, split again.
+// Phase 2 makes phase 1's V orthogonal in FP64 (Newton-Schulz iteration for
+// the polar factor, V <- V (3I - V^T V)/2) and forms X' = X V' in FP64.
+// Phase 3 sweeps X' in FP64 with the same block structure (DMMA GEMMs) until
+// no pair rotates.  This is the mixed-precision preconditioned one-sided
+// Jacobi scheme: a low-precision V, orthogonalised in working precision, then
+// working-precision Jacobi (Zhou; Higham, Tisseur, Webb and Zhou, SIMAX 2021,
+// for the symmetric eigenproblem).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "dgemm.hpp"
+#include "internal.hpp"
+#include "jsvd.h"
+#include "mixed.hpp"
+#include "plain.hpp"
+#include "ptx.cuh"
+
+namespace jsvd {
+namespace {
+
+constexpr int kB = 32;          // columns per block
+constexpr int kW = 2 * kB;      // panel width (a block pair)
+constexpr int kTileRows = 128;  // rows per rotation tile; working rows are padded to a multiple
+constexpr int kColPad = 128;    // working columns padded to a multiple (block count stays even)
+
+// ============================================================================
+// Phase 1 kernels (tcgen05, 3xTF32)
+// ============================================================================
+
+constexpr int kGramStages = 4;
+constexpr int kGramStageBytes = 4 * 4096;  // [h_i h_j l_i l_j], 32 rows x 32 columns each
+constexpr size_t kGramTcSmem = 1024 + kGramStages * kGramStageBytes + 128;
+constexpr int kGramTcThreads = 192;        // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
+
+__device__ __forceinline__ uint8_t *align1024(uint8_t *p)
+{
+    const uint32_t a = smem_u32(p);
+    return p + ((1024u - (a & 1023u)) & 1023u);
+}
+
+__device__ __forceinline__ void record_status(int *status, int code) { atomicCAS(status, 0, code); }
+
+// Partial Gram of block pair blockIdx.y over row chunks [c0, c1) (32 rows
+// each) of split blockIdx.x.  Output: the raw 128 x 64 FP32 accumulator,
+// column-major, at part + (pair * splits + split) * 8192.
+__global__ void __launch_bounds__(kGramTcThreads)
+    mx_gram_tc(const __grid_constant__ CUtensorMap mh, const __grid_constant__ CUtensorMap ml, int nb, int round,
+               int kchunks, int chunks_per_split, float *__restrict__ part, int *__restrict__ status)
+{
+    extern __shared__ uint8_t smraw[];
+    uint8_t *sm = align1024(smraw);
+    uint8_t *tiles = sm;
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + kGramStages * kGramStageBytes);
+    uint64_t *empty = full + kGramStages;
+    uint64_t *accf = empty + kGramStages;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(accf + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pair = blockIdx.y, split = blockIdx.x;
+    const int2 bp = round_robin_pair(nb, round, pair);
+    const int c0 = split * chunks_per_split;
+    const int nck = min(kchunks, c0 + chunks_per_split) - c0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kGramStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(accf, 1);
+        mbar_fence_init();
+    }
+    if (warp == 5) tmem_alloc(tslot, 64);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 4) {
+        if (lane == 0) {
+            tma_prefetch_desc(&mh);
+            tma_prefetch_desc(&ml);
+            for (int it = 0; it < nck; ++it) {
+                const int s = it % kGramStages;
+                const uint32_t ph = (uint32_t)(it / kGramStages) & 1u;
+                if (!mbar_wait(&empty[s], ph ^ 1u)) {
+                    record_status(status, kDevWaitTimeout);
+                    break;
+                }
+                mbar_arrive_expect_tx(&full[s], kGramStageBytes);
+                uint8_t *t = tiles + s * kGramStageBytes;
+                const int row = (c0 + it) * 32;
+                tma_load_2d(t, &mh, &full[s], row, bp.x * kB);
+                tma_load_2d(t + 4096, &mh, &full[s], row, bp.y * kB);
+                tma_load_2d(t + 8192, &ml, &full[s], row, bp.x * kB);
+                tma_load_2d(t + 12288, &ml, &full[s], row, bp.y * kB);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 5) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_tf32(128, 64, 0, 0);
+            for (int it = 0; it < nck; ++it) {
+                const int s = it % kGramStages;
+                const uint32_t ph = (uint32_t)(it / kGramStages) & 1u;
+                if (!mbar_wait(&full[s], ph)) {
+                    record_status(status, kDevWaitTimeout);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t base = smem_u32(tiles + s * kGramStageBytes);
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) {  // K = 8 TF32 per MMA = 32 bytes of the 128-byte row
+                    const uint64_t a = smem_desc_sw128(base + ks * 32, 16, 1024);
+                    const uint64_t bh = smem_desc_sw128(base + ks * 32, 16, 1024);
+                    const uint64_t bl = smem_desc_sw128(base + 8192 + ks * 32, 16, 1024);
+                    tc_mma_tf32(tmem, a, bh, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+                    tc_mma_tf32(tmem, a, bl, idesc, 1u);
+                }
+                tc_commit(&empty[s]);
+            }
+            tc_commit(accf);
+        }
+        __syncwarp();
+    }
+    if (warp < 4) {
+        const bool ok = mbar_wait(accf, 0);
+        tc_fence_after();
+        if (!ok) {
+            record_status(status, kDevWaitTimeout);
+        } else {
+            float *out = part + ((size_t)pair * gridDim.x + split) * (128 * 64);
+            const int r = warp * 32 + lane;
+            float v[32];
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + half * 32, v);
+#pragma unroll
+                for (int c = 0; c < 32; ++c) out[(size_t)(half * 32 + c) * 128 + r] = v[c];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 5) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 64);
+    }
+}
+
+constexpr int kRotTcThreads = 128;
+constexpr int kRotAOff = 0;      // A: [h|l] x [block i|block j] x 4 row atoms x 4 KB = 64 KB
+constexpr int kRotBOff = 65536;  // B: 2 K-atoms x 128 rows x 128 bytes = 32 KB
+constexpr int kRotBarOff = 98304;
+constexpr size_t kRotTcSmem = 1024 + 98304 + 64;
+
+// Rotation of one 128-row tile of the block pair blockIdx.y, in X (tiles
+// [0, x_tiles)) or in V (tiles from x_tiles on): [h + l] <- [h + l] W.  The
+// tensor maps are the 32-byte-atom swizzled ones (A is MN-major): each 4 KB box
+// is 32 K rows (columns of P) of 128 bytes (32 rows of P), groups of 4 K rows
+// 512 bytes apart (SBO), the four 32-row atoms of the tile 4096 bytes apart
+// (LBO).
+__global__ void __launch_bounds__(kRotTcThreads)
+    mx_rot_tc(const __grid_constant__ CUtensorMap mxh, const __grid_constant__ CUtensorMap mxl,
+              const __grid_constant__ CUtensorMap mvh, const __grid_constant__ CUtensorMap mvl,
+              float *__restrict__ xh, float *__restrict__ xl, long ldx, int x_tiles, float *__restrict__ vh,
+              float *__restrict__ vl, long ldv, int nb, int round, const double *__restrict__ W,
+              const int *__restrict__ flags, int *__restrict__ status)
+{
+    const int pair = blockIdx.y;
+    if (flags[pair] == 0) return;  // W = I: the tile stays as it is
+    extern __shared__ uint8_t smraw[];
+    uint8_t *sm = align1024(smraw);
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + kRotBarOff);
+    uint64_t *accf = full + 1;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(accf + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool onV = (int)blockIdx.x >= x_tiles;
+    const CUtensorMap *mh = onV ? &mvh : &mxh;
+    const CUtensorMap *ml = onV ? &mvl : &mxl;
+    float *oh = onV ? vh : xh;
+    float *ol = onV ? vl : xl;
+    const long ld = onV ? ldv : ldx;
+    const int row0 = (onV ? (int)blockIdx.x - x_tiles : (int)blockIdx.x) * kTileRows;
+    const int2 bp = round_robin_pair(nb, round, pair);
+
+    if (threadIdx.x == 0) {
+        mbar_init(full, 1);
+        mbar_init(accf, 1);
+        mbar_fence_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, 128);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(full, 65536);
+#pragma unroll
+        for (int hl = 0; hl < 2; ++hl)
+#pragma unroll
+            for (int half = 0; half < 2; ++half)
+#pragma unroll
+                for (int g = 0; g < 4; ++g)
+                    tma_load_2d(sm + kRotAOff + hl * 32768 + half * 16384 + g * 4096, hl ? ml : mh, full,
+                                row0 + g * 32, (half ? bp.y : bp.x) * kB);
+    }
+    __syncwarp();
+    // B = [W_h | W_l]: row n (0..63 head, 64..127 tail) holds column n of W
+    // along K (K-major, 128-byte swizzle, two 32-float K atoms).
+    const double *wp = W + (size_t)pair * kW * kW;
+    for (int e = threadIdx.x; e < kW * kW; e += kRotTcThreads) {
+        const int k = e & 63, n = e >> 6;  // W(k, n) at k + 64 n: consecutive threads read consecutive k
+        float h, l;
+        split_tf32((float)wp[e], h, l);
+        const int atom = k >> 5, kk = k & 31;
+#pragma unroll
+        for (int hl = 0; hl < 2; ++hl) {
+            const int row = n + hl * 64;
+            const uint32_t off = kRotBOff + atom * 16384 + row * 128 + (((kk >> 2) ^ (row & 7)) << 4) + (kk & 3) * 4;
+            *reinterpret_cast<float *>(sm + off) = hl ? l : h;
+        }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        constexpr uint32_t idesc = idesc_tf32(128, 128, 1, 0);
+        if (!mbar_wait(full, 0)) {
+            record_status(status, kDevWaitTimeout);
+        } else {
+            tc_fence_after();
+            const uint32_t abase = smem_u32(sm + kRotAOff), bbase = smem_u32(sm + kRotBOff);
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) {
+                const int half = ks >> 2, g8 = ks & 3;
+                const uint64_t b = smem_desc_sw128(bbase + half * 16384 + g8 * 32, 16, 1024);
+                const uint64_t ah = smem_desc(abase + half * 16384 + g8 * 1024, 4096, 512, kSwizzle128B32BAtom);
+                const uint64_t al =
+                    smem_desc(abase + 32768 + half * 16384 + g8 * 1024, 4096, 512, kSwizzle128B32BAtom);
+                tc_mma_tf32(tmem, ah, b, idesc, ks > 0 ? 1u : 0u);
+                tc_mma_tf32(tmem, al, b, idesc, 1u);
+            }
+        }
+        tc_commit(accf);
+    }
+    __syncwarp();
+    const bool ok = mbar_wait(accf, 0);
+    tc_fence_after();
+    if (!ok) {
+        record_status(status, kDevWaitTimeout);
+    } else {
+        const int r = row0 + warp * 32 + lane;
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            float a[32], b[32];
+            tmem_ld32(lane_addr + cc * 32, a);
+            tmem_ld32(lane_addr + 64 + cc * 32, b);
+            const int col0 = (cc ? bp.y : bp.x) * kB;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                float h, l;
+                split_tf32(a[c] + b[c], h, l);
+                const size_t idx = (size_t)r + (size_t)(col0 + c) * ld;
+                oh[idx] = h;
+                ol[idx] = l;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 128);
+    }
+}
+
+// ============================================================================
+// Phase 3 kernels (FP64, DMMA)
+// ============================================================================
+
+constexpr int kGram64Threads = 256;
+constexpr int kGram64Rows = 32;             // rows of P per stage
+constexpr int kGram64LD = kGram64Rows + 4;  // Ps[col][row]
+constexpr int kGram64Stages = 3;
+constexpr size_t kGram64Smem = sizeof(double) * kGram64Stages * kW * kGram64LD;
+
+// Partial Gram of block pair blockIdx.y over rows [r0, r1) of split
+// blockIdx.x; output 64 x 64 FP64 column-major at part + (pair*splits+split)*4096.
+// Warp w computes rows 8w..8w+7 of G (eight 8 x 8 DMMA tiles).
+__global__ void __launch_bounds__(kGram64Threads)
+    mx_gram_f64(const double *__restrict__ X, long ldx, int nb, int round, int rows_per_split, int rows,
+                double *__restrict__ part)
+{
+    extern __shared__ double dsm[];
+    const int pair = blockIdx.y, split = blockIdx.x;
+    const int2 bp = round_robin_pair(nb, round, pair);
+    const int r0 = split * rows_per_split, r1 = min(rows, r0 + rows_per_split);
+    const int nst = (r1 - r0 + kGram64Rows - 1) / kGram64Rows;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int fr = lane >> 2, fk = lane & 3;
+    auto issue = [&](int st) {
+        double *s = dsm + (st % kGram64Stages) * kW * kGram64LD;
+        const int rb = r0 + st * kGram64Rows;
+        for (int e = threadIdx.x; e < kW * kGram64Rows; e += kGram64Threads) {
+            const int k = e & 31, c = e >> 5;
+            const int gc = (c < kB ? bp.x * kB + c : bp.y * kB + (c - kB));
+            const int gr = rb + k;
+            double *d = s + c * kGram64LD + k;
+            if (gr < r1)
+                cp_async8(d, X + (size_t)gr + (size_t)gc * ldx);
+            else
+                *d = 0.0;
+        }
+    };
+    double acc[8][2];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+#pragma unroll
+    for (int s = 0; s < kGram64Stages - 1; ++s) {
+        if (s < nst) issue(s);
+        cp_async_commit();
+    }
+    for (int st = 0; st < nst; ++st) {
+        cp_async_wait<kGram64Stages - 2>();
+        __syncthreads();
+        if (st + kGram64Stages - 1 < nst) issue(st + kGram64Stages - 1);
+        cp_async_commit();
+        const double *s = dsm + (st % kGram64Stages) * kW * kGram64LD;
+#pragma unroll
+        for (int kk = 0; kk < kGram64Rows; kk += 4) {
+            // A = P^T (row i of A = column i of P), B = P
+            const double a = s[(warp * 8 + fr) * kGram64LD + kk + fk];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const double b = s[(j * 8 + fr) * kGram64LD + kk + fk];
+                dmma_m8n8k4(acc[j], a, b);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    double *out = part + ((size_t)pair * gridDim.x + split) * (kW * kW);
+    const int row = warp * 8 + fr;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int col = j * 8 + 2 * fk;
+        out[(size_t)col * kW + row] = acc[j][0];
+        out[(size_t)(col + 1) * kW + row] = acc[j][1];
+    }
+}
+
+constexpr int kRot64Threads = 256;
+constexpr int kRot64PLD = kTileRows + 8;  // Pt[col][row]
+constexpr int kRot64WLD = kW + 4;         // Ws[col][k]
+constexpr size_t kRot64Smem = sizeof(double) * (kW * kRot64PLD + kW * kRot64WLD);
+
+// Rotation of one 128-row tile of block pair blockIdx.y (X tiles, then V
+// tiles), FP64: P <- P W.  Warp w computes rows 16w..16w+15 x 64 columns.
+__global__ void __launch_bounds__(kRot64Threads)
+    mx_rot_f64(double *__restrict__ X, long ldx, int x_tiles, double *__restrict__ V, long ldv, int nb, int round,
+               const double *__restrict__ W, const int *__restrict__ flags)
+{
+    const int pair = blockIdx.y;
+    if (flags[pair] == 0) return;
+    extern __shared__ double dsm[];
+    double *Pt = dsm;                   // [64 cols][136]
+    double *Ws = dsm + kW * kRot64PLD;  // [64 cols][68]
+    const bool onV = (int)blockIdx.x >= x_tiles;
+    double *M = onV ? V : X;
+    const long ld = onV ? ldv : ldx;
+    const int row0 = (onV ? (int)blockIdx.x - x_tiles : (int)blockIdx.x) * kTileRows;
+    const int2 bp = round_robin_pair(nb, round, pair);
+    const double *wp = W + (size_t)pair * kW * kW;
+    for (int e = threadIdx.x; e < kW * kW; e += kRot64Threads) {
+        const int k = e & 63, c = e >> 6;
+        cp_async8(Ws + c * kRot64WLD + k, wp + e);
+    }
+    for (int e = threadIdx.x; e < kW * kTileRows; e += kRot64Threads) {
+        const int r = e & (kTileRows - 1), c = e >> 7;
+        const int gc = c < kB ? bp.x * kB + c : bp.y * kB + (c - kB);
+        cp_async8(Pt + c * kRot64PLD + r, M + (size_t)(row0 + r) + (size_t)gc * ld);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int fr = lane >> 2, fk = lane & 3;
+    double acc[2][8][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < kW; kk += 4) {
+        double a[2], b[8];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) a[i] = Pt[(kk + fk) * kRot64PLD + warp * 16 + i * 8 + fr];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) b[j] = Ws[(j * 8 + fr) * kRot64WLD + kk + fk];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) dmma_m8n8k4(acc[i][j], a[i], b[j]);
+    }
+    __syncthreads();  // every warp is done reading Pt
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int r = warp * 16 + i * 8 + fr, c = j * 8 + 2 * fk;
+            Pt[c * kRot64PLD + r] = acc[i][j][0];
+            Pt[(c + 1) * kRot64PLD + r] = acc[i][j][1];
+        }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kW * kTileRows; e += kRot64Threads) {
+        const int r = e & (kTileRows - 1), c = e >> 7;
+        const int gc = c < kB ? bp.x * kB + c : bp.y * kB + (c - kB);
+        M[(size_t)(row0 + r) + (size_t)gc * ld] = Pt[c * kRot64PLD + r];
+    }
+}
+
+// ============================================================================
+// Block eigen-solve (FP64, both phases)
+// ============================================================================
+
+constexpr int kEvdThreads = 256;
+constexpr int kEvdLD = kW + 1;
+constexpr int kTriBlocks = (kW / 2) * (kW / 2 + 1) / 2;  // 2x2 blocks (a <= b) of the 32 x 32 block grid
+constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD;
+
+struct EvdTables {
+    unsigned char pairs[kW - 1][kW / 2][2];  // (p, q) of pair k in inner round r (circle over 64 indices)
+    unsigned char tri[kTriBlocks][2];        // (a, b), a <= b
+};
+__constant__ EvdTables c_evd;
+
+// Input Gram of block pair blockIdx.x from `splits` partials: kind 0 = the
+// tensor-core layout (128 x 64 FP32, rows r and r + 64 summed), kind 1 =
+// 64 x 64 FP64.  Writes W (64 x 64, column-major) and flags[pair] = 1 when
+// some pair rotated (else flags[pair] = 0 and W is left as it was).  stats[0]
+// (as double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over the input
+// Grams, stats[1] = number of block pairs that rotated.
+__global__ void __launch_bounds__(kEvdThreads)
+    mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps,
+           double *__restrict__ Wout, int *__restrict__ flags, unsigned long long *__restrict__ stats)
+{
+    extern __shared__ double dsm[];
+    double *G = dsm;                 // [64][65]
+    double *Wm = dsm + kW * kEvdLD;  // [64][65], Wm[row][col]
+    __shared__ double cs_c[kW / 2], cs_s[kW / 2], cs_t[kW / 2];
+    __shared__ int rot_k[kW / 2];
+    __shared__ int any_round, any_sweep;
+    __shared__ unsigned long long off_bits;
+    const int pair = blockIdx.x;
+    const int tid = threadIdx.x;
+    if (tid == 0) off_bits = 0ull;
+    for (int e = tid; e < kW * kW; e += kEvdThreads) {
+        const int r = e & 63, c = e >> 6;  // consecutive threads, consecutive rows of a column
+        double g = 0.0;
+        if (kind == 0) {
+            const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
+            for (int s = 0; s < splits; ++s)
+                g += (double)p[(size_t)s * 8192 + c * 128 + r] + (double)p[(size_t)s * 8192 + c * 128 + r + 64];
+        } else {
+            const double *p = static_cast<const double *>(part) + (size_t)pair * splits * 4096;
+            for (int s = 0; s < splits; ++s) g += p[(size_t)s * 4096 + c * 64 + r];
+        }
+        G[r * kEvdLD + c] = g;
+        Wm[r * kEvdLD + c] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    // symmetrise (the two triangles come from different accumulation orders)
+    // and measure the input's largest scaled off-diagonal entry
+    double off = 0.0;
+    for (int e = tid; e < kW * kW; e += kEvdThreads) {
+        const int r = e >> 6, c = e & 63;
+        if (r < c) {
+            const double g = 0.5 * (G[r * kEvdLD + c] + G[c * kEvdLD + r]);
+            G[r * kEvdLD + c] = g;
+            G[c * kEvdLD + r] = g;
+            const double d = sqrt(fmax(G[r * kEvdLD + r], 0.0) * fmax(G[c * kEvdLD + c], 0.0));
+            if (d > 0.0) off = fmax(off, fabs(g) / d);
+        }
+    }
+    if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
+    bool rotated_any = false;
+    for (int sw = 0; sw < inner_sweeps; ++sw) {
+        if (tid == 0) any_sweep = 0;
+        __syncthreads();
+        for (int r = 0; r < kW - 1; ++r) {
+            if (tid < kW / 2) {
+                const int p = c_evd.pairs[r][tid][0], q = c_evd.pairs[r][tid][1];
+                double c, s;
+                const bool rot = rotation_params(G[p * kEvdLD + p], G[q * kEvdLD + q], G[p * kEvdLD + q], tau, c, s);
+                cs_c[tid] = rot ? c : 1.0;
+                cs_s[tid] = rot ? s : 0.0;
+                cs_t[tid] = rot ? s / c : 0.0;
+                rot_k[tid] = rot ? 1 : 0;
+                const unsigned any = __ballot_sync(0xffffffffu, rot);
+                if (tid == 0) any_round = any != 0u;
+            }
+            __syncthreads();
+            if (any_round) {
+                // G <- J^T G J by 2 x 2 blocks of index pairs (a, b), a <= b
+                for (int e = tid; e < kTriBlocks; e += kEvdThreads) {
+                    const int a = c_evd.tri[e][0], b = c_evd.tri[e][1];
+                    if (!rot_k[a] && !rot_k[b]) continue;
+                    const int pa = c_evd.pairs[r][a][0], qa = c_evd.pairs[r][a][1];
+                    const int pb = c_evd.pairs[r][b][0], qb = c_evd.pairs[r][b][1];
+                    if (a == b) {
+                        // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
+                        const double t = cs_t[a], o = G[pa * kEvdLD + qa];
+                        G[pa * kEvdLD + pa] = fma(-t, o, G[pa * kEvdLD + pa]);
+                        G[qa * kEvdLD + qa] = fma(t, o, G[qa * kEvdLD + qa]);
+                        G[pa * kEvdLD + qa] = 0.0;
+                        G[qa * kEvdLD + pa] = 0.0;
+                        continue;
+                    }
+                    const double ca = cs_c[a], sa = cs_s[a], cb = cs_c[b], sb = cs_s[b];
+                    const double g11 = G[pa * kEvdLD + pb], g12 = G[pa * kEvdLD + qb];
+                    const double g21 = G[qa * kEvdLD + pb], g22 = G[qa * kEvdLD + qb];
+                    // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
+                    const double h11 = fma(cb, g11, -(sb * g12)), h12 = fma(sb, g11, cb * g12);
+                    const double h21 = fma(cb, g21, -(sb * g22)), h22 = fma(sb, g21, cb * g22);
+                    // rows (on the left, pair a)
+                    const double n11 = fma(ca, h11, -(sa * h21)), n21 = fma(sa, h11, ca * h21);
+                    const double n12 = fma(ca, h12, -(sa * h22)), n22 = fma(sa, h12, ca * h22);
+                    G[pa * kEvdLD + pb] = n11;
+                    G[pa * kEvdLD + qb] = n12;
+                    G[qa * kEvdLD + pb] = n21;
+                    G[qa * kEvdLD + qb] = n22;
+                    G[pb * kEvdLD + pa] = n11;
+                    G[qb * kEvdLD + pa] = n12;
+                    G[pb * kEvdLD + qa] = n21;
+                    G[qb * kEvdLD + qa] = n22;
+                }
+                // W <- W J (row-local)
+                for (int e = tid; e < kW * (kW / 2); e += kEvdThreads) {
+                    const int k = e >> 6, row = e & 63;
+                    if (!rot_k[k]) continue;
+                    const int p = c_evd.pairs[r][k][0], q = c_evd.pairs[r][k][1];
+                    const double c = cs_c[k], s = cs_s[k];
+                    const double wp = Wm[row * kEvdLD + p], wq = Wm[row * kEvdLD + q];
+                    Wm[row * kEvdLD + p] = fma(c, wp, -(s * wq));
+                    Wm[row * kEvdLD + q] = fma(s, wp, c * wq);
+                }
+                if (tid == 0) any_sweep = 1;
+            }
+            __syncthreads();
+        }
+        const bool had = any_sweep != 0;
+        __syncthreads();  // every thread has read any_sweep before thread 0 resets it
+        rotated_any = rotated_any || had;
+        if (!had) break;
+    }
+    if (rotated_any) {
+        double *wo = Wout + (size_t)pair * kW * kW;
+        for (int e = tid; e < kW * kW; e += kEvdThreads) {
+            const int r = e & 63, c = e >> 6;
+            wo[e] = Wm[r * kEvdLD + c];  // column-major W(r, c)
+        }
+    }
+    __syncthreads();  // off_bits complete
+    if (tid == 0) {
+        flags[pair] = rotated_any ? 1 : 0;
+        if (rotated_any) atomicAdd(&stats[1], 1ull);
+        if (off_bits) atomicMax(&stats[0], off_bits);
+    }
+}
+
+// ============================================================================
+// Layout kernels
+// ============================================================================
+
+constexpr int kT = 32, kTR = 8;
+
+// row-major (rows x cols) -> column-major padded (ld = rows_pad, cols_pad
+// columns; the padding is zero)
+__global__ void __launch_bounds__(kT *kTR)
+    mx_rowmajor_to_padded(const double *__restrict__ src, int rows, int cols, double *__restrict__ dst, long ld,
+                          int rows_pad, int cols_pad)
+{
+    __shared__ double tile[kT][kT + 1];
+    const int c0 = blockIdx.x * kT, r0 = blockIdx.y * kT;
+    for (int k = threadIdx.y; k < kT; k += kTR) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        tile[k][threadIdx.x] = (r < rows && c < cols) ? src[(size_t)r * cols + c] : 0.0;
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < kT; k += kTR) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows_pad && c < cols_pad) dst[(size_t)c * ld + r] = tile[threadIdx.x][k];
+    }
+}
+
+// column-major (ld) -> row-major (rows x cols); with sigma, column c is
+// divided by sigma[c] (zero when sigma[c] <= eps)
+__global__ void __launch_bounds__(kT *kTR)
+    mx_padded_to_rowmajor(const double *__restrict__ src, long ld, int rows, int cols, double *__restrict__ dst,
+                          const double *__restrict__ sigma, double eps)
+{
+    __shared__ double tile[kT][kT + 1];
+    const int r0 = blockIdx.x * kT, c0 = blockIdx.y * kT;
+    for (int k = threadIdx.y; k < kT; k += kTR) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) tile[k][threadIdx.x] = src[(size_t)c * ld + r];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < kT; k += kTR) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) {
+            double v = tile[threadIdx.x][k];
+            if (sigma) {
+                const double sg = sigma[c];
+                v = (sg > eps) ? v / sg : 0.0;
+            }
+            dst[(size_t)r * cols + c] = v;
+        }
+    }
+}
+
+// FP64 -> TF32 head + FP32 tail, elementwise
+__global__ void mx_split(const double *__restrict__ x, size_t count, float *__restrict__ h, float *__restrict__ l)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x) {
+        float hh, ll;
+        split_tf32((float)x[e], hh, ll);
+        h[e] = hh;
+        l[e] = ll;
+    }
+}
+
+__global__ void mx_join(const float *__restrict__ h, const float *__restrict__ l, size_t count, double *__restrict__ x)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x)
+        x[e] = (double)h[e] + (double)l[e];
+}
+
+// identity (n x n, ld = n): FP64 and/or the TF32 head/tail pair
+__global__ void mx_identity(double *__restrict__ v, float *__restrict__ vh, float *__restrict__ vl, int n)
+{
+    const size_t total = (size_t)n * n;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const double d = (e / n == e % n) ? 1.0 : 0.0;
+        if (v) v[e] = d;
+        if (vh) vh[e] = (float)d;
+        if (vl) vl[e] = 0.0f;
+    }
+}
+
+// E = V^T V - I (in place) and *maxabs = max |E_ij| (double bits)
+__global__ void mx_minus_identity_max(double *__restrict__ E, int n, unsigned long long *__restrict__ maxabs)
+{
+    const size_t total = (size_t)n * n;
+    double m = 0.0;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        double v = E[e];
+        if (e / n == e % n) v -= 1.0;
+        E[e] = v;
+        m = fmax(m, fabs(v));
+        if (v != v) m = INFINITY;  // NaN
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(maxabs, (unsigned long long)__double_as_longlong(m));
+}
+
+// M = I - E / 2 (in place)
+__global__ void mx_half_step(double *__restrict__ E, int n)
+{
+    const size_t total = (size_t)n * n;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+        E[e] = ((e / n == e % n) ? 1.0 : 0.0) - 0.5 * E[e];
+}
+
+// g[pair] (64 x 64 column-major FP64) = sum of the pair's Gram partials
+__global__ void mx_sum_partials(const void *__restrict__ part, int kind, int splits, int npairs, double *__restrict__ g)
+{
+    const size_t total = (size_t)npairs * kW * kW;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int pair = (int)(e / (kW * kW)), rc = (int)(e % (kW * kW));
+        const int r = rc & 63, c = rc >> 6;
+        double acc = 0.0;
+        if (kind == 0) {
+            const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
+            for (int s = 0; s < splits; ++s)
+                acc += (double)p[(size_t)s * 8192 + c * 128 + r] + (double)p[(size_t)s * 8192 + c * 128 + r + 64];
+        } else {
+            const double *p = static_cast<const double *>(part) + (size_t)pair * splits * 4096;
+            for (int s = 0; s < splits; ++s) acc += p[(size_t)s * 4096 + c * 64 + r];
+        }
+        g[e] = acc;
+    }
+}
+
+__global__ void mx_fill_int(int *__restrict__ p, int n, int v)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// sigma_j = ||x_j|| (one warp per column, FP64)
+__global__ void mx_sigma(const double *__restrict__ X, long ld, int rows, int cols, double *__restrict__ sigma)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= cols) return;
+    const double *x = X + (size_t)w * ld;
+    double acc = 0.0;
+    for (int i = lane; i < rows; i += 32) acc = fma(x[i], x[i], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) sigma[w] = sqrt(acc);
+}
+
+// ============================================================================
+// Host side
+// ============================================================================
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int get_encode_fn(EncodeTiledFn *out)
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q{};
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    if (!fn) {
+        set_last_error(JSVD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the CUDA driver.");
+        return JSVD_ERR_CUDA;
+    }
+    *out = fn;
+    return JSVD_OK;
+}
+
+// 2-D map of a column-major FP32 array (rows x cols, ld = rows), box 32 x 32,
+// 128-byte swizzle of 16-byte chunks (K-major operand tiles) or of 32-byte
+// chunks (MN-major TF32 operand tiles).
+int make_map(CUtensorMap *map, float *base, long rows, long cols, bool atom32 = false)
+{
+    EncodeTiledFn enc = nullptr;
+    if (int rc = get_encode_fn(&enc); rc != JSVD_OK) return rc;
+    const cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)rows * sizeof(float)};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           atom32 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_last_error(JSVD_ERR_CUDA, "cuTensorMapEncodeTiled failed (CUresult " + std::to_string((int)r) + ").");
+        return JSVD_ERR_CUDA;
+    }
+    return JSVD_OK;
+}
+
+int init_tables_once()
+{
+    static std::once_flag once;
+    static EvdTables t{};
+    std::call_once(once, [] {
+        for (int r = 0; r < kW - 1; ++r)
+            for (int k = 0; k < kW / 2; ++k) {
+                const int2 pq = round_robin_pair(kW, r, k);
+                t.pairs[r][k][0] = (unsigned char)pq.x;
+                t.pairs[r][k][1] = (unsigned char)pq.y;
+            }
+        int e = 0;
+        for (int a = 0; a < kW / 2; ++a)
+            for (int b = a; b < kW / 2; ++b) {
+                t.tri[e][0] = (unsigned char)a;
+                t.tri[e][1] = (unsigned char)b;
+                ++e;
+            }
+    });
+    // constant memory and function attributes are per device
+    static thread_local unsigned long long done_mask = 0;
+    int dev = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64 || !(done_mask & (1ull << dev))) {
+        JSVD_CUDA_TRY(cudaMemcpyToSymbol(c_evd, &t, sizeof(t)));
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGramTcSmem));
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_rot_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRotTcSmem));
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_rot_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRot64Smem));
+        JSVD_CUDA_TRY(
+            cudaFuncSetAttribute(mx_gram_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGram64Smem));
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_evd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEvdSmem));
+        if (dev < 64) done_mask |= 1ull << dev;
+    }
+    return JSVD_OK;
+}
+
+struct MixedStats {
+    unsigned long long solves = 0, tc_sweeps = 0, f64_sweeps = 0, block_rounds = 0, fallbacks = 0;
+    double qr_ms = 0, tc_ms = 0, orth_ms = 0, refine_ms = 0, out_ms = 0;
+    double last_tc_off = 0, last_f64_off = 0;
+    int last_tc_sweeps = 0, last_f64_sweeps = 0;
+    unsigned long long tc_gram = 0, tc_rot = 0, f64_gram = 0, f64_rot = 0, evd = 0;
+    unsigned long long tc_discarded = 0;
+};
+
+MixedStats &mixed_stats()
+{
+    thread_local MixedStats s;
+    return s;
+}
+
+jsvd_mixed_options default_options()
+{
+    jsvd_mixed_options o{};
+    o.precondition = 1;
+    o.tc_max_sweeps = 10;
+    o.tc_tol = 2e-5;
+    o.inner_sweeps = 2;
+    o.refine = 0;
+    o.f64_max_sweeps = 0;
+    o.gram_splits = 0;
+    return o;
+}
+
+jsvd_mixed_options &thread_options()
+{
+    thread_local jsvd_mixed_options o = default_options();
+    return o;
+}
+
+// Device workspace of one shape.
+struct Work {
+    int rows = 0, cols = 0, rows_pad = 0, cols_pad = 0, nb = 0, rounds = 0, npairs = 0;
+    int x_tiles = 0, v_tiles = 0;
+    int tc_splits = 1, tc_chunks = 0, tc_chunks_per_split = 0;
+    int f64_splits = 1, f64_rows_per_split = 0;
+    double *x64 = nullptr, *xr = nullptr, *v64 = nullptr, *vo = nullptr, *e64 = nullptr;
+    float *xh = nullptr, *xl = nullptr, *vh = nullptr, *vl = nullptr;
+    void *part = nullptr;
+    double *W = nullptr, *sg = nullptr;
+    int *flags = nullptr, *status = nullptr;
+    unsigned long long *stats = nullptr;    // [0] max off (double bits) [1] rotated pairs [2] orth max
+    unsigned long long *h_stats = nullptr;  // pinned copy
+    CUtensorMap mxh{}, mxl{}, mvh{}, mvl{};  // 16-byte-chunk swizzle (Gram operands)
+    CUtensorMap rxh{}, rxl{}, rvh{}, rvl{};  // 32-byte-chunk swizzle (rotation A operands)
+    void *block = nullptr;
+};
+
+int split_count(int chunks, int npairs, int requested)
+{
+    if (requested > 0) return std::max(1, std::min(requested, chunks));
+    // enough CTAs to cover the SMs about twice, at least 4 chunks per split
+    int s = (2 * 148 + npairs - 1) / std::max(1, npairs);
+    s = std::min(s, std::max(1, chunks / 4));
+    return std::max(1, s);
+}
+
+int make_work(int rows, int cols, const jsvd_mixed_options &o, bool tc, cudaStream_t st, Work &w)
+{
+    w.rows = rows;
+    w.cols = cols;
+    w.rows_pad = (rows + kTileRows - 1) / kTileRows * kTileRows;
+    w.cols_pad = (cols + kColPad - 1) / kColPad * kColPad;
+    w.nb = w.cols_pad / kB;
+    w.rounds = w.nb - 1;
+    w.npairs = w.nb / 2;
+    w.x_tiles = w.rows_pad / kTileRows;
+    w.v_tiles = w.cols_pad / kTileRows;
+    w.tc_chunks = w.rows_pad / 32;
+    w.tc_splits = split_count(w.tc_chunks, w.npairs, o.gram_splits);
+    w.tc_chunks_per_split = (w.tc_chunks + w.tc_splits - 1) / w.tc_splits;
+    w.tc_splits = (w.tc_chunks + w.tc_chunks_per_split - 1) / w.tc_chunks_per_split;  // no empty split
+    const int r32 = w.rows_pad / 32;
+    w.f64_splits = split_count(r32, w.npairs, o.gram_splits);
+    w.f64_rows_per_split = (r32 + w.f64_splits - 1) / w.f64_splits * 32;
+    w.f64_splits = (w.rows_pad + w.f64_rows_per_split - 1) / w.f64_rows_per_split;
+    const size_t mn = (size_t)w.rows_pad * w.cols_pad, nn = (size_t)w.cols_pad * w.cols_pad;
+    const int splits = std::max(w.tc_splits, w.f64_splits);
+    const size_t part_bytes = (size_t)w.npairs * splits * 4096 * sizeof(double);
+    size_t bytes = 0;
+    auto take = [&](size_t b) {
+        const size_t off = bytes;
+        bytes += (b + 255) / 256 * 256;
+        return off;
+    };
+    const size_t o_x64 = take(mn * 8), o_xr = take(mn * 8), o_v64 = take(nn * 8), o_vo = take(nn * 8),
+                 o_e = take(nn * 8);
+    const size_t o_xh = tc ? take(mn * 4) : 0, o_xl = tc ? take(mn * 4) : 0, o_vh = tc ? take(nn * 4) : 0,
+                 o_vl = tc ? take(nn * 4) : 0;
+    const size_t o_part = take(part_bytes), o_w = take((size_t)w.npairs * kW * kW * 8), o_sg = take(w.cols_pad * 8),
+                 o_flags = take(w.npairs * 4), o_status = take(4), o_stats = take(4 * 8);
+    JSVD_CUDA_TRY(cudaMallocAsync(&w.block, bytes, st));
+    uint8_t *b = static_cast<uint8_t *>(w.block);
+    w.x64 = reinterpret_cast<double *>(b + o_x64);
+    w.xr = reinterpret_cast<double *>(b + o_xr);
+    w.v64 = reinterpret_cast<double *>(b + o_v64);
+    w.vo = reinterpret_cast<double *>(b + o_vo);
+    w.e64 = reinterpret_cast<double *>(b + o_e);
+    if (tc) {
+        w.xh = reinterpret_cast<float *>(b + o_xh);
+        w.xl = reinterpret_cast<float *>(b + o_xl);
+        w.vh = reinterpret_cast<float *>(b + o_vh);
+        w.vl = reinterpret_cast<float *>(b + o_vl);
+    }
+    w.part = b + o_part;
+    w.W = reinterpret_cast<double *>(b + o_w);
+    w.sg = reinterpret_cast<double *>(b + o_sg);
+    w.flags = reinterpret_cast<int *>(b + o_flags);
+    w.status = reinterpret_cast<int *>(b + o_status);
+    w.stats = reinterpret_cast<unsigned long long *>(b + o_stats);
+    JSVD_CUDA_TRY(cudaMallocHost((void **)&w.h_stats, 4 * sizeof(unsigned long long)));
+    if (tc) {
+        if (int rc = make_map(&w.mxh, w.xh, w.rows_pad, w.cols_pad); rc != JSVD_OK) return rc;
+        if (int rc = make_map(&w.mxl, w.xl, w.rows_pad, w.cols_pad); rc != JSVD_OK) return rc;
+        if (int rc = make_map(&w.mvh, w.vh, w.cols_pad, w.cols_pad); rc != JSVD_OK) return rc;
+        if (int rc = make_map(&w.mvl, w.vl, w.cols_pad, w.cols_pad); rc != JSVD_OK) return rc;
+        if (int rc = make_map(&w.rxh, w.xh, w.rows_pad, w.cols_pad, true); rc != JSVD_OK) return rc;
+        if (int rc = make_map(&w.rxl, w.xl, w.rows_pad, w.cols_pad, true); rc != JSVD_OK) return rc;
+        if (int rc = make_map(&w.rvh, w.vh, w.cols_pad, w.cols_pad, true); rc != JSVD_OK) return rc;
+        if (int rc = make_map(&w.rvl, w.vl, w.cols_pad, w.cols_pad, true); rc != JSVD_OK) return rc;
+    }
+    return JSVD_OK;
+}
+
+void free_work(Work &w, cudaStream_t st)
+{
+    if (w.block) cudaFreeAsync(w.block, st);
+    if (w.h_stats) cudaFreeHost(w.h_stats);
+    w.block = nullptr;
+    w.h_stats = nullptr;
+}
+
+unsigned grid_for(size_t count) { return (unsigned)std::min<size_t>(148 * 8, (count + 255) / 256); }
+
+// One sweep (every block round) of phase 1 or phase 3; reads back the
+// sweep's statistics.
+int run_sweep(Work &w, bool tc, double tau, int inner, cudaStream_t st, double *max_off, unsigned long long *rotated)
+{
+    MixedStats &ms = mixed_stats();
+    JSVD_CUDA_TRY(cudaMemsetAsync(w.stats, 0, 2 * sizeof(unsigned long long), st));
+    for (int r = 0; r < w.rounds; ++r) {
+        if (tc) {
+            mx_gram_tc<<<dim3(w.tc_splits, w.npairs), kGramTcThreads, kGramTcSmem, st>>>(
+                w.mxh, w.mxl, w.nb, r, w.tc_chunks, w.tc_chunks_per_split, static_cast<float *>(w.part), w.status);
+            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.W, w.flags,
+                                                            w.stats);
+            mx_rot_tc<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
+                w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, w.rows_pad, w.x_tiles, w.vh, w.vl, w.cols_pad, w.nb, r, w.W,
+                w.flags, w.status);
+            ms.tc_gram += 1;
+            ms.tc_rot += 1;
+        } else {
+            mx_gram_f64<<<dim3(w.f64_splits, w.npairs), kGram64Threads, kGram64Smem, st>>>(
+                w.xr, w.rows_pad, w.nb, r, w.f64_rows_per_split, w.rows_pad, static_cast<double *>(w.part));
+            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 1, w.f64_splits, tau, inner, w.W, w.flags,
+                                                            w.stats);
+            mx_rot_f64<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRot64Threads, kRot64Smem, st>>>(
+                w.xr, w.rows_pad, w.x_tiles, w.v64, w.cols_pad, w.nb, r, w.W, w.flags);
+            ms.f64_gram += 1;
+            ms.f64_rot += 1;
+        }
+        ms.evd += 1;
+    }
+    JSVD_CUDA_TRY(cudaGetLastError());
+    ms.block_rounds += (unsigned long long)w.rounds;
+    JSVD_CUDA_TRY(cudaMemcpyAsync(w.h_stats, w.stats, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    int dstatus = 0;
+    JSVD_CUDA_TRY(cudaMemcpyAsync(&dstatus, w.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (dstatus != 0) {
+        set_last_error(JSVD_ERR_RUNTIME, "mixed engine: a tensor-core kernel gave up waiting for its operands "
+                                         "(device status " +
+                                             std::to_string(dstatus) + ").");
+        return JSVD_ERR_RUNTIME;
+    }
+    const unsigned long long bits = w.h_stats[0];
+    double off;
+    std::memcpy(&off, &bits, sizeof(off));
+    *max_off = off;
+    *rotated = w.h_stats[1];
+    return JSVD_OK;
+}
+
+// V <- polar factor of V (Newton-Schulz), at most `steps` steps; stops once
+// max |V^T V - I| <= 4u.  Result in w.v64; *residual = max |V^T V - I| of the
+// last iterate measured.
+int orthogonalise(Work &w, cudaStream_t st, int steps, double *residual)
+{
+    *residual = INFINITY;
+    const int n = w.cols_pad;
+    const size_t nn = (size_t)n * n;
+    for (int i = 0; i < steps; ++i) {
+        if (int rc = dgemm(st, 'T', 'N', n, n, n, 1.0, w.v64, n, w.v64, n, 0.0, w.e64, n); rc != JSVD_OK) return rc;
+        JSVD_CUDA_TRY(cudaMemsetAsync(w.stats + 2, 0, sizeof(unsigned long long), st));
+        mx_minus_identity_max<<<grid_for(nn), 256, 0, st>>>(w.e64, n, w.stats + 2);
+        JSVD_CUDA_TRY(cudaGetLastError());
+        JSVD_CUDA_TRY(
+            cudaMemcpyAsync(w.h_stats + 2, w.stats + 2, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+        double e;
+        std::memcpy(&e, &w.h_stats[2], sizeof(e));
+        *residual = e;
+        if (!(e <= 0.25)) break;  // not near orthogonal (or NaN): the iteration would not converge
+        if (e <= 4.0 * 1.1102230246251565e-16) break;
+        mx_half_step<<<grid_for(nn), 256, 0, st>>>(w.e64, n);
+        if (int rc = dgemm(st, 'N', 'N', n, n, n, 1.0, w.v64, n, w.e64, n, 0.0, w.vo, n); rc != JSVD_OK) return rc;
+        std::swap(w.v64, w.vo);
+    }
+    return JSVD_OK;
+}
+
+}  // namespace
+
+const jsvd_mixed_options &mixed_options() { return thread_options(); }
+
+int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const jsvd_mixed_options &o, double *u,
+                double *sigma, double *v, int *sweeps, cudaStream_t st)
+{
+    if (int rc = init_tables_once(); rc != JSVD_OK) return rc;
+    const bool tc = o.tc_max_sweeps > 0;
+    Work w;
+    ScopeExit release([&] { free_work(w, st); });
+    if (int rc = make_work(rows, cols, o, tc, st, w); rc != JSVD_OK) return rc;
+    MixedStats &ms = mixed_stats();
+    cudaEvent_t ev[5] = {};
+    for (auto &e : ev) cudaEventCreate(&e);
+    ScopeExit destroy([&] {
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    });
+    const size_t mn = (size_t)w.rows_pad * w.cols_pad, nn = (size_t)w.cols_pad * w.cols_pad;
+    cudaEventRecord(ev[0], st);
+    JSVD_CUDA_TRY(cudaMemsetAsync(w.status, 0, sizeof(int), st));
+    mx_rowmajor_to_padded<<<dim3(w.cols_pad / kT, w.rows_pad / kT), dim3(kT, kTR), 0, st>>>(
+        x, rows, cols, w.x64, w.rows_pad, w.rows_pad, w.cols_pad);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    int tc_sweeps = 0, f64_sweeps = 0;
+    double tc_off = 0.0;
+    const double u53 = 1.1102230246251565e-16;
+    if (tc) {
+        mx_split<<<grid_for(mn), 256, 0, st>>>(w.x64, mn, w.xh, w.xl);
+        mx_identity<<<grid_for(nn), 256, 0, st>>>(nullptr, w.vh, w.vl, w.cols_pad);
+        JSVD_CUDA_TRY(cudaGetLastError());
+        // Phase 1 rotates every pair the FP32-accurate Gram resolves: its
+        // entries carry relative errors of about 2^-21 + sqrt(m) 2^-24.
+        const double tau = std::max(o.tc_tol * 0.25, 4.0 * std::sqrt((double)w.rows_pad) * 5.96e-8);
+        for (int s = 0; s < o.tc_max_sweeps; ++s) {
+            unsigned long long rotated = 0;
+            if (int rc = run_sweep(w, true, tau, o.inner_sweeps, st, &tc_off, &rotated); rc != JSVD_OK) return rc;
+            ++tc_sweeps;
+            if (rotated == 0 || tc_off <= o.tc_tol) break;
+        }
+        cudaEventRecord(ev[1], st);
+        mx_join<<<grid_for(nn), 256, 0, st>>>(w.vh, w.vl, nn, w.v64);
+        JSVD_CUDA_TRY(cudaGetLastError());
+        double orth = INFINITY;
+        if (int rc = orthogonalise(w, st, 4, &orth); rc != JSVD_OK) return rc;
+        if (orth <= 1e-12) {
+            if (int rc = dgemm(st, 'N', 'N', w.rows_pad, w.cols_pad, w.cols_pad, 1.0, w.x64, w.rows_pad, w.v64,
+                               w.cols_pad, 0.0, w.xr, w.rows_pad);
+                rc != JSVD_OK)
+                return rc;
+        } else {
+            // phase 1 did not leave a usable V: the FP64 sweeps start from X
+            ms.tc_discarded += 1;
+            JSVD_CUDA_TRY(cudaMemcpyAsync(w.xr, w.x64, mn * 8, cudaMemcpyDeviceToDevice, st));
+            mx_identity<<<grid_for(nn), 256, 0, st>>>(w.v64, nullptr, nullptr, w.cols_pad);
+            JSVD_CUDA_TRY(cudaGetLastError());
+        }
+        cudaEventRecord(ev[2], st);
+    } else {
+        JSVD_CUDA_TRY(cudaMemcpyAsync(w.xr, w.x64, mn * 8, cudaMemcpyDeviceToDevice, st));
+        mx_identity<<<grid_for(nn), 256, 0, st>>>(w.v64, nullptr, nullptr, w.cols_pad);
+        JSVD_CUDA_TRY(cudaGetLastError());
+        cudaEventRecord(ev[1], st);
+        cudaEventRecord(ev[2], st);
+    }
+    // Phase 3: FP64 blocked sweeps.  The Gram's own rounding (about
+    // sqrt(m) u relative) sets the smallest threshold it can decide.
+    const double tau64 = std::max(c.epsilon, 4.0 * std::sqrt((double)w.rows_pad) * u53);
+    const int cap = o.f64_max_sweeps > 0 ? o.f64_max_sweeps : c.max_sweeps;
+    double f64_off = 0.0;
+    for (int s = 0; s < cap; ++s) {
+        unsigned long long rotated = 0;
+        if (int rc = run_sweep(w, false, tau64, o.inner_sweeps, st, &f64_off, &rotated); rc != JSVD_OK) return rc;
+        ++f64_sweeps;
+        if (rotated == 0) break;
+    }
+    cudaEventRecord(ev[3], st);
+    double *sg = sigma ? sigma : w.sg;
+    mx_sigma<<<(cols * 32 + 255) / 256, 256, 0, st>>>(w.xr, w.rows_pad, rows, cols, sg);
+    if (u)
+        mx_padded_to_rowmajor<<<dim3((rows + kT - 1) / kT, (cols + kT - 1) / kT), dim3(kT, kTR), 0, st>>>(
+            w.xr, w.rows_pad, rows, cols, u, sg, c.epsilon);
+    if (v)
+        mx_padded_to_rowmajor<<<dim3((cols + kT - 1) / kT, (cols + kT - 1) / kT), dim3(kT, kTR), 0, st>>>(
+            w.v64, w.cols_pad, cols, cols, v, nullptr, 0.0);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    cudaEventRecord(ev[4], st);
+    JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+    float t01 = 0, t12 = 0, t23 = 0, t34 = 0;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    cudaEventElapsedTime(&t34, ev[3], ev[4]);
+    ms.tc_ms += t01;
+    ms.orth_ms += t12;
+    ms.refine_ms += t23;
+    ms.out_ms += t34;
+    ms.tc_sweeps += tc_sweeps;
+    ms.f64_sweeps += f64_sweeps;
+    ms.last_tc_sweeps = tc_sweeps;
+    ms.last_f64_sweeps = f64_sweeps;
+    ms.last_tc_off = tc_off;
+    ms.last_f64_off = f64_off;
+    if (sweeps) *sweeps = tc_sweeps + f64_sweeps;
+    return JSVD_OK;
+}
+
+void mixed_note_solve(double qr_ms, bool fallback)
+{
+    MixedStats &ms = mixed_stats();
+    ms.solves += 1;
+    ms.qr_ms += qr_ms;
+    if (fallback) ms.fallbacks += 1;
+}
+
+}  // namespace jsvd
+
+using namespace jsvd;
+
+// Kernel-level test hook: one block round of the engine's kernels on X
+// (rows x cols, column-major FP64, device; rows and cols multiples of 128).
+//   kind 0: tensor-core Gram of every block pair of `round` -> gw
+//           (npairs x 64 x 64, column-major FP64, the partials summed);
+//   kind 1: the FP64 Gram -> gw;
+//   kind 2: tensor-core rotation X_pair <- X_pair W_pair with W from gw (X is
+//           split into TF32 head and tail first and joined afterwards);
+//   kind 3: the FP64 rotation.
+extern "C" int jsvd_mixed_test_round(int kind, double *d_x, int rows, int cols, int round, double *d_gw)
+{
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (!d_x || !d_gw || rows <= 0 || cols <= 0 || rows % kTileRows || cols % kColPad || kind < 0 || kind > 3 ||
+            round < 0 || round >= cols / kB - 1)
+            return invalid_argument("jsvd_mixed_test_round: bad arguments.");
+        cudaStream_t st = nullptr;
+        if (const int e = entry_stream(nullptr, &st); e != JSVD_OK) return e;
+        if (int rc = init_tables_once(); rc != JSVD_OK) return rc;
+        const bool tc = (kind == 0 || kind == 2);
+        jsvd_mixed_options o = default_options();
+        Work w;
+        ScopeExit release([&] { free_work(w, st); });
+        if (int rc = make_work(rows, cols, o, tc, st, w); rc != JSVD_OK) return rc;
+        const size_t mn = (size_t)rows * cols;
+        JSVD_CUDA_TRY(cudaMemsetAsync(w.status, 0, sizeof(int), st));
+        if (tc) mx_split<<<grid_for(mn), 256, 0, st>>>(d_x, mn, w.xh, w.xl);
+        if (kind == 0) {
+            mx_gram_tc<<<dim3(w.tc_splits, w.npairs), kGramTcThreads, kGramTcSmem, st>>>(
+                w.mxh, w.mxl, w.nb, round, w.tc_chunks, w.tc_chunks_per_split, static_cast<float *>(w.part), w.status);
+            mx_sum_partials<<<grid_for((size_t)w.npairs * 4096), 256, 0, st>>>(w.part, 0, w.tc_splits, w.npairs, d_gw);
+        } else if (kind == 1) {
+            mx_gram_f64<<<dim3(w.f64_splits, w.npairs), kGram64Threads, kGram64Smem, st>>>(
+                d_x, rows, w.nb, round, w.f64_rows_per_split, rows, static_cast<double *>(w.part));
+            mx_sum_partials<<<grid_for((size_t)w.npairs * 4096), 256, 0, st>>>(w.part, 1, w.f64_splits, w.npairs,
+                                                                                d_gw);
+        } else {
+            mx_fill_int<<<1, 256, 0, st>>>(w.flags, w.npairs, 1);
+            if (kind == 2) {
+                mx_rot_tc<<<dim3(w.x_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
+                    w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, rows, w.x_tiles, w.vh, w.vl, cols, w.nb, round, d_gw,
+                    w.flags, w.status);
+                mx_join<<<grid_for(mn), 256, 0, st>>>(w.xh, w.xl, mn, d_x);
+            } else {
+                mx_rot_f64<<<dim3(w.x_tiles, w.npairs), kRot64Threads, kRot64Smem, st>>>(
+                    d_x, rows, w.x_tiles, w.v64, cols, w.nb, round, d_gw, w.flags);
+            }
+        }
+        JSVD_CUDA_TRY(cudaGetLastError());
+        int dstatus = 0;
+        JSVD_CUDA_TRY(cudaMemcpyAsync(&dstatus, w.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+        if (dstatus != 0) {
+            set_last_error(JSVD_ERR_RUNTIME, "jsvd_mixed_test_round: device status " + std::to_string(dstatus));
+            return JSVD_ERR_RUNTIME;
+        }
+        return JSVD_OK;
+    });
+}
+
+extern "C" void jsvd_mixed_options_default(jsvd_mixed_options *o)
+{
+    if (o) *o = default_options();
+}
+
+extern "C" void jsvd_mixed_set_options(const jsvd_mixed_options *o) { thread_options() = o ? *o : default_options(); }
+
+extern "C" void jsvd_mixed_stats_get(jsvd_mixed_stats *out)
+{
+    if (!out) return;
+    const MixedStats &s = mixed_stats();
+    out->solves = s.solves;
+    out->tc_sweeps = s.tc_sweeps;
+    out->f64_sweeps = s.f64_sweeps;
+    out->block_rounds = s.block_rounds;
+    out->fallbacks = s.fallbacks;
+    out->qr_ms = s.qr_ms;
+    out->tc_ms = s.tc_ms;
+    out->orth_ms = s.orth_ms;
+    out->refine_ms = s.refine_ms;
+    out->out_ms = s.out_ms;
+    out->last_tc_offdiag = s.last_tc_off;
+    out->last_f64_offdiag = s.last_f64_off;
+    out->last_tc_sweeps = s.last_tc_sweeps;
+    out->last_f64_sweeps = s.last_f64_sweeps;
+    out->tc_gram_launches = s.tc_gram;
+    out->tc_rot_launches = s.tc_rot;
+    out->f64_gram_launches = s.f64_gram;
+    out->f64_rot_launches = s.f64_rot;
+    out->evd_launches = s.evd;
+    out->tc_discarded = s.tc_discarded;
+}
+
+extern "C" void jsvd_mixed_stats_reset(void) { mixed_stats() = MixedStats{}; }

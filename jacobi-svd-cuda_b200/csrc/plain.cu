@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "dgemm.hpp"
 #include "internal.hpp"
 #include "layout.cuh"
 #include "plain.hpp"
@@ -663,7 +664,6 @@ PlainPlan::~PlainPlan()
                     (void *)gram_count})
         if (p) cudaFreeAsync(p, stream);
     if (h_gram_count) cudaFreeHost(h_gram_count);
-    if (cublas) cublasDestroy(cublas);
     if (prev >= 0) cudaSetDevice(prev);
 }
 
@@ -848,21 +848,9 @@ int PlainPlan::gram_converged(cudaStream_t st, bool &converged)
         JSVD_CUDA_TRY(cudaMallocHost((void **)&h_gram_count, sizeof(unsigned)));
         JSVD_CUDA_TRY(cudaStreamSynchronize(stream));
     }
-    if (cublas == nullptr) {
-        const cublasStatus_t cs0 = cublasCreate(&cublas);
-        if (cs0 != CUBLAS_STATUS_SUCCESS) {
-            cublas = nullptr;
-            set_last_error(JSVD_ERR_CUDA, "cublasCreate failed (status " + std::to_string((int)cs0) + ").");
-            return JSVD_ERR_CUDA;
-        }
-    }
-    const double one = 1.0, zero = 0.0;
-    if (cublasSetStream(cublas, st) != CUBLAS_STATUS_SUCCESS ||
-        cublasDsyrk(cublas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)n, (int)m, &one, a_w, (int)lda, &zero, gram,
-                    (int)n) != CUBLAS_STATUS_SUCCESS) {
-        set_last_error(JSVD_ERR_CUDA, "cublasDsyrk failed in the Gram convergence test.");
-        return JSVD_ERR_CUDA;
-    }
+    if (const int rc = dgemm(st, 'T', 'N', (int)n, (int)n, (int)m, 1.0, a_w, lda, a_w, lda, 0.0, gram, (long)n, 1);
+        rc != JSVD_OK)
+        return rc;
     JSVD_CUDA_TRY(cudaMemsetAsync(gram_count, 0, sizeof(unsigned), st));
     gram_offdiag_count<<<std::min<size_t>(1184, (n * n + 255) / 256), 256, 0, st>>>(gram, (int)n, eps, gram_count);
     JSVD_CUDA_TRY(cudaGetLastError());

@@ -4,7 +4,6 @@
 // graph instantiation once.
 #pragma once
 
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -58,7 +57,6 @@ struct PlainPlan {
     double *gram = nullptr;            // n x n, lower triangle
     unsigned *gram_count = nullptr;    // pairs that would rotate
     unsigned *h_gram_count = nullptr;  // pinned
-    cublasHandle_t cublas = nullptr;
 
     cudaGraphExec_t sweep_exec = nullptr;   // rounds of even sweeps
     cudaGraphExec_t sweep_exec2 = nullptr;  // rounds of odd sweeps
@@ -82,7 +80,7 @@ struct PlainPlan {
     int capture_rounds(cudaStream_t st, int parity);
     // Runs the whole solve on device buffers; outputs may be null.  With
     // gram_stop and eps >= 1e-12, a sweep that rotated few pairs is followed
-    // by a test of every pair on G = A^T A (one DSYRK): when no pair would
+    // by a test of every pair on G = A^T A (one lower-triangle GEMM): when no pair would
     // rotate, the next sweep would change nothing and is not run (it is
     // counted in `sweeps`).  The
     // dot products then come from the GEMM, not the reference's reduction

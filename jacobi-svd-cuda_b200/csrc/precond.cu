@@ -14,11 +14,10 @@
 //   3. X V_x = U_x Sigma  =>  A = Q R = Q V_x Sigma U_x^T, so
 //      V_A = U_x (normalised columns of the rotated X), U_A = Q V_x, Sigma_A =
 //      Sigma_x (unsorted, in X's column order).
-// Gram products and triangular updates are plain DGEMM/DSYRK calls (cuBLAS);
-// the Cholesky diagonal blocks, the triangular row solves, the shift and the
-// layout kernels are written here.  If a Cholesky pivot is not positive the
-// solve falls back to the plain path on A.
-#include <cublas_v2.h>
+// Gram products and triangular updates run on this library's FP64 tensor-core
+// GEMM (dgemm.cu); the Cholesky diagonal blocks, the triangular row solves,
+// the shift and the layout kernels are written here.  If a Cholesky pivot is
+// not positive the solve falls back to the plain path on A.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -31,9 +30,11 @@
 #include <vector>
 
 #include "blockpair.hpp"
+#include "dgemm.hpp"
 #include "internal.hpp"
 #include "jsvd.h"
 #include "layout.cuh"
+#include "mixed.hpp"
 #include "plain.hpp"
 
 namespace jsvd {
@@ -41,29 +42,10 @@ namespace {
 
 constexpr int kNb = 64;  // Cholesky / triangular block size
 
-const char *cublas_name(cublasStatus_t s)
-{
-    switch (s) {
-    case CUBLAS_STATUS_SUCCESS: return "CUBLAS_STATUS_SUCCESS";
-    case CUBLAS_STATUS_NOT_INITIALIZED: return "CUBLAS_STATUS_NOT_INITIALIZED";
-    case CUBLAS_STATUS_ALLOC_FAILED: return "CUBLAS_STATUS_ALLOC_FAILED";
-    case CUBLAS_STATUS_INVALID_VALUE: return "CUBLAS_STATUS_INVALID_VALUE";
-    case CUBLAS_STATUS_EXECUTION_FAILED: return "CUBLAS_STATUS_EXECUTION_FAILED";
-    default: return "CUBLAS error";
-    }
-}
-
-int cublas_failure(cublasStatus_t s, const char *expr, const char *file, int line)
-{
-    set_last_error(JSVD_ERR_CUDA, std::string("cuBLAS call failed: ") + expr + " @ " + file + ":" +
-                                      std::to_string(line) + ", status=" + cublas_name(s));
-    return JSVD_ERR_CUDA;
-}
-
-#define JSVD_CUBLAS_TRY(EXPR)                                                              \
-    do {                                                                                   \
-        cublasStatus_t st_ = (EXPR);                                                       \
-        if (st_ != CUBLAS_STATUS_SUCCESS) return cublas_failure(st_, #EXPR, __FILE__, __LINE__); \
+#define JSVD_GEMM_TRY(EXPR)                       \
+    do {                                          \
+        const int gemm_rc_ = (EXPR);              \
+        if (gemm_rc_ != JSVD_OK) return gemm_rc_; \
     } while (0)
 
 // row-major (rows x cols) -> column-major (ld = rows), one launch (the n x n
@@ -237,40 +219,15 @@ __global__ void pc_lower_to_upper(const double *__restrict__ L, double *__restri
     }
 }
 
-struct CublasHandle {
-    cublasHandle_t h = nullptr;
-    int device = -1;
-    ~CublasHandle()
-    {
-        if (h) cublasDestroy(h);
-    }
-};
-
-int thread_cublas(int dev, cudaStream_t st, cublasHandle_t *out)
-{
-    thread_local CublasHandle ch;
-    if (ch.h == nullptr || ch.device != dev) {
-        if (ch.h) cublasDestroy(ch.h);
-        ch.h = nullptr;
-        JSVD_CUBLAS_TRY(cublasCreate(&ch.h));
-        ch.device = dev;
-    }
-    JSVD_CUBLAS_TRY(cublasSetStream(ch.h, st));
-    *out = ch.h;
-    return JSVD_OK;
-}
-
 // One Cholesky QR pass: G = Q^T Q (+ shift), G = L L^T (blocked,
 // right-looking; diagonal blocks factored and inverted by pc_chol_inv_diag,
-// panels L21 = G21 L11^{-T} and trailing updates as DGEMM/DSYRK), then
+// panels L21 = G21 L11^{-T} and trailing updates as GEMMs), then
 // Qout = Q L^{-T} by a blocked right-looking solve (Qout_J = Q_J Linv_J^T,
 // Q_{>J} -= Qout_J L_{>J,J}^T; Q is overwritten) and R = L^T.
-int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Q, double *Qout, int m, int n, double *G, double *Lm,
-                 double *Linv, double *R, bool shift, int *d_status)
+int chol_qr_pass(cudaStream_t st, double *Q, double *Qout, int m, int n, double *G, double *Lm, double *Linv,
+                 double *R, bool shift, int *d_status)
 {
-    const double one = 1.0, zero = 0.0, mone = -1.0;
-    JSVD_CUDA_TRY(cudaFuncSetAttribute(pc_chol_inv_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
-    JSVD_CUBLAS_TRY(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, m, &one, Q, m, &zero, G, n));
+    JSVD_GEMM_TRY(dgemm(st, 'T', 'N', n, n, m, 1.0, Q, m, Q, m, 0.0, G, n, 1));
     if (shift) {
         pc_shift_diagonal<<<1, 256, 0, st>>>(G, n, m);
         JSVD_CUDA_TRY(cudaGetLastError());
@@ -283,23 +240,22 @@ int chol_qr_pass(cublasHandle_t hb, cudaStream_t st, double *Q, double *Qout, in
         const int rest = n - k0 - kb;
         if (rest > 0) {
             // L21 = G21 L11^{-T}
-            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, rest, kb, kb, &one, G + (size_t)k0 * n + k0 + kb,
-                                        n, li, kNb, &zero, Lm + (size_t)k0 * n + k0 + kb, n));
+            JSVD_GEMM_TRY(dgemm(st, 'N', 'T', rest, kb, kb, 1.0, G + (size_t)k0 * n + k0 + kb, n, li, kNb, 0.0,
+                                Lm + (size_t)k0 * n + k0 + kb, n));
             // G22 -= L21 L21^T (lower)
-            JSVD_CUBLAS_TRY(cublasDsyrk(hb, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, rest, kb, &mone,
-                                        Lm + (size_t)k0 * n + k0 + kb, n, &one, G + (size_t)(k0 + kb) * n + k0 + kb,
-                                        n));
+            JSVD_GEMM_TRY(dgemm(st, 'N', 'T', rest, rest, kb, -1.0, Lm + (size_t)k0 * n + k0 + kb, n,
+                                Lm + (size_t)k0 * n + k0 + kb, n, 1.0, G + (size_t)(k0 + kb) * n + k0 + kb, n, 1));
         }
     }
     for (int j0 = 0, blk = 0; j0 < n; j0 += kNb, ++blk) {
         const int kb = std::min(kNb, n - j0);
         const double *li = Linv + (size_t)blk * kNb * kNb;
-        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, kb, kb, &one, Q + (size_t)j0 * m, m, li, kNb,
-                                    &zero, Qout + (size_t)j0 * m, m));
+        JSVD_GEMM_TRY(
+            dgemm(st, 'N', 'T', m, kb, kb, 1.0, Q + (size_t)j0 * m, m, li, kNb, 0.0, Qout + (size_t)j0 * m, m));
         const int rest = n - j0 - kb;
         if (rest > 0)
-            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, m, rest, kb, &mone, Qout + (size_t)j0 * m, m,
-                                        Lm + (size_t)j0 * n + j0 + kb, n, &one, Q + (size_t)(j0 + kb) * m, m));
+            JSVD_GEMM_TRY(dgemm(st, 'N', 'T', m, rest, kb, -1.0, Qout + (size_t)j0 * m, m, Lm + (size_t)j0 * n + j0 + kb,
+                                n, 1.0, Q + (size_t)(j0 + kb) * m, m));
     }
     pc_lower_to_upper<<<std::min<size_t>(1184, ((size_t)n * n + 255) / 256), 256, 0, st>>>(Lm, R, n);
     JSVD_CUDA_TRY(cudaGetLastError());
@@ -314,10 +270,16 @@ std::atomic<int> g_gram_stop{1};
 // measured faster on B200 for the 1024-column factor of a 4096 x 1024 input
 // (4.0 us per round, 1023 rounds per sweep, against 18 us per block-pair outer
 // round, 255 per sweep).
+// Engine 2 is the blocked mixed-precision sweep (mixed.cu), used by
+// jsvd_mixed_svd*.
+constexpr int kEngineMixed = 2;
+
 int inner_jacobi(const double *x, size_t cols, const jsvd_config &c, double *u, double *sigma, double *v, int *sweeps,
-                 cudaStream_t st)
+                 cudaStream_t st, int engine)
 {
-    if (g_inner.load() == 0 && bp_supported(cols, cols))
+    if (engine == kEngineMixed && cols >= (size_t)kMixedMinCols)
+        return mixed_solve(x, (int)cols, (int)cols, c, mixed_options(), u, sigma, v, sweeps, st);
+    if (engine == 0 && bp_supported(cols, cols))
         return bp_solve(x, cols, cols, c.epsilon, c.max_sweeps, u, sigma, v, sweeps, st);
     // The last, rotation-free sweep is replaced by a test of every pair on the
     // Gram matrix (this path is held to a tolerance, not to the bits).
@@ -337,18 +299,14 @@ PrecondStats &precond_stats()
 }
 
 // Per-thread cached resources of the QR stage for one shape: the workspace,
-// a stream for allocation and graph capture, a cuBLAS handle with its own
-// fixed workspace (so the captured GEMMs never allocate and the handle never
-// refers to another plan's memory), and the two shifted CholeskyQR3 stages
-// captured as graphs on the plan's second use.  The stage is ~500 small
+// a stream for allocation and graph capture, and the two shifted CholeskyQR3
+// stages captured as graphs on the plan's second use.  The stage is ~500 small
 // launches whose enqueueing, not their device time, set its duration.
 struct PcPlan {
     int device = -1;
     size_t m = 0, n = 0;
     double *ws = nullptr;
-    void *blas_ws = nullptr;
     cudaStream_t own = nullptr;
-    cublasHandle_t blas = nullptr;
     cudaGraphExec_t qr1 = nullptr, qr2 = nullptr;
     bool no_graph = false;  // a capture failed: launch directly from then on
     unsigned long long uses = 0;
@@ -356,17 +314,14 @@ struct PcPlan {
     {
         if (qr1) cudaGraphExecDestroy(qr1);
         if (qr2) cudaGraphExecDestroy(qr2);
-        if (blas) cublasDestroy(blas);
         if (own) {
             if (ws) cudaFreeAsync(ws, own);
-            if (blas_ws) cudaFreeAsync(blas_ws, own);
             cudaStreamSynchronize(own);
             cudaStreamDestroy(own);
         }
     }
 };
 
-constexpr size_t kPcBlasWorkspace = size_t(32) << 20;
 constexpr size_t kPcMaxPlanBytes = size_t(2) << 30;  // larger shapes allocate per call, no graphs
 constexpr size_t kPcMaxPlans = 2;
 
@@ -402,10 +357,7 @@ int acquire_pc_plan(int dev, size_t m, size_t n, size_t ws_doubles, PcPlan **out
         }
     }
     JSVD_CUDA_TRY(cudaMallocAsync((void **)&p->ws, sizeof(double) * ws_doubles, p->own));
-    JSVD_CUDA_TRY(cudaMallocAsync(&p->blas_ws, kPcBlasWorkspace, p->own));
     JSVD_CUDA_TRY(cudaStreamSynchronize(p->own));
-    JSVD_CUBLAS_TRY(cublasCreate(&p->blas));
-    JSVD_CUBLAS_TRY(cublasSetWorkspace(p->blas, p->blas_ws, kPcBlasWorkspace));
     JSVD_CUDA_TRY(cudaFuncSetAttribute(pc_chol_inv_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
     plans.insert(plans.begin(), std::move(p));
     while (plans.size() > kPcMaxPlans) plans.pop_back();
@@ -414,7 +366,7 @@ int acquire_pc_plan(int dev, size_t m, size_t n, size_t ws_doubles, PcPlan **out
 }
 
 int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config &c, double *d_u, double *d_sigma,
-                 double *d_v, int *sweeps, cudaStream_t st)
+                 double *d_v, int *sweeps, cudaStream_t st, int engine)
 {
     const int m = (int)rows, n = (int)cols;
     int dev = 0;
@@ -427,14 +379,7 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     PcPlan *plan = nullptr;
     int rc = acquire_pc_plan(dev, rows, cols, ws_doubles, &plan);
     if (rc != JSVD_OK) return rc;
-    cublasHandle_t hb = nullptr;
-    if (plan) {
-        hb = plan->blas;
-        JSVD_CUBLAS_TRY(cublasSetStream(hb, st));
-    } else {
-        rc = thread_cublas(dev, st, &hb);
-        if (rc != JSVD_OK) return rc;
-    }
+    JSVD_CUDA_TRY(cudaFuncSetAttribute(pc_chol_inv_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem));
     double *ws = plan ? plan->ws : nullptr;
     if (!plan) JSVD_CUDA_TRY(cudaMallocAsync((void **)&ws, sizeof(double) * ws_doubles, st));
     double *Qa = ws, *Qb = Qa + mn, *G = Qb + mn, *Lm = G + nn, *R1 = Lm + nn, *R2 = R1 + nn, *R3 = R2 + nn,
@@ -460,24 +405,22 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     };
     // every return below, the early ones of the status macros included, releases them
     ScopeExit guard([&] { cleanup(); });
-    const double one = 1.0, zero = 0.0;
     // Shifted CholeskyQR3 of Xa (rows x n, column-major, overwritten): the
     // orthonormal factor ends in Xb, R = R3 R2 R1 in Ra (upper, column-major);
     // Rb, Rc are scratch.
     auto scqr3 = [&](cudaStream_t s2, double *Xa, double *Xb, int rows, double *Ra, double *Rb, double *Rc) -> int {
-        int r = chol_qr_pass(hb, s2, Xa, Xb, rows, n, G, Lm, Linv, Ra, true, d_status);
-        if (r == JSVD_OK) r = chol_qr_pass(hb, s2, Xb, Xa, rows, n, G, Lm, Linv, Rb, false, d_status);
-        if (r == JSVD_OK) r = chol_qr_pass(hb, s2, Xa, Xb, rows, n, G, Lm, Linv, Rc, false, d_status);
+        int r = chol_qr_pass(s2, Xa, Xb, rows, n, G, Lm, Linv, Ra, true, d_status);
+        if (r == JSVD_OK) r = chol_qr_pass(s2, Xb, Xa, rows, n, G, Lm, Linv, Rb, false, d_status);
+        if (r == JSVD_OK) r = chol_qr_pass(s2, Xa, Xb, rows, n, G, Lm, Linv, Rc, false, d_status);
         if (r != JSVD_OK) return r;
-        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Rb, n, Ra, n, &zero, Tm, n));
-        JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, Rc, n, Tm, n, &zero, Ra, n));
+        JSVD_GEMM_TRY(dgemm(s2, 'N', 'N', n, n, n, 1.0, Rb, n, Ra, n, 0.0, Tm, n));
+        JSVD_GEMM_TRY(dgemm(s2, 'N', 'N', n, n, n, 1.0, Rc, n, Tm, n, 0.0, Ra, n));
         return JSVD_OK;
     };
     // Runs a QR stage: directly, or (a plan on its second use onwards) as a
     // graph captured once on the plan's own stream and replayed on st.
     auto run_stage = [&](cudaGraphExec_t *exec, auto &&enqueue) -> int {
         if (plan && !plan->no_graph && *exec == nullptr && plan->uses >= 1) {
-            JSVD_CUBLAS_TRY(cublasSetStream(hb, plan->own));
             cudaGraph_t graph = nullptr;
             int r = JSVD_OK;
             cudaError_t ce = cudaStreamBeginCapture(plan->own, cudaStreamCaptureModeThreadLocal);
@@ -494,7 +437,6 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
                 cudaGetLastError();
                 set_last_error(JSVD_OK, "");
             }
-            JSVD_CUBLAS_TRY(cublasSetStream(hb, st));
         }
         if (plan && *exec != nullptr) {
             JSVD_CUDA_TRY(cudaGraphLaunch(*exec, st));
@@ -525,6 +467,7 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
         cudaEventRecord(e1, st);
         cleanup();
         ps.fallbacks += 1;
+        if (engine == kEngineMixed) mixed_note_solve(0.0, true);
         return jsvd_plain_svd_device(d_a, rows, cols, &c, d_u, d_sigma, d_v, sweeps, st);
     }
     // R^T = Q1 P (P upper): R1's column-major buffer read as row-major is R^T.
@@ -545,7 +488,7 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     if (status2 == 0) {
         // A = Q R = Q P^T Q1^T.  Jacobi on X = P^T (P1's column-major buffer read
         // as row-major): X = Ux S Vx^T, so U_A = Q Ux and V_A = Q1 Vx.
-        rc = inner_jacobi(P1, cols, c, d_u ? Ux : nullptr, sout, d_v ? Vx : nullptr, sweeps, st);
+        rc = inner_jacobi(P1, cols, c, d_u ? Ux : nullptr, sout, d_v ? Vx : nullptr, sweeps, st, engine);
         if (rc != JSVD_OK) {
             cleanup();
             return rc;
@@ -554,22 +497,22 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
         // Row-major U_A (m x n) is column-major U_A^T = Ux^T Q^T; Ux's row-major
         // buffer is Ux^T column-major.  The same for V_A^T = Vx^T Q1^T.
         if (d_u)
-            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, n, m, n, &one, Ux, n, Q, m, &zero, d_u, n));
+            JSVD_GEMM_TRY(dgemm(st, 'N', 'T', n, m, n, 1.0, Ux, n, Q, m, 0.0, d_u, n));
         if (d_v)
-            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, n, n, n, &one, Vx, n, Q1, n, &zero, d_v, n));
+            JSVD_GEMM_TRY(dgemm(st, 'N', 'T', n, n, n, 1.0, Vx, n, Q1, n, 0.0, d_v, n));
     } else {
         // Second factorisation failed: Jacobi on X = R^T, A = Q X^T =
         // (Q Vx) S Ux^T, so U_A = Q Vx and V_A = Ux.
         ps.fallbacks += 1;
         double *vout = d_v ? d_v : Ux;
-        rc = inner_jacobi(R1, cols, c, vout, sout, Vx, sweeps, st);
+        rc = inner_jacobi(R1, cols, c, vout, sout, Vx, sweeps, st, engine);
         if (rc != JSVD_OK) {
             cleanup();
             return rc;
         }
         cudaEventRecord(e2, st);
         if (d_u)
-            JSVD_CUBLAS_TRY(cublasDgemm(hb, CUBLAS_OP_N, CUBLAS_OP_T, n, m, n, &one, Vx, n, Q, m, &zero, d_u, n));
+            JSVD_GEMM_TRY(dgemm(st, 'N', 'T', n, m, n, 1.0, Vx, n, Q, m, 0.0, d_u, n));
     }
     cudaEventRecord(e3, st);
     JSVD_CUDA_TRY(cudaStreamSynchronize(st));
@@ -582,6 +525,7 @@ int precond_impl(const double *d_a, size_t rows, size_t cols, const jsvd_config 
     ps.jacobi_ms += b;
     ps.u_ms += d;
     ps.last_sweeps = sweeps ? *sweeps : 0;
+    if (engine == kEngineMixed) mixed_note_solve(a, status2 != 0);
     if (plan) plan->uses += 1;
     cleanup();
     return JSVD_OK;
@@ -604,7 +548,7 @@ extern "C" int jsvd_precond_svd_device(const double *d_a, size_t rows, size_t co
         cudaStream_t st = nullptr;
         if (const int e = entry_stream(stream, &st); e != JSVD_OK) return e;
         if (columns == 1) return jsvd_plain_svd_device(d_a, rows, columns, &c, d_u, d_sigma, d_v, sweeps, st);
-        return precond_impl(d_a, rows, columns, c, d_u, d_sigma, d_v, sweeps, st);
+        return precond_impl(d_a, rows, columns, c, d_u, d_sigma, d_v, sweeps, st, g_inner.load());
     });
 }
 
@@ -619,6 +563,40 @@ extern "C" int jsvd_precond_svd(const double *a, size_t rows, size_t columns, co
 namespace jsvd {
 void pc_release_thread_plans() { pc_plans().clear(); }
 }  // namespace jsvd
+
+extern "C" int jsvd_mixed_svd_device(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg,
+                                     double *d_u, double *d_sigma, double *d_v, int *sweeps, void *stream)
+{
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        jsvd_config def;
+        const jsvd_config &c = config_or_default(cfg, def);
+        int rc = validate_plain_request(d_a, rows, columns, c);
+        if (rc != JSVD_OK) return rc;
+        cudaStream_t st = nullptr;
+        if (const int e = entry_stream(stream, &st); e != JSVD_OK) return e;
+        if (columns == 1) return jsvd_plain_svd_device(d_a, rows, columns, &c, d_u, d_sigma, d_v, sweeps, st);
+        const jsvd_mixed_options &o = mixed_options();
+        if (!o.precondition && columns >= (size_t)kMixedMinCols) {
+            // the blocked sweeps directly on A (row tiles of 32 along the
+            // transpose grid's y dimension bound the rows)
+            if (rows > (size_t)65535 * 32)
+                return invalid_argument("jsvd_mixed_svd: too many rows for the unpreconditioned blocked sweep.");
+            rc = mixed_solve(d_a, (int)rows, (int)columns, c, o, d_u, d_sigma, d_v, sweeps, st);
+            if (rc == JSVD_OK) mixed_note_solve(0.0, false);
+            return rc;
+        }
+        return precond_impl(d_a, rows, columns, c, d_u, d_sigma, d_v, sweeps, st, kEngineMixed);
+    });
+}
+
+extern "C" int jsvd_mixed_svd(const double *a, size_t rows, size_t columns, const jsvd_config *cfg, double *u,
+                              double *sigma, double *v, int *sweeps)
+{
+    return c_entry([&]() -> int {
+        return host_buffer_solve(jsvd_mixed_svd_device, a, rows, columns, cfg, u, sigma, v, sweeps);
+    });
+}
 
 extern "C" void jsvd_precond_set_inner(int engine) { g_inner.store(engine == 0 ? 0 : 1); }
 

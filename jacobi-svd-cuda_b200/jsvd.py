@@ -137,6 +137,24 @@ class BlockedStats(ctypes.Structure):
                 ("block_rounds", ctypes.c_ulonglong), ("sweep_ms", ctypes.c_double)]
 
 
+class MixedOptions(ctypes.Structure):
+    _fields_ = [("precondition", ctypes.c_int), ("tc_max_sweeps", ctypes.c_int), ("tc_tol", ctypes.c_double),
+                ("inner_sweeps", ctypes.c_int), ("refine", ctypes.c_int), ("f64_max_sweeps", ctypes.c_int),
+                ("gram_splits", ctypes.c_int)]
+
+
+class MixedStats(ctypes.Structure):
+    _fields_ = [("solves", ctypes.c_ulonglong), ("tc_sweeps", ctypes.c_ulonglong), ("f64_sweeps", ctypes.c_ulonglong),
+                ("block_rounds", ctypes.c_ulonglong), ("fallbacks", ctypes.c_ulonglong),
+                ("qr_ms", ctypes.c_double), ("tc_ms", ctypes.c_double), ("orth_ms", ctypes.c_double),
+                ("refine_ms", ctypes.c_double), ("out_ms", ctypes.c_double),
+                ("last_tc_offdiag", ctypes.c_double), ("last_f64_offdiag", ctypes.c_double),
+                ("last_tc_sweeps", ctypes.c_int), ("last_f64_sweeps", ctypes.c_int),
+                ("tc_gram_launches", ctypes.c_ulonglong), ("tc_rot_launches", ctypes.c_ulonglong),
+                ("f64_gram_launches", ctypes.c_ulonglong), ("f64_rot_launches", ctypes.c_ulonglong),
+                ("evd_launches", ctypes.c_ulonglong), ("tc_discarded", ctypes.c_ulonglong)]
+
+
 class JsvdError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[{code}] {message}")
@@ -173,6 +191,8 @@ def exported_symbols() -> list[str]:
         "jsvd_blockpair_stats_get", "jsvd_blockpair_stats_reset", "jsvd_precond_set_inner",
         "jsvd_precond_set_gram_stop", "jsvd_batch_builtin_tuning", "jsvd_batch_autotune", "jsvd_residuals",
         "jsvd_round_robin_schedule", "jsvd_plain_set_vpass_in_global", "jsvd_server_poll",
+        "jsvd_mixed_options_default", "jsvd_mixed_set_options", "jsvd_mixed_svd", "jsvd_mixed_svd_device",
+        "jsvd_mixed_stats_get", "jsvd_mixed_stats_reset", "jsvd_dgemm_device", "jsvd_mixed_test_round",
     ]
 
 
@@ -262,6 +282,22 @@ def lib() -> ctypes.CDLL:
         L.jsvd_precond_set_inner.restype = None
         L.jsvd_precond_set_gram_stop.argtypes = [I]
         L.jsvd_precond_set_gram_stop.restype = None
+        L.jsvd_mixed_options_default.argtypes = [ctypes.POINTER(MixedOptions)]
+        L.jsvd_mixed_options_default.restype = None
+        L.jsvd_mixed_set_options.argtypes = [ctypes.POINTER(MixedOptions)]
+        L.jsvd_mixed_set_options.restype = None
+        L.jsvd_mixed_svd.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P]
+        L.jsvd_mixed_svd.restype = I
+        L.jsvd_mixed_svd_device.argtypes = [P, S, S, ctypes.POINTER(Config), P, P, P, P, P]
+        L.jsvd_mixed_svd_device.restype = I
+        L.jsvd_mixed_stats_get.argtypes = [ctypes.POINTER(MixedStats)]
+        L.jsvd_mixed_stats_get.restype = None
+        L.jsvd_mixed_stats_reset.restype = None
+        D, LG = ctypes.c_double, ctypes.c_long
+        L.jsvd_dgemm_device.argtypes = [ctypes.c_char, ctypes.c_char, I, I, I, D, P, LG, P, LG, D, P, LG, I]
+        L.jsvd_dgemm_device.restype = I
+        L.jsvd_mixed_test_round.argtypes = [I, P, I, I, I, P]
+        L.jsvd_mixed_test_round.restype = I
         _LIB = L
     return _LIB
 
@@ -300,15 +336,15 @@ class SvdResult(NamedTuple):
 
 
 _HOST_ENTRIES = {"plain": "jsvd_plain_svd", "precond": "jsvd_precond_svd", "blockpair": "jsvd_blockpair_svd",
-                 "blocked": "jsvd_blocked_svd"}
+                 "blocked": "jsvd_blocked_svd", "mixed": "jsvd_mixed_svd"}
 
 
 def svd(a: np.ndarray, solver: str = "plain", cfg: Config | None = None, want_u: bool = True,
         want_v: bool = True) -> SvdResult:
     """One-sided Jacobi SVD of a row-major host matrix (rows >= columns)
     through the chosen solver's host-buffer entry point.  "plain" is the
-    reference's arithmetic bit for bit; "precond", "blockpair" and "blocked"
-    are accurate to working precision.  sigma is unsorted, as the reference
+    reference's arithmetic bit for bit; "precond", "blockpair", "blocked" and
+    "mixed" are accurate to working precision.  sigma is unsorted, as the reference
     returns it; U and V are row-major."""
     if solver not in _HOST_ENTRIES:
         raise ValueError(f"solver must be one of {sorted(_HOST_ENTRIES)}")
@@ -422,6 +458,61 @@ def precond_stats() -> PrecondStats:
 
 def precond_stats_reset() -> None:
     lib().jsvd_precond_stats_reset()
+
+
+def mixed_options(**overrides) -> MixedOptions:
+    """The library's default mixed-path options with `overrides` applied."""
+    o = MixedOptions()
+    lib().jsvd_mixed_options_default(ctypes.byref(o))
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+def mixed_set_options(opts: MixedOptions | None = None, **overrides) -> None:
+    """Sets the calling thread's mixed-path options (defaults when None)."""
+    if opts is None and not overrides:
+        lib().jsvd_mixed_set_options(None)
+        return
+    o = opts if opts is not None else mixed_options()
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    lib().jsvd_mixed_set_options(ctypes.byref(o))
+
+
+def mixed_svd(a: np.ndarray, cfg: Config | None = None, want_u: bool = True, want_v: bool = True) -> SvdResult:
+    """Host-buffer blocked mixed-precision solve (tcgen05 3xTF32 phase + FP64 refinement)."""
+    return svd(a, "mixed", cfg, want_u, want_v)
+
+
+def mixed_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:
+    cfg = cfg or default_config()
+    sw = ctypes.c_int(0)
+    check(lib().jsvd_mixed_svd_device(d_a, m, n, ctypes.byref(cfg), d_u, d_sigma, d_v, ctypes.byref(sw),
+                                      stream or None))
+    return sw.value
+
+
+def mixed_stats() -> MixedStats:
+    st = MixedStats()
+    lib().jsvd_mixed_stats_get(ctypes.byref(st))
+    return st
+
+
+def mixed_stats_reset() -> None:
+    lib().jsvd_mixed_stats_reset()
+
+
+def mixed_test_round(kind: int, d_x, rows: int, cols: int, rnd: int, d_gw) -> None:
+    """One block round of the mixed engine's kernels (0 TC Gram, 1 FP64 Gram, 2 TC rotation, 3 FP64 rotation)."""
+    check(lib().jsvd_mixed_test_round(kind, d_x, rows, cols, rnd, d_gw))
+
+
+def dgemm_device(op_a: str, op_b: str, m: int, n: int, k: int, alpha: float, d_a, lda: int, d_b, ldb: int,
+                 beta: float, d_c, ldc: int, lower: bool = False) -> None:
+    """C = alpha op(A) op(B) + beta C on column-major device buffers (the library's DMMA GEMM)."""
+    check(lib().jsvd_dgemm_device(op_a.encode(), op_b.encode(), m, n, k, alpha, d_a, lda, d_b, ldb, beta, d_c, ldc,
+                                  1 if lower else 0))
 
 
 def plain_svd_device(d_a, m: int, n: int, d_u, d_sigma, d_v, cfg: Config | None = None, stream: int = 0) -> int:
