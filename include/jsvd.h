@@ -102,10 +102,17 @@ int jsvd_plain_svd_device(const double *d_a, size_t rows, size_t columns, const 
  * legacy default stream), and the working copies live in one fixed 16 MiB
  * device array inside the library, so rows*columns + columns*columns +
  * columns + 1 must not exceed 2097152 and rows 2097120 (larger requests fail
- * with JSVD_ERR_INVALID_ARGUMENT).  That array is held by every GPU that loads the
- * library until exit and is shared by all calls: calls that overlap on the GPU
- * race and must be serialised by the caller.  The first call on a device looks
- * up the array's device address; make it before any stream capture begins.
+ * with JSVD_ERR_INVALID_ARGUMENT).  The array is committed on a device when
+ * the library's module is loaded there; CUDA loads modules lazily by default,
+ * so that happens on the first call on each device: a caller that reserves
+ * the rest of the device afterwards makes one warm-up call per device first
+ * (or sets CUDA_MODULE_LOADING=EAGER).  It then stays until the process
+ * exits.  The array is shared by all calls and keeps the last call's
+ * contents: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on a device, and again the first call after the
+ * device's context is replaced (cudaDeviceReset), looks up the array's device
+ * address.  Each sweep waits on the host for a device-to-host copy, so the
+ * entry cannot be used while its stream is being captured into a graph.
  * Results are bit-identical to jsvd_plain_svd_device.
  */
 int jsvd_plain_svd_noalloc(const double *d_a, size_t rows, size_t columns, const jsvd_config *cfg, double *d_u,

@@ -21,13 +21,27 @@
 // results: serialise them.
 //
 // Host code cannot use the array's name as a device address (it names a host
-// shadow).  The first call on each device looks the address up with
-// cudaGetSymbolAddress while that device is current and caches it; make that
-// first call before any stream capture begins on the device.
+// shadow).  The first call on each device (more precisely, in each CUDA
+// context: after cudaDeviceReset the device gets a new primary context and the
+// module, with the array, is loaded again, possibly at another address) looks
+// the address up with cudaGetSymbolAddress while that device is current and
+// caches it together with the context's process-unique ID; later calls in the
+// same context reuse it, a call in a new context looks it up again.
+//
+// Memory is committed when the module is loaded.  CUDA loads modules lazily by
+// default (CUDA_MODULE_LOADING=LAZY since 12.2), so on each device the array is
+// committed by the first call, not when the library is loaded: a caller that
+// reserves the rest of the device afterwards must make one warm-up call per
+// device first (or run with CUDA_MODULE_LOADING=EAGER).
+//
+// Each sweep reads its rotation count back with a device-to-host copy and
+// waits for it on the host, so the entry cannot be used while its stream is
+// being captured into a CUDA graph.
 //
 // The arithmetic is the plain path's: same reduction order, same rotation,
 // same cyclic round-robin order; V is rotated inside the round kernel (no
 // (c, s) table), so results are bit-identical to jsvd_plain_svd_device.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -44,21 +58,64 @@ constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 
-std::mutex g_noalloc_mutex;
-double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+struct ScratchAddress {
+    unsigned long long context_id = 0;  // 0: not looked up yet
+    double *ptr = nullptr;
+};
 
-// Device address of the scratch array on the current device (set-up on the
-// first call per device).
+std::mutex g_noalloc_mutex;
+ScratchAddress g_noalloc_addr[kNoAllocMaxDevices];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// Process-unique ID of the current CUDA context (driver entry points fetched
+// through the runtime, so the library needs no link against libcuda).
+int current_context_id(unsigned long long *id)
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q{};
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(p);
+    });
+    if (!get_current || !get_id) {
+        set_last_error(JSVD_ERR_CUDA, "cuCtxGetCurrent/cuCtxGetId are not available from the CUDA driver.");
+        return JSVD_ERR_CUDA;
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr || get_id(ctx, id) != CUDA_SUCCESS) {
+        set_last_error(JSVD_ERR_CUDA, "jsvd_plain_svd_noalloc: no current CUDA context on the device.");
+        return JSVD_ERR_CUDA;
+    }
+    return JSVD_OK;
+}
+
+// Device address of the scratch array on the current device: looked up once
+// per device and context (the caller has made `dev` current and initialised
+// its primary context).
 int noalloc_scratch(int dev, double **out)
 {
     if (dev < 0 || dev >= kNoAllocMaxDevices) return invalid_argument("Device ordinal out of range.");
+    unsigned long long ctx_id = 0;
+    if (int rc = current_context_id(&ctx_id); rc != JSVD_OK) return rc;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_ptr[dev] == nullptr) {
+    ScratchAddress &slot = g_noalloc_addr[dev];
+    if (slot.context_id != ctx_id || slot.ptr == nullptr) {
         double *ptr = nullptr;
         JSVD_CUDA_TRY(cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = ptr;
+        slot.ptr = ptr;
+        slot.context_id = ctx_id;
     }
-    *out = g_noalloc_ptr[dev];
+    *out = slot.ptr;
     return JSVD_OK;
 }
 
@@ -281,6 +338,9 @@ extern "C" int jsvd_plain_svd_noalloc(const double *d_a, size_t rows, size_t col
             return invalid_argument("jsvd_plain_svd_noalloc: at most 2097120 rows.");
         int dev = 0;
         JSVD_CUDA_TRY(cudaGetDevice(&dev));
+        // since CUDA 12 this also initialises the device's primary context, so
+        // the context ID below exists on the very first call
+        JSVD_CUDA_TRY(cudaSetDevice(dev));
         double *scratch = nullptr;
         rc = noalloc_scratch(dev, &scratch);
         if (rc != JSVD_OK) return rc;

@@ -4,8 +4,9 @@ that cannot take the device synchronisation of cudaMalloc/cudaFree, plugin hosts
 that forbid allocation).  It must give the same results as the allocating entry
 point jsvd_plain_svd_device - the tolerance of the plain-path tests is
 bit-for-bit equality - on two calls in a row (the second call reuses the shared
-scratch array that the first one left dirty), and it must refuse requests larger
-than its fixed scratch with a clear error.
+scratch array that the first one left dirty), it must leave the device's free
+memory unchanged once a warm-up call has loaded it, and it must refuse requests
+larger than its fixed scratch with a clear error.
 
 Kept in its own file, collected last, so a run that stops at the first failure
 has already run every other test.
@@ -63,6 +64,34 @@ def test_noalloc_matches_allocating_entry_on_two_calls(cuda_device):
         assert got[3] == exp[3]
         for x, y in zip(got[:3], exp[:3]):
             assert np.array_equal(x, y)
+
+
+def test_noalloc_allocates_nothing_after_warm_up(cuda_device):
+    """After one warm-up call (module loaded, scratch committed, kernels of
+    this reduction width loaded), a call of a new shape must leave the device's
+    free memory exactly as it was.  Every buffer the call touches is made
+    before the first reading of free memory."""
+    import torch
+
+    fn = _bind()
+    cfg = jsvd.default_config(epsilon=1e-12)
+    _solve(fn, W.gaussian_splitmix(96, 64, 5), cfg, cuda_device)  # warm-up
+    m, n = 300, 200
+    a = W.gaussian_splitmix(m, n, 6)
+    da = torch.from_numpy(a).to(cuda_device)
+    du = torch.empty((m, n), dtype=torch.float64, device=cuda_device)
+    ds = torch.empty((n,), dtype=torch.float64, device=cuda_device)
+    dv = torch.empty((n, n), dtype=torch.float64, device=cuda_device)
+    sw = ctypes.c_int(0)
+    torch.cuda.synchronize(cuda_device)
+    free_before, _ = torch.cuda.mem_get_info(cuda_device)
+    rc = fn(da.data_ptr(), m, n, ctypes.byref(cfg), du.data_ptr(), ds.data_ptr(), dv.data_ptr(), ctypes.byref(sw),
+            None)
+    torch.cuda.synchronize(cuda_device)
+    free_after, _ = torch.cuda.mem_get_info(cuda_device)
+    jsvd.check(rc)
+    assert sw.value >= 1
+    assert free_after == free_before
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch(cuda_device):
