@@ -461,20 +461,47 @@ __global__ void __launch_bounds__(kRot64Threads)
 constexpr int kEvdThreads = 256;
 constexpr int kEvdLD = kW + 1;
 constexpr int kTriBlocks = (kW / 2) * (kW / 2 + 1) / 2;  // 2x2 blocks (a <= b) of the 32 x 32 block grid
-constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD;
+constexpr int kEvdRounds = kW - 1;
+constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD + kEvdRounds * (kW / 2) * 2 + kTriBlocks * 2;
 
+// Round-robin pair tables of the block eigen-solve, in global memory so that
+// a CTA copies them into shared memory with coalesced loads.
 struct EvdTables {
-    unsigned char pairs[kW - 1][kW / 2][2];  // (p, q) of pair k in inner round r (circle over 64 indices)
-    unsigned char tri[kTriBlocks][2];        // (a, b), a <= b
+    unsigned char pairs[kEvdRounds][kW / 2][2];  // (p, q) of pair k in inner round r (circle over 64 indices)
+    unsigned char tri[kTriBlocks][2];            // (a, b), a <= b
 };
-__constant__ EvdTables c_evd;
+__device__ EvdTables g_evd_tables;
+
+// Rutishauser rotation of [pp pq; pq qq] with the threshold test of the
+// reference (|pq| > tau sqrt(pp qq), squared, and |pq| > 1e-300); c, s, t = s/c.
+__device__ __forceinline__ bool evd_rotation(double pp, double qq, double pq, double tau, double &c, double &s,
+                                             double &t)
+{
+    const double a = fmax(pp, 0.0) * fmax(qq, 0.0);
+    if (fabs(pq) > 1.0e-300 && pq * pq > (tau * tau) * a) {
+        const double zeta = (qq - pp) / (2.0 * pq);
+        const double h = sqrt(fma(zeta, zeta, 1.0));
+        t = (zeta >= 0.0) ? 1.0 / (zeta + h) : -1.0 / (-zeta + h);
+        c = 1.0 / sqrt(fma(t, t, 1.0));
+        s = t * c;
+        return true;
+    }
+    c = 1.0;
+    s = 0.0;
+    t = 0.0;
+    return false;
+}
 
 // Input Gram of block pair blockIdx.x from `splits` partials: kind 0 = the
 // tensor-core layout (128 x 64 FP32, rows r and r + 64 summed), kind 1 =
-// 64 x 64 FP64.  Writes W (64 x 64, column-major) and flags[pair] = 1 when
-// some pair rotated (else flags[pair] = 0 and W is left as it was).  stats[0]
-// (as double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over the input
-// Grams, stats[1] = number of block pairs that rotated.
+// 64 x 64 FP64.  Cyclic two-sided Jacobi, at most inner_sweeps sweeps of 63
+// rounds of 32 disjoint index pairs.  Every warp derives all 32 angles of a
+// round itself (lane k = pair k; identical inputs give identical results in
+// every warp) and takes (c, s) of the pairs it updates by shuffle; a round
+// without rotations costs one barrier, others two.  Writes W (64 x 64, column-major) and flags[pair] = 1
+// when some pair rotated (else flags[pair] = 0 and W is left as it was).
+// stats[0] (as double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over
+// the input Grams, stats[1] = number of block pairs that rotated.
 __global__ void __launch_bounds__(kEvdThreads)
     mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps,
            double *__restrict__ Wout, int *__restrict__ flags, unsigned long long *__restrict__ stats)
@@ -482,13 +509,16 @@ __global__ void __launch_bounds__(kEvdThreads)
     extern __shared__ double dsm[];
     double *G = dsm;                 // [64][65]
     double *Wm = dsm + kW * kEvdLD;  // [64][65], Wm[row][col]
-    __shared__ double cs_c[kW / 2], cs_s[kW / 2], cs_t[kW / 2];
-    __shared__ int rot_k[kW / 2];
-    __shared__ int any_round, any_sweep;
+    unsigned char *tp = reinterpret_cast<unsigned char *>(dsm + 2 * kW * kEvdLD);  // [63][32][2]
+    unsigned char *tt = tp + kEvdRounds * (kW / 2) * 2;                            // [528][2]
     __shared__ unsigned long long off_bits;
     const int pair = blockIdx.x;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     if (tid == 0) off_bits = 0ull;
+    {
+        const unsigned char *src = reinterpret_cast<const unsigned char *>(&g_evd_tables);
+        for (int e = tid; e < (int)sizeof(EvdTables); e += kEvdThreads) tp[e] = src[e];
+    }
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
         const int r = e & 63, c = e >> 6;  // consecutive threads, consecutive rows of a column
         double g = 0.0;
@@ -518,40 +548,41 @@ __global__ void __launch_bounds__(kEvdThreads)
         }
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
+    __syncthreads();
     bool rotated_any = false;
     for (int sw = 0; sw < inner_sweeps; ++sw) {
-        if (tid == 0) any_sweep = 0;
-        __syncthreads();
-        for (int r = 0; r < kW - 1; ++r) {
-            if (tid < kW / 2) {
-                const int p = c_evd.pairs[r][tid][0], q = c_evd.pairs[r][tid][1];
-                double c, s;
-                const bool rot = rotation_params(G[p * kEvdLD + p], G[q * kEvdLD + q], G[p * kEvdLD + q], tau, c, s);
-                cs_c[tid] = rot ? c : 1.0;
-                cs_s[tid] = rot ? s : 0.0;
-                cs_t[tid] = rot ? s / c : 0.0;
-                rot_k[tid] = rot ? 1 : 0;
-                const unsigned any = __ballot_sync(0xffffffffu, rot);
-                if (tid == 0) any_round = any != 0u;
+        bool sweep_any = false;
+        for (int r = 0; r < kEvdRounds; ++r) {
+            const unsigned char *rp = tp + r * kW;  // (p, q) of pair k at rp[2k], rp[2k+1]
+            double c, s, t;
+            {
+                const int p = rp[2 * lane], q = rp[2 * lane + 1];
+                evd_rotation(G[p * kEvdLD + p], G[q * kEvdLD + q], G[p * kEvdLD + q], tau, c, s, t);
             }
-            __syncthreads();
-            if (any_round) {
+            const unsigned rot = __ballot_sync(0xffffffffu, s != 0.0);
+            // every warp has read its angle inputs before any warp updates G
+            // (identical in every warp, so the branch is uniform)
+            if (rot) __syncthreads();
+            if (rot) {
+                sweep_any = true;
                 // G <- J^T G J by 2 x 2 blocks of index pairs (a, b), a <= b
-                for (int e = tid; e < kTriBlocks; e += kEvdThreads) {
-                    const int a = c_evd.tri[e][0], b = c_evd.tri[e][1];
-                    if (!rot_k[a] && !rot_k[b]) continue;
-                    const int pa = c_evd.pairs[r][a][0], qa = c_evd.pairs[r][a][1];
-                    const int pb = c_evd.pairs[r][b][0], qb = c_evd.pairs[r][b][1];
+                for (int e = tid; e < kTriBlocks + kEvdThreads - 1; e += kEvdThreads) {
+                    const bool live = e < kTriBlocks;
+                    const int a = live ? tt[2 * e] : 0, b = live ? tt[2 * e + 1] : 0;
+                    const double ca = __shfl_sync(0xffffffffu, c, a), sa = __shfl_sync(0xffffffffu, s, a);
+                    const double ta = __shfl_sync(0xffffffffu, t, a);
+                    const double cb = __shfl_sync(0xffffffffu, c, b), sb = __shfl_sync(0xffffffffu, s, b);
+                    if (!live || !(((rot >> a) | (rot >> b)) & 1u)) continue;
+                    const int pa = rp[2 * a], qa = rp[2 * a + 1], pb = rp[2 * b], qb = rp[2 * b + 1];
                     if (a == b) {
                         // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
-                        const double t = cs_t[a], o = G[pa * kEvdLD + qa];
-                        G[pa * kEvdLD + pa] = fma(-t, o, G[pa * kEvdLD + pa]);
-                        G[qa * kEvdLD + qa] = fma(t, o, G[qa * kEvdLD + qa]);
+                        const double o = G[pa * kEvdLD + qa];
+                        G[pa * kEvdLD + pa] = fma(-ta, o, G[pa * kEvdLD + pa]);
+                        G[qa * kEvdLD + qa] = fma(ta, o, G[qa * kEvdLD + qa]);
                         G[pa * kEvdLD + qa] = 0.0;
                         G[qa * kEvdLD + pa] = 0.0;
                         continue;
                     }
-                    const double ca = cs_c[a], sa = cs_s[a], cb = cs_c[b], sb = cs_s[b];
                     const double g11 = G[pa * kEvdLD + pb], g12 = G[pa * kEvdLD + qb];
                     const double g21 = G[qa * kEvdLD + pb], g22 = G[qa * kEvdLD + qb];
                     // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
@@ -569,24 +600,23 @@ __global__ void __launch_bounds__(kEvdThreads)
                     G[pb * kEvdLD + qa] = n21;
                     G[qb * kEvdLD + qa] = n22;
                 }
-                // W <- W J (row-local)
-                for (int e = tid; e < kW * (kW / 2); e += kEvdThreads) {
+                // W <- W J (row-local); a warp covers 32 rows of one pair k
+#pragma unroll
+                for (int j = 0; j < kW * (kW / 2) / kEvdThreads; ++j) {
+                    const int e = tid + j * kEvdThreads;
                     const int k = e >> 6, row = e & 63;
-                    if (!rot_k[k]) continue;
-                    const int p = c_evd.pairs[r][k][0], q = c_evd.pairs[r][k][1];
-                    const double c = cs_c[k], s = cs_s[k];
+                    const double ck = __shfl_sync(0xffffffffu, c, k), sk = __shfl_sync(0xffffffffu, s, k);
+                    if (!((rot >> k) & 1u)) continue;
+                    const int p = rp[2 * k], q = rp[2 * k + 1];
                     const double wp = Wm[row * kEvdLD + p], wq = Wm[row * kEvdLD + q];
-                    Wm[row * kEvdLD + p] = fma(c, wp, -(s * wq));
-                    Wm[row * kEvdLD + q] = fma(s, wp, c * wq);
+                    Wm[row * kEvdLD + p] = fma(ck, wp, -(sk * wq));
+                    Wm[row * kEvdLD + q] = fma(sk, wp, ck * wq);
                 }
-                if (tid == 0) any_sweep = 1;
             }
             __syncthreads();
         }
-        const bool had = any_sweep != 0;
-        __syncthreads();  // every thread has read any_sweep before thread 0 resets it
-        rotated_any = rotated_any || had;
-        if (!had) break;
+        rotated_any = rotated_any || sweep_any;
+        if (!sweep_any) break;  // identical in every warp: every thread leaves together
     }
     if (rotated_any) {
         double *wo = Wout + (size_t)pair * kW * kW;
@@ -595,7 +625,6 @@ __global__ void __launch_bounds__(kEvdThreads)
             wo[e] = Wm[r * kEvdLD + c];  // column-major W(r, c)
         }
     }
-    __syncthreads();  // off_bits complete
     if (tid == 0) {
         flags[pair] = rotated_any ? 1 : 0;
         if (rotated_any) atomicAdd(&stats[1], 1ull);
@@ -817,7 +846,7 @@ int init_tables_once()
     int dev = 0;
     JSVD_CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64 || !(done_mask & (1ull << dev))) {
-        JSVD_CUDA_TRY(cudaMemcpyToSymbol(c_evd, &t, sizeof(t)));
+        JSVD_CUDA_TRY(cudaMemcpyToSymbol(g_evd_tables, &t, sizeof(t)));
         JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGramTcSmem));
         JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_rot_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRotTcSmem));
         JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_rot_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRot64Smem));

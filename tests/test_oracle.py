@@ -245,3 +245,20 @@ def test_batch_workload_matches_its_description():
     for a in mats[:5]:
         s = np.linalg.svd(a.astype(np.float64), compute_uv=False)
         assert s[0] <= 1.0 + 1e-6 and s[-1] > 0.0
+
+
+def test_tall_oracle_fixture_matches_its_input():
+    """tests/golden/tall_4096x1024_oracle.npz (made by make_tall_sigma.py with
+    the oracle, 30 sweeps on the seeded 4096 x 1024 input) belongs to the input
+    that workloads.tall_case() generates here, and its sigma is the analytic one
+    to the reference arithmetic's accuracy (normwise 2e-13, per value 1e-11)."""
+    import hashlib
+
+    d = np.load(os.path.join(GOLDEN, "tall_4096x1024_oracle.npz"))
+    a, sig = W.tall_case()
+    assert hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest() == str(d["a_sha256"])
+    assert np.array_equal(d["sigma_analytic"], sig)
+    assert int(d["sweeps"]) == 30
+    s = np.sort(d["sigma"])[::-1]
+    assert np.max(np.abs(s - sig)) / sig[0] <= 2e-13
+    assert np.max(np.abs(s - sig) / sig) <= 1e-11
