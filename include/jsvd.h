@@ -445,7 +445,7 @@ typedef struct jsvd_server_options {
     int large_workers;          /* concurrent large solves, one stream each (0 = 4) */
     int max_batch;              /* requests per batched launch (0 = 4096)           */
     jsvd_config cfg;            /* epsilon, max_sweeps, threads_per_block           */
-    int large_path;             /* 0 = plain sweep, 1 = QR-preconditioned           */
+    int large_path;             /* 0 = plain sweep, 1 = QR-preconditioned, 2 = mixed  */
 } jsvd_server_options;
 
 typedef struct jsvd_server_stats {

@@ -17,7 +17,9 @@ namespace jacobi::svd
         precond,   ///< two CholeskyQR factorisations, then the sweep on the
                    ///< triangular factor (accurate to working precision)
         blockpair, ///< block-pair ordering of the FP64 sweep (working precision)
-        blocked    ///< Gram-blocked FP64 sweep (working precision)
+        blocked,   ///< Gram-blocked FP64 sweep (working precision)
+        mixed      ///< blocked sweeps with a tensor-core (3xTF32) phase and FP64
+                   ///< refinement after the QR stage (working precision)
     };
 
     /// one_sided_jacobi_svd through the chosen solver.  Same arguments,

@@ -11,8 +11,11 @@ namespace jacobi::svd::pipeline
     enum class LargeSolver
     {
         plain,   ///< the plain sweep: bit-identical to the reference (default)
-        precond  ///< shifted CholeskyQR3 + Jacobi on R^T: faster on tall and
+        precond, ///< shifted CholeskyQR3 + Jacobi on R^T: faster on tall and
                  ///< ill-conditioned inputs, accurate to working precision
+        mixed    ///< the QR stage + blocked sweeps, tensor-core (3xTF32) phase
+                 ///< and FP64 refinement (jsvd_mixed_svd): fastest on large
+                 ///< inputs, accurate to working precision
     };
 
     /// Selects the large-testcase solver for pipelines run afterwards in this

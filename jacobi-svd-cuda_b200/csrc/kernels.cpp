@@ -178,6 +178,9 @@ namespace jacobi::svd
         case SvdSolver::blocked:
             entry = jsvd_blocked_svd;
             break;
+        case SvdSolver::mixed:
+            entry = jsvd_mixed_svd;
+            break;
         default:
             throw std::invalid_argument("Unknown SvdSolver.");
         }

@@ -49,7 +49,7 @@ namespace
         std::size_t queue_capacity = 4;
         bool force = false, dry_run = false, print_config = false, json = false, quiet = false;
         bool help = false, version = false;
-        bool precond = false;
+        std::string solver = "plain";  // plain | precond | mixed
         std::filesystem::path residual_report;  // empty: off
         std::filesystem::path verify;           // empty: solve; else check this result file
     };
@@ -84,7 +84,7 @@ namespace
         {"print-config", '\0', false, "", "Print effective config before execution."},
         {"json-report", '\0', false, "", "Print execution report in JSON."},
         {"quiet", 'q', false, "", "Suppress text report."},
-        {"solver", '\0', true, "NAME", "Large-testcase solver: plain (bit-identical, default) | precond."},
+        {"solver", '\0', true, "NAME", "Large-testcase solver: plain (bit-identical, default) | precond | mixed."},
         {"residual-report", '\0', true, "PATH",
          "Write each testcase's rows, columns, epsilon, sweeps, rho_A, rho_U, rho_V as a JSON line."},
         {"verify", '\0', true, "PATH",
@@ -191,9 +191,9 @@ namespace
         else if (n == "solver")
         {
             const std::string l = lower(v);
-            if (l != "plain" && l != "precond")
-                throw ArgError("Invalid value for --solver: expected plain|precond.");
-            o.precond = l == "precond";
+            if (l != "plain" && l != "precond" && l != "mixed")
+                throw ArgError("Invalid value for --solver: expected plain|precond|mixed.");
+            o.solver = l;
         }
         else if (n == "residual-report") o.residual_report = std::string(v);
         else if (n == "verify") o.verify = std::string(v);
@@ -450,7 +450,7 @@ namespace
                   << "layout-bench-swp: " << o.layout_bench_sweeps << '\n'
                   << "queue-capacity  : " << o.queue_capacity << '\n'
                   << "force-overwrite : " << (o.force ? "true" : "false") << '\n'
-                  << "solver          : " << (o.precond ? "precond" : "plain") << '\n'
+                  << "solver          : " << o.solver << '\n'
                   << "residual-report : " << (o.residual_report.empty() ? "off" : o.residual_report.string())
                   << '\n';
     }
@@ -488,8 +488,10 @@ int main(int argc, char **argv)
             std::cout << '\n';
         }
         jacobi::svd::pipeline::set_residual_report(o.residual_report);
-        jacobi::svd::pipeline::set_large_solver(o.precond ? jacobi::svd::pipeline::LargeSolver::precond
-                                                          : jacobi::svd::pipeline::LargeSolver::plain);
+        using jacobi::svd::pipeline::LargeSolver;
+        jacobi::svd::pipeline::set_large_solver(o.solver == "precond" ? LargeSolver::precond
+                                                : o.solver == "mixed" ? LargeSolver::mixed
+                                                                      : LargeSolver::plain);
         jacobi::svd::pipeline::PipelineConfig cfg;
         cfg.input_path = o.input;
         cfg.output_path = o.output;

@@ -208,11 +208,15 @@ namespace jacobi::svd::pipeline
         return os.str();
     }
 
-    void set_large_solver(LargeSolver solver) noexcept { g_large_solver.store(solver == LargeSolver::precond ? 1 : 0); }
+    void set_large_solver(LargeSolver solver) noexcept
+    {
+        g_large_solver.store(solver == LargeSolver::precond ? 1 : solver == LargeSolver::mixed ? 2 : 0);
+    }
 
     LargeSolver large_solver() noexcept
     {
-        return g_large_solver.load() == 1 ? LargeSolver::precond : LargeSolver::plain;
+        const int s = g_large_solver.load();
+        return s == 1 ? LargeSolver::precond : s == 2 ? LargeSolver::mixed : LargeSolver::plain;
     }
 
     JacobiSvdPipeline::JacobiSvdPipeline(PipelineConfig config) : config_(std::move(config)) {}
@@ -246,7 +250,7 @@ namespace jacobi::svd::pipeline
         jsvd_server_options opt;
         jsvd_server_options_default(&opt);
         opt.cfg = to_c(kernel);
-        opt.large_path = large_solver() == LargeSolver::precond ? 1 : 0;
+        opt.large_path = static_cast<int>(g_large_solver.load());
         ServerHandle server;
         if (const int rc = jsvd_server_create(&opt, &server.s); rc != JSVD_OK)
             rethrow_status(rc);

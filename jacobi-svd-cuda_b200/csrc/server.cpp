@@ -49,12 +49,15 @@ size_t small_footprint(size_t m, size_t n, bool want_u)
     return sizeof(double) * (m * n + n + 2 * n * n + (want_u ? m * n : 0));
 }
 
-size_t large_footprint(size_t m, size_t n)
+size_t large_footprint(size_t m, size_t n, int path)
 {
     // I/O buffers (A, U, sigma, V) + plan (A_w, V_w, sigma, schedule and
-    // angles) + the preconditioned path's Q and seven n x n scratch matrices
+    // angles) + the preconditioned path's Q and seven n x n scratch matrices;
+    // the mixed path adds its working set on the padded n x n factor (five
+    // FP64 and four FP32 matrices)
+    const size_t np = (n + 127) / 128 * 128;
     return sizeof(double) * (2 * m * n + n + n * n) + sizeof(double) * (m * n + n * n + n) + 24 * n * n +
-           sizeof(double) * (m * n + 7 * n * n);
+           sizeof(double) * (m * n + 7 * n * n) + (path == 2 ? (5 * 8 + 4 * 4) * np * np : 0);
 }
 
 struct Request {
@@ -131,7 +134,7 @@ public:
         r->want_u = want_u != 0;
         // The batched solver reduces with T = 256; other widths take the plain path.
         r->small = is_small(m, n) && reduction_lanes(opt_.cfg.threads_per_block) == 256;
-        r->footprint = r->small ? small_footprint(m, n, r->want_u) : large_footprint(m, n);
+        r->footprint = r->small ? small_footprint(m, n, r->want_u) : large_footprint(m, n, opt_.large_path);
         if (r->footprint > opt_.device_budget_bytes) {
             set_last_error(JSVD_ERR_BUDGET, "Request needs " + std::to_string(r->footprint) +
                                                 " bytes of device memory, more than the serving budget of " +
@@ -397,8 +400,9 @@ private:
         ScopeExit free_d([&] { cudaFreeAsync(d, st); });  // stream-ordered, on every path
         JSVD_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double) * m * n, cudaMemcpyHostToDevice, st));
         double *ds = d + m * n, *dv = ds + n, *du = r->want_u ? dv + n * n : nullptr;
-        rc = opt_.large_path == 1 ? jsvd_precond_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st)
-                                  : jsvd_plain_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st);
+        rc = opt_.large_path == 1   ? jsvd_precond_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st)
+             : opt_.large_path == 2 ? jsvd_mixed_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st)
+                                    : jsvd_plain_svd_device(d, m, n, &opt_.cfg, du, ds, dv, &r->sweeps, st);
         if (rc != JSVD_OK) return rc;
         JSVD_CUDA_TRY(cudaMemcpyAsync(h + m * n, ds, sizeof(double) * (doubles - m * n), cudaMemcpyDeviceToHost, st));
         JSVD_CUDA_TRY(cudaStreamSynchronize(st));

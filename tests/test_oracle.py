@@ -83,7 +83,12 @@ def test_identity_converges_in_one_sweep():
 
 
 def _golden_cases():
-    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+    """The fixtures recorded from the reference's own runs (summary.json);
+    other .npz files in the folder (the oracle-made tall-case sigma) are not
+    reference outputs."""
+    summ = _summary() or {"cases": {}}
+    return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if os.path.basename(p)[:-4] in summ["cases"])
 
 
 def _summary():
