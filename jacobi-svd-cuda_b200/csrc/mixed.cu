@@ -536,21 +536,26 @@ __global__ void __launch_bounds__(kEvdThreads)
     __syncthreads();
     // symmetrise (the two triangles come from different accumulation orders)
     // and measure the input's largest scaled off-diagonal entry
+    // and whether any index pair passes the rotation test at all: if none
+    // does, no round can rotate (G never changes) and the solve is skipped
     double off = 0.0;
+    int need = 0;
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
         const int r = e >> 6, c = e & 63;
         if (r < c) {
             const double g = 0.5 * (G[r * kEvdLD + c] + G[c * kEvdLD + r]);
             G[r * kEvdLD + c] = g;
             G[c * kEvdLD + r] = g;
-            const double d = sqrt(fmax(G[r * kEvdLD + r], 0.0) * fmax(G[c * kEvdLD + c], 0.0));
+            const double a = fmax(G[r * kEvdLD + r], 0.0) * fmax(G[c * kEvdLD + c], 0.0);
+            const double d = sqrt(a);
             if (d > 0.0) off = fmax(off, fabs(g) / d);
+            if (fabs(g) > 1.0e-300 && g * g > (tau * tau) * a) need = 1;
         }
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
-    __syncthreads();
+    const bool work = __syncthreads_or(need) != 0;
     bool rotated_any = false;
-    for (int sw = 0; sw < inner_sweeps; ++sw) {
+    for (int sw = 0; sw < (work ? inner_sweeps : 0); ++sw) {
         bool sweep_any = false;
         for (int r = 0; r < kEvdRounds; ++r) {
             const unsigned char *rp = tp + r * kW;  // (p, q) of pair k at rp[2k], rp[2k+1]
@@ -625,6 +630,7 @@ __global__ void __launch_bounds__(kEvdThreads)
             wo[e] = Wm[r * kEvdLD + c];  // column-major W(r, c)
         }
     }
+    __syncthreads();  // off_bits complete (a skipped solve has no barrier after the atomics)
     if (tid == 0) {
         flags[pair] = rotated_any ? 1 : 0;
         if (rotated_any) atomicAdd(&stats[1], 1ull);
