@@ -571,7 +571,12 @@ __global__ void __launch_bounds__(kEvdThreads)
             if (rot) {
                 sweep_any = true;
                 // G <- J^T G J by 2 x 2 blocks of index pairs (a, b), a <= b
-                for (int e = tid; e < kTriBlocks + kEvdThreads - 1; e += kEvdThreads) {
+                // the same trip count in every thread: the shuffles below need
+                // all 32 lanes of each warp
+                constexpr int kTriIters = (kTriBlocks + kEvdThreads - 1) / kEvdThreads;
+#pragma unroll
+                for (int j = 0; j < kTriIters; ++j) {
+                    const int e = tid + j * kEvdThreads;
                     const bool live = e < kTriBlocks;
                     const int a = live ? tt[2 * e] : 0, b = live ? tt[2 * e + 1] : 0;
                     const double ca = __shfl_sync(0xffffffffu, c, a), sa = __shfl_sync(0xffffffffu, s, a);
