@@ -409,10 +409,22 @@ typedef struct jsvd_mixed_stats {
     int last_tc_sweeps, last_f64_sweeps;
     unsigned long long tc_gram_launches, tc_rot_launches, f64_gram_launches, f64_rot_launches, evd_launches;
     unsigned long long tc_discarded; /* solves whose phase-1 V did not orthogonalise (FP64 sweeps from X) */
+    /* device time of the Gram, eigen-solve and rotation kernels of sampled
+     * block rounds (rounds 0 and rounds/2 of every sweep; events around each
+     * launch), per phase, and the number of sampled rounds */
+    double tc_gram_ms, tc_evd_ms, tc_rot_ms, f64_gram_ms, f64_evd_ms, f64_rot_ms;
+    unsigned long long tc_sampled_rounds, f64_sampled_rounds;
 } jsvd_mixed_stats;
 
 void jsvd_mixed_stats_get(jsvd_mixed_stats *out);
 void jsvd_mixed_stats_reset(void);
+
+/* Sweeps of the calling thread's last mixed solve, in order: phase (1 tensor
+ * core, 3 FP64 refinement), the largest scaled off-diagonal Gram entry the
+ * sweep saw, and the block pairs it rotated.  Fills at most `capacity`
+ * entries (any pointer may be NULL) and returns the number of sweeps
+ * recorded (at most 64). */
+int jsvd_mixed_sweep_history(int *phase, double *offdiag, unsigned long long *rotated, int capacity);
 
 /* Kernel-level test hook of the mixed path: one block round (`round`) of its
  * kernels on X (rows x cols, column-major FP64, device, both multiples of

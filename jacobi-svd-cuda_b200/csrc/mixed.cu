@@ -458,11 +458,12 @@ __global__ void __launch_bounds__(kRot64Threads)
 // Block eigen-solve (FP64, both phases)
 // ============================================================================
 
-constexpr int kEvdThreads = 256;
+constexpr int kEvdThreads = 256;  // warps 0-3: W rows in registers; warps 4-7: G; warp 4 also the angles
 constexpr int kEvdLD = kW + 1;
 constexpr int kTriBlocks = (kW / 2) * (kW / 2 + 1) / 2;  // 2x2 blocks (a <= b) of the 32 x 32 block grid
 constexpr int kEvdRounds = kW - 1;
-constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD + kEvdRounds * (kW / 2) * 2 + kTriBlocks * 2;
+constexpr int kEvdMaxInner = 8;
+constexpr size_t kEvdSmem = sizeof(double) * kW * kEvdLD + kEvdRounds * (kW / 2) * 2 + kTriBlocks * 2;
 
 // Round-robin pair tables of the block eigen-solve, in global memory so that
 // a CTA copies them into shared memory with coalesced loads.
@@ -492,29 +493,82 @@ __device__ __forceinline__ bool evd_rotation(double pp, double qq, double pq, do
     return false;
 }
 
+// W in registers.  In inner round r, pair k rotates the columns at circle
+// positions k and 63 - k; slot 2k holds position k and slot 2k+1 position
+// 63 - k, so the pairs sit at fixed slots and the round-robin advance
+// (positions 1..62 move up by one, 63 wraps to 1, 0 stays) is a fixed
+// permutation of slots:
+//   first'[0] = first[0], first'[1] = second[0], first'[k] = first[k-1],
+//   second'[k] = second[k+1] (k < 31), second'[31] = first[31].
+// Row `row` of W is held by two threads: half h owns pairs 16h .. 16h+15
+// (slots 32h .. 32h+31, local index j <-> pair 16h + j), w[2j] = first,
+// w[2j+1] = second.  Across the halves one value moves per round:
+// first[15] -> first'[16] and second[16] -> second'[15] (one xor shuffle).
+// After 63 rounds every column is back at its starting slot: slot 2k holds
+// column k, slot 2k+1 column 63 - k.
+__device__ __forceinline__ int evd_slot_column(int slot) { return (slot & 1) ? 63 - (slot >> 1) : (slot >> 1); }
+
+__device__ __forceinline__ void evd_w_rotate(double (&w)[32], const double *cs_c, const double *cs_s, int half)
+{
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const double c = cs_c[16 * half + j], s = cs_s[16 * half + j];
+        const double x = w[2 * j], y = w[2 * j + 1];
+        w[2 * j] = fma(c, x, -(s * y));
+        w[2 * j + 1] = fma(s, x, c * y);
+    }
+}
+
+// Advance of the circle for one thread's half row (lane partner = lane ^ 1).
+__device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
+{
+    const double send = half ? w[1] : w[30];  // half 1: second[16]; half 0: first[15]
+    const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
+    double f[16], s[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        f[j] = w[2 * j];
+        s[j] = w[2 * j + 1];
+    }
+    // first'
+    w[0] = half ? recv : f[0];
+    w[2] = half ? f[0] : s[0];
+#pragma unroll
+    for (int j = 2; j < 16; ++j) w[2 * j] = f[j - 1];
+    // second'
+#pragma unroll
+    for (int j = 0; j < 15; ++j) w[2 * j + 1] = s[j + 1];
+    w[31] = half ? f[15] : recv;
+}
+
 // Input Gram of block pair blockIdx.x from `splits` partials: kind 0 = the
 // tensor-core layout (128 x 64 FP32, rows r and r + 64 summed), kind 1 =
 // 64 x 64 FP64.  Cyclic two-sided Jacobi, at most inner_sweeps sweeps of 63
-// rounds of 32 disjoint index pairs.  Every warp derives all 32 angles of a
-// round itself (lane k = pair k; identical inputs give identical results in
-// every warp) and takes (c, s) of the pairs it updates by shuffle; a round
-// without rotations costs one barrier, others two.  Writes W (64 x 64, column-major) and flags[pair] = 1
-// when some pair rotated (else flags[pair] = 0 and W is left as it was).
-// stats[0] (as double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over
-// the input Grams, stats[1] = number of block pairs that rotated.
+// rounds of 32 disjoint index pairs.  Per round: warp 4 derives the 32 angles
+// from G (shared memory) and publishes them; then warps 4-7 apply
+// G <- J^T G J by 2 x 2 blocks while warps 0-3 apply W <- W J to the rows they
+// hold in registers and advance the circle.  Writes W (64 x 64,
+// column-major) and flags[pair] = 1 when some pair rotated (else
+// flags[pair] = 0 and W is left as it was).  stats[0] (as double bits) =
+// running max of |g_pq| / sqrt(g_pp g_qq) over the input Grams, stats[1] =
+// number of block pairs that rotated.
 __global__ void __launch_bounds__(kEvdThreads)
     mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps,
            double *__restrict__ Wout, int *__restrict__ flags, unsigned long long *__restrict__ stats)
 {
     extern __shared__ double dsm[];
-    double *G = dsm;                 // [64][65]
-    double *Wm = dsm + kW * kEvdLD;  // [64][65], Wm[row][col]
-    unsigned char *tp = reinterpret_cast<unsigned char *>(dsm + 2 * kW * kEvdLD);  // [63][32][2]
-    unsigned char *tt = tp + kEvdRounds * (kW / 2) * 2;                            // [528][2]
+    double *G = dsm;  // [64][65]
+    unsigned char *tp = reinterpret_cast<unsigned char *>(dsm + kW * kEvdLD);  // [63][32][2]
+    unsigned char *tt = tp + kEvdRounds * (kW / 2) * 2;                       // [528][2]
+    __shared__ double cs_c[kW / 2], cs_s[kW / 2], cs_t[kW / 2];
+    __shared__ unsigned rot_mask;
+    __shared__ int sweep_any[kEvdMaxInner];
     __shared__ unsigned long long off_bits;
     const int pair = blockIdx.x;
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nsweeps = min(inner_sweeps, kEvdMaxInner);
     if (tid == 0) off_bits = 0ull;
+    if (tid < kEvdMaxInner) sweep_any[tid] = 0;
     {
         const unsigned char *src = reinterpret_cast<const unsigned char *>(&g_evd_tables);
         for (int e = tid; e < (int)sizeof(EvdTables); e += kEvdThreads) tp[e] = src[e];
@@ -531,13 +585,17 @@ __global__ void __launch_bounds__(kEvdThreads)
             for (int s = 0; s < splits; ++s) g += p[(size_t)s * 4096 + c * 64 + r];
         }
         G[r * kEvdLD + c] = g;
-        Wm[r * kEvdLD + c] = (r == c) ? 1.0 : 0.0;
     }
+    // W rows: thread tid < 128 holds row tid/2, half tid&1 (slot layout above)
+    const int wrow = (tid >> 1) & 63, half = tid & 1;
+    double w[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) w[j] = (evd_slot_column(32 * half + j) == wrow) ? 1.0 : 0.0;
     __syncthreads();
-    // symmetrise (the two triangles come from different accumulation orders)
-    // and measure the input's largest scaled off-diagonal entry
-    // and whether any index pair passes the rotation test at all: if none
-    // does, no round can rotate (G never changes) and the solve is skipped
+    // symmetrise (the two triangles come from different accumulation orders),
+    // measure the input's largest scaled off-diagonal entry, and find whether
+    // any index pair passes the rotation test at all: if none does, no round
+    // can rotate (G never changes) and the solve is skipped
     double off = 0.0;
     int need = 0;
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
@@ -555,44 +613,43 @@ __global__ void __launch_bounds__(kEvdThreads)
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
     const bool work = __syncthreads_or(need) != 0;
     bool rotated_any = false;
-    for (int sw = 0; sw < (work ? inner_sweeps : 0); ++sw) {
-        bool sweep_any = false;
+    for (int sw = 0; sw < (work ? nsweeps : 0); ++sw) {
         for (int r = 0; r < kEvdRounds; ++r) {
             const unsigned char *rp = tp + r * kW;  // (p, q) of pair k at rp[2k], rp[2k+1]
-            double c, s, t;
-            {
+            if (warp == 4) {
                 const int p = rp[2 * lane], q = rp[2 * lane + 1];
-                evd_rotation(G[p * kEvdLD + p], G[q * kEvdLD + q], G[p * kEvdLD + q], tau, c, s, t);
+                double c, s, t;
+                const bool rot = evd_rotation(G[p * kEvdLD + p], G[q * kEvdLD + q], G[p * kEvdLD + q], tau, c, s, t);
+                cs_c[lane] = c;
+                cs_s[lane] = s;
+                cs_t[lane] = t;
+                const unsigned m = __ballot_sync(0xffffffffu, rot);
+                if (lane == 0) {
+                    rot_mask = m;
+                    if (m) sweep_any[sw] = 1;
+                }
             }
-            const unsigned rot = __ballot_sync(0xffffffffu, s != 0.0);
-            // every warp has read its angle inputs before any warp updates G
-            // (identical in every warp, so the branch is uniform)
-            if (rot) __syncthreads();
-            if (rot) {
-                sweep_any = true;
+            __syncthreads();
+            const unsigned rot = rot_mask;
+            if (warp < 4) {
+                if (rot) evd_w_rotate(w, cs_c, cs_s, half);
+                evd_w_shift(w, half);
+            } else if (rot) {
                 // G <- J^T G J by 2 x 2 blocks of index pairs (a, b), a <= b
-                // the same trip count in every thread: the shuffles below need
-                // all 32 lanes of each warp
-                constexpr int kTriIters = (kTriBlocks + kEvdThreads - 1) / kEvdThreads;
-#pragma unroll
-                for (int j = 0; j < kTriIters; ++j) {
-                    const int e = tid + j * kEvdThreads;
-                    const bool live = e < kTriBlocks;
-                    const int a = live ? tt[2 * e] : 0, b = live ? tt[2 * e + 1] : 0;
-                    const double ca = __shfl_sync(0xffffffffu, c, a), sa = __shfl_sync(0xffffffffu, s, a);
-                    const double ta = __shfl_sync(0xffffffffu, t, a);
-                    const double cb = __shfl_sync(0xffffffffu, c, b), sb = __shfl_sync(0xffffffffu, s, b);
-                    if (!live || !(((rot >> a) | (rot >> b)) & 1u)) continue;
+                for (int e = tid - 128; e < kTriBlocks; e += 128) {
+                    const int a = tt[2 * e], b = tt[2 * e + 1];
+                    if (!(((rot >> a) | (rot >> b)) & 1u)) continue;
                     const int pa = rp[2 * a], qa = rp[2 * a + 1], pb = rp[2 * b], qb = rp[2 * b + 1];
                     if (a == b) {
                         // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
-                        const double o = G[pa * kEvdLD + qa];
+                        const double ta = cs_t[a], o = G[pa * kEvdLD + qa];
                         G[pa * kEvdLD + pa] = fma(-ta, o, G[pa * kEvdLD + pa]);
                         G[qa * kEvdLD + qa] = fma(ta, o, G[qa * kEvdLD + qa]);
                         G[pa * kEvdLD + qa] = 0.0;
                         G[qa * kEvdLD + pa] = 0.0;
                         continue;
                     }
+                    const double ca = cs_c[a], sa = cs_s[a], cb = cs_c[b], sb = cs_s[b];
                     const double g11 = G[pa * kEvdLD + pb], g12 = G[pa * kEvdLD + qb];
                     const double g21 = G[qa * kEvdLD + pb], g22 = G[qa * kEvdLD + qb];
                     // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
@@ -610,32 +667,21 @@ __global__ void __launch_bounds__(kEvdThreads)
                     G[pb * kEvdLD + qa] = n21;
                     G[qb * kEvdLD + qa] = n22;
                 }
-                // W <- W J (row-local); a warp covers 32 rows of one pair k
-#pragma unroll
-                for (int j = 0; j < kW * (kW / 2) / kEvdThreads; ++j) {
-                    const int e = tid + j * kEvdThreads;
-                    const int k = e >> 6, row = e & 63;
-                    const double ck = __shfl_sync(0xffffffffu, c, k), sk = __shfl_sync(0xffffffffu, s, k);
-                    if (!((rot >> k) & 1u)) continue;
-                    const int p = rp[2 * k], q = rp[2 * k + 1];
-                    const double wp = Wm[row * kEvdLD + p], wq = Wm[row * kEvdLD + q];
-                    Wm[row * kEvdLD + p] = fma(ck, wp, -(sk * wq));
-                    Wm[row * kEvdLD + q] = fma(sk, wp, ck * wq);
-                }
             }
             __syncthreads();
         }
-        rotated_any = rotated_any || sweep_any;
-        if (!sweep_any) break;  // identical in every warp: every thread leaves together
+        // sweep_any[sw] was last written before the round's first barrier
+        const bool had = sweep_any[sw] != 0;
+        rotated_any = rotated_any || had;
+        if (!had) break;  // the same value in every thread
     }
-    if (rotated_any) {
+    if (rotated_any && tid < 128) {
+        // every sweep ran all 63 rounds: slot s holds column evd_slot_column(s)
         double *wo = Wout + (size_t)pair * kW * kW;
-        for (int e = tid; e < kW * kW; e += kEvdThreads) {
-            const int r = e & 63, c = e >> 6;
-            wo[e] = Wm[r * kEvdLD + c];  // column-major W(r, c)
-        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) wo[(size_t)evd_slot_column(32 * half + j) * kW + wrow] = w[j];
     }
-    __syncthreads();  // off_bits complete (a skipped solve has no barrier after the atomics)
+    __syncthreads();  // off_bits complete
     if (tid == 0) {
         flags[pair] = rotated_any ? 1 : 0;
         if (rotated_any) atomicAdd(&stats[1], 1ull);
@@ -876,6 +922,17 @@ struct MixedStats {
     int last_tc_sweeps = 0, last_f64_sweeps = 0;
     unsigned long long tc_gram = 0, tc_rot = 0, f64_gram = 0, f64_rot = 0, evd = 0;
     unsigned long long tc_discarded = 0;
+    // device time of the three kernels of sampled block rounds (rounds 0 and
+    // rounds/2 of every sweep, events around each launch)
+    double tc_gram_ms = 0, tc_evd_ms = 0, tc_rot_ms = 0, f64_gram_ms = 0, f64_evd_ms = 0, f64_rot_ms = 0;
+    unsigned long long tc_sampled = 0, f64_sampled = 0;
+    // per sweep of the last solve: phase (1 tensor core, 3 FP64), largest
+    // scaled off-diagonal Gram entry seen, block pairs that rotated
+    static constexpr int kHist = 64;
+    int hist_len = 0;
+    int hist_phase[kHist] = {};
+    double hist_off[kHist] = {};
+    unsigned long long hist_rot[kHist] = {};
 };
 
 MixedStats &mixed_stats()
@@ -919,6 +976,7 @@ struct Work {
     CUtensorMap mxh{}, mxl{}, mvh{}, mvl{};  // 16-byte-chunk swizzle (Gram operands)
     CUtensorMap rxh{}, rxl{}, rvh{}, rvl{};  // 32-byte-chunk swizzle (rotation A operands)
     void *block = nullptr;
+    cudaEvent_t tev[2][4] = {};  // kernel timing of two sampled rounds per sweep
 };
 
 int split_count(int chunks, int npairs, int requested)
@@ -984,6 +1042,8 @@ int make_work(int rows, int cols, const jsvd_mixed_options &o, bool tc, cudaStre
     w.status = reinterpret_cast<int *>(b + o_status);
     w.stats = reinterpret_cast<unsigned long long *>(b + o_stats);
     JSVD_CUDA_TRY(cudaMallocHost((void **)&w.h_stats, 4 * sizeof(unsigned long long)));
+    for (auto &row : w.tev)
+        for (auto &e : row) JSVD_CUDA_TRY(cudaEventCreate(&e));
     if (tc) {
         if (int rc = make_map(&w.mxh, w.xh, w.rows_pad, w.cols_pad); rc != JSVD_OK) return rc;
         if (int rc = make_map(&w.mxl, w.xl, w.rows_pad, w.cols_pad); rc != JSVD_OK) return rc;
@@ -1001,6 +1061,9 @@ void free_work(Work &w, cudaStream_t st)
 {
     if (w.block) cudaFreeAsync(w.block, st);
     if (w.h_stats) cudaFreeHost(w.h_stats);
+    for (auto &row : w.tev)
+        for (auto &e : row)
+            if (e) cudaEventDestroy(e);
     w.block = nullptr;
     w.h_stats = nullptr;
 }
@@ -1013,12 +1076,20 @@ int run_sweep(Work &w, bool tc, double tau, int inner, cudaStream_t st, double *
 {
     MixedStats &ms = mixed_stats();
     JSVD_CUDA_TRY(cudaMemsetAsync(w.stats, 0, 2 * sizeof(unsigned long long), st));
+    const int sample_round[2] = {0, w.rounds / 2};
+    const int nsample = w.rounds > 2 ? 2 : 1;
     for (int r = 0; r < w.rounds; ++r) {
+        int si = -1;
+        for (int i = 0; i < nsample; ++i)
+            if (r == sample_round[i]) si = i;
+        if (si >= 0) cudaEventRecord(w.tev[si][0], st);
         if (tc) {
             mx_gram_tc<<<dim3(w.tc_splits, w.npairs), kGramTcThreads, kGramTcSmem, st>>>(
                 w.mxh, w.mxl, w.nb, r, w.tc_chunks, w.tc_chunks_per_split, static_cast<float *>(w.part), w.status);
+            if (si >= 0) cudaEventRecord(w.tev[si][1], st);
             mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.W, w.flags,
                                                             w.stats);
+            if (si >= 0) cudaEventRecord(w.tev[si][2], st);
             mx_rot_tc<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
                 w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, w.rows_pad, w.x_tiles, w.vh, w.vl, w.cols_pad, w.nb, r, w.W,
                 w.flags, w.status);
@@ -1027,13 +1098,16 @@ int run_sweep(Work &w, bool tc, double tau, int inner, cudaStream_t st, double *
         } else {
             mx_gram_f64<<<dim3(w.f64_splits, w.npairs), kGram64Threads, kGram64Smem, st>>>(
                 w.xr, w.rows_pad, w.nb, r, w.f64_rows_per_split, w.rows_pad, static_cast<double *>(w.part));
+            if (si >= 0) cudaEventRecord(w.tev[si][1], st);
             mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 1, w.f64_splits, tau, inner, w.W, w.flags,
                                                             w.stats);
+            if (si >= 0) cudaEventRecord(w.tev[si][2], st);
             mx_rot_f64<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRot64Threads, kRot64Smem, st>>>(
                 w.xr, w.rows_pad, w.x_tiles, w.v64, w.cols_pad, w.nb, r, w.W, w.flags);
             ms.f64_gram += 1;
             ms.f64_rot += 1;
         }
+        if (si >= 0) cudaEventRecord(w.tev[si][3], st);
         ms.evd += 1;
     }
     JSVD_CUDA_TRY(cudaGetLastError());
@@ -1053,6 +1127,22 @@ int run_sweep(Work &w, bool tc, double tau, int inner, cudaStream_t st, double *
     std::memcpy(&off, &bits, sizeof(off));
     *max_off = off;
     *rotated = w.h_stats[1];
+    for (int i = 0; i < nsample; ++i) {
+        float g = 0.f, e = 0.f, t = 0.f;
+        cudaEventElapsedTime(&g, w.tev[i][0], w.tev[i][1]);
+        cudaEventElapsedTime(&e, w.tev[i][1], w.tev[i][2]);
+        cudaEventElapsedTime(&t, w.tev[i][2], w.tev[i][3]);
+        (tc ? ms.tc_gram_ms : ms.f64_gram_ms) += g;
+        (tc ? ms.tc_evd_ms : ms.f64_evd_ms) += e;
+        (tc ? ms.tc_rot_ms : ms.f64_rot_ms) += t;
+        (tc ? ms.tc_sampled : ms.f64_sampled) += 1;
+    }
+    if (ms.hist_len < MixedStats::kHist) {
+        ms.hist_phase[ms.hist_len] = tc ? 1 : 3;
+        ms.hist_off[ms.hist_len] = off;
+        ms.hist_rot[ms.hist_len] = *rotated;
+        ++ms.hist_len;
+    }
     return JSVD_OK;
 }
 
@@ -1097,6 +1187,7 @@ int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const
     ScopeExit release([&] { free_work(w, st); });
     if (int rc = make_work(rows, cols, o, tc, st, w); rc != JSVD_OK) return rc;
     MixedStats &ms = mixed_stats();
+    ms.hist_len = 0;
     cudaEvent_t ev[5] = {};
     for (auto &e : ev) cudaEventCreate(&e);
     ScopeExit destroy([&] {
@@ -1294,6 +1385,26 @@ extern "C" void jsvd_mixed_stats_get(jsvd_mixed_stats *out)
     out->f64_rot_launches = s.f64_rot;
     out->evd_launches = s.evd;
     out->tc_discarded = s.tc_discarded;
+    out->tc_gram_ms = s.tc_gram_ms;
+    out->tc_evd_ms = s.tc_evd_ms;
+    out->tc_rot_ms = s.tc_rot_ms;
+    out->f64_gram_ms = s.f64_gram_ms;
+    out->f64_evd_ms = s.f64_evd_ms;
+    out->f64_rot_ms = s.f64_rot_ms;
+    out->tc_sampled_rounds = s.tc_sampled;
+    out->f64_sampled_rounds = s.f64_sampled;
+}
+
+extern "C" int jsvd_mixed_sweep_history(int *phase, double *offdiag, unsigned long long *rotated, int capacity)
+{
+    const MixedStats &s = mixed_stats();
+    const int n = std::min(s.hist_len, std::max(0, capacity));
+    for (int i = 0; i < n; ++i) {
+        if (phase) phase[i] = s.hist_phase[i];
+        if (offdiag) offdiag[i] = s.hist_off[i];
+        if (rotated) rotated[i] = s.hist_rot[i];
+    }
+    return s.hist_len;
 }
 
 extern "C" void jsvd_mixed_stats_reset(void) { mixed_stats() = MixedStats{}; }

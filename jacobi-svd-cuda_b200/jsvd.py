@@ -152,7 +152,10 @@ class MixedStats(ctypes.Structure):
                 ("last_tc_sweeps", ctypes.c_int), ("last_f64_sweeps", ctypes.c_int),
                 ("tc_gram_launches", ctypes.c_ulonglong), ("tc_rot_launches", ctypes.c_ulonglong),
                 ("f64_gram_launches", ctypes.c_ulonglong), ("f64_rot_launches", ctypes.c_ulonglong),
-                ("evd_launches", ctypes.c_ulonglong), ("tc_discarded", ctypes.c_ulonglong)]
+                ("evd_launches", ctypes.c_ulonglong), ("tc_discarded", ctypes.c_ulonglong),
+                ("tc_gram_ms", ctypes.c_double), ("tc_evd_ms", ctypes.c_double), ("tc_rot_ms", ctypes.c_double),
+                ("f64_gram_ms", ctypes.c_double), ("f64_evd_ms", ctypes.c_double), ("f64_rot_ms", ctypes.c_double),
+                ("tc_sampled_rounds", ctypes.c_ulonglong), ("f64_sampled_rounds", ctypes.c_ulonglong)]
 
 
 class JsvdError(RuntimeError):
@@ -193,6 +196,7 @@ def exported_symbols() -> list[str]:
         "jsvd_round_robin_schedule", "jsvd_plain_set_vpass_in_global", "jsvd_server_poll",
         "jsvd_mixed_options_default", "jsvd_mixed_set_options", "jsvd_mixed_svd", "jsvd_mixed_svd_device",
         "jsvd_mixed_stats_get", "jsvd_mixed_stats_reset", "jsvd_dgemm_device", "jsvd_mixed_test_round",
+        "jsvd_mixed_sweep_history",
     ]
 
 
@@ -298,6 +302,9 @@ def lib() -> ctypes.CDLL:
         L.jsvd_dgemm_device.restype = I
         L.jsvd_mixed_test_round.argtypes = [I, P, I, I, I, P]
         L.jsvd_mixed_test_round.restype = I
+        L.jsvd_mixed_sweep_history.argtypes = [ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_ulonglong), I]
+        L.jsvd_mixed_sweep_history.restype = I
         _LIB = L
     return _LIB
 
@@ -501,6 +508,16 @@ def mixed_stats() -> MixedStats:
 
 def mixed_stats_reset() -> None:
     lib().jsvd_mixed_stats_reset()
+
+
+def mixed_sweep_history() -> list[tuple[int, float, int]]:
+    """(phase, largest scaled off-diagonal, rotated block pairs) per sweep of the last mixed solve."""
+    cap = 64
+    ph = (ctypes.c_int * cap)()
+    off = (ctypes.c_double * cap)()
+    rot = (ctypes.c_ulonglong * cap)()
+    n = lib().jsvd_mixed_sweep_history(ph, off, rot, cap)
+    return [(int(ph[i]), float(off[i]), int(rot[i])) for i in range(min(n, cap))]
 
 
 def mixed_test_round(kind: int, d_x, rows: int, cols: int, rnd: int, d_gw) -> None:
