@@ -389,6 +389,8 @@ typedef struct jsvd_mixed_options {
     int refine;         /* refinement: 0 = blocked FP64 sweeps (default), 1 = plain scalar sweep */
     int f64_max_sweeps; /* cap on refinement sweeps; 0 = the config's max_sweeps                  */
     int gram_splits;    /* row splits of each block-pair Gram; 0 = automatic                      */
+    int sort;           /* 1 (default): each block eigen-solve gives the larger eigenvalues to the
+                           lower-numbered block (decreasing column norms, de Rijk's ordering)   */
 } jsvd_mixed_options;
 
 void jsvd_mixed_options_default(jsvd_mixed_options *o);

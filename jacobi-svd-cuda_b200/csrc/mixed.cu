@@ -321,8 +321,20 @@ constexpr int kGram64Stages = 3;
 constexpr size_t kGram64Smem = sizeof(double) * kGram64Stages * kW * kGram64LD;
 
 // Partial Gram of block pair blockIdx.y over rows [r0, r1) of split
-// blockIdx.x; output 64 x 64 FP64 column-major at part + (pair*splits+split)*4096.
-// Warp w computes rows 8w..8w+7 of G (eight 8 x 8 DMMA tiles).
+// blockIdx.x; output 64 x 64 FP64 column-major at part + (pair*splits+split)*4096,
+// upper triangle only (the 36 8 x 8 tiles (i, j), i <= j; the lower halves of
+// the diagonal tiles are written too and ignored).  Warp w computes tiles
+// w, w + 8, ... of the row-major list of upper tiles (4 or 5 DMMA tiles).
+__device__ __forceinline__ int2 upper_tile(int t)
+{
+    int i = 0;
+    while (t >= 8 - i) {
+        t -= 8 - i;
+        ++i;
+    }
+    return make_int2(i, i + t);
+}
+
 __global__ void __launch_bounds__(kGram64Threads)
     mx_gram_f64(const double *__restrict__ X, long ldx, int nb, int round, int rows_per_split, int rows,
                 double *__restrict__ part)
@@ -348,9 +360,19 @@ __global__ void __launch_bounds__(kGram64Threads)
                 *d = 0.0;
         }
     };
-    double acc[8][2];
+    constexpr int kTiles = 36, kPerWarp = 5;
+    int ti[kPerWarp], tj[kPerWarp];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+    for (int u = 0; u < kPerWarp; ++u) {
+        const int t = warp + 8 * u;
+        const int2 ij = upper_tile(t < kTiles ? t : 0);
+        ti[u] = ij.x;
+        tj[u] = ij.y;
+    }
+    const int ntiles = warp < kTiles - 32 ? kPerWarp : kPerWarp - 1;  // warps 0-3: 5 tiles, 4-7: 4
+    double acc[kPerWarp][2];
+#pragma unroll
+    for (int u = 0; u < kPerWarp; ++u) acc[u][0] = acc[u][1] = 0.0;
 #pragma unroll
     for (int s = 0; s < kGram64Stages - 1; ++s) {
         if (s < nst) issue(s);
@@ -365,22 +387,25 @@ __global__ void __launch_bounds__(kGram64Threads)
 #pragma unroll
         for (int kk = 0; kk < kGram64Rows; kk += 4) {
             // A = P^T (row i of A = column i of P), B = P
-            const double a = s[(warp * 8 + fr) * kGram64LD + kk + fk];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const double b = s[(j * 8 + fr) * kGram64LD + kk + fk];
-                dmma_m8n8k4(acc[j], a, b);
+            for (int u = 0; u < kPerWarp; ++u) {
+                if (u < ntiles) {
+                    const double a = s[(ti[u] * 8 + fr) * kGram64LD + kk + fk];
+                    const double b = s[(tj[u] * 8 + fr) * kGram64LD + kk + fk];
+                    dmma_m8n8k4(acc[u], a, b);
+                }
             }
         }
     }
     cp_async_wait<0>();
     double *out = part + ((size_t)pair * gridDim.x + split) * (kW * kW);
-    const int row = warp * 8 + fr;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int col = j * 8 + 2 * fk;
-        out[(size_t)col * kW + row] = acc[j][0];
-        out[(size_t)(col + 1) * kW + row] = acc[j][1];
+    for (int u = 0; u < kPerWarp; ++u) {
+        if (u < ntiles) {
+            const int row = ti[u] * 8 + fr, col = tj[u] * 8 + 2 * fk;
+            out[(size_t)col * kW + row] = acc[u][0];
+            out[(size_t)(col + 1) * kW + row] = acc[u][1];
+        }
     }
 }
 
@@ -553,8 +578,8 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
 // running max of |g_pq| / sqrt(g_pp g_qq) over the input Grams, stats[1] =
 // number of block pairs that rotated.
 __global__ void __launch_bounds__(kEvdThreads)
-    mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps,
-           double *__restrict__ Wout, int *__restrict__ flags, unsigned long long *__restrict__ stats)
+    mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps, int nb, int round,
+           int sort, double *__restrict__ Wout, int *__restrict__ flags, unsigned long long *__restrict__ stats)
 {
     extern __shared__ double dsm[];
     double *G = dsm;  // [64][65]
@@ -563,6 +588,7 @@ __global__ void __launch_bounds__(kEvdThreads)
     __shared__ double cs_c[kW / 2], cs_s[kW / 2], cs_t[kW / 2];
     __shared__ unsigned rot_mask;
     __shared__ int sweep_any[kEvdMaxInner];
+    __shared__ int out_col[kW];
     __shared__ unsigned long long off_bits;
     const int pair = blockIdx.x;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -580,11 +606,13 @@ __global__ void __launch_bounds__(kEvdThreads)
             const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
             for (int s = 0; s < splits; ++s)
                 g += (double)p[(size_t)s * 8192 + c * 128 + r] + (double)p[(size_t)s * 8192 + c * 128 + r + 64];
-        } else {
+            G[r * kEvdLD + c] = g;
+        } else if (r <= c) {  // the FP64 Gram kernel writes the upper triangle only: mirror it
             const double *p = static_cast<const double *>(part) + (size_t)pair * splits * 4096;
             for (int s = 0; s < splits; ++s) g += p[(size_t)s * 4096 + c * 64 + r];
+            G[r * kEvdLD + c] = g;
+            G[c * kEvdLD + r] = g;
         }
-        G[r * kEvdLD + c] = g;
     }
     // W rows: thread tid < 128 holds row tid/2, half tid&1 (slot layout above)
     const int wrow = (tid >> 1) & 63, half = tid & 1;
@@ -675,11 +703,31 @@ __global__ void __launch_bounds__(kEvdThreads)
         rotated_any = rotated_any || had;
         if (!had) break;  // the same value in every thread
     }
+    // Output order of W's columns.  With `sort`, the eigenvalues (G's
+    // diagonal) are ranked and the lower-numbered block of the pair receives
+    // the larger ones (decreasing norms across the blocks, de Rijk's
+    // ordering for one-sided Jacobi), which speeds convergence on graded
+    // spectra; it is a column permutation of W.
+    if (rotated_any && tid < kW) {
+        int pos = tid;
+        if (sort) {
+            const double lam = G[tid * kEvdLD + tid];
+            int rank = 0;
+            for (int c = 0; c < kW; ++c) {
+                const double l2 = G[c * kEvdLD + c];
+                rank += (l2 > lam || (l2 == lam && c < tid)) ? 1 : 0;
+            }
+            const int2 bp = round_robin_pair(nb, round, pair);
+            pos = bp.x < bp.y ? rank : kW - 1 - rank;
+        }
+        out_col[tid] = pos;
+    }
+    __syncthreads();
     if (rotated_any && tid < 128) {
         // every sweep ran all 63 rounds: slot s holds column evd_slot_column(s)
         double *wo = Wout + (size_t)pair * kW * kW;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) wo[(size_t)evd_slot_column(32 * half + j) * kW + wrow] = w[j];
+        for (int j = 0; j < 32; ++j) wo[(size_t)out_col[evd_slot_column(32 * half + j)] * kW + wrow] = w[j];
     }
     __syncthreads();  // off_bits complete
     if (tid == 0) {
@@ -799,7 +847,12 @@ __global__ void mx_sum_partials(const void *__restrict__ part, int kind, int spl
     const size_t total = (size_t)npairs * kW * kW;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
         const int pair = (int)(e / (kW * kW)), rc = (int)(e % (kW * kW));
-        const int r = rc & 63, c = rc >> 6;
+        int r = rc & 63, c = rc >> 6;
+        if (kind != 0 && r > c) {  // the FP64 Gram holds the upper triangle: read the mirror
+            const int t = r;
+            r = c;
+            c = t;
+        }
         double acc = 0.0;
         if (kind == 0) {
             const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
@@ -951,6 +1004,7 @@ jsvd_mixed_options default_options()
     o.refine = 0;
     o.f64_max_sweeps = 0;
     o.gram_splits = 0;
+    o.sort = 1;
     return o;
 }
 
@@ -1072,7 +1126,8 @@ unsigned grid_for(size_t count) { return (unsigned)std::min<size_t>(148 * 8, (co
 
 // One sweep (every block round) of phase 1 or phase 3; reads back the
 // sweep's statistics.
-int run_sweep(Work &w, bool tc, double tau, int inner, cudaStream_t st, double *max_off, unsigned long long *rotated)
+int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st, double *max_off,
+              unsigned long long *rotated)
 {
     MixedStats &ms = mixed_stats();
     JSVD_CUDA_TRY(cudaMemsetAsync(w.stats, 0, 2 * sizeof(unsigned long long), st));
@@ -1087,8 +1142,8 @@ int run_sweep(Work &w, bool tc, double tau, int inner, cudaStream_t st, double *
             mx_gram_tc<<<dim3(w.tc_splits, w.npairs), kGramTcThreads, kGramTcSmem, st>>>(
                 w.mxh, w.mxl, w.nb, r, w.tc_chunks, w.tc_chunks_per_split, static_cast<float *>(w.part), w.status);
             if (si >= 0) cudaEventRecord(w.tev[si][1], st);
-            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.W, w.flags,
-                                                            w.stats);
+            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.nb, r, sort, w.W,
+                                                            w.flags, w.stats);
             if (si >= 0) cudaEventRecord(w.tev[si][2], st);
             mx_rot_tc<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
                 w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, w.rows_pad, w.x_tiles, w.vh, w.vl, w.cols_pad, w.nb, r, w.W,
@@ -1099,8 +1154,8 @@ int run_sweep(Work &w, bool tc, double tau, int inner, cudaStream_t st, double *
             mx_gram_f64<<<dim3(w.f64_splits, w.npairs), kGram64Threads, kGram64Smem, st>>>(
                 w.xr, w.rows_pad, w.nb, r, w.f64_rows_per_split, w.rows_pad, static_cast<double *>(w.part));
             if (si >= 0) cudaEventRecord(w.tev[si][1], st);
-            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 1, w.f64_splits, tau, inner, w.W, w.flags,
-                                                            w.stats);
+            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 1, w.f64_splits, tau, inner, w.nb, r, sort,
+                                                            w.W, w.flags, w.stats);
             if (si >= 0) cudaEventRecord(w.tev[si][2], st);
             mx_rot_f64<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRot64Threads, kRot64Smem, st>>>(
                 w.xr, w.rows_pad, w.x_tiles, w.v64, w.cols_pad, w.nb, r, w.W, w.flags);
@@ -1212,7 +1267,8 @@ int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const
         const double tau = std::max(o.tc_tol * 0.25, 4.0 * std::sqrt((double)w.rows_pad) * 5.96e-8);
         for (int s = 0; s < o.tc_max_sweeps; ++s) {
             unsigned long long rotated = 0;
-            if (int rc = run_sweep(w, true, tau, o.inner_sweeps, st, &tc_off, &rotated); rc != JSVD_OK) return rc;
+            if (int rc = run_sweep(w, true, tau, o.inner_sweeps, o.sort, st, &tc_off, &rotated); rc != JSVD_OK)
+                return rc;
             ++tc_sweeps;
             if (rotated == 0 || tc_off <= o.tc_tol) break;
         }
@@ -1248,7 +1304,8 @@ int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const
     double f64_off = 0.0;
     for (int s = 0; s < cap; ++s) {
         unsigned long long rotated = 0;
-        if (int rc = run_sweep(w, false, tau64, o.inner_sweeps, st, &f64_off, &rotated); rc != JSVD_OK) return rc;
+        if (int rc = run_sweep(w, false, tau64, o.inner_sweeps, o.sort, st, &f64_off, &rotated); rc != JSVD_OK)
+            return rc;
         ++f64_sweeps;
         if (rotated == 0) break;
     }

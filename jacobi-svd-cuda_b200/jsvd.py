@@ -140,7 +140,7 @@ class BlockedStats(ctypes.Structure):
 class MixedOptions(ctypes.Structure):
     _fields_ = [("precondition", ctypes.c_int), ("tc_max_sweeps", ctypes.c_int), ("tc_tol", ctypes.c_double),
                 ("inner_sweeps", ctypes.c_int), ("refine", ctypes.c_int), ("f64_max_sweeps", ctypes.c_int),
-                ("gram_splits", ctypes.c_int)]
+                ("gram_splits", ctypes.c_int), ("sort", ctypes.c_int)]
 
 
 class MixedStats(ctypes.Structure):

@@ -124,8 +124,8 @@ def test_mixed_accuracy(cuda_device, name, make, kappa):
 
 
 @pytest.mark.parametrize("opts", [dict(tc_max_sweeps=0), dict(precondition=0), dict(inner_sweeps=1),
-                                  dict(gram_splits=1), dict(tc_max_sweeps=2)],
-                         ids=["fp64_only", "no_qr", "inner1", "splits1", "tc2"])
+                                  dict(gram_splits=1), dict(tc_max_sweeps=2), dict(sort=0)],
+                         ids=["fp64_only", "no_qr", "inner1", "splits1", "tc2", "unsorted"])
 def test_mixed_options(cuda_device, opts):
     a = W.spectrum_matrix(1024, 384, W.geometric_sigma(384, 1e-6), 51)
     jsvd.mixed_set_options(**opts)
