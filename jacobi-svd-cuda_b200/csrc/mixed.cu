@@ -579,7 +579,8 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
 // number of block pairs that rotated.
 __global__ void __launch_bounds__(kEvdThreads)
     mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps, int nb, int round,
-           int sort, double *__restrict__ Wout, int *__restrict__ flags, unsigned long long *__restrict__ stats)
+           int sort, int ncols, double *__restrict__ Wout, int *__restrict__ flags,
+           unsigned long long *__restrict__ stats)
 {
     extern __shared__ double dsm[];
     double *G = dsm;  // [64][65]
@@ -707,18 +708,32 @@ __global__ void __launch_bounds__(kEvdThreads)
     // diagonal) are ranked and the lower-numbered block of the pair receives
     // the larger ones (decreasing norms across the blocks, de Rijk's
     // ordering for one-sided Jacobi), which speeds convergence on graded
-    // spectra; it is a column permutation of W.
+    // spectra; it is a column permutation of W.  Only the pair's real columns
+    // (global index < ncols) are reordered, among their own positions: the
+    // zero padding columns never rotate and must stay at the end.
     if (rotated_any && tid < kW) {
         int pos = tid;
         if (sort) {
-            const double lam = G[tid * kEvdLD + tid];
-            int rank = 0;
-            for (int c = 0; c < kW; ++c) {
-                const double l2 = G[c * kEvdLD + c];
-                rank += (l2 > lam || (l2 == lam && c < tid)) ? 1 : 0;
-            }
             const int2 bp = round_robin_pair(nb, round, pair);
-            pos = bp.x < bp.y ? rank : kW - 1 - rank;
+            auto gcol = [&](int c) { return c < kB ? bp.x * kB + c : bp.y * kB + (c - kB); };
+            if (gcol(tid) < ncols) {
+                const bool desc = bp.x < bp.y;  // local order follows global order when bp.x < bp.y
+                const double lam = G[tid * kEvdLD + tid];
+                int rank = 0;
+                for (int c = 0; c < kW; ++c) {
+                    if (gcol(c) >= ncols) continue;
+                    const double l2 = G[c * kEvdLD + c];
+                    const bool before = desc ? (l2 > lam) : (l2 < lam);
+                    rank += (before || (l2 == lam && c < tid)) ? 1 : 0;
+                }
+                for (int c = 0, k = 0; c < kW; ++c) {
+                    if (gcol(c) >= ncols) continue;
+                    if (k++ == rank) {
+                        pos = c;
+                        break;
+                    }
+                }
+            }
         }
         out_col[tid] = pos;
     }
@@ -1142,8 +1157,8 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
             mx_gram_tc<<<dim3(w.tc_splits, w.npairs), kGramTcThreads, kGramTcSmem, st>>>(
                 w.mxh, w.mxl, w.nb, r, w.tc_chunks, w.tc_chunks_per_split, static_cast<float *>(w.part), w.status);
             if (si >= 0) cudaEventRecord(w.tev[si][1], st);
-            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.nb, r, sort, w.W,
-                                                            w.flags, w.stats);
+            mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.nb, r, sort, w.cols,
+                                                            w.W, w.flags, w.stats);
             if (si >= 0) cudaEventRecord(w.tev[si][2], st);
             mx_rot_tc<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
                 w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, w.rows_pad, w.x_tiles, w.vh, w.vl, w.cols_pad, w.nb, r, w.W,
@@ -1155,7 +1170,7 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
                 w.xr, w.rows_pad, w.nb, r, w.f64_rows_per_split, w.rows_pad, static_cast<double *>(w.part));
             if (si >= 0) cudaEventRecord(w.tev[si][1], st);
             mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 1, w.f64_splits, tau, inner, w.nb, r, sort,
-                                                            w.W, w.flags, w.stats);
+                                                            w.cols, w.W, w.flags, w.stats);
             if (si >= 0) cudaEventRecord(w.tev[si][2], st);
             mx_rot_f64<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRot64Threads, kRot64Smem, st>>>(
                 w.xr, w.rows_pad, w.x_tiles, w.v64, w.cols_pad, w.nb, r, w.W, w.flags);
