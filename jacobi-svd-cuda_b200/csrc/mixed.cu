@@ -498,17 +498,31 @@ struct EvdTables {
 };
 __device__ EvdTables g_evd_tables;
 
-// Rutishauser rotation of [pp pq; pq qq] with the threshold test of the
-// reference (|pq| > tau sqrt(pp qq), squared, and |pq| > 1e-300); c, s, t = s/c.
+// Rotation of [pp pq; pq qq] that annihilates pq, with the reference's
+// threshold test (|pq| > tau sqrt(pp qq), squared, and |pq| > 1e-300).
+// t = tan(theta) is the smaller root of t^2 + 2 zeta t - 1 = 0,
+// zeta = (qq - pp) / (2 pq), in the form
+//   t = sign * |e| / (|d| + sqrt(d^2 + e^2)),  d = qq - pp, e = 2 pq,
+// with sign = sign(e) for d >= 0 and -sign(e) otherwise (Rutishauser's t);
+// then c = 1 / sqrt(1 + t^2), s = t c.  One square root, one division and
+// one reciprocal square root on the serial chain.  d and e are scaled by a
+// power of two when their magnitude could over- or underflow d^2 + e^2.
 __device__ __forceinline__ bool evd_rotation(double pp, double qq, double pq, double tau, double &c, double &s,
                                              double &t)
 {
     const double a = fmax(pp, 0.0) * fmax(qq, 0.0);
     if (fabs(pq) > 1.0e-300 && pq * pq > (tau * tau) * a) {
-        const double zeta = (qq - pp) / (2.0 * pq);
-        const double h = sqrt(fma(zeta, zeta, 1.0));
-        t = (zeta >= 0.0) ? 1.0 / (zeta + h) : -1.0 / (-zeta + h);
-        c = 1.0 / sqrt(fma(t, t, 1.0));
+        double d = qq - pp, e = 2.0 * pq;
+        const double f = fmax(fabs(d), fabs(e));
+        if (f > 1.0e150 || f < 1.0e-150) {
+            const int k = ilogb(f);
+            d = scalbn(d, -k);
+            e = scalbn(e, -k);
+        }
+        const double h = sqrt(fma(d, d, e * e));
+        const double tt = fabs(e) / (fabs(d) + h);
+        t = ((d >= 0.0) == (e >= 0.0)) ? tt : -tt;
+        c = rsqrt(fma(t, t, 1.0));
         s = t * c;
         return true;
     }
@@ -570,14 +584,14 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
 // tensor-core layout (128 x 64 FP32, rows r and r + 64 summed), kind 1 =
 // 64 x 64 FP64.  Cyclic two-sided Jacobi, at most inner_sweeps sweeps of 63
 // rounds of 32 disjoint index pairs.  Per round: warp 4 derives the 32 angles
-// from G (shared memory) and publishes them; then warps 4-7 apply
-// G <- J^T G J by 2 x 2 blocks while warps 0-3 apply W <- W J to the rows they
-// hold in registers and advance the circle.  Writes W (64 x 64,
+// from G (shared memory) and publishes them; then warps 0-3 apply W <- W J
+// to the rows they hold in registers and advance the circle, and all eight
+// warps apply G <- J^T G J by 2 x 2 blocks.  Writes W (64 x 64,
 // column-major) and flags[pair] = 1 when some pair rotated (else
 // flags[pair] = 0 and W is left as it was).  stats[0] (as double bits) =
 // running max of |g_pq| / sqrt(g_pp g_qq) over the input Grams, stats[1] =
 // number of block pairs that rotated.
-__global__ void __launch_bounds__(kEvdThreads)
+__global__ void __launch_bounds__(kEvdThreads, 1)
     mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps, int nb, int round,
            int sort, int ncols, double *__restrict__ Wout, int *__restrict__ flags,
            unsigned long long *__restrict__ stats)
@@ -641,6 +655,15 @@ __global__ void __launch_bounds__(kEvdThreads)
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
     const bool work = __syncthreads_or(need) != 0;
+    // the 2 x 2 blocks of G this thread updates in every round
+    constexpr int kTriIters = (kTriBlocks + kEvdThreads - 1) / kEvdThreads;
+    int blk_a[kTriIters], blk_b[kTriIters];
+#pragma unroll
+    for (int j = 0; j < kTriIters; ++j) {
+        const int e = tid + j * kEvdThreads;
+        blk_a[j] = e < kTriBlocks ? tt[2 * e] : -1;
+        blk_b[j] = e < kTriBlocks ? tt[2 * e + 1] : -1;
+    }
     bool rotated_any = false;
     for (int sw = 0; sw < (work ? nsweeps : 0); ++sw) {
         for (int r = 0; r < kEvdRounds; ++r) {
@@ -663,11 +686,14 @@ __global__ void __launch_bounds__(kEvdThreads)
             if (warp < 4) {
                 if (rot) evd_w_rotate(w, cs_c, cs_s, half);
                 evd_w_shift(w, half);
-            } else if (rot) {
-                // G <- J^T G J by 2 x 2 blocks of index pairs (a, b), a <= b
-                for (int e = tid - 128; e < kTriBlocks; e += 128) {
-                    const int a = tt[2 * e], b = tt[2 * e + 1];
-                    if (!(((rot >> a) | (rot >> b)) & 1u)) continue;
+            }
+            if (rot) {
+                // G <- J^T G J by 2 x 2 blocks of index pairs (a, b), a <= b;
+                // thread tid owns blocks tid, tid + 256, tid + 512
+#pragma unroll
+                for (int j = 0; j < kTriIters; ++j) {
+                    const int a = blk_a[j], b = blk_b[j];
+                    if (a < 0 || !(((rot >> a) | (rot >> b)) & 1u)) continue;
                     const int pa = rp[2 * a], qa = rp[2 * a + 1], pb = rp[2 * b], qb = rp[2 * b + 1];
                     if (a == b) {
                         // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
