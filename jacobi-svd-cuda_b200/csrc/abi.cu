@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "blockpair.hpp"
 #include "internal.hpp"
+#include "mixed.hpp"
 #include "jsvd.h"
 #include "plain.hpp"
 
@@ -431,6 +432,7 @@ void jsvd_release_thread_cache(void)
     cache.plans.clear();
     bp_release_thread_plans();
     pc_release_thread_plans();
+    mixed_release_thread_cache();
 }
 
 }  // extern "C"

@@ -1270,18 +1270,88 @@ int orthogonalise(Work &w, cudaStream_t st, int steps, double *residual)
     return JSVD_OK;
 }
 
+// Per-thread cache of workspaces (at most two shapes, 16 GiB), so that
+// repeated solves of one shape allocate nothing and create no events.  A
+// workspace depends on the device, the shape, whether phase 1 runs and the
+// Gram row splits.
+struct CachedWork {
+    int device = -1, rows = 0, cols = 0, splits = 0;
+    bool tc = false;
+    Work w;
+    ~CachedWork()
+    {
+        if (w.block) cudaFree(w.block);
+        if (w.h_stats) cudaFreeHost(w.h_stats);
+        for (auto &row : w.tev)
+            for (auto &e : row)
+                if (e) cudaEventDestroy(e);
+    }
+};
+
+std::vector<std::unique_ptr<CachedWork>> &work_cache()
+{
+    thread_local std::vector<std::unique_ptr<CachedWork>> cache;
+    return cache;
+}
+
+constexpr size_t kMaxCachedWorkBytes = size_t(16) << 30;
+
+size_t work_bytes_estimate(int rows, int cols, bool tc)
+{
+    const size_t rp = (rows + kTileRows - 1) / kTileRows * kTileRows, cp = (cols + kColPad - 1) / kColPad * kColPad;
+    return 8 * (2 * rp * cp + 3 * cp * cp) + (tc ? 8 * (rp * cp + cp * cp) : 0);
+}
+
+// The calling thread's workspace for this request: cached (repeated
+// shapes) or made for this call only (*owned is then set and the caller
+// frees it).
+int acquire_work(int rows, int cols, const jsvd_mixed_options &o, bool tc, cudaStream_t st, Work **out, Work *owned)
+{
+    int dev = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    auto &cache = work_cache();
+    for (size_t i = 0; i < cache.size(); ++i) {
+        CachedWork &c = *cache[i];
+        if (c.device == dev && c.rows == rows && c.cols == cols && c.tc == tc && c.splits == o.gram_splits) {
+            std::rotate(cache.begin(), cache.begin() + i, cache.begin() + i + 1);
+            *out = &cache.front()->w;
+            return JSVD_OK;
+        }
+    }
+    if (work_bytes_estimate(rows, cols, tc) > kMaxCachedWorkBytes) {
+        if (int rc = make_work(rows, cols, o, tc, st, *owned); rc != JSVD_OK) return rc;
+        *out = owned;
+        return JSVD_OK;
+    }
+    auto c = std::make_unique<CachedWork>();
+    c->device = dev;
+    c->rows = rows;
+    c->cols = cols;
+    c->tc = tc;
+    c->splits = o.gram_splits;
+    if (int rc = make_work(rows, cols, o, tc, st, c->w); rc != JSVD_OK) return rc;
+    cache.insert(cache.begin(), std::move(c));
+    while (cache.size() > 2) cache.pop_back();
+    *out = &cache.front()->w;
+    return JSVD_OK;
+}
+
 }  // namespace
 
 const jsvd_mixed_options &mixed_options() { return thread_options(); }
+
+void mixed_release_thread_cache() { work_cache().clear(); }
 
 int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const jsvd_mixed_options &o, double *u,
                 double *sigma, double *v, int *sweeps, cudaStream_t st)
 {
     if (int rc = init_tables_once(); rc != JSVD_OK) return rc;
     const bool tc = o.tc_max_sweeps > 0;
-    Work w;
-    ScopeExit release([&] { free_work(w, st); });
-    if (int rc = make_work(rows, cols, o, tc, st, w); rc != JSVD_OK) return rc;
+    Work owned;
+    ScopeExit release([&] { free_work(owned, st); });
+    Work *wp = nullptr;
+    if (int rc = acquire_work(rows, cols, o, tc, st, &wp, &owned); rc != JSVD_OK) return rc;
+    Work &w = *wp;
     MixedStats &ms = mixed_stats();
     ms.hist_len = 0;
     cudaEvent_t ev[5] = {};

@@ -18,6 +18,9 @@ int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const
 // Counts one solve of the mixed path (and a fallback to the plain sweep).
 void mixed_note_solve(double qr_ms, bool fallback);
 
+// Drops the calling thread's cached mixed-path workspaces.
+void mixed_release_thread_cache();
+
 // The calling thread's options (jsvd_mixed_set_options).
 const jsvd_mixed_options &mixed_options();
 
