@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload tall|square512|batch|serve|large]
-                    [--path auto|plain|precond|blocked|blockpair]
+                    [--path auto|plain|precond|mixed|blocked|blockpair]
 
 One step = one pass of the hot path over one batch of synthetic input (for the
 single-matrix workloads: one full SVD).  `value` is whole-job SVDs/s with the
@@ -180,7 +180,7 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
     ds = torch.empty(n, dtype=torch.float64, device=device)
     dv = torch.empty((n, n), dtype=torch.float64, device=device)
     fn = {"precond": jsvd.precond_svd_device, "blocked": jsvd.blocked_svd_device,
-          "blockpair": jsvd.blockpair_svd_device}.get(path, jsvd.plain_svd_device)
+          "blockpair": jsvd.blockpair_svd_device, "mixed": jsvd.mixed_svd_device}.get(path, jsvd.plain_svd_device)
 
     def step():
         return fn(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg, stream.cuda_stream)
@@ -192,6 +192,7 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
     jsvd.precond_stats_reset()
     jsvd.blocked_stats_reset()
     jsvd.blockpair_stats_reset()
+    jsvd.mixed_stats_reset()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(device)
@@ -208,7 +209,7 @@ def time_single(args, wl, path, device, stream, steps, warmup, flush, world):
     torch.cuda.synchronize(device)
     total_ms = max_over_ranks(total_ms, world, device)
     return total_ms, sweeps, (jsvd.plain_stats(), jsvd.precond_stats(), jsvd.blocked_stats(),
-                              jsvd.blockpair_stats()), ds.cpu().numpy(), (du, dv)
+                              jsvd.blockpair_stats(), jsvd.mixed_stats()), ds.cpu().numpy(), (du, dv)
 
 
 def nominal_rate(m: int, n: int, plain_sweeps: int | None, svd_per_s: float | None) -> dict | None:
@@ -231,6 +232,75 @@ def blocked_sweep_flops(rows: int, n: int, b: int = 32) -> float:
     return nb * (nb - 1) / 2 * (2.0 * rows * w * w + 2.0 * (rows + n) * w * w)
 
 
+ORACLE_FIXTURES = {"tall": os.path.join(ROOT, "tests", "golden", "tall_4096x1024_oracle.npz")}
+
+
+def oracle_sigma_check(wl, sigma) -> dict | None:
+    """Error of `sigma` against the FP64 oracle's sigma on the same input (the
+    reference's arithmetic; tests/golden/tall_4096x1024_oracle.npz, made by
+    tests/golden/make_tall_sigma.py), when the fixture belongs to this input."""
+    import hashlib
+
+    p = ORACLE_FIXTURES.get(wl["name"])
+    if not p or not os.path.exists(p):
+        return None
+    d = np.load(p)
+    if hashlib.sha256(np.ascontiguousarray(wl["a"]).tobytes()).hexdigest() != str(d["a_sha256"]):
+        return {"oracle": "fixture does not match this input (not compared)"}
+    ref = np.sort(d["sigma"])[::-1]
+    got = np.sort(np.asarray(sigma))[::-1]
+    err = np.abs(got - ref)
+    return {"sigma_max_rel_vs_oracle": float(np.max(err / ref)),
+            "sigma_normwise_vs_oracle": float(err.max() / ref[0]),
+            "oracle_vs_analytic_max_rel": float(np.max(np.abs(ref - np.sort(d["sigma_analytic"])[::-1])
+                                                       / np.sort(d["sigma_analytic"])[::-1])),
+            "oracle_sweeps": int(d["sweeps"])}
+
+
+def mixed_roofline(mst, hbm_peak: float, peak_kind: str, step_ms: float) -> dict:
+    """Roofline of the mixed path's dominant kernel from the block rounds
+    sampled inside the timed solves (events around each launch; rounds 0 and
+    rounds/2 of every sweep).  Algorithmic bytes per launch: a Gram launch
+    reads the whole swept factor once (rows_pad x cols_pad elements, 8 bytes
+    each: FP64, or the TF32 head and tail); a rotation launch reads and
+    writes the 64 columns of X and of V of every block pair that rotated
+    ((rows_pad + cols_pad) x 64 x 16 bytes per pair).  The eigen-solve moves
+    no DRAM bytes of note (a 64 x 64 Gram per pair): it is latency-bound, and
+    its share of the sampled time is reported beside."""
+    k = {}
+    for ph, g, e, r, n, pairs in (("tc", mst.tc_gram_ms, mst.tc_evd_ms, mst.tc_rot_ms, mst.tc_sampled_rounds,
+                                   mst.tc_sampled_pairs),
+                                  ("f64", mst.f64_gram_ms, mst.f64_evd_ms, mst.f64_rot_ms, mst.f64_sampled_rounds,
+                                   mst.f64_sampled_pairs)):
+        if n:
+            k[ph] = {"gram_us": 1e3 * g / n, "evd_us": 1e3 * e / n, "rot_us": 1e3 * r / n,
+                     "rot_pairs_per_launch": pairs / n, "rounds": int(n)}
+    rp, cp = mst.rows_pad, mst.cols_pad
+    total = {name: sum(v[name + "_us"] * v["rounds"] for v in k.values()) for name in ("gram", "evd", "rot")}
+    cands = []
+    for ph, v in k.items():
+        gb = rp * cp * 8.0
+        cands.append((v["gram_us"] * v["rounds"], {"kernel": "mx_gram_tc" if ph == "tc" else "mx_gram_f64",
+                                                     "bytes": gb, "us": v["gram_us"]}))
+        rb = v["rot_pairs_per_launch"] * (rp + cp) * 64 * 16.0
+        cands.append((v["rot_us"] * v["rounds"], {"kernel": "mx_rot_tc" if ph == "tc" else "mx_rot_f64",
+                                                    "bytes": rb, "us": v["rot_us"]}))
+    if not cands:
+        return {"bound": "hbm", "kernel": None, "achieved": 0.0, "peak": hbm_peak, "unit": "GB/s", "frac": 0.0,
+                "traffic": None}
+    _, top = max(cands, key=lambda x: x[0])
+    achieved = top["bytes"] / (top["us"] * 1e-6) / 1e9
+    tsum = max(1e-9, sum(total.values()))
+    return {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "peak_kind": peak_kind, "frac": achieved / hbm_peak,
+            "traffic": PROFILED_TRAFFIC.get((top["kernel"], rp, cp)),
+            "avg_launch_us": top["us"], "algorithmic_bytes_per_launch": top["bytes"],
+            "sampled_kernel_share": {kk: vv / tsum for kk, vv in total.items()},
+            "per_phase": k, "note": "the eigen-solve (mx_evd) is latency-bound (64 x 64 FP64 Jacobi per block "
+                                    "pair, no DRAM traffic); its share of the sampled kernel time is under "
+                                    "sampled_kernel_share"}
+
+
 def run_ours(args, rank: int, world: int, device):
     import ctypes
 
@@ -249,8 +319,8 @@ def run_ours(args, rank: int, world: int, device):
 
     sampler = ClockSampler(device.index if device.index is not None else 0)
     sampler.start()
-    total_ms, sweeps, (pst, cst, bst, kst), sig, (du, dv) = time_single(args, wl, path, device, stream, args.steps,
-                                                                       args.warmup, flush, world)
+    total_ms, sweeps, (pst, cst, bst, kst, mst), sig, (du, dv) = time_single(args, wl, path, device, stream,
+                                                                            args.steps, args.warmup, flush, world)
     clocks = sampler.stop()
     ms_per_step = total_ms / args.steps
     value = replica_rate(args.steps, world, total_ms / 1e3)
@@ -258,10 +328,15 @@ def run_ours(args, rank: int, world: int, device):
     if kst.solves:
         # outer rounds + per solve: layout in, identity, sigma, U and V layout out
         launches += int(kst.round_launches) + 5 * int(kst.solves)
-    if path == "precond":
-        # per solve: layout kernel, 3 passes x (shift?, ceil(n/64) x (chol + trsm) + ceil(n/64) trsm + 1), status
+    if path in ("precond", "mixed"):
+        # per solve, the QR stage: 2 factorisations x 3 passes x (Gram, shift?, ceil(n/64) x (diagonal block,
+        # panel, trailing update) + ceil(n/64) x (solve, update) + R copy) + 2 R products, and the U, V products
         blocks = (n + 63) // 64
-        launches += args.steps * (1 + 3 * (3 * blocks + 1) + 1)
+        launches += args.steps * (2 * 3 * (2 + 5 * blocks + 1) + 4 + 4)
+    if path == "mixed":
+        # block rounds (Gram, eigen-solve, rotation) + layout, split, identity, polar steps, X V', sigma, U, V
+        launches += int(mst.tc_gram_launches + mst.tc_rot_launches + mst.f64_gram_launches + mst.f64_rot_launches
+                        + mst.evd_launches) + args.steps * 16
 
     # accuracy guard on the timed configuration (sigma vs the analytic spectrum,
     # and the reference's residual metrics on the returned factors)
@@ -274,6 +349,9 @@ def run_ours(args, rank: int, world: int, device):
                  "sigma_normwise_vs_analytic": float(np.max(np.abs(sig - t)) / t[0])}
     if m * n <= (1 << 22):  # the library's validation metrics (jsvd_residuals, host threads)
         guard = dict(guard or {}, **jsvd.residuals(a, du.cpu().numpy(), sig_cols, dv.cpu().numpy()))
+    oc = oracle_sigma_check(wl, sig_cols)
+    if oc:
+        guard = dict(guard or {}, **oc)
 
     # e2e through the host-buffer C-ABI call, pinned host memory
     ha = torch.from_numpy(a).pin_memory().numpy()
@@ -282,7 +360,7 @@ def run_ours(args, rank: int, world: int, device):
     hv = torch.empty((n, n), dtype=torch.float64).pin_memory().numpy()
     lib = jsvd.lib()
     entry = {"precond": lib.jsvd_precond_svd, "blocked": lib.jsvd_blocked_svd,
-             "blockpair": lib.jsvd_blockpair_svd}.get(path, lib.jsvd_plain_svd)
+             "blockpair": lib.jsvd_blockpair_svd, "mixed": lib.jsvd_mixed_svd}.get(path, lib.jsvd_plain_svd)
     sw = ctypes.c_int(0)
     e2e_steps = 0 if args.no_e2e else args.steps
     for _ in range(max(1, args.warmup) if e2e_steps else 0):
@@ -302,12 +380,17 @@ def run_ours(args, rank: int, world: int, device):
     # the plain drop-in on the same input, for the speed-up of the fast path
     plain = None
     if path != "plain" and not args.no_plain_compare:
-        p_ms, p_sw, _, _, _ = time_single(args, wl, "plain", device, stream, 2, 1, flush, world)
+        p_ms, p_sw, _, p_sig, _ = time_single(args, wl, "plain", device, stream, 2, 1, flush, world)
         plain = {"value": world * 2 / (p_ms / 1e3), "ms_per_step": p_ms / 2, "sweeps_per_svd": p_sw[0]}
+        oc = oracle_sigma_check(wl, p_sig)
+        if oc:
+            plain["check"] = oc
 
     hbm_peak, _, peak_kind = peaks()
-    mx = n if path == "precond" else m  # rows of the swept matrix
-    if kst.round_launches:
+    mx = n if path in ("precond", "mixed") else m  # rows of the swept matrix
+    if path == "mixed":
+        roof = mixed_roofline(mst, hbm_peak, peak_kind, total_ms / world)
+    elif kst.round_launches:
         # block-pair outer round: every column of X (mx rows) and of V (n rows)
         # is read and written once per launch
         avg_ms = kst.round_ms / kst.round_launches
@@ -346,6 +429,13 @@ def run_ours(args, rank: int, world: int, device):
         phases = {"qr_ms": cst.qr_ms / cst.solves, "jacobi_ms": cst.jacobi_ms / cst.solves,
                   "u_ms": cst.u_ms / cst.solves, "fallbacks": int(cst.fallbacks),
                   "gram_checks": pst.gram_checks / cst.solves}
+    if path == "mixed" and mst.solves:
+        phases = {"qr_ms": mst.qr_ms / mst.solves, "tensor_core_phase_ms": mst.tc_ms / mst.solves,
+                  "orthogonalise_ms": mst.orth_ms / mst.solves, "fp64_refine_ms": mst.refine_ms / mst.solves,
+                  "output_ms": mst.out_ms / mst.solves, "tc_sweeps": mst.tc_sweeps / mst.solves,
+                  "fp64_sweeps": mst.f64_sweeps / mst.solves, "fallbacks": int(mst.fallbacks),
+                  "tc_discarded": int(mst.tc_discarded),
+                  "sweep_history": [[p, o, r] for p, o, r in jsvd.mixed_sweep_history()]}
     if bst.solves:
         phases = dict(phases or {}, blocked_sweeps=bst.sweeps / bst.solves,
                       blocked_sweep_ms=bst.sweep_ms / max(1, bst.sweeps),
@@ -368,6 +458,10 @@ def run_ours(args, rank: int, world: int, device):
                                        "R^T = Q1 P) + FP64 Jacobi on P^T (" +
                                        ("block-pair" if kst.solves else "plain round-robin") + " sweep)",
                             "blocked": "blocked FP64 one-sided Jacobi on A (32-column blocks)",
+                            "mixed": "blocked mixed precision: the QR stage, then block-pair sweeps with tcgen05 "
+                                     "3xTF32 Gram and rotation GEMMs (TMA-fed, TMEM accumulators) and FP64 block "
+                                     "eigen-solves, FP64 re-orthogonalisation of V, FP64 blocked refinement "
+                                     "sweeps (DMMA)",
                             "blockpair": "block-pair FP64 one-sided Jacobi on A"}.get(
                        path, "plain FP64 drop-in (reference arithmetic, round-robin)"),
                    "epsilon": wl["eps"], "sweeps_per_svd": sweeps[0] if sweeps else None,
@@ -385,7 +479,110 @@ def run_ours(args, rank: int, world: int, device):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, PLAIN_SWEEPS.get(wl["name"], 12), budget_s=args.cpu_budget)
+    if wl["name"] == "tall" and world == 1 and not args.no_extras:
+        line["other_configs"] = run_extras(args, path, device, stream, flush)
     return line
+
+
+def run_extras(args, path: str, device, stream, flush) -> dict:
+    """Short measurements of the other configurations beside the headline
+    line (device-resident inputs, L2 flushed between steps, CUDA events):
+    the other fast path on the same 4096 x 1024 input, config 1 (512 x 512
+    N(0,1), plain drop-in, checked bit for bit against the reference's own
+    output), config 3 (the 20,000-matrix batch) and the 16384 x 8192 graded
+    and clustered matrix through the mixed path."""
+    import jsvd
+
+    out = {}
+    other = "precond" if path == "mixed" else "mixed"
+    wl = make_workload("tall")
+    o_ms, o_sw, _, o_sig, _ = time_single(args, wl, other, device, stream, 3, 1, flush, 1)
+    out[f"tall_{other}"] = {"value": 3 / (o_ms / 1e3), "unit": "SVD/s", "ms_per_step": o_ms / 3,
+                            "sweeps_per_svd": o_sw[0], "check": oracle_sigma_check(wl, o_sig)}
+    wl1 = make_workload("square512")
+    s_ms, s_sw, _, s_sig, _ = time_single(args, wl1, "plain", device, stream, 3, 1, flush, 1)
+    g = np.load(os.path.join(ROOT, "tests", "golden", "cfg1_512x512.npz"))
+    out["square512_plain"] = {"value": 3 / (s_ms / 1e3), "unit": "SVD/s", "ms_per_step": s_ms / 3,
+                              "sweeps_per_svd": s_sw[0], "epsilon": wl1["eps"],
+                              "sigma_bitwise_equal_to_reference": bool(np.array_equal(s_sig, g["sigma"])) if float(
+                                  g["eps"]) == wl1["eps"] else None}
+    bargs = argparse.Namespace(**vars(args))
+    bargs.steps, bargs.warmup, bargs.no_cpu_baseline = 2, 1, True
+    b = run_batch(bargs, 0, 1, device)
+    out["batch"] = {"value": b["value"], "unit": "SVD/s", "ms_per_step": b["ms_per_step"],
+                    "matrices": BATCH_COUNT if bargs.batch_count == BATCH_COUNT else bargs.batch_count,
+                    "class_ms_per_step": b["config"]["classes"]["ms_per_step"], "roofline": b["roofline"]}
+    out["large_mixed"] = run_large_device(args, device, "mixed")
+    return out
+
+
+def run_large_device(args, device, path: str, steps: int = 1, warmup: int = 1) -> dict:
+    """The 16384 x 8192 graded and clustered matrix (sigma_i = 10^(-10 i/n),
+    8 clusters of 16 with gaps 1e-10, Haar U and V, seed 5), generated on the
+    GPU and solved from device memory by one path (CUDA events)."""
+    import torch
+    import jsvd
+    import workloads as W
+
+    m, n = args.large_m, args.large_n
+    sig = np.ascontiguousarray(W.graded_clustered_sigma(n))
+    t0 = time.time()
+    da = large_matrix_device(m, n, sig, device)
+    gen_s = time.time() - t0
+    du = torch.empty((m, n), dtype=torch.float64, device=device)
+    ds = torch.empty(n, dtype=torch.float64, device=device)
+    dv = torch.empty((n, n), dtype=torch.float64, device=device)
+    cfg = jsvd.default_config(epsilon=1e-14)
+    fn = {"mixed": jsvd.mixed_svd_device, "precond": jsvd.precond_svd_device}[path]
+    st = torch.cuda.current_stream(device)
+    for _ in range(warmup):
+        fn(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg, st.cuda_stream)
+    jsvd.mixed_stats_reset()
+    torch.cuda.synchronize(device)
+    total, sw = 0.0, 0
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sw = fn(da.data_ptr(), m, n, du.data_ptr(), ds.data_ptr(), dv.data_ptr(), cfg, st.cuda_stream)
+        e1.record(st)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    ref = np.sort(sig)[::-1]
+    got = np.sort(ds.cpu().numpy())[::-1]
+    err = np.abs(got - ref)
+    mst = jsvd.mixed_stats()
+    res = {"value": steps / (total / 1e3), "unit": "SVD/s", "s_per_svd": total / 1e3 / steps, "sweeps_per_svd": sw,
+           "path": path, "generation_s": gen_s,
+           "check": {"sigma_normwise_vs_analytic": float(err.max() / ref[0]),
+                     "sigma_max_rel_top_half": float(np.max((err / ref)[: n // 2]))}}
+    if path == "mixed" and mst.solves:
+        res["phases_ms"] = {"qr": mst.qr_ms / mst.solves, "tensor_core_phase": mst.tc_ms / mst.solves,
+                            "orthogonalise": mst.orth_ms / mst.solves, "fp64_refine": mst.refine_ms / mst.solves,
+                            "tc_sweeps": mst.tc_sweeps / mst.solves, "fp64_sweeps": mst.f64_sweeps / mst.solves}
+        res["roofline"] = mixed_roofline(mst, peaks()[0], peaks()[2], total / steps)
+    del da, du, dv
+    torch.cuda.empty_cache()
+    return res
+
+
+def large_matrix_device(m: int, n: int, sig: np.ndarray, device):
+    """A = U diag(sig) V^T on the GPU, U (m x n) and V (n x n) Haar from QR of
+    seeded Gaussians (torch, FP64), row-major."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(5)
+    qu, ru = torch.linalg.qr(torch.randn((m, n), generator=g, dtype=torch.float64, device=device))
+    qu *= torch.sign(torch.diagonal(ru))[None, :]
+    del ru
+    qv, rv = torch.linalg.qr(torch.randn((n, n), generator=g, dtype=torch.float64, device=device))
+    qv *= torch.sign(torch.diagonal(rv))[None, :]
+    del rv
+    qu *= torch.from_numpy(sig).to(device)[None, :]
+    a = (qu @ qv.T).contiguous()
+    del qu, qv
+    torch.cuda.empty_cache()
+    return a
 
 
 def cpu_baseline(wl, sweeps: int, budget_s: float = 12.0, threads: int | None = None) -> dict:
@@ -650,26 +847,17 @@ def run_large(args, rank: int, world: int, device):
     """Large streamed case: an m x n FP64 matrix with sigma_i = 10^(-10 i / n)
     and 8 clusters of 16 values with relative gaps 1e-10, Haar U and V, written
     to disk in the *.mat format and solved by the CLI pipeline (mmap reader,
-    serving core, QR-preconditioned solver, mmap writer).  One step = one run
-    of the CLI on the file; timed on the host wall clock (file in, file out)."""
-    import torch
+    serving core, the chosen solver - mixed by default, or precond or plain -
+    mmap writer).  One step = one run of the CLI on the file; timed on the
+    host wall clock (file in, file out).  The line also carries the same
+    matrix solved from device memory (`device_resident`, CUDA events)."""
     import workloads as W
 
     m, n = args.large_m, args.large_n
+    solver = args.path if args.path in ("mixed", "precond", "plain") else "mixed"
     sig = np.ascontiguousarray(W.graded_clustered_sigma(n))
-    g = torch.Generator(device=device)
-    g.manual_seed(5)
     t0 = time.time()
-    qu, ru = torch.linalg.qr(torch.randn((m, n), generator=g, dtype=torch.float64, device=device))
-    qu *= torch.sign(torch.diagonal(ru))[None, :]
-    del ru
-    qv, rv = torch.linalg.qr(torch.randn((n, n), generator=g, dtype=torch.float64, device=device))
-    qv *= torch.sign(torch.diagonal(rv))[None, :]
-    del rv
-    qu *= torch.from_numpy(sig).to(device)[None, :]
-    a = (qu @ qv.T).cpu().numpy()
-    del qu, qv
-    torch.cuda.empty_cache()
+    a = large_matrix_device(m, n, sig, device).cpu().numpy()
     gen_s = time.time() - t0
     work = args.large_dir or "/tmp/jsvd_large"
     os.makedirs(work, exist_ok=True)
@@ -679,7 +867,7 @@ def run_large(args, rank: int, world: int, device):
         a.astype(">f8").tofile(f)
     del a
     cli = os.path.join(ROOT, "jacobi-svd-cuda_b200", "jacobi-svd-b200")
-    cmd = [cli, src, dst, "-e", "1e-14", "--solver", "precond", "--force", "-q", "--json-report"]
+    cmd = [cli, src, dst, "-e", "1e-14", "--solver", solver, "--force", "-q", "--json-report"]
     times = []
     for i in range(args.warmup + args.steps):
         t1 = time.perf_counter()
@@ -714,7 +902,7 @@ def run_large(args, rank: int, world: int, device):
         "data": "synthetic (seeded)",
         "config": {"workload": f"{m}x{n} FP64, sigma_i = 10^(-10 i/n) with 8 clusters of 16 (gaps 1e-10), Haar U,V "
                                f"(seed 5), streamed from a *.mat file through the CLI pipeline",
-                   "path": "CLI pipeline -> serving core -> QR-preconditioned solver", "epsilon": 1e-14,
+                   "path": f"CLI pipeline -> serving core -> {solver} solver", "epsilon": 1e-14,
                    "pipeline_report": report, "generation_s": gen_s, "sigma_header": hdr.tolist()},
         "e2e": {"value": 1.0 / elapsed, "unit": "SVD/s", "h2d_bytes_per_step": 8 * m * n,
                 "d2h_bytes_per_step": 8 * (m * n + n + n * n), "timer": "host wall clock around the CLI process"},
@@ -722,6 +910,7 @@ def run_large(args, rank: int, world: int, device):
                   "sigma_max_rel_vs_analytic": float(np.max(err / ref)),
                   "sigma_max_rel_top_half": float(np.max((err / ref)[: n // 2]))},
         "gpu_launches": None,
+        "device_resident": run_large_device(args, device, solver if solver != "plain" else "precond"),
     }
 
 
@@ -811,6 +1000,8 @@ def main():
                     help="threads_per_block (reduction width T) of the config; 0 = the reference default 256")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the host-buffer leg (profiling runs: only the warm-up and timed solves launch)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="tall workload: skip the other-configuration sub-objects (other_configs)")
     ap.add_argument("--precond-inner", type=int, default=1, choices=[0, 1],
                     help="Jacobi stage of the QR-preconditioned path: 0 block-pair where it applies, 1 plain")
     args = ap.parse_args()

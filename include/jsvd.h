@@ -416,6 +416,10 @@ typedef struct jsvd_mixed_stats {
      * launch), per phase, and the number of sampled rounds */
     double tc_gram_ms, tc_evd_ms, tc_rot_ms, f64_gram_ms, f64_evd_ms, f64_rot_ms;
     unsigned long long tc_sampled_rounds, f64_sampled_rounds;
+    /* block pairs rotated in the sampled rounds (each rotation kernel moves
+     * (rows_pad + cols_pad) x 64 elements of X and V per rotated pair) */
+    unsigned long long tc_sampled_pairs, f64_sampled_pairs;
+    int rows_pad, cols_pad, block_pairs; /* working shape of the last sweep */
 } jsvd_mixed_stats;
 
 void jsvd_mixed_stats_get(jsvd_mixed_stats *out);

@@ -1020,6 +1020,10 @@ struct MixedStats {
     // rounds/2 of every sweep, events around each launch)
     double tc_gram_ms = 0, tc_evd_ms = 0, tc_rot_ms = 0, f64_gram_ms = 0, f64_evd_ms = 0, f64_rot_ms = 0;
     unsigned long long tc_sampled = 0, f64_sampled = 0;
+    // block pairs that rotated in the sampled rounds (their rotation kernels
+    // moved (rows_pad + cols_pad) x 64 elements each)
+    unsigned long long tc_sampled_pairs = 0, f64_sampled_pairs = 0;
+    int rows_pad = 0, cols_pad = 0, npairs = 0;  // of the last sweep's workspace
     // per sweep of the last solve: phase (1 tensor core, 3 FP64), largest
     // scaled off-diagonal Gram entry seen, block pairs that rotated
     static constexpr int kHist = 64;
@@ -1066,7 +1070,9 @@ struct Work {
     void *part = nullptr;
     double *W = nullptr, *sg = nullptr;
     int *flags = nullptr, *status = nullptr;
-    unsigned long long *stats = nullptr;    // [0] max off (double bits) [1] rotated pairs [2] orth max
+    // [0] max off (double bits) [1] rotated pairs [2] orth max [4..7] rotated
+    // pairs before/after the eigen-solve of the two sampled rounds
+    unsigned long long *stats = nullptr;
     unsigned long long *h_stats = nullptr;  // pinned copy
     CUtensorMap mxh{}, mxl{}, mvh{}, mvl{};  // 16-byte-chunk swizzle (Gram operands)
     CUtensorMap rxh{}, rxl{}, rvh{}, rvl{};  // 32-byte-chunk swizzle (rotation A operands)
@@ -1116,7 +1122,7 @@ int make_work(int rows, int cols, const jsvd_mixed_options &o, bool tc, cudaStre
     const size_t o_xh = tc ? take(mn * 4) : 0, o_xl = tc ? take(mn * 4) : 0, o_vh = tc ? take(nn * 4) : 0,
                  o_vl = tc ? take(nn * 4) : 0;
     const size_t o_part = take(part_bytes), o_w = take((size_t)w.npairs * kW * kW * 8), o_sg = take(w.cols_pad * 8),
-                 o_flags = take(w.npairs * 4), o_status = take(4), o_stats = take(4 * 8);
+                 o_flags = take(w.npairs * 4), o_status = take(4), o_stats = take(8 * 8);
     JSVD_CUDA_TRY(cudaMallocAsync(&w.block, bytes, st));
     uint8_t *b = static_cast<uint8_t *>(w.block);
     w.x64 = reinterpret_cast<double *>(b + o_x64);
@@ -1136,7 +1142,7 @@ int make_work(int rows, int cols, const jsvd_mixed_options &o, bool tc, cudaStre
     w.flags = reinterpret_cast<int *>(b + o_flags);
     w.status = reinterpret_cast<int *>(b + o_status);
     w.stats = reinterpret_cast<unsigned long long *>(b + o_stats);
-    JSVD_CUDA_TRY(cudaMallocHost((void **)&w.h_stats, 4 * sizeof(unsigned long long)));
+    JSVD_CUDA_TRY(cudaMallocHost((void **)&w.h_stats, 8 * sizeof(unsigned long long)));
     for (auto &row : w.tev)
         for (auto &e : row) JSVD_CUDA_TRY(cudaEventCreate(&e));
     if (tc) {
@@ -1182,10 +1188,16 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
         if (tc) {
             mx_gram_tc<<<dim3(w.tc_splits, w.npairs), kGramTcThreads, kGramTcSmem, st>>>(
                 w.mxh, w.mxl, w.nb, r, w.tc_chunks, w.tc_chunks_per_split, static_cast<float *>(w.part), w.status);
-            if (si >= 0) cudaEventRecord(w.tev[si][1], st);
+            if (si >= 0) {
+                cudaEventRecord(w.tev[si][1], st);
+                cudaMemcpyAsync(w.stats + 4 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
+            }
             mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.nb, r, sort, w.cols,
                                                             w.W, w.flags, w.stats);
-            if (si >= 0) cudaEventRecord(w.tev[si][2], st);
+            if (si >= 0) {
+                cudaMemcpyAsync(w.stats + 5 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
+                cudaEventRecord(w.tev[si][2], st);
+            }
             mx_rot_tc<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
                 w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, w.rows_pad, w.x_tiles, w.vh, w.vl, w.cols_pad, w.nb, r, w.W,
                 w.flags, w.status);
@@ -1194,10 +1206,16 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
         } else {
             mx_gram_f64<<<dim3(w.f64_splits, w.npairs), kGram64Threads, kGram64Smem, st>>>(
                 w.xr, w.rows_pad, w.nb, r, w.f64_rows_per_split, w.rows_pad, static_cast<double *>(w.part));
-            if (si >= 0) cudaEventRecord(w.tev[si][1], st);
+            if (si >= 0) {
+                cudaEventRecord(w.tev[si][1], st);
+                cudaMemcpyAsync(w.stats + 4 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
+            }
             mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 1, w.f64_splits, tau, inner, w.nb, r, sort,
                                                             w.cols, w.W, w.flags, w.stats);
-            if (si >= 0) cudaEventRecord(w.tev[si][2], st);
+            if (si >= 0) {
+                cudaMemcpyAsync(w.stats + 5 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
+                cudaEventRecord(w.tev[si][2], st);
+            }
             mx_rot_f64<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRot64Threads, kRot64Smem, st>>>(
                 w.xr, w.rows_pad, w.x_tiles, w.v64, w.cols_pad, w.nb, r, w.W, w.flags);
             ms.f64_gram += 1;
@@ -1209,6 +1227,8 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
     JSVD_CUDA_TRY(cudaGetLastError());
     ms.block_rounds += (unsigned long long)w.rounds;
     JSVD_CUDA_TRY(cudaMemcpyAsync(w.h_stats, w.stats, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    JSVD_CUDA_TRY(
+        cudaMemcpyAsync(w.h_stats + 4, w.stats + 4, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     int dstatus = 0;
     JSVD_CUDA_TRY(cudaMemcpyAsync(&dstatus, w.status, sizeof(int), cudaMemcpyDeviceToHost, st));
     JSVD_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1232,7 +1252,11 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
         (tc ? ms.tc_evd_ms : ms.f64_evd_ms) += e;
         (tc ? ms.tc_rot_ms : ms.f64_rot_ms) += t;
         (tc ? ms.tc_sampled : ms.f64_sampled) += 1;
+        (tc ? ms.tc_sampled_pairs : ms.f64_sampled_pairs) += w.h_stats[5 + 2 * i] - w.h_stats[4 + 2 * i];
     }
+    ms.rows_pad = w.rows_pad;
+    ms.cols_pad = w.cols_pad;
+    ms.npairs = w.npairs;
     if (ms.hist_len < MixedStats::kHist) {
         ms.hist_phase[ms.hist_len] = tc ? 1 : 3;
         ms.hist_off[ms.hist_len] = off;
@@ -1561,6 +1585,11 @@ extern "C" void jsvd_mixed_stats_get(jsvd_mixed_stats *out)
     out->f64_rot_ms = s.f64_rot_ms;
     out->tc_sampled_rounds = s.tc_sampled;
     out->f64_sampled_rounds = s.f64_sampled;
+    out->tc_sampled_pairs = s.tc_sampled_pairs;
+    out->f64_sampled_pairs = s.f64_sampled_pairs;
+    out->rows_pad = s.rows_pad;
+    out->cols_pad = s.cols_pad;
+    out->block_pairs = s.npairs;
 }
 
 extern "C" int jsvd_mixed_sweep_history(int *phase, double *offdiag, unsigned long long *rotated, int capacity)

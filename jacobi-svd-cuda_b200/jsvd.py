@@ -155,7 +155,9 @@ class MixedStats(ctypes.Structure):
                 ("evd_launches", ctypes.c_ulonglong), ("tc_discarded", ctypes.c_ulonglong),
                 ("tc_gram_ms", ctypes.c_double), ("tc_evd_ms", ctypes.c_double), ("tc_rot_ms", ctypes.c_double),
                 ("f64_gram_ms", ctypes.c_double), ("f64_evd_ms", ctypes.c_double), ("f64_rot_ms", ctypes.c_double),
-                ("tc_sampled_rounds", ctypes.c_ulonglong), ("f64_sampled_rounds", ctypes.c_ulonglong)]
+                ("tc_sampled_rounds", ctypes.c_ulonglong), ("f64_sampled_rounds", ctypes.c_ulonglong),
+                ("tc_sampled_pairs", ctypes.c_ulonglong), ("f64_sampled_pairs", ctypes.c_ulonglong),
+                ("rows_pad", ctypes.c_int), ("cols_pad", ctypes.c_int), ("block_pairs", ctypes.c_int)]
 
 
 class JsvdError(RuntimeError):
