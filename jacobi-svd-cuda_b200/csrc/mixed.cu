@@ -483,12 +483,12 @@ __global__ void __launch_bounds__(kRot64Threads)
 // Block eigen-solve (FP64, both phases)
 // ============================================================================
 
-constexpr int kEvdThreads = 256;  // warps 0-3: W rows in registers; warps 4-7: G; warp 4 also the angles
+constexpr int kEvdThreads = 256;  // warps 0-3: W rows in registers; warps 0-6: G; warp 7: the angles
 constexpr int kEvdLD = kW + 1;
 constexpr int kTriBlocks = (kW / 2) * (kW / 2 + 1) / 2;  // 2x2 blocks (a <= b) of the 32 x 32 block grid
 constexpr int kEvdRounds = kW - 1;
 constexpr int kEvdMaxInner = 8;
-constexpr size_t kEvdSmem = sizeof(double) * kW * kEvdLD + kEvdRounds * (kW / 2) * 2 + kTriBlocks * 2;
+constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD + kEvdRounds * (kW / 2) * 2 + kTriBlocks * 2;
 
 // Round-robin pair tables of the block eigen-solve, in global memory so that
 // a CTA copies them into shared memory with coalesced loads.
@@ -582,38 +582,51 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
 
 // Input Gram of block pair blockIdx.x from `splits` partials: kind 0 = the
 // tensor-core layout (128 x 64 FP32, rows r and r + 64 summed), kind 1 =
-// 64 x 64 FP64.  Cyclic two-sided Jacobi, at most inner_sweeps sweeps of 63
-// rounds of 32 disjoint index pairs.  Per round: warp 4 derives the 32 angles
-// from G (shared memory) and publishes them; then warps 0-3 apply W <- W J
-// to the rows they hold in registers and advance the circle, and all eight
-// warps apply G <- J^T G J by 2 x 2 blocks.  Writes W (64 x 64,
-// column-major) and flags[pair] = 1 when some pair rotated (else
-// flags[pair] = 0 and W is left as it was).  stats[0] (as double bits) =
-// running max of |g_pq| / sqrt(g_pp g_qq) over the input Grams, stats[1] =
-// number of block pairs that rotated.
+// 64 x 64 FP64 upper triangle.  Cyclic two-sided Jacobi, at most
+// inner_sweeps sweeps of 63 rounds of 32 disjoint index pairs, software
+// pipelined so that a round costs one barrier and the angle chain runs beside
+// the update:
+//   * G is double-buffered: round r reads buffer r%2 and writes r+1%2;
+//   * warps 0-6 apply round r to G (2 x 2 blocks, every block written, the
+//     unrotated ones copied) and warps 0-3 apply it to W (registers);
+//   * warp 7 meanwhile derives the angles of round r+1 from buffer r%2 and
+//     round r's rotations: in the circle, pair k of round r+1 takes its first
+//     column from pair k-1 of round r (pair 0 for k <= 1) and its second from
+//     pair k+1 (pair 31 for k = 31), so its diagonal entries are round r's
+//     annihilated diagonals and its off-diagonal entry is one element of one
+//     2 x 2 block update, computed with the same operations as the update
+//     itself (bit-identical to what lands in the buffer).
+// Writes W (64 x 64, column-major) and flags[pair] = 1 when some pair
+// rotated (else flags[pair] = 0 and W is left as it was).  stats[0] (as
+// double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over the input
+// Grams, stats[1] = number of block pairs that rotated.
+constexpr int kEvdBulkThreads = 224;  // warps 0-6
+constexpr int kEvdBulkIters = (kTriBlocks + kEvdBulkThreads - 1) / kEvdBulkThreads;
+
 __global__ void __launch_bounds__(kEvdThreads, 1)
     mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps, int nb, int round,
            int sort, int ncols, double *__restrict__ Wout, int *__restrict__ flags,
            unsigned long long *__restrict__ stats)
 {
     extern __shared__ double dsm[];
-    double *G = dsm;  // [64][65]
-    unsigned char *tp = reinterpret_cast<unsigned char *>(dsm + kW * kEvdLD);  // [63][32][2]
-    unsigned char *tt = tp + kEvdRounds * (kW / 2) * 2;                       // [528][2]
-    __shared__ double cs_c[kW / 2], cs_s[kW / 2], cs_t[kW / 2];
-    __shared__ unsigned rot_mask;
-    __shared__ int sweep_any[kEvdMaxInner];
+    double *Gbuf[2] = {dsm, dsm + kW * kEvdLD};  // [64][65] each
+    unsigned char *tp = reinterpret_cast<unsigned char *>(dsm + 2 * kW * kEvdLD);  // [63][32][2]
+    unsigned char *tt = tp + kEvdRounds * (kW / 2) * 2;                           // [528][2]
+    __shared__ double cs_c[2][kW / 2], cs_s[2][kW / 2], cs_t[2][kW / 2];
+    __shared__ unsigned rot_mask[2];
+    __shared__ int sweep_any[kEvdMaxInner + 1];
     __shared__ int out_col[kW];
     __shared__ unsigned long long off_bits;
     const int pair = blockIdx.x;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nsweeps = min(inner_sweeps, kEvdMaxInner);
     if (tid == 0) off_bits = 0ull;
-    if (tid < kEvdMaxInner) sweep_any[tid] = 0;
+    if (tid <= kEvdMaxInner) sweep_any[tid] = 0;
     {
         const unsigned char *src = reinterpret_cast<const unsigned char *>(&g_evd_tables);
         for (int e = tid; e < (int)sizeof(EvdTables); e += kEvdThreads) tp[e] = src[e];
     }
+    double *G0 = Gbuf[0];
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
         const int r = e & 63, c = e >> 6;  // consecutive threads, consecutive rows of a column
         double g = 0.0;
@@ -621,12 +634,12 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
             for (int s = 0; s < splits; ++s)
                 g += (double)p[(size_t)s * 8192 + c * 128 + r] + (double)p[(size_t)s * 8192 + c * 128 + r + 64];
-            G[r * kEvdLD + c] = g;
+            G0[r * kEvdLD + c] = g;
         } else if (r <= c) {  // the FP64 Gram kernel writes the upper triangle only: mirror it
             const double *p = static_cast<const double *>(part) + (size_t)pair * splits * 4096;
             for (int s = 0; s < splits; ++s) g += p[(size_t)s * 4096 + c * 64 + r];
-            G[r * kEvdLD + c] = g;
-            G[c * kEvdLD + r] = g;
+            G0[r * kEvdLD + c] = g;
+            G0[c * kEvdLD + r] = g;
         }
     }
     // W rows: thread tid < 128 holds row tid/2, half tid&1 (slot layout above)
@@ -644,10 +657,10 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
         const int r = e >> 6, c = e & 63;
         if (r < c) {
-            const double g = 0.5 * (G[r * kEvdLD + c] + G[c * kEvdLD + r]);
-            G[r * kEvdLD + c] = g;
-            G[c * kEvdLD + r] = g;
-            const double a = fmax(G[r * kEvdLD + r], 0.0) * fmax(G[c * kEvdLD + c], 0.0);
+            const double g = 0.5 * (G0[r * kEvdLD + c] + G0[c * kEvdLD + r]);
+            G0[r * kEvdLD + c] = g;
+            G0[c * kEvdLD + r] = g;
+            const double a = fmax(G0[r * kEvdLD + r], 0.0) * fmax(G0[c * kEvdLD + c], 0.0);
             const double d = sqrt(a);
             if (d > 0.0) off = fmax(off, fabs(g) / d);
             if (fabs(g) > 1.0e-300 && g * g > (tau * tau) * a) need = 1;
@@ -655,81 +668,143 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
     const bool work = __syncthreads_or(need) != 0;
-    // the 2 x 2 blocks of G this thread updates in every round
-    constexpr int kTriIters = (kTriBlocks + kEvdThreads - 1) / kEvdThreads;
-    int blk_a[kTriIters], blk_b[kTriIters];
+    // the 2 x 2 blocks of G this thread updates in every round (warps 0-6)
+    int blk_a[kEvdBulkIters], blk_b[kEvdBulkIters];
 #pragma unroll
-    for (int j = 0; j < kTriIters; ++j) {
-        const int e = tid + j * kEvdThreads;
-        blk_a[j] = e < kTriBlocks ? tt[2 * e] : -1;
-        blk_b[j] = e < kTriBlocks ? tt[2 * e + 1] : -1;
+    for (int j = 0; j < kEvdBulkIters; ++j) {
+        const int e = tid + j * kEvdBulkThreads;
+        const bool live = tid < kEvdBulkThreads && e < kTriBlocks;
+        blk_a[j] = live ? tt[2 * e] : -1;
+        blk_b[j] = live ? tt[2 * e + 1] : -1;
+    }
+    // warp 7: round 0's angles from buffer 0; it keeps its pair's indices,
+    // input entries and rotation in registers from round to round
+    int my_p = 0, my_q = 0;
+    double a_pp = 0.0, a_qq = 0.0, a_pq = 0.0, a_c = 1.0, a_s = 0.0, a_t = 0.0;
+    if (warp == 7 && work) {
+        my_p = tp[2 * lane];
+        my_q = tp[2 * lane + 1];
+        a_pp = G0[my_p * kEvdLD + my_p];
+        a_qq = G0[my_q * kEvdLD + my_q];
+        a_pq = G0[my_p * kEvdLD + my_q];
+        const bool rot = evd_rotation(a_pp, a_qq, a_pq, tau, a_c, a_s, a_t);
+        cs_c[0][lane] = a_c;
+        cs_s[0][lane] = a_s;
+        cs_t[0][lane] = a_t;
+        const unsigned m = __ballot_sync(0xffffffffu, rot);
+        if (lane == 0) {
+            rot_mask[0] = m;
+            if (m) sweep_any[0] = 1;
+        }
     }
     bool rotated_any = false;
+    int gr = 0;  // rounds executed so far (buffer parity)
     for (int sw = 0; sw < (work ? nsweeps : 0); ++sw) {
-        for (int r = 0; r < kEvdRounds; ++r) {
+        for (int r = 0; r < kEvdRounds; ++r, ++gr) {
+            __syncthreads();  // round gr's angles published, its input buffer complete
+            const int cur = gr & 1;
+            const double *Gin = Gbuf[cur];
+            double *Gout = Gbuf[cur ^ 1];
+            const unsigned rot = rot_mask[cur];
             const unsigned char *rp = tp + r * kW;  // (p, q) of pair k at rp[2k], rp[2k+1]
-            if (warp == 4) {
-                const int p = rp[2 * lane], q = rp[2 * lane + 1];
-                double c, s, t;
-                const bool rot = evd_rotation(G[p * kEvdLD + p], G[q * kEvdLD + q], G[p * kEvdLD + q], tau, c, s, t);
-                cs_c[lane] = c;
-                cs_s[lane] = s;
-                cs_t[lane] = t;
-                const unsigned m = __ballot_sync(0xffffffffu, rot);
-                if (lane == 0) {
-                    rot_mask = m;
-                    if (m) sweep_any[sw] = 1;
+            if (warp < 7) {
+                if (warp < 4) {
+                    if (rot) evd_w_rotate(w, cs_c[cur], cs_s[cur], half);
+                    evd_w_shift(w, half);
                 }
-            }
-            __syncthreads();
-            const unsigned rot = rot_mask;
-            if (warp < 4) {
-                if (rot) evd_w_rotate(w, cs_c, cs_s, half);
-                evd_w_shift(w, half);
-            }
-            if (rot) {
-                // G <- J^T G J by 2 x 2 blocks of index pairs (a, b), a <= b;
-                // thread tid owns blocks tid, tid + 256, tid + 512
+                // G_out = J^T G_in J by 2 x 2 blocks of index pairs (a, b), a <= b
 #pragma unroll
-                for (int j = 0; j < kTriIters; ++j) {
+                for (int j = 0; j < kEvdBulkIters; ++j) {
                     const int a = blk_a[j], b = blk_b[j];
-                    if (a < 0 || !(((rot >> a) | (rot >> b)) & 1u)) continue;
+                    if (a < 0) continue;
                     const int pa = rp[2 * a], qa = rp[2 * a + 1], pb = rp[2 * b], qb = rp[2 * b + 1];
+                    const bool ra = (rot >> a) & 1u, rb = (rot >> b) & 1u;
                     if (a == b) {
                         // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
-                        const double ta = cs_t[a], o = G[pa * kEvdLD + qa];
-                        G[pa * kEvdLD + pa] = fma(-ta, o, G[pa * kEvdLD + pa]);
-                        G[qa * kEvdLD + qa] = fma(ta, o, G[qa * kEvdLD + qa]);
-                        G[pa * kEvdLD + qa] = 0.0;
-                        G[qa * kEvdLD + pa] = 0.0;
+                        const double gpp = Gin[pa * kEvdLD + pa], gqq = Gin[qa * kEvdLD + qa];
+                        const double o = Gin[pa * kEvdLD + qa];
+                        if (ra) {
+                            const double t = cs_t[cur][a];
+                            Gout[pa * kEvdLD + pa] = fma(-t, o, gpp);
+                            Gout[qa * kEvdLD + qa] = fma(t, o, gqq);
+                            Gout[pa * kEvdLD + qa] = 0.0;
+                            Gout[qa * kEvdLD + pa] = 0.0;
+                        } else {
+                            Gout[pa * kEvdLD + pa] = gpp;
+                            Gout[qa * kEvdLD + qa] = gqq;
+                            Gout[pa * kEvdLD + qa] = o;
+                            Gout[qa * kEvdLD + pa] = o;
+                        }
                         continue;
                     }
-                    const double ca = cs_c[a], sa = cs_s[a], cb = cs_c[b], sb = cs_s[b];
-                    const double g11 = G[pa * kEvdLD + pb], g12 = G[pa * kEvdLD + qb];
-                    const double g21 = G[qa * kEvdLD + pb], g22 = G[qa * kEvdLD + qb];
-                    // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
-                    const double h11 = fma(cb, g11, -(sb * g12)), h12 = fma(sb, g11, cb * g12);
-                    const double h21 = fma(cb, g21, -(sb * g22)), h22 = fma(sb, g21, cb * g22);
-                    // rows (on the left, pair a)
-                    const double n11 = fma(ca, h11, -(sa * h21)), n21 = fma(sa, h11, ca * h21);
-                    const double n12 = fma(ca, h12, -(sa * h22)), n22 = fma(sa, h12, ca * h22);
-                    G[pa * kEvdLD + pb] = n11;
-                    G[pa * kEvdLD + qb] = n12;
-                    G[qa * kEvdLD + pb] = n21;
-                    G[qa * kEvdLD + qb] = n22;
-                    G[pb * kEvdLD + pa] = n11;
-                    G[qb * kEvdLD + pa] = n12;
-                    G[pb * kEvdLD + qa] = n21;
-                    G[qb * kEvdLD + qa] = n22;
+                    const double g11 = Gin[pa * kEvdLD + pb], g12 = Gin[pa * kEvdLD + qb];
+                    const double g21 = Gin[qa * kEvdLD + pb], g22 = Gin[qa * kEvdLD + qb];
+                    double n11 = g11, n12 = g12, n21 = g21, n22 = g22;
+                    if (ra || rb) {
+                        const double ca = cs_c[cur][a], sa = cs_s[cur][a], cb = cs_c[cur][b], sb = cs_s[cur][b];
+                        // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
+                        const double h11 = fma(cb, g11, -(sb * g12)), h12 = fma(sb, g11, cb * g12);
+                        const double h21 = fma(cb, g21, -(sb * g22)), h22 = fma(sb, g21, cb * g22);
+                        // rows (on the left, pair a)
+                        n11 = fma(ca, h11, -(sa * h21));
+                        n21 = fma(sa, h11, ca * h21);
+                        n12 = fma(ca, h12, -(sa * h22));
+                        n22 = fma(sa, h12, ca * h22);
+                    }
+                    Gout[pa * kEvdLD + pb] = n11;
+                    Gout[pa * kEvdLD + qb] = n12;
+                    Gout[qa * kEvdLD + pb] = n21;
+                    Gout[qa * kEvdLD + qb] = n22;
+                    Gout[pb * kEvdLD + pa] = n11;
+                    Gout[qb * kEvdLD + pa] = n12;
+                    Gout[pb * kEvdLD + qa] = n21;
+                    Gout[qb * kEvdLD + qa] = n22;
+                }
+            } else {
+                // warp 7: the angles of round gr + 1, from G_in and round gr's
+                // rotations (lane k held pair k of round gr)
+                const bool me = (rot >> lane) & 1u;
+                const double nd0 = me ? fma(-a_t, a_pq, a_pp) : a_pp;  // new diagonal of my first column
+                const double nd1 = me ? fma(a_t, a_pq, a_qq) : a_qq;   // ... of my second column
+                const int A = lane <= 1 ? 0 : lane - 1, RA = lane == 1 ? 1 : 0;
+                const int B = lane <= 30 ? lane + 1 : 31, RB = lane <= 30 ? 1 : 0;
+                const double dA0 = __shfl_sync(0xffffffffu, nd0, A), dA1 = __shfl_sync(0xffffffffu, nd1, A);
+                const double dB0 = __shfl_sync(0xffffffffu, nd0, B), dB1 = __shfl_sync(0xffffffffu, nd1, B);
+                const double ca = __shfl_sync(0xffffffffu, a_c, A), sa = __shfl_sync(0xffffffffu, a_s, A);
+                const double cb = __shfl_sync(0xffffffffu, a_c, B), sb = __shfl_sync(0xffffffffu, a_s, B);
+                const int pa = __shfl_sync(0xffffffffu, my_p, A), qa = __shfl_sync(0xffffffffu, my_q, A);
+                const int pb = __shfl_sync(0xffffffffu, my_p, B), qb = __shfl_sync(0xffffffffu, my_q, B);
+                const double g11 = Gin[pa * kEvdLD + pb], g12 = Gin[pa * kEvdLD + qb];
+                const double g21 = Gin[qa * kEvdLD + pb], g22 = Gin[qa * kEvdLD + qb];
+                // element (RA, RB) of block (A, B) of G_out, as the update computes it
+                double gpq = RA ? (RB ? g22 : g21) : (RB ? g12 : g11);
+                if (((rot >> A) | (rot >> B)) & 1u) {
+                    const double h1 = RB ? fma(sb, g11, cb * g12) : fma(cb, g11, -(sb * g12));  // h1RB
+                    const double h2 = RB ? fma(sb, g21, cb * g22) : fma(cb, g21, -(sb * g22));  // h2RB
+                    gpq = RA ? fma(sa, h1, ca * h2) : fma(ca, h1, -(sa * h2));
+                }
+                a_pp = RA ? dA1 : dA0;
+                a_qq = RB ? dB1 : dB0;
+                a_pq = gpq;
+                my_p = RA ? qa : pa;
+                my_q = RB ? qb : pb;
+                const bool rot_next = evd_rotation(a_pp, a_qq, a_pq, tau, a_c, a_s, a_t);
+                cs_c[cur ^ 1][lane] = a_c;
+                cs_s[cur ^ 1][lane] = a_s;
+                cs_t[cur ^ 1][lane] = a_t;
+                const unsigned m = __ballot_sync(0xffffffffu, rot_next);
+                if (lane == 0) {
+                    rot_mask[cur ^ 1] = m;
+                    if (m) sweep_any[r + 1 < kEvdRounds ? sw : sw + 1] = 1;
                 }
             }
-            __syncthreads();
         }
-        // sweep_any[sw] was last written before the round's first barrier
-        const bool had = sweep_any[sw] != 0;
-        rotated_any = rotated_any || had;
-        if (!had) break;  // the same value in every thread
+        // sweep_any[sw] was last written before this sweep's final barrier
+        if (!sweep_any[sw]) break;  // the same value in every thread
+        rotated_any = true;
     }
+    __syncthreads();  // the last round's output buffer is complete
+    const double *Gf = Gbuf[gr & 1];
     // Output order of W's columns.  With `sort`, the eigenvalues (G's
     // diagonal) are ranked and the lower-numbered block of the pair receives
     // the larger ones (decreasing norms across the blocks, de Rijk's
@@ -744,11 +819,11 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             auto gcol = [&](int c) { return c < kB ? bp.x * kB + c : bp.y * kB + (c - kB); };
             if (gcol(tid) < ncols) {
                 const bool desc = bp.x < bp.y;  // local order follows global order when bp.x < bp.y
-                const double lam = G[tid * kEvdLD + tid];
+                const double lam = Gf[tid * kEvdLD + tid];
                 int rank = 0;
                 for (int c = 0; c < kW; ++c) {
                     if (gcol(c) >= ncols) continue;
-                    const double l2 = G[c * kEvdLD + c];
+                    const double l2 = Gf[c * kEvdLD + c];
                     const bool before = desc ? (l2 > lam) : (l2 < lam);
                     rank += (before || (l2 == lam && c < tid)) ? 1 : 0;
                 }
@@ -770,7 +845,6 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
 #pragma unroll
         for (int j = 0; j < 32; ++j) wo[(size_t)out_col[evd_slot_column(32 * half + j)] * kW + wrow] = w[j];
     }
-    __syncthreads();  // off_bits complete
     if (tid == 0) {
         flags[pair] = rotated_any ? 1 : 0;
         if (rotated_any) atomicAdd(&stats[1], 1ull);
