@@ -484,19 +484,11 @@ __global__ void __launch_bounds__(kRot64Threads)
 // ============================================================================
 
 constexpr int kEvdThreads = 256;  // warps 0-3: W rows in registers; warps 0-6: G; warp 7: the angles
-constexpr int kEvdLD = kW + 1;
+constexpr int kEvdLD = kW + 2;    // even: every row starts on a 16-byte boundary (vector loads of slot pairs)
 constexpr int kTriBlocks = (kW / 2) * (kW / 2 + 1) / 2;  // 2x2 blocks (a <= b) of the 32 x 32 block grid
 constexpr int kEvdRounds = kW - 1;
 constexpr int kEvdMaxInner = 8;
-constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD + kEvdRounds * (kW / 2) * 2 + kTriBlocks * 2;
-
-// Round-robin pair tables of the block eigen-solve, in global memory so that
-// a CTA copies them into shared memory with coalesced loads.
-struct EvdTables {
-    unsigned char pairs[kEvdRounds][kW / 2][2];  // (p, q) of pair k in inner round r (circle over 64 indices)
-    unsigned char tri[kTriBlocks][2];            // (a, b), a <= b
-};
-__device__ EvdTables g_evd_tables;
+constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD;
 
 // Rotation of [pp pq; pq qq] that annihilates pq, with the reference's
 // threshold test (|pq| > tau sqrt(pp qq), squared, and |pq| > 1e-300).
@@ -532,29 +524,41 @@ __device__ __forceinline__ bool evd_rotation(double pp, double qq, double pq, do
     return false;
 }
 
-// W in registers.  In inner round r, pair k rotates the columns at circle
-// positions k and 63 - k; slot 2k holds position k and slot 2k+1 position
-// 63 - k, so the pairs sit at fixed slots and the round-robin advance
-// (positions 1..62 move up by one, 63 wraps to 1, 0 stays) is a fixed
-// permutation of slots:
+// Slots.  The 64 indices of the eigen-solve move through the circle of the
+// round-robin ordering; instead of looking the pairs up per round, every
+// index lives in a slot: in each inner round, pair k rotates slots 2k (its
+// first index) and 2k + 1 (its second), and the round-robin advance between
+// rounds is one fixed permutation of the slots, evd_next_slot:
 //   first'[0] = first[0], first'[1] = second[0], first'[k] = first[k-1],
 //   second'[k] = second[k+1] (k < 31), second'[31] = first[31].
-// Row `row` of W is held by two threads: half h owns pairs 16h .. 16h+15
-// (slots 32h .. 32h+31, local index j <-> pair 16h + j), w[2j] = first,
-// w[2j+1] = second.  Across the halves one value moves per round:
-// first[15] -> first'[16] and second[16] -> second'[15] (one xor shuffle).
-// After 63 rounds every column is back at its starting slot: slot 2k holds
-// column k, slot 2k+1 column 63 - k.
+// At the start (and after every full sweep of 63 rounds, the permutation's
+// order) slot 2k holds index k and slot 2k+1 index 63 - k, which is pair k of
+// round 0 of the circle (round_robin_pair).
 __device__ __forceinline__ int evd_slot_column(int slot) { return (slot & 1) ? 63 - (slot >> 1) : (slot >> 1); }
+__device__ __forceinline__ int evd_column_slot(int col) { return col < 32 ? 2 * col : 127 - 2 * col; }
+__device__ __forceinline__ int evd_next_slot(int s)
+{
+    if (s == 0) return 0;
+    if (s == 1) return 2;
+    if (s == 62) return 63;
+    return (s & 1) ? s - 2 : s + 2;
+}
+// G is symmetric and only its upper triangle (in slot coordinates) is kept.
+__device__ __forceinline__ int evd_upper(int s, int t) { return s <= t ? s * kEvdLD + t : t * kEvdLD + s; }
 
-__device__ __forceinline__ void evd_w_rotate(double (&w)[32], const double *cs_c, const double *cs_s, int half)
+// W in registers, in slots.  Row `row` of W is held by two threads: half h
+// owns pairs 16h .. 16h+15 (slots 32h .. 32h+31, local index j <-> pair
+// 16h + j), w[2j] = first, w[2j+1] = second.  Across the halves one value
+// moves per round: first[15] -> first'[16] and second[16] -> second'[15]
+// (one xor shuffle).
+__device__ __forceinline__ void evd_w_rotate(double (&w)[32], const double2 *cs, int half)
 {
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        const double c = cs_c[16 * half + j], s = cs_s[16 * half + j];
+        const double2 r = cs[16 * half + j];
         const double x = w[2 * j], y = w[2 * j + 1];
-        w[2 * j] = fma(c, x, -(s * y));
-        w[2 * j + 1] = fma(s, x, c * y);
+        w[2 * j] = fma(r.x, x, -(r.y * y));
+        w[2 * j + 1] = fma(r.y, x, r.x * y);
     }
 }
 
@@ -583,19 +587,23 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
 // Input Gram of block pair blockIdx.x from `splits` partials: kind 0 = the
 // tensor-core layout (128 x 64 FP32, rows r and r + 64 summed), kind 1 =
 // 64 x 64 FP64 upper triangle.  Cyclic two-sided Jacobi, at most
-// inner_sweeps sweeps of 63 rounds of 32 disjoint index pairs, software
-// pipelined so that a round costs one barrier and the angle chain runs beside
-// the update:
-//   * G is double-buffered: round r reads buffer r%2 and writes r+1%2;
-//   * warps 0-6 apply round r to G (2 x 2 blocks, every block written, the
-//     unrotated ones copied) and warps 0-3 apply it to W (registers);
+// inner_sweeps sweeps of 63 rounds of 32 disjoint index pairs, in slot
+// coordinates (above), software pipelined so that a round costs one barrier
+// and the angle chain runs beside the update:
+//   * G (upper triangle, slot coordinates) is double-buffered: round r reads
+//     buffer r%2 and writes buffer (r+1)%2 already advanced to round r+1's
+//     slots, so every thread reads and writes the same addresses in every
+//     round (kept in registers, no table lookups);
+//   * warps 0-6 apply round r to G by 2 x 2 blocks of slot pairs (a, b),
+//     a <= b (two 16-byte loads, every output written once, the unrotated
+//     ones copied), and warps 0-3 apply it to W (registers);
 //   * warp 7 meanwhile derives the angles of round r+1 from buffer r%2 and
-//     round r's rotations: in the circle, pair k of round r+1 takes its first
-//     column from pair k-1 of round r (pair 0 for k <= 1) and its second from
-//     pair k+1 (pair 31 for k = 31), so its diagonal entries are round r's
-//     annihilated diagonals and its off-diagonal entry is one element of one
-//     2 x 2 block update, computed with the same operations as the update
-//     itself (bit-identical to what lands in the buffer).
+//     round r's rotations: pair k of round r+1 takes its first index from
+//     pair k-1 of round r (pair 0 for k <= 1) and its second from pair k+1
+//     (pair 31 for k = 31), so its diagonal entries are round r's annihilated
+//     diagonals and its off-diagonal entry is one element of one 2 x 2 block
+//     update, computed with the same operations as the update itself
+//     (bit-identical to what lands in the buffer).
 // Writes W (64 x 64, column-major) and flags[pair] = 1 when some pair
 // rotated (else flags[pair] = 0 and W is left as it was).  stats[0] (as
 // double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over the input
@@ -608,11 +616,11 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
            int sort, int ncols, double *__restrict__ Wout, int *__restrict__ flags,
            unsigned long long *__restrict__ stats)
 {
-    extern __shared__ double dsm[];
-    double *Gbuf[2] = {dsm, dsm + kW * kEvdLD};  // [64][65] each
-    unsigned char *tp = reinterpret_cast<unsigned char *>(dsm + 2 * kW * kEvdLD);  // [63][32][2]
-    unsigned char *tt = tp + kEvdRounds * (kW / 2) * 2;                           // [528][2]
-    __shared__ double cs_c[2][kW / 2], cs_s[2][kW / 2], cs_t[2][kW / 2];
+    extern __shared__ __align__(16) double dsm[];
+    double *const G0 = dsm;                 // [64][66], buffer 0
+    double *const G1 = dsm + kW * kEvdLD;   // [64][66], buffer 1
+    __shared__ double2 cs[2][kW / 2];       // (c, s) of the 32 pairs, by round parity
+    __shared__ double cs_t[2][kW / 2];      // t
     __shared__ unsigned rot_mask[2];
     __shared__ int sweep_any[kEvdMaxInner + 1];
     __shared__ int out_col[kW];
@@ -622,11 +630,7 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     const int nsweeps = min(inner_sweeps, kEvdMaxInner);
     if (tid == 0) off_bits = 0ull;
     if (tid <= kEvdMaxInner) sweep_any[tid] = 0;
-    {
-        const unsigned char *src = reinterpret_cast<const unsigned char *>(&g_evd_tables);
-        for (int e = tid; e < (int)sizeof(EvdTables); e += kEvdThreads) tp[e] = src[e];
-    }
-    double *G0 = Gbuf[0];
+    // the input Gram in column coordinates, in buffer 1
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
         const int r = e & 63, c = e >> 6;  // consecutive threads, consecutive rows of a column
         double g = 0.0;
@@ -634,12 +638,12 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
             for (int s = 0; s < splits; ++s)
                 g += (double)p[(size_t)s * 8192 + c * 128 + r] + (double)p[(size_t)s * 8192 + c * 128 + r + 64];
-            G0[r * kEvdLD + c] = g;
+            G1[r * kEvdLD + c] = g;
         } else if (r <= c) {  // the FP64 Gram kernel writes the upper triangle only: mirror it
             const double *p = static_cast<const double *>(part) + (size_t)pair * splits * 4096;
             for (int s = 0; s < splits; ++s) g += p[(size_t)s * 4096 + c * 64 + r];
-            G0[r * kEvdLD + c] = g;
-            G0[c * kEvdLD + r] = g;
+            G1[r * kEvdLD + c] = g;
+            G1[c * kEvdLD + r] = g;
         }
     }
     // W rows: thread tid < 128 holds row tid/2, half tid&1 (slot layout above)
@@ -648,48 +652,66 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
 #pragma unroll
     for (int j = 0; j < 32; ++j) w[j] = (evd_slot_column(32 * half + j) == wrow) ? 1.0 : 0.0;
     __syncthreads();
-    // symmetrise (the two triangles come from different accumulation orders),
-    // measure the input's largest scaled off-diagonal entry, and find whether
-    // any index pair passes the rotation test at all: if none does, no round
-    // can rotate (G never changes) and the solve is skipped
+    // symmetrise (the two triangles come from different accumulation orders)
+    // into buffer 0 in slot coordinates, measure the input's largest scaled
+    // off-diagonal entry, and find whether any index pair passes the rotation
+    // test at all: if none does, no round can rotate (G never changes) and the
+    // solve is skipped
     double off = 0.0;
     int need = 0;
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
         const int r = e >> 6, c = e & 63;
-        if (r < c) {
-            const double g = 0.5 * (G0[r * kEvdLD + c] + G0[c * kEvdLD + r]);
-            G0[r * kEvdLD + c] = g;
-            G0[c * kEvdLD + r] = g;
-            const double a = fmax(G0[r * kEvdLD + r], 0.0) * fmax(G0[c * kEvdLD + c], 0.0);
-            const double d = sqrt(a);
-            if (d > 0.0) off = fmax(off, fabs(g) / d);
-            if (fabs(g) > 1.0e-300 && g * g > (tau * tau) * a) need = 1;
+        if (r <= c) {
+            const double g = r < c ? 0.5 * (G1[r * kEvdLD + c] + G1[c * kEvdLD + r]) : G1[r * kEvdLD + r];
+            G0[evd_upper(evd_column_slot(r), evd_column_slot(c))] = g;
+            if (r < c) {
+                const double a = fmax(G1[r * kEvdLD + r], 0.0) * fmax(G1[c * kEvdLD + c], 0.0);
+                const double d = sqrt(a);
+                if (d > 0.0) off = fmax(off, fabs(g) / d);
+                if (fabs(g) > 1.0e-300 && g * g > (tau * tau) * a) need = 1;
+            }
         }
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
-    const bool work = __syncthreads_or(need) != 0;
-    // the 2 x 2 blocks of G this thread updates in every round (warps 0-6)
-    int blk_a[kEvdBulkIters], blk_b[kEvdBulkIters];
+    // the 2 x 2 blocks this thread updates in every round (warps 0-6): pair
+    // indices (a | b << 8), the offset of the block's first row, and the four
+    // destinations (slot coordinates of round r+1, upper triangle), two per int
+    int blk[kEvdBulkIters], rd[kEvdBulkIters], wr01[kEvdBulkIters], wr23[kEvdBulkIters];
 #pragma unroll
     for (int j = 0; j < kEvdBulkIters; ++j) {
-        const int e = tid + j * kEvdBulkThreads;
-        const bool live = tid < kEvdBulkThreads && e < kTriBlocks;
-        blk_a[j] = live ? tt[2 * e] : -1;
-        blk_b[j] = live ? tt[2 * e + 1] : -1;
+        int e = tid + j * kEvdBulkThreads;
+        blk[j] = -1;
+        rd[j] = wr01[j] = wr23[j] = 0;
+        if (tid < kEvdBulkThreads && e < kTriBlocks) {
+            int a = 0;
+            while (e >= kW / 2 - a) {  // row-major over a <= b
+                e -= kW / 2 - a;
+                ++a;
+            }
+            const int b = a + e;
+            const int pa = evd_next_slot(2 * a), qa = evd_next_slot(2 * a + 1);
+            const int pb = evd_next_slot(2 * b), qb = evd_next_slot(2 * b + 1);
+            blk[j] = a | (b << 8);
+            rd[j] = 2 * a * kEvdLD + 2 * b;
+            if (a == b) {  // (pp, pq) and qq
+                wr01[j] = evd_upper(pa, pa) | (evd_upper(pa, qa) << 16);
+                wr23[j] = evd_upper(qa, qa);
+            } else {       // (11, 12) and (21, 22)
+                wr01[j] = evd_upper(pa, pb) | (evd_upper(pa, qb) << 16);
+                wr23[j] = evd_upper(qa, pb) | (evd_upper(qa, qb) << 16);
+            }
+        }
     }
-    // warp 7: round 0's angles from buffer 0; it keeps its pair's indices,
-    // input entries and rotation in registers from round to round
-    int my_p = 0, my_q = 0;
+    const bool work = __syncthreads_or(need) != 0;
+    // warp 7: round 0's angles from buffer 0; it keeps its pair's input
+    // entries and rotation in registers from round to round
     double a_pp = 0.0, a_qq = 0.0, a_pq = 0.0, a_c = 1.0, a_s = 0.0, a_t = 0.0;
     if (warp == 7 && work) {
-        my_p = tp[2 * lane];
-        my_q = tp[2 * lane + 1];
-        a_pp = G0[my_p * kEvdLD + my_p];
-        a_qq = G0[my_q * kEvdLD + my_q];
-        a_pq = G0[my_p * kEvdLD + my_q];
+        a_pp = G0[2 * lane * kEvdLD + 2 * lane];
+        a_qq = G0[(2 * lane + 1) * kEvdLD + 2 * lane + 1];
+        a_pq = G0[2 * lane * kEvdLD + 2 * lane + 1];
         const bool rot = evd_rotation(a_pp, a_qq, a_pq, tau, a_c, a_s, a_t);
-        cs_c[0][lane] = a_c;
-        cs_s[0][lane] = a_s;
+        cs[0][lane] = make_double2(a_c, a_s);
         cs_t[0][lane] = a_t;
         const unsigned m = __ballot_sync(0xffffffffu, rot);
         if (lane == 0) {
@@ -703,45 +725,41 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         for (int r = 0; r < kEvdRounds; ++r, ++gr) {
             __syncthreads();  // round gr's angles published, its input buffer complete
             const int cur = gr & 1;
-            const double *Gin = Gbuf[cur];
-            double *Gout = Gbuf[cur ^ 1];
+            const double *Gin = cur ? G1 : G0;
+            double *Gout = cur ? G0 : G1;
             const unsigned rot = rot_mask[cur];
-            const unsigned char *rp = tp + r * kW;  // (p, q) of pair k at rp[2k], rp[2k+1]
             if (warp < 7) {
                 if (warp < 4) {
-                    if (rot) evd_w_rotate(w, cs_c[cur], cs_s[cur], half);
+                    if (rot) evd_w_rotate(w, cs[cur], half);
                     evd_w_shift(w, half);
                 }
-                // G_out = J^T G_in J by 2 x 2 blocks of index pairs (a, b), a <= b
 #pragma unroll
                 for (int j = 0; j < kEvdBulkIters; ++j) {
-                    const int a = blk_a[j], b = blk_b[j];
-                    if (a < 0) continue;
-                    const int pa = rp[2 * a], qa = rp[2 * a + 1], pb = rp[2 * b], qb = rp[2 * b + 1];
+                    if (blk[j] < 0) continue;
+                    const int a = blk[j] & 255, b = blk[j] >> 8;
                     const bool ra = (rot >> a) & 1u, rb = (rot >> b) & 1u;
+                    const double2 x1 = *reinterpret_cast<const double2 *>(Gin + rd[j]);
                     if (a == b) {
                         // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
-                        const double gpp = Gin[pa * kEvdLD + pa], gqq = Gin[qa * kEvdLD + qa];
-                        const double o = Gin[pa * kEvdLD + qa];
+                        const double gqq = Gin[rd[j] + kEvdLD + 1];
+                        double npp = x1.x, nqq = gqq, npq = x1.y;
                         if (ra) {
                             const double t = cs_t[cur][a];
-                            Gout[pa * kEvdLD + pa] = fma(-t, o, gpp);
-                            Gout[qa * kEvdLD + qa] = fma(t, o, gqq);
-                            Gout[pa * kEvdLD + qa] = 0.0;
-                            Gout[qa * kEvdLD + pa] = 0.0;
-                        } else {
-                            Gout[pa * kEvdLD + pa] = gpp;
-                            Gout[qa * kEvdLD + qa] = gqq;
-                            Gout[pa * kEvdLD + qa] = o;
-                            Gout[qa * kEvdLD + pa] = o;
+                            npp = fma(-t, x1.y, x1.x);
+                            nqq = fma(t, x1.y, gqq);
+                            npq = 0.0;
                         }
+                        Gout[wr01[j] & 0xffff] = npp;
+                        Gout[wr01[j] >> 16] = npq;
+                        Gout[wr23[j]] = nqq;
                         continue;
                     }
-                    const double g11 = Gin[pa * kEvdLD + pb], g12 = Gin[pa * kEvdLD + qb];
-                    const double g21 = Gin[qa * kEvdLD + pb], g22 = Gin[qa * kEvdLD + qb];
+                    const double2 x2 = *reinterpret_cast<const double2 *>(Gin + rd[j] + kEvdLD);
+                    const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
                     double n11 = g11, n12 = g12, n21 = g21, n22 = g22;
                     if (ra || rb) {
-                        const double ca = cs_c[cur][a], sa = cs_s[cur][a], cb = cs_c[cur][b], sb = cs_s[cur][b];
+                        const double2 A = cs[cur][a], B = cs[cur][b];
+                        const double ca = A.x, sa = A.y, cb = B.x, sb = B.y;
                         // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
                         const double h11 = fma(cb, g11, -(sb * g12)), h12 = fma(sb, g11, cb * g12);
                         const double h21 = fma(cb, g21, -(sb * g22)), h22 = fma(sb, g21, cb * g22);
@@ -751,31 +769,27 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
                         n12 = fma(ca, h12, -(sa * h22));
                         n22 = fma(sa, h12, ca * h22);
                     }
-                    Gout[pa * kEvdLD + pb] = n11;
-                    Gout[pa * kEvdLD + qb] = n12;
-                    Gout[qa * kEvdLD + pb] = n21;
-                    Gout[qa * kEvdLD + qb] = n22;
-                    Gout[pb * kEvdLD + pa] = n11;
-                    Gout[qb * kEvdLD + pa] = n12;
-                    Gout[pb * kEvdLD + qa] = n21;
-                    Gout[qb * kEvdLD + qa] = n22;
+                    Gout[wr01[j] & 0xffff] = n11;
+                    Gout[wr01[j] >> 16] = n12;
+                    Gout[wr23[j] & 0xffff] = n21;
+                    Gout[wr23[j] >> 16] = n22;
                 }
             } else {
                 // warp 7: the angles of round gr + 1, from G_in and round gr's
                 // rotations (lane k held pair k of round gr)
                 const bool me = (rot >> lane) & 1u;
-                const double nd0 = me ? fma(-a_t, a_pq, a_pp) : a_pp;  // new diagonal of my first column
-                const double nd1 = me ? fma(a_t, a_pq, a_qq) : a_qq;   // ... of my second column
+                const double nd0 = me ? fma(-a_t, a_pq, a_pp) : a_pp;  // new diagonal of my first slot
+                const double nd1 = me ? fma(a_t, a_pq, a_qq) : a_qq;   // ... of my second slot
                 const int A = lane <= 1 ? 0 : lane - 1, RA = lane == 1 ? 1 : 0;
                 const int B = lane <= 30 ? lane + 1 : 31, RB = lane <= 30 ? 1 : 0;
                 const double dA0 = __shfl_sync(0xffffffffu, nd0, A), dA1 = __shfl_sync(0xffffffffu, nd1, A);
                 const double dB0 = __shfl_sync(0xffffffffu, nd0, B), dB1 = __shfl_sync(0xffffffffu, nd1, B);
                 const double ca = __shfl_sync(0xffffffffu, a_c, A), sa = __shfl_sync(0xffffffffu, a_s, A);
                 const double cb = __shfl_sync(0xffffffffu, a_c, B), sb = __shfl_sync(0xffffffffu, a_s, B);
-                const int pa = __shfl_sync(0xffffffffu, my_p, A), qa = __shfl_sync(0xffffffffu, my_q, A);
-                const int pb = __shfl_sync(0xffffffffu, my_p, B), qb = __shfl_sync(0xffffffffu, my_q, B);
-                const double g11 = Gin[pa * kEvdLD + pb], g12 = Gin[pa * kEvdLD + qb];
-                const double g21 = Gin[qa * kEvdLD + pb], g22 = Gin[qa * kEvdLD + qb];
+                // block (A, B), A < B: rows 2A and 2A+1, columns 2B and 2B+1
+                const double2 x1 = *reinterpret_cast<const double2 *>(Gin + 2 * A * kEvdLD + 2 * B);
+                const double2 x2 = *reinterpret_cast<const double2 *>(Gin + (2 * A + 1) * kEvdLD + 2 * B);
+                const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
                 // element (RA, RB) of block (A, B) of G_out, as the update computes it
                 double gpq = RA ? (RB ? g22 : g21) : (RB ? g12 : g11);
                 if (((rot >> A) | (rot >> B)) & 1u) {
@@ -786,11 +800,8 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
                 a_pp = RA ? dA1 : dA0;
                 a_qq = RB ? dB1 : dB0;
                 a_pq = gpq;
-                my_p = RA ? qa : pa;
-                my_q = RB ? qb : pb;
                 const bool rot_next = evd_rotation(a_pp, a_qq, a_pq, tau, a_c, a_s, a_t);
-                cs_c[cur ^ 1][lane] = a_c;
-                cs_s[cur ^ 1][lane] = a_s;
+                cs[cur ^ 1][lane] = make_double2(a_c, a_s);
                 cs_t[cur ^ 1][lane] = a_t;
                 const unsigned m = __ballot_sync(0xffffffffu, rot_next);
                 if (lane == 0) {
@@ -804,28 +815,33 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         rotated_any = true;
     }
     __syncthreads();  // the last round's output buffer is complete
-    const double *Gf = Gbuf[gr & 1];
+    const double *Gf = (gr & 1) ? G1 : G0;
     // Output order of W's columns.  With `sort`, the eigenvalues (G's
     // diagonal) are ranked and the lower-numbered block of the pair receives
     // the larger ones (decreasing norms across the blocks, de Rijk's
     // ordering for one-sided Jacobi), which speeds convergence on graded
     // spectra; it is a column permutation of W.  Only the pair's real columns
     // (global index < ncols) are reordered, among their own positions: the
-    // zero padding columns never rotate and must stay at the end.
+    // zero padding columns never rotate and must stay at the end.  After full
+    // sweeps the slots are back at their starting columns.
     if (rotated_any && tid < kW) {
         int pos = tid;
         if (sort) {
             const int2 bp = round_robin_pair(nb, round, pair);
             auto gcol = [&](int c) { return c < kB ? bp.x * kB + c : bp.y * kB + (c - kB); };
+            auto lam = [&](int c) {
+                const int s = evd_column_slot(c);
+                return Gf[s * kEvdLD + s];
+            };
             if (gcol(tid) < ncols) {
                 const bool desc = bp.x < bp.y;  // local order follows global order when bp.x < bp.y
-                const double lam = Gf[tid * kEvdLD + tid];
+                const double l1 = lam(tid);
                 int rank = 0;
                 for (int c = 0; c < kW; ++c) {
                     if (gcol(c) >= ncols) continue;
-                    const double l2 = Gf[c * kEvdLD + c];
-                    const bool before = desc ? (l2 > lam) : (l2 < lam);
-                    rank += (before || (l2 == lam && c < tid)) ? 1 : 0;
+                    const double l2 = lam(c);
+                    const bool before = desc ? (l2 > l1) : (l2 < l1);
+                    rank += (before || (l2 == l1 && c < tid)) ? 1 : 0;
                 }
                 for (int c = 0, k = 0; c < kW; ++c) {
                     if (gcol(c) >= ncols) continue;
@@ -1047,31 +1063,13 @@ int make_map(CUtensorMap *map, float *base, long rows, long cols, bool atom32 = 
     return JSVD_OK;
 }
 
-int init_tables_once()
+int init_kernel_attributes()
 {
-    static std::once_flag once;
-    static EvdTables t{};
-    std::call_once(once, [] {
-        for (int r = 0; r < kW - 1; ++r)
-            for (int k = 0; k < kW / 2; ++k) {
-                const int2 pq = round_robin_pair(kW, r, k);
-                t.pairs[r][k][0] = (unsigned char)pq.x;
-                t.pairs[r][k][1] = (unsigned char)pq.y;
-            }
-        int e = 0;
-        for (int a = 0; a < kW / 2; ++a)
-            for (int b = a; b < kW / 2; ++b) {
-                t.tri[e][0] = (unsigned char)a;
-                t.tri[e][1] = (unsigned char)b;
-                ++e;
-            }
-    });
-    // constant memory and function attributes are per device
+    // function attributes are per device
     static thread_local unsigned long long done_mask = 0;
     int dev = 0;
     JSVD_CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64 || !(done_mask & (1ull << dev))) {
-        JSVD_CUDA_TRY(cudaMemcpyToSymbol(g_evd_tables, &t, sizeof(t)));
         JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGramTcSmem));
         JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_rot_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRotTcSmem));
         JSVD_CUDA_TRY(cudaFuncSetAttribute(mx_rot_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRot64Smem));
@@ -1443,7 +1441,7 @@ void mixed_release_thread_cache() { work_cache().clear(); }
 int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const jsvd_mixed_options &o, double *u,
                 double *sigma, double *v, int *sweeps, cudaStream_t st)
 {
-    if (int rc = init_tables_once(); rc != JSVD_OK) return rc;
+    if (int rc = init_kernel_attributes(); rc != JSVD_OK) return rc;
     const bool tc = o.tc_max_sweeps > 0;
     Work owned;
     ScopeExit release([&] { free_work(owned, st); });
@@ -1578,7 +1576,7 @@ extern "C" int jsvd_mixed_test_round(int kind, double *d_x, int rows, int cols, 
             return invalid_argument("jsvd_mixed_test_round: bad arguments.");
         cudaStream_t st = nullptr;
         if (const int e = entry_stream(nullptr, &st); e != JSVD_OK) return e;
-        if (int rc = init_tables_once(); rc != JSVD_OK) return rc;
+        if (int rc = init_kernel_attributes(); rc != JSVD_OK) return rc;
         const bool tc = (kind == 0 || kind == 2);
         jsvd_mixed_options o = default_options();
         Work w;
