@@ -630,20 +630,71 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     const int nsweeps = min(inner_sweeps, kEvdMaxInner);
     if (tid == 0) off_bits = 0ull;
     if (tid <= kEvdMaxInner) sweep_any[tid] = 0;
-    // the input Gram in column coordinates, in buffer 1
-    for (int e = tid; e < kW * kW; e += kEvdThreads) {
-        const int r = e & 63, c = e >> 6;  // consecutive threads, consecutive rows of a column
-        double g = 0.0;
+    // the input Gram in column coordinates, in buffer 1.  Thread t sums rows
+    // 4j .. 4j+3 of column c for (c, j) = ((t + 256 i) >> 4, (t + 256 i) & 15),
+    // i = 0..3, over the splits: 16-byte loads, eight per split in flight
+    // (kind 0 adds rows r and r + 64 of the partial in the same order as the
+    // element-wise sum: g += lo + hi).
+    {
+        double acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[i][k] = 0.0;
         if (kind == 0) {
             const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
-            for (int s = 0; s < splits; ++s)
-                g += (double)p[(size_t)s * 8192 + c * 128 + r] + (double)p[(size_t)s * 8192 + c * 128 + r + 64];
-            G1[r * kEvdLD + c] = g;
-        } else if (r <= c) {  // the FP64 Gram kernel writes the upper triangle only: mirror it
+#pragma unroll 2
+            for (int s = 0; s < splits; ++s) {
+                float4 lo[4], hi[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int o = tid + kEvdThreads * i, c = o >> 4, j = o & 15;
+                    const float *q = p + (size_t)s * 8192 + c * 128 + 4 * j;
+                    lo[i] = __ldg(reinterpret_cast<const float4 *>(q));
+                    hi[i] = __ldg(reinterpret_cast<const float4 *>(q + 64));
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    acc[i][0] += (double)lo[i].x + (double)hi[i].x;
+                    acc[i][1] += (double)lo[i].y + (double)hi[i].y;
+                    acc[i][2] += (double)lo[i].z + (double)hi[i].z;
+                    acc[i][3] += (double)lo[i].w + (double)hi[i].w;
+                }
+            }
+        } else {
             const double *p = static_cast<const double *>(part) + (size_t)pair * splits * 4096;
-            for (int s = 0; s < splits; ++s) g += p[(size_t)s * 4096 + c * 64 + r];
-            G1[r * kEvdLD + c] = g;
-            G1[c * kEvdLD + r] = g;
+#pragma unroll 2
+            for (int s = 0; s < splits; ++s) {
+                double2 x0[4], x1[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int o = tid + kEvdThreads * i, c = o >> 4, j = o & 15;
+                    const double *q = p + (size_t)s * 4096 + c * 64 + 4 * j;
+                    x0[i] = __ldg(reinterpret_cast<const double2 *>(q));
+                    x1[i] = __ldg(reinterpret_cast<const double2 *>(q + 2));
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    acc[i][0] += x0[i].x;
+                    acc[i][1] += x0[i].y;
+                    acc[i][2] += x1[i].x;
+                    acc[i][3] += x1[i].y;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int o = tid + kEvdThreads * i, c = o >> 4, j = o & 15;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int r = 4 * j + k;
+                if (kind == 0) {
+                    G1[r * kEvdLD + c] = acc[i][k];
+                } else if (r <= c) {  // the FP64 Gram kernel writes the upper triangle only: mirror it
+                    G1[r * kEvdLD + c] = acc[i][k];
+                    G1[c * kEvdLD + r] = acc[i][k];
+                }
+            }
         }
     }
     // W rows: thread tid < 128 holds row tid/2, half tid&1 (slot layout above)
