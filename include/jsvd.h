@@ -383,9 +383,10 @@ void jsvd_precond_stats_reset(void);
  * precision (normwise), not bit-identical to the plain path. */
 typedef struct jsvd_mixed_options {
     int precondition;   /* 1 (default): blocked sweeps on X = P^T after the two QRs; 0: on A   */
-    int tc_max_sweeps;  /* tensor-core sweeps at most (default 10); 0 = FP64 blocked sweeps only */
+    int tc_max_sweeps;  /* tensor-core sweeps at most; 0 = FP64 blocked sweeps only; -1 (default) =
+                           automatic: 4 for at most 2048 columns, else 10                       */
     double tc_tol;      /* phase 1 ends when no pair's |g_pq| / sqrt(g_pp g_qq) exceeds this    */
-    int inner_sweeps;   /* two-sided sweeps per 64 x 64 block eigen-solve (default 2)           */
+    int inner_sweeps;   /* two-sided sweeps per 64 x 64 block eigen-solve (default 1)           */
     int refine;         /* refinement: 0 = blocked FP64 sweeps (default), 1 = plain scalar sweep */
     int f64_max_sweeps; /* cap on refinement sweeps; 0 = the config's max_sweeps                  */
     int gram_splits;    /* row splits of each block-pair Gram; 0 = automatic                      */

@@ -483,45 +483,52 @@ __global__ void __launch_bounds__(kRot64Threads)
 // Block eigen-solve (FP64, both phases)
 // ============================================================================
 
-constexpr int kEvdThreads = 256;  // warps 0-3: W rows in registers; warps 0-6: G; warp 7: the angles
-constexpr int kEvdLD = kW + 2;    // even: every row starts on a 16-byte boundary (vector loads of slot pairs)
+constexpr int kEvdThreads = 512;      // warps 0-7: W; warps 8-14: G; warp 15: the angles
+constexpr int kEvdWThreads = 256;     // 4 threads per row of W
+constexpr int kEvdBulkFirst = 256;    // first thread of the G update
+constexpr int kEvdBulkThreads = 224;  // warps 8-14
+constexpr int kEvdLD = kW + 2;        // even: every row starts on a 16-byte boundary (vector loads of slot pairs)
 constexpr int kTriBlocks = (kW / 2) * (kW / 2 + 1) / 2;  // 2x2 blocks (a <= b) of the 32 x 32 block grid
+constexpr int kEvdBulkIters = (kTriBlocks + kEvdBulkThreads - 1) / kEvdBulkThreads;
 constexpr int kEvdRounds = kW - 1;
 constexpr int kEvdMaxInner = 8;
 constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD;
 
 // Rotation of [pp pq; pq qq] that annihilates pq, with the reference's
 // threshold test (|pq| > tau sqrt(pp qq), squared, and |pq| > 1e-300).
-// t = tan(theta) is the smaller root of t^2 + 2 zeta t - 1 = 0,
-// zeta = (qq - pp) / (2 pq), in the form
-//   t = sign * |e| / (|d| + sqrt(d^2 + e^2)),  d = qq - pp, e = 2 pq,
-// with sign = sign(e) for d >= 0 and -sign(e) otherwise (Rutishauser's t);
-// then c = 1 / sqrt(1 + t^2), s = t c.  One square root, one division and
-// one reciprocal square root on the serial chain.  d and e are scaled by a
-// power of two when their magnitude could over- or underflow d^2 + e^2.
+// With d = qq - pp, e = 2 pq and rho = 1 / sqrt(d^2 + e^2), the double angle
+// has cos 2theta = |d| rho and sin 2theta = |e| rho (the smaller rotation,
+// |theta| <= pi/4, Rutishauser's choice of root), and the half-angle
+// identities give
+//   c^2 = (1 + cos 2theta) / 2 in [1/2, 1],  c = c^2 / sqrt(c^2),
+//   |s| = sin 2theta / (2c),  |t| = |s| / c,
+// with sign(t) = sign(s) = sign(e) for d >= 0 and -sign(e) otherwise: two
+// reciprocal square roots and no division on the serial chain, no
+// cancellation (c^2 >= 1/2).  d and e are scaled by a power of two when
+// their magnitude could over- or underflow d^2 + e^2.  The rotation is
+// computed unconditionally and replaced by the identity when the test fails.
 __device__ __forceinline__ bool evd_rotation(double pp, double qq, double pq, double tau, double &c, double &s,
                                              double &t)
 {
     const double a = fmax(pp, 0.0) * fmax(qq, 0.0);
-    if (fabs(pq) > 1.0e-300 && pq * pq > (tau * tau) * a) {
-        double d = qq - pp, e = 2.0 * pq;
-        const double f = fmax(fabs(d), fabs(e));
-        if (f > 1.0e150 || f < 1.0e-150) {
-            const int k = ilogb(f);
-            d = scalbn(d, -k);
-            e = scalbn(e, -k);
-        }
-        const double h = sqrt(fma(d, d, e * e));
-        const double tt = fabs(e) / (fabs(d) + h);
-        t = ((d >= 0.0) == (e >= 0.0)) ? tt : -tt;
-        c = rsqrt(fma(t, t, 1.0));
-        s = t * c;
-        return true;
+    const bool rot = fabs(pq) > 1.0e-300 && pq * pq > (tau * tau) * a;
+    double d = qq - pp, e = 2.0 * pq;
+    const double f = fmax(fabs(d), fabs(e));
+    if (rot && (f > 1.0e150 || f < 1.0e-150)) {
+        const int k = ilogb(f);
+        d = scalbn(d, -k);
+        e = scalbn(e, -k);
     }
-    c = 1.0;
-    s = 0.0;
-    t = 0.0;
-    return false;
+    const double rho = rsqrt(fma(d, d, e * e));
+    const double c2 = fma(0.5 * fabs(d), rho, 0.5);
+    const double hs = (0.5 * fabs(e)) * rho;  // sin 2theta / 2
+    const double rc = rsqrt(c2);              // 1 / c
+    const double sg = ((d >= 0.0) == (e >= 0.0)) ? 1.0 : -1.0;
+    const double sa = hs * rc;
+    c = rot ? c2 * rc : 1.0;
+    s = rot ? sg * sa : 0.0;
+    t = rot ? sg * (sa * rc) : 0.0;
+    return rot;
 }
 
 // Slots.  The 64 indices of the eigen-solve move through the circle of the
@@ -546,42 +553,40 @@ __device__ __forceinline__ int evd_next_slot(int s)
 // G is symmetric and only its upper triangle (in slot coordinates) is kept.
 __device__ __forceinline__ int evd_upper(int s, int t) { return s <= t ? s * kEvdLD + t : t * kEvdLD + s; }
 
-// W in registers, in slots.  Row `row` of W is held by two threads: half h
-// owns pairs 16h .. 16h+15 (slots 32h .. 32h+31, local index j <-> pair
-// 16h + j), w[2j] = first, w[2j+1] = second.  Across the halves one value
-// moves per round: first[15] -> first'[16] and second[16] -> second'[15]
-// (one xor shuffle).
-__device__ __forceinline__ void evd_w_rotate(double (&w)[32], const double2 *cs, int half)
+// W in registers, in slots.  Row `row` of W is held by four consecutive
+// lanes: quarter q owns pairs 8q .. 8q+7 (slots 16q .. 16q+15, local index
+// j <-> pair 8q + j), w[2j] = first, w[2j+1] = second.
+__device__ __forceinline__ void evd_w_rotate(double (&w)[16], const double2 *cs, int q)
 {
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        const double2 r = cs[16 * half + j];
+    for (int j = 0; j < 8; ++j) {
+        const double2 r = cs[8 * q + j];
         const double x = w[2 * j], y = w[2 * j + 1];
         w[2 * j] = fma(r.x, x, -(r.y * y));
         w[2 * j + 1] = fma(r.y, x, r.x * y);
     }
 }
 
-// Advance of the circle for one thread's half row (lane partner = lane ^ 1).
-__device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
+// Advance of the circle for one thread's quarter row: first[8q - 1] comes in
+// from the quarter below (lane - 1), second[8q + 8] from the quarter above
+// (lane + 1).
+__device__ __forceinline__ void evd_w_shift(double (&w)[16], int q)
 {
-    const double send = half ? w[1] : w[30];  // half 1: second[16]; half 0: first[15]
-    const double recv = __shfl_xor_sync(0xffffffffu, send, 1);
-    double f[16], s[16];
+    const double up = __shfl_up_sync(0xffffffffu, w[14], 1);    // first[8q - 1]
+    const double down = __shfl_down_sync(0xffffffffu, w[1], 1);  // second[8q + 8]
+    double f[8], s[8];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
+    for (int j = 0; j < 8; ++j) {
         f[j] = w[2 * j];
         s[j] = w[2 * j + 1];
     }
-    // first'
-    w[0] = half ? recv : f[0];
-    w[2] = half ? f[0] : s[0];
+    w[0] = q == 0 ? f[0] : up;
+    w[2] = q == 0 ? s[0] : f[0];
 #pragma unroll
-    for (int j = 2; j < 16; ++j) w[2 * j] = f[j - 1];
-    // second'
+    for (int j = 2; j < 8; ++j) w[2 * j] = f[j - 1];
 #pragma unroll
-    for (int j = 0; j < 15; ++j) w[2 * j + 1] = s[j + 1];
-    w[31] = half ? f[15] : recv;
+    for (int j = 0; j < 7; ++j) w[2 * j + 1] = s[j + 1];
+    w[15] = q == 3 ? f[7] : down;
 }
 
 // Input Gram of block pair blockIdx.x from `splits` partials: kind 0 = the
@@ -589,15 +594,16 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
 // 64 x 64 FP64 upper triangle.  Cyclic two-sided Jacobi, at most
 // inner_sweeps sweeps of 63 rounds of 32 disjoint index pairs, in slot
 // coordinates (above), software pipelined so that a round costs one barrier
-// and the angle chain runs beside the update:
+// and the angle chain runs beside the update, on three groups of warps:
 //   * G (upper triangle, slot coordinates) is double-buffered: round r reads
 //     buffer r%2 and writes buffer (r+1)%2 already advanced to round r+1's
 //     slots, so every thread reads and writes the same addresses in every
 //     round (kept in registers, no table lookups);
-//   * warps 0-6 apply round r to G by 2 x 2 blocks of slot pairs (a, b),
+//   * warps 8-14 apply round r to G by 2 x 2 blocks of slot pairs (a, b),
 //     a <= b (two 16-byte loads, every output written once, the unrotated
-//     ones copied), and warps 0-3 apply it to W (registers);
-//   * warp 7 meanwhile derives the angles of round r+1 from buffer r%2 and
+//     ones copied: c = 1, s = 0 reproduce them);
+//   * warps 0-7 apply it to W (registers, 4 lanes per row);
+//   * warp 15 meanwhile derives the angles of round r+1 from buffer r%2 and
 //     round r's rotations: pair k of round r+1 takes its first index from
 //     pair k-1 of round r (pair 0 for k <= 1) and its second from pair k+1
 //     (pair 31 for k = 31), so its diagonal entries are round r's annihilated
@@ -608,9 +614,6 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[32], int half)
 // rotated (else flags[pair] = 0 and W is left as it was).  stats[0] (as
 // double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over the input
 // Grams, stats[1] = number of block pairs that rotated.
-constexpr int kEvdBulkThreads = 224;  // warps 0-6
-constexpr int kEvdBulkIters = (kTriBlocks + kEvdBulkThreads - 1) / kEvdBulkThreads;
-
 __global__ void __launch_bounds__(kEvdThreads, 1)
     mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps, int nb, int round,
            int sort, int ncols, double *__restrict__ Wout, int *__restrict__ flags,
@@ -631,30 +634,31 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     if (tid == 0) off_bits = 0ull;
     if (tid <= kEvdMaxInner) sweep_any[tid] = 0;
     // the input Gram in column coordinates, in buffer 1.  Thread t sums rows
-    // 4j .. 4j+3 of column c for (c, j) = ((t + 256 i) >> 4, (t + 256 i) & 15),
-    // i = 0..3, over the splits: 16-byte loads, eight per split in flight
+    // 4j .. 4j+3 of column c for (c, j) = ((t + 512 i) >> 4, (t + 512 i) & 15),
+    // i = 0..1, over the splits: 16-byte loads, four per split in flight
     // (kind 0 adds rows r and r + 64 of the partial in the same order as the
     // element-wise sum: g += lo + hi).
     {
-        double acc[4][4];
+        constexpr int kI = kW * kW / 4 / kEvdThreads;
+        double acc[kI][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < kI; ++i)
 #pragma unroll
             for (int k = 0; k < 4; ++k) acc[i][k] = 0.0;
         if (kind == 0) {
             const float *p = static_cast<const float *>(part) + (size_t)pair * splits * 8192;
-#pragma unroll 2
+#pragma unroll 4
             for (int s = 0; s < splits; ++s) {
-                float4 lo[4], hi[4];
+                float4 lo[kI], hi[kI];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < kI; ++i) {
                     const int o = tid + kEvdThreads * i, c = o >> 4, j = o & 15;
                     const float *q = p + (size_t)s * 8192 + c * 128 + 4 * j;
                     lo[i] = __ldg(reinterpret_cast<const float4 *>(q));
                     hi[i] = __ldg(reinterpret_cast<const float4 *>(q + 64));
                 }
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < kI; ++i) {
                     acc[i][0] += (double)lo[i].x + (double)hi[i].x;
                     acc[i][1] += (double)lo[i].y + (double)hi[i].y;
                     acc[i][2] += (double)lo[i].z + (double)hi[i].z;
@@ -663,18 +667,18 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             }
         } else {
             const double *p = static_cast<const double *>(part) + (size_t)pair * splits * 4096;
-#pragma unroll 2
+#pragma unroll 4
             for (int s = 0; s < splits; ++s) {
-                double2 x0[4], x1[4];
+                double2 x0[kI], x1[kI];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < kI; ++i) {
                     const int o = tid + kEvdThreads * i, c = o >> 4, j = o & 15;
                     const double *q = p + (size_t)s * 4096 + c * 64 + 4 * j;
                     x0[i] = __ldg(reinterpret_cast<const double2 *>(q));
                     x1[i] = __ldg(reinterpret_cast<const double2 *>(q + 2));
                 }
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < kI; ++i) {
                     acc[i][0] += x0[i].x;
                     acc[i][1] += x0[i].y;
                     acc[i][2] += x1[i].x;
@@ -683,7 +687,7 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             }
         }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < kI; ++i) {
             const int o = tid + kEvdThreads * i, c = o >> 4, j = o & 15;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -697,11 +701,11 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             }
         }
     }
-    // W rows: thread tid < 128 holds row tid/2, half tid&1 (slot layout above)
-    const int wrow = (tid >> 1) & 63, half = tid & 1;
-    double w[32];
+    // W rows: thread tid < 256 holds row tid/4, quarter tid&3 (slot layout above)
+    const int wrow = (tid >> 2) & 63, quarter = tid & 3;
+    double w[16];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) w[j] = (evd_slot_column(32 * half + j) == wrow) ? 1.0 : 0.0;
+    for (int j = 0; j < 16; ++j) w[j] = (evd_slot_column(16 * quarter + j) == wrow) ? 1.0 : 0.0;
     __syncthreads();
     // symmetrise (the two triangles come from different accumulation orders)
     // into buffer 0 in slot coordinates, measure the input's largest scaled
@@ -724,16 +728,17 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         }
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
-    // the 2 x 2 blocks this thread updates in every round (warps 0-6): pair
-    // indices (a | b << 8), the offset of the block's first row, and the four
+    // the 2 x 2 blocks a G thread updates in every round: pair indices
+    // (a | b << 8), the offset of the block's first row, and the four
     // destinations (slot coordinates of round r+1, upper triangle), two per int
     int blk[kEvdBulkIters], rd[kEvdBulkIters], wr01[kEvdBulkIters], wr23[kEvdBulkIters];
 #pragma unroll
     for (int j = 0; j < kEvdBulkIters; ++j) {
-        int e = tid + j * kEvdBulkThreads;
+        const int bt = tid - kEvdBulkFirst;
+        int e = bt + j * kEvdBulkThreads;
         blk[j] = -1;
         rd[j] = wr01[j] = wr23[j] = 0;
-        if (tid < kEvdBulkThreads && e < kTriBlocks) {
+        if (bt >= 0 && bt < kEvdBulkThreads && e < kTriBlocks) {
             int a = 0;
             while (e >= kW / 2 - a) {  // row-major over a <= b
                 e -= kW / 2 - a;
@@ -754,10 +759,10 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         }
     }
     const bool work = __syncthreads_or(need) != 0;
-    // warp 7: round 0's angles from buffer 0; it keeps its pair's input
+    // warp 15: round 0's angles from buffer 0; it keeps its pair's input
     // entries and rotation in registers from round to round
     double a_pp = 0.0, a_qq = 0.0, a_pq = 0.0, a_c = 1.0, a_s = 0.0, a_t = 0.0;
-    if (warp == 7 && work) {
+    if (warp == 15 && work) {
         a_pp = G0[2 * lane * kEvdLD + 2 * lane];
         a_qq = G0[(2 * lane + 1) * kEvdLD + 2 * lane + 1];
         a_pq = G0[2 * lane * kEvdLD + 2 * lane + 1];
@@ -779,62 +784,50 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             const double *Gin = cur ? G1 : G0;
             double *Gout = cur ? G0 : G1;
             const unsigned rot = rot_mask[cur];
-            if (warp < 7) {
-                if (warp < 4) {
-                    if (rot) evd_w_rotate(w, cs[cur], half);
-                    evd_w_shift(w, half);
-                }
+            if (warp < 8) {
+                if (rot) evd_w_rotate(w, cs[cur], quarter);
+                evd_w_shift(w, quarter);
+            } else if (warp < 15) {
 #pragma unroll
                 for (int j = 0; j < kEvdBulkIters; ++j) {
                     if (blk[j] < 0) continue;
                     const int a = blk[j] & 255, b = blk[j] >> 8;
-                    const bool ra = (rot >> a) & 1u, rb = (rot >> b) & 1u;
+                    const double2 A = cs[cur][a], B = cs[cur][b];
                     const double2 x1 = *reinterpret_cast<const double2 *>(Gin + rd[j]);
                     if (a == b) {
                         // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
                         const double gqq = Gin[rd[j] + kEvdLD + 1];
-                        double npp = x1.x, nqq = gqq, npq = x1.y;
-                        if (ra) {
-                            const double t = cs_t[cur][a];
-                            npp = fma(-t, x1.y, x1.x);
-                            nqq = fma(t, x1.y, gqq);
-                            npq = 0.0;
-                        }
-                        Gout[wr01[j] & 0xffff] = npp;
-                        Gout[wr01[j] >> 16] = npq;
-                        Gout[wr23[j]] = nqq;
+                        const double t = cs_t[cur][a];
+                        const bool ra = (rot >> a) & 1u;
+                        Gout[wr01[j] & 0xffff] = fma(-t, x1.y, x1.x);
+                        Gout[wr01[j] >> 16] = ra ? 0.0 : x1.y;
+                        Gout[wr23[j]] = fma(t, x1.y, gqq);
                         continue;
                     }
                     const double2 x2 = *reinterpret_cast<const double2 *>(Gin + rd[j] + kEvdLD);
                     const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
-                    double n11 = g11, n12 = g12, n21 = g21, n22 = g22;
-                    if (ra || rb) {
-                        const double2 A = cs[cur][a], B = cs[cur][b];
-                        const double ca = A.x, sa = A.y, cb = B.x, sb = B.y;
-                        // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
-                        const double h11 = fma(cb, g11, -(sb * g12)), h12 = fma(sb, g11, cb * g12);
-                        const double h21 = fma(cb, g21, -(sb * g22)), h22 = fma(sb, g21, cb * g22);
-                        // rows (on the left, pair a)
-                        n11 = fma(ca, h11, -(sa * h21));
-                        n21 = fma(sa, h11, ca * h21);
-                        n12 = fma(ca, h12, -(sa * h22));
-                        n22 = fma(sa, h12, ca * h22);
-                    }
-                    Gout[wr01[j] & 0xffff] = n11;
-                    Gout[wr01[j] >> 16] = n12;
-                    Gout[wr23[j] & 0xffff] = n21;
-                    Gout[wr23[j] >> 16] = n22;
+                    const double ca = A.x, sa = A.y, cb = B.x, sb = B.y;
+                    // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
+                    const double h11 = fma(cb, g11, -(sb * g12)), h12 = fma(sb, g11, cb * g12);
+                    const double h21 = fma(cb, g21, -(sb * g22)), h22 = fma(sb, g21, cb * g22);
+                    // rows (on the left, pair a)
+                    Gout[wr01[j] & 0xffff] = fma(ca, h11, -(sa * h21));
+                    Gout[wr01[j] >> 16] = fma(ca, h12, -(sa * h22));
+                    Gout[wr23[j] & 0xffff] = fma(sa, h11, ca * h21);
+                    Gout[wr23[j] >> 16] = fma(sa, h12, ca * h22);
                 }
             } else {
-                // warp 7: the angles of round gr + 1, from G_in and round gr's
+                // warp 15: the angles of round gr + 1, from G_in and round gr's
                 // rotations (lane k held pair k of round gr)
-                const bool me = (rot >> lane) & 1u;
-                const double nd0 = me ? fma(-a_t, a_pq, a_pp) : a_pp;  // new diagonal of my first slot
-                const double nd1 = me ? fma(a_t, a_pq, a_qq) : a_qq;   // ... of my second slot
+                const double nd0 = fma(-a_t, a_pq, a_pp);  // new diagonal of my first slot
+                const double nd1 = fma(a_t, a_pq, a_qq);   // ... of my second slot
+                // first index of pair k: pair k-1's first (k >= 2), pair 0's
+                // second (k = 1), its own (k = 0); second index: pair k+1's
+                // second (k <= 30), its own first (k = 31)
+                const double up = __shfl_up_sync(0xffffffffu, lane == 0 ? nd1 : nd0, 1);
+                const double dn = __shfl_down_sync(0xffffffffu, nd1, 1);
                 const int A = lane <= 1 ? 0 : lane - 1, RA = lane == 1 ? 1 : 0;
                 const int B = lane <= 30 ? lane + 1 : 31, RB = lane <= 30 ? 1 : 0;
-                const double dA0 = __shfl_sync(0xffffffffu, nd0, A), dA1 = __shfl_sync(0xffffffffu, nd1, A);
-                const double dB0 = __shfl_sync(0xffffffffu, nd0, B), dB1 = __shfl_sync(0xffffffffu, nd1, B);
                 const double ca = __shfl_sync(0xffffffffu, a_c, A), sa = __shfl_sync(0xffffffffu, a_s, A);
                 const double cb = __shfl_sync(0xffffffffu, a_c, B), sb = __shfl_sync(0xffffffffu, a_s, B);
                 // block (A, B), A < B: rows 2A and 2A+1, columns 2B and 2B+1
@@ -842,15 +835,11 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
                 const double2 x2 = *reinterpret_cast<const double2 *>(Gin + (2 * A + 1) * kEvdLD + 2 * B);
                 const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
                 // element (RA, RB) of block (A, B) of G_out, as the update computes it
-                double gpq = RA ? (RB ? g22 : g21) : (RB ? g12 : g11);
-                if (((rot >> A) | (rot >> B)) & 1u) {
-                    const double h1 = RB ? fma(sb, g11, cb * g12) : fma(cb, g11, -(sb * g12));  // h1RB
-                    const double h2 = RB ? fma(sb, g21, cb * g22) : fma(cb, g21, -(sb * g22));  // h2RB
-                    gpq = RA ? fma(sa, h1, ca * h2) : fma(ca, h1, -(sa * h2));
-                }
-                a_pp = RA ? dA1 : dA0;
-                a_qq = RB ? dB1 : dB0;
-                a_pq = gpq;
+                const double h1 = RB ? fma(sb, g11, cb * g12) : fma(cb, g11, -(sb * g12));  // h1RB
+                const double h2 = RB ? fma(sb, g21, cb * g22) : fma(cb, g21, -(sb * g22));  // h2RB
+                a_pq = RA ? fma(sa, h1, ca * h2) : fma(ca, h1, -(sa * h2));
+                a_pp = lane == 0 ? nd0 : up;
+                a_qq = lane == 31 ? nd0 : dn;
                 const bool rot_next = evd_rotation(a_pp, a_qq, a_pq, tau, a_c, a_s, a_t);
                 cs[cur ^ 1][lane] = make_double2(a_c, a_s);
                 cs_t[cur ^ 1][lane] = a_t;
@@ -906,11 +895,11 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         out_col[tid] = pos;
     }
     __syncthreads();
-    if (rotated_any && tid < 128) {
+    if (rotated_any && tid < kEvdWThreads) {
         // every sweep ran all 63 rounds: slot s holds column evd_slot_column(s)
         double *wo = Wout + (size_t)pair * kW * kW;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) wo[(size_t)out_col[evd_slot_column(32 * half + j)] * kW + wrow] = w[j];
+        for (int j = 0; j < 16; ++j) wo[(size_t)out_col[evd_slot_column(16 * quarter + j)] * kW + wrow] = w[j];
     }
     if (tid == 0) {
         flags[pair] = rotated_any ? 1 : 0;
@@ -1166,9 +1155,9 @@ jsvd_mixed_options default_options()
 {
     jsvd_mixed_options o{};
     o.precondition = 1;
-    o.tc_max_sweeps = 10;
+    o.tc_max_sweeps = -1;
     o.tc_tol = 2e-5;
-    o.inner_sweeps = 2;
+    o.inner_sweeps = 1;
     o.refine = 0;
     o.f64_max_sweeps = 0;
     o.gram_splits = 0;
@@ -1493,7 +1482,13 @@ int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const
                 double *sigma, double *v, int *sweeps, cudaStream_t st)
 {
     if (int rc = init_kernel_attributes(); rc != JSVD_OK) return rc;
-    const bool tc = o.tc_max_sweeps > 0;
+    // automatic cap on the tensor-core sweeps: on narrow inputs (few block
+    // pairs per round) a round costs about the same in either phase, the
+    // block eigen-solves dominating, so the FP64 phase, which converges
+    // quadratically, takes over early; on wide ones the 3xTF32 rounds are
+    // the cheaper and phase 1 runs until tc_tol
+    const int tc_max = o.tc_max_sweeps >= 0 ? o.tc_max_sweeps : (cols <= 2048 ? 4 : 10);
+    const bool tc = tc_max > 0;
     Work owned;
     ScopeExit release([&] { free_work(owned, st); });
     Work *wp = nullptr;
@@ -1523,7 +1518,7 @@ int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const
         // Phase 1 rotates every pair the FP32-accurate Gram resolves: its
         // entries carry relative errors of about 2^-21 + sqrt(m) 2^-24.
         const double tau = std::max(o.tc_tol * 0.25, 4.0 * std::sqrt((double)w.rows_pad) * 5.96e-8);
-        for (int s = 0; s < o.tc_max_sweeps; ++s) {
+        for (int s = 0; s < tc_max; ++s) {
             unsigned long long rotated = 0;
             if (int rc = run_sweep(w, true, tau, o.inner_sweeps, o.sort, st, &tc_off, &rotated); rc != JSVD_OK)
                 return rc;
