@@ -491,7 +491,49 @@ def run_ours(args, rank: int, world: int, device):
         line["cpu_baseline"] = cpu_baseline(wl, PLAIN_SWEEPS.get(wl["name"], 12), budget_s=args.cpu_budget)
     if wl["name"] == "tall" and world == 1 and not args.no_extras:
         line["other_configs"] = run_extras(args, path, device, stream, flush)
+        line["reference_gpu"] = reference_gpu_timing()
     return line
+
+
+REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "libjsvd_ref.so")
+
+
+def reference_gpu_timing() -> dict:
+    """The reference's own GPU solver (jacobi::svd::one_sided_jacobi_svd,
+    compiled unmodified from its sources into oracle/_ref/libjsvd_ref.so by
+    oracle/Makefile) timed through its full host path (its own cudaMalloc,
+    host<->device copies and per-round synchronisations) on the config-2
+    input (one solve) and on config 1 (best of two): the GPU comparator of the
+    plain drop-in.  Wall clock around the call, host buffers in and out."""
+    import ctypes
+
+    if not os.path.exists(REF_GPU_LIB):
+        return {"unavailable": "oracle/_ref/libjsvd_ref.so not built (build() compiles it where the "
+                               "reference sources are present)"}
+    L = ctypes.CDLL(REF_GPU_LIB)
+    P, S, I, D = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double
+    L.ref_plain_svd.argtypes = [P, S, S, D, I, I, I, P, P, P, P]
+    L.ref_plain_svd.restype = I
+    out = {"kind": "reference GPU binary (unmodified sources, oracle/_ref)", "unit": "SVD/s"}
+    for name, reps in (("tall", 1), ("square512", 2)):
+        wl = make_workload(name)
+        a = np.ascontiguousarray(wl["a"])
+        m, n = a.shape
+        u, sg, v = np.empty((m, n)), np.empty(n), np.empty((n, n))
+        sw = ctypes.c_int(0)
+        best = None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            rc = L.ref_plain_svd(a.ctypes.data, m, n, wl["eps"], 128, 256, 0, u.ctypes.data, sg.ctypes.data,
+                                 v.ctypes.data, ctypes.byref(sw))
+            dt = time.perf_counter() - t0
+            if rc != 0:
+                out[name] = {"error": f"ref_plain_svd returned {rc}"}
+                break
+            best = dt if best is None else min(best, dt)
+        else:
+            out[name] = {"value": 1.0 / best, "seconds": best, "sweeps": int(sw.value), "epsilon": wl["eps"]}
+    return out
 
 
 def run_extras(args, path: str, device, stream, flush) -> dict:

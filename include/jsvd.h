@@ -440,6 +440,17 @@ int jsvd_mixed_sweep_history(int *phase, double *offdiag, unsigned long long *ro
  * X_pair <- X_pair W_pair with W read from gw, in place; 3: FP64 rotation. */
 int jsvd_mixed_test_round(int kind, double *d_x, int rows, int cols, int round, double *d_gw);
 
+/* Failure-detection check of the bounded device waits: one wait with a
+ * limit of limit_ms (1..2000) on something nothing completes during the
+ * launch.  which 0: the persistent sweep's acquire-load wait on another CTA's
+ * round flag; 1: the tensor-core kernels' mbarrier wait.  preset != 0 sets
+ * the flag (arrives on the barrier) first, so the wait ends at once.  On
+ * expiry the kernel writes status 2 (wait timeout) and returns, the context
+ * stays usable, and the call returns JSVD_ERR_RUNTIME with a last-error
+ * message, as a sweep stopped at its limit does.  *device_status and
+ * *elapsed_ms (launch time) may be NULL. */
+int jsvd_test_wait_limit(int which, int limit_ms, int preset, int *device_status, double *elapsed_ms);
+
 /* FP64 GEMM of the library (DMMA tensor cores), for tests and tools:
  * C = alpha op(A) op(B) + beta C, column-major device buffers, op 'N' or 'T';
  * lower != 0 writes only C's lower triangle.  Synchronous on the calling

@@ -864,35 +864,36 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     // (global index < ncols) are reordered, among their own positions: the
     // zero padding columns never rotate and must stay at the end.  After full
     // sweeps the slots are back at their starting columns.
-    if (rotated_any && tid < kW) {
-        int pos = tid;
-        if (sort) {
-            const int2 bp = round_robin_pair(nb, round, pair);
-            auto gcol = [&](int c) { return c < kB ? bp.x * kB + c : bp.y * kB + (c - kB); };
-            auto lam = [&](int c) {
-                const int s = evd_column_slot(c);
-                return Gf[s * kEvdLD + s];
-            };
-            if (gcol(tid) < ncols) {
-                const bool desc = bp.x < bp.y;  // local order follows global order when bp.x < bp.y
-                const double l1 = lam(tid);
-                int rank = 0;
-                for (int c = 0; c < kW; ++c) {
-                    if (gcol(c) >= ncols) continue;
-                    const double l2 = lam(c);
-                    const bool before = desc ? (l2 > l1) : (l2 < l1);
-                    rank += (before || (l2 == l1 && c < tid)) ? 1 : 0;
-                }
-                for (int c = 0, k = 0; c < kW; ++c) {
-                    if (gcol(c) >= ncols) continue;
-                    if (k++ == rank) {
-                        pos = c;
-                        break;
-                    }
-                }
-            }
+    if (rotated_any) {  // the same value in every thread
+        // column col = tid / 8 is compared with columns 8 part .. 8 part + 7
+        // (part = tid % 8) and the 8 counts meet over lanes xor 1, 2, 4
+        const int col = tid >> 3, part = tid & 7;
+        const int2 bp = round_robin_pair(nb, round, pair);
+        const int real0 = min(max(ncols - bp.x * kB, 0), kB), real1 = min(max(ncols - bp.y * kB, 0), kB);
+        auto real = [&](int c) { return c < kB ? c < real0 : c - kB < real1; };
+        auto lam = [&](int c) {
+            const int s = evd_column_slot(c);
+            return Gf[s * kEvdLD + s];
+        };
+        const bool desc = bp.x < bp.y;  // local order follows global order when bp.x < bp.y
+        const double l1 = lam(col);
+        int rank = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int c = 8 * part + k;
+            const double l2 = lam(c);
+            const bool before = desc ? (l2 > l1) : (l2 < l1);
+            rank += (real(c) && (before || (l2 == l1 && c < col))) ? 1 : 0;
         }
-        out_col[tid] = pos;
+        rank += __shfl_xor_sync(0xffffffffu, rank, 1);
+        rank += __shfl_xor_sync(0xffffffffu, rank, 2);
+        rank += __shfl_xor_sync(0xffffffffu, rank, 4);
+        if (part == 0) {
+            // the rank-th real column (the real columns are a prefix of each block)
+            int pos = col;
+            if (sort && real(col)) pos = rank < real0 ? rank : kB + (rank - real0);
+            out_col[col] = pos;
+        }
     }
     __syncthreads();
     if (rotated_any && tid < kEvdWThreads) {
@@ -906,6 +907,17 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         if (rotated_any) atomicAdd(&stats[1], 1ull);
         if (off_bits) atomicMax(&stats[0], off_bits);
     }
+}
+
+// Wait-limit check of mbar_wait (see mixed_wait_limit_check).
+__global__ void mx_wait_limit_check(long long limit_ns, int arrive, int *status)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    if (arrive) mbar_arrive(&bar);
+    if (!mbar_wait(&bar, 0, limit_ns)) record_status(status, kDevWaitTimeout);
 }
 
 // ============================================================================
@@ -1590,6 +1602,13 @@ int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const
     ms.last_tc_off = tc_off;
     ms.last_f64_off = f64_off;
     if (sweeps) *sweeps = tc_sweeps + f64_sweeps;
+    return JSVD_OK;
+}
+
+int mixed_wait_limit_check(long long limit_ns, bool arrive, int *status, cudaStream_t st)
+{
+    mx_wait_limit_check<<<1, 32, 0, st>>>(limit_ns, arrive ? 1 : 0, status);
+    JSVD_CUDA_TRY(cudaGetLastError());
     return JSVD_OK;
 }
 

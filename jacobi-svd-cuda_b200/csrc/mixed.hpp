@@ -24,6 +24,12 @@ void mixed_release_thread_cache();
 // The calling thread's options (jsvd_mixed_set_options).
 const jsvd_mixed_options &mixed_options();
 
+// Wait-limit check of the tensor-core kernels' mbarrier wait: one thread
+// initialises an mbarrier and waits on its first phase with limit_ns;
+// `arrive` makes it arrive first (the wait then completes at once).  On
+// expiry kDevWaitTimeout is written to *status.
+int mixed_wait_limit_check(long long limit_ns, bool arrive, int *status, cudaStream_t st);
+
 // Smallest column count the blocked engine takes (narrower inputs go to the
 // plain sweep).
 constexpr int kMixedMinCols = 128;

@@ -40,6 +40,7 @@
 #include "dgemm.hpp"
 #include "internal.hpp"
 #include "layout.cuh"
+#include "mixed.hpp"
 #include "plain.hpp"
 
 namespace jsvd {
@@ -394,6 +395,29 @@ __device__ __forceinline__ long long global_ns()
     return t;
 }
 
+// Waits until the CTAs lo and hi (and CTA 0 when need0) have completed g
+// rounds (acquire loads of their flags); false after limit_ns.
+__device__ __forceinline__ bool wait_for_rounds(const int *flags, int lo, int hi, bool need0, int g,
+                                                long long limit_ns)
+{
+    const long long t0 = global_ns();
+    for (;;) {
+        const int f1 = ld_acquire_gpu(flags + lo);
+        const int f2 = ld_acquire_gpu(flags + hi);
+        const int f3 = ld_acquire_gpu(flags + 0);
+        if (f1 >= g && f2 >= g && (!need0 || f3 >= g)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+
+// Wait-limit check: thread 0 waits, as a persistent-sweep CTA does, for
+// flags[0] to reach round 1, with a short limit; on expiry it records
+// kDevWaitTimeout like the sweep.  Nothing sets the flag during the launch.
+__global__ void wait_limit_check_kernel(const int *flags, long long limit_ns, int *status)
+{
+    if (threadIdx.x == 0 && !wait_for_rounds(flags, 0, 0, false, 1, limit_ns)) atomicExch(status, (int)kDevWaitTimeout);
+}
+
 // Column of circle position pos in round r (-1 for the dummy of an odd n).
 __device__ __forceinline__ int circle_col(int n, int L, int r, int pos)
 {
@@ -421,22 +445,8 @@ __global__ void __launch_bounds__(T) plain_sweep_persistent(double *__restrict__
     for (int r = 0; r < rounds; ++r) {
         const int g = g0 + r;
         if (r > 0) {
-            if (t == 0) {
-                int ok = 1;
-                const long long t0 = global_ns();
-                for (;;) {
-                    const int f1 = ld_acquire_gpu(flags + dep_lo);
-                    const int f2 = ld_acquire_gpu(flags + dep_hi);
-                    const int f3 = ld_acquire_gpu(flags + 0);
-                    if (f1 >= g && f2 >= g && (k_lo != 1 || f3 >= g)) break;
-                    if (global_ns() - t0 > kSpinLimitNs) {
-                        atomicExch(status, (int)kDevWaitTimeout);
-                        ok = 0;
-                        break;
-                    }
-                }
-                s_ok = ok;
-            }
+            if (t == 0) s_ok = wait_for_rounds(flags, dep_lo, dep_hi, k_lo == 1, g, kSpinLimitNs) ? 1 : 0;
+            if (t == 0 && !s_ok) atomicExch(status, (int)kDevWaitTimeout);
             __syncthreads();
             if (!s_ok) return;
         }
@@ -1018,6 +1028,48 @@ int PlainPlan::run(const double *d_a, double *out_u, double *out_sigma, double *
 }  // namespace jsvd
 
 using namespace jsvd;
+
+extern "C" int jsvd_test_wait_limit(int which, int limit_ms, int preset, int *device_status, double *elapsed_ms)
+{
+    return c_entry([&]() -> int {
+        set_last_error(JSVD_OK, "");
+        if (which != 0 && which != 1) return invalid_argument("which must be 0 (round flags) or 1 (mbarrier).");
+        if (limit_ms < 1 || limit_ms > 2000) return invalid_argument("limit_ms must be in [1, 2000].");
+        int *d = nullptr;  // [0] the awaited flag, [1] the device status word
+        JSVD_CUDA_TRY(cudaMalloc(&d, 2 * sizeof(int)));
+        ScopeExit release([&] { cudaFree(d); });
+        const int init[2] = {preset ? 1 : 0, 0};
+        JSVD_CUDA_TRY(cudaMemcpy(d, init, sizeof(init), cudaMemcpyHostToDevice));
+        cudaEvent_t ev[2] = {};
+        for (auto &e : ev) JSVD_CUDA_TRY(cudaEventCreate(&e));
+        ScopeExit destroy([&] {
+            for (auto &e : ev) cudaEventDestroy(e);
+        });
+        const long long limit_ns = (long long)limit_ms * 1000000LL;
+        JSVD_CUDA_TRY(cudaEventRecord(ev[0], 0));
+        if (which == 0) {
+            wait_limit_check_kernel<<<1, 32>>>(d, limit_ns, d + 1);
+            JSVD_CUDA_TRY(cudaGetLastError());
+        } else if (int rc = mixed_wait_limit_check(limit_ns, preset != 0, d + 1, 0); rc != JSVD_OK) {
+            return rc;
+        }
+        JSVD_CUDA_TRY(cudaEventRecord(ev[1], 0));
+        JSVD_CUDA_TRY(cudaEventSynchronize(ev[1]));
+        int st = 0;
+        JSVD_CUDA_TRY(cudaMemcpy(&st, d + 1, sizeof(int), cudaMemcpyDeviceToHost));
+        float ms = 0.f;
+        JSVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        if (device_status) *device_status = st;
+        if (elapsed_ms) *elapsed_ms = ms;
+        if (st == kDevWaitTimeout) {
+            set_last_error(JSVD_ERR_RUNTIME, std::string(which == 0 ? "A round-flag" : "An mbarrier") +
+                                                 " wait stopped at its limit (device status " + std::to_string(st) +
+                                                 ").");
+            return JSVD_ERR_RUNTIME;
+        }
+        return JSVD_OK;
+    });
+}
 
 extern "C" int jsvd_round_robin_schedule(int n, int form, int *out, size_t capacity, size_t *needed)
 {

@@ -81,14 +81,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 // Waits for the phase with the given parity to complete; false after
-// kTcWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// limit_ns (kTcWaitLimitNs in the kernels; shorter in the wait-limit check).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit_ns = kTcWaitLimitNs)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = tc_global_ns();
     for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (tc_global_ns() - t0 > kTcWaitLimitNs) return false;
+        if (tc_global_ns() - t0 > limit_ns) return false;
     }
 }
 

@@ -198,6 +198,7 @@ def exported_symbols() -> list[str]:
         "jsvd_round_robin_schedule", "jsvd_plain_set_vpass_in_global", "jsvd_server_poll",
         "jsvd_mixed_options_default", "jsvd_mixed_set_options", "jsvd_mixed_svd", "jsvd_mixed_svd_device",
         "jsvd_mixed_stats_get", "jsvd_mixed_stats_reset", "jsvd_dgemm_device", "jsvd_mixed_test_round",
+        "jsvd_test_wait_limit",
         "jsvd_mixed_sweep_history",
     ]
 
@@ -304,6 +305,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_dgemm_device.restype = I
         L.jsvd_mixed_test_round.argtypes = [I, P, I, I, I, P]
         L.jsvd_mixed_test_round.restype = I
+        L.jsvd_test_wait_limit.argtypes = [I, I, I, ctypes.POINTER(I), ctypes.POINTER(D)]
+        L.jsvd_test_wait_limit.restype = I
         L.jsvd_mixed_sweep_history.argtypes = [ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double),
                                                ctypes.POINTER(ctypes.c_ulonglong), I]
         L.jsvd_mixed_sweep_history.restype = I
@@ -525,6 +528,18 @@ def mixed_sweep_history() -> list[tuple[int, float, int]]:
 def mixed_test_round(kind: int, d_x, rows: int, cols: int, rnd: int, d_gw) -> None:
     """One block round of the mixed engine's kernels (0 TC Gram, 1 FP64 Gram, 2 TC rotation, 3 FP64 rotation)."""
     check(lib().jsvd_mixed_test_round(kind, d_x, rows, cols, rnd, d_gw))
+
+
+def test_wait_limit(which: int, limit_ms: int, preset: bool = False) -> tuple[int, int, float]:
+    """Runs one bounded device wait with a short limit: which 0 = the
+    persistent sweep's wait on another CTA's round flag, 1 = the tensor-core
+    kernels' mbarrier wait.  With preset the awaited flag is set (the barrier
+    arrived on) beforehand.  Returns (return code, device status word,
+    elapsed ms); a wait that ran out gives JSVD_ERR_RUNTIME and status 2."""
+    st = ctypes.c_int(-1)
+    ms = ctypes.c_double(0.0)
+    rc = lib().jsvd_test_wait_limit(which, limit_ms, 1 if preset else 0, ctypes.byref(st), ctypes.byref(ms))
+    return int(rc), int(st.value), float(ms.value)
 
 
 def dgemm_device(op_a: str, op_b: str, m: int, n: int, k: int, alpha: float, d_a, lda: int, d_b, ldb: int,

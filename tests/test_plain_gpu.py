@@ -107,7 +107,10 @@ def _golden():
     if not os.path.exists(p):
         return None, []
     with open(p) as f:
-        return json.load(f), sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+        summ = json.load(f)
+    # only the fixtures recorded from the reference's own runs; other .npz
+    # files in the folder (the oracle-made tall-case sigma) are not
+    return summ, sorted(q for q in glob.glob(os.path.join(GOLDEN, "*.npz")) if os.path.basename(q)[:-4] in summ["cases"])
 
 
 _SUMMARY, _CASES = _golden()
