@@ -483,51 +483,80 @@ __global__ void __launch_bounds__(kRot64Threads)
 // Block eigen-solve (FP64, both phases)
 // ============================================================================
 
-constexpr int kEvdThreads = 512;      // warps 0-7: W; warps 8-14: G; warp 15: the angles
-constexpr int kEvdWThreads = 256;     // 4 threads per row of W
+constexpr int kEvdThreads = 512;      // warps 0-7: W (and 48 blocks of G); warps 8-14: G; warp 15: the angles
+constexpr int kEvdWThreads = 256;     // a warp per (half of the rows, quarter of the slots) of W
 constexpr int kEvdBulkFirst = 256;    // first thread of the G update
 constexpr int kEvdBulkThreads = 224;  // warps 8-14
 constexpr int kEvdLD = kW + 2;        // even: every row starts on a 16-byte boundary (vector loads of slot pairs)
-constexpr int kTriBlocks = (kW / 2) * (kW / 2 + 1) / 2;  // 2x2 blocks (a <= b) of the 32 x 32 block grid
-constexpr int kEvdBulkIters = (kTriBlocks + kEvdBulkThreads - 1) / kEvdBulkThreads;
+constexpr int kOffBlocks = (kW / 2) * (kW / 2 - 1) / 2;  // 2x2 blocks (a < b) of the 32 x 32 block grid
+constexpr int kEvdBulkIters = 2;      // blocks per G thread (the last 48 go to W threads 0-47)
 constexpr int kEvdRounds = kW - 1;
 constexpr int kEvdMaxInner = 8;
 constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD;
+static_assert(kOffBlocks - kEvdBulkIters * kEvdBulkThreads <= kEvdWThreads, "G blocks left for the W warps");
 
 // Rotation of [pp pq; pq qq] that annihilates pq, with the reference's
-// threshold test (|pq| > tau sqrt(pp qq), squared, and |pq| > 1e-300).
-// With d = qq - pp, e = 2 pq and rho = 1 / sqrt(d^2 + e^2), the double angle
-// has cos 2theta = |d| rho and sin 2theta = |e| rho (the smaller rotation,
-// |theta| <= pi/4, Rutishauser's choice of root), and the half-angle
-// identities give
+// threshold test (|pq| > tau sqrt(pp qq), squared, and |pq| > 1e-300), in
+// two parts: evd_prepare takes what depends on the diagonal only (known a
+// round ahead), evd_rotation the rest once pq is known.
+//   t = tan(theta), the smaller root of t^2 + 2 zeta t - 1 = 0 with
+//   zeta = (qq - pp) / (2 pq) (Rutishauser's choice), c = 1 / sqrt(1 + t^2),
+//   s = t c, sign(t) = sign(e) for d = qq - pp >= 0 and -sign(e) otherwise
+//   (e = 2 pq).
+// Small angles (x = |e| / (2 |d|) <= 2^-15): the series t = x - x^3 + 2x^5
+// and c = 1 - t^2/2 + 3t^4/8 are exact to rounding without their last
+// terms (relative size below 2^-59), so t = x (1 - x^2), c = 1 - t^2 / 2:
+// one multiplication by the precomputed 1 / (2 |d|) and three fused
+// operations.  Otherwise, with rho = 1 / sqrt(d^2 + e^2), cos 2theta =
+// |d| rho and sin 2theta = |e| rho, and the half-angle identities give
 //   c^2 = (1 + cos 2theta) / 2 in [1/2, 1],  c = c^2 / sqrt(c^2),
-//   |s| = sin 2theta / (2c),  |t| = |s| / c,
-// with sign(t) = sign(s) = sign(e) for d >= 0 and -sign(e) otherwise: two
-// reciprocal square roots and no division on the serial chain, no
-// cancellation (c^2 >= 1/2).  d and e are scaled by a power of two when
-// their magnitude could over- or underflow d^2 + e^2.  The rotation is
-// computed unconditionally and replaced by the identity when the test fails.
-__device__ __forceinline__ bool evd_rotation(double pp, double qq, double pq, double tau, double &c, double &s,
-                                             double &t)
+//   |s| = sin 2theta / (2c),  |t| = |s| / c:
+// two reciprocal square roots, no cancellation; d and e are scaled by a
+// power of two when their magnitude could over- or underflow d^2 + e^2.
+struct EvdPre {
+    double d;    // qq - pp
+    double thr;  // tau^2 max(pp, 0) max(qq, 0)
+    double r2;   // 1 / (2 |d|) (infinite for d = 0)
+};
+
+__device__ __forceinline__ EvdPre evd_prepare(double pp, double qq, double tau)
 {
-    const double a = fmax(pp, 0.0) * fmax(qq, 0.0);
-    const bool rot = fabs(pq) > 1.0e-300 && pq * pq > (tau * tau) * a;
-    double d = qq - pp, e = 2.0 * pq;
-    const double f = fmax(fabs(d), fabs(e));
-    if (rot && (f > 1.0e150 || f < 1.0e-150)) {
-        const int k = ilogb(f);
-        d = scalbn(d, -k);
-        e = scalbn(e, -k);
-    }
-    const double rho = rsqrt(fma(d, d, e * e));
-    const double c2 = fma(0.5 * fabs(d), rho, 0.5);
-    const double hs = (0.5 * fabs(e)) * rho;  // sin 2theta / 2
-    const double rc = rsqrt(c2);              // 1 / c
+    EvdPre p;
+    p.d = qq - pp;
+    p.thr = (tau * tau) * (fmax(pp, 0.0) * fmax(qq, 0.0));
+    p.r2 = 0.5 / fabs(p.d);
+    return p;
+}
+
+__device__ __forceinline__ bool evd_rotation(const EvdPre &p, double pq, double &c, double &s, double &t)
+{
+    const bool rot = fabs(pq) > 1.0e-300 && pq * pq > p.thr;
+    double d = p.d, e = 2.0 * pq;
     const double sg = ((d >= 0.0) == (e >= 0.0)) ? 1.0 : -1.0;
-    const double sa = hs * rc;
-    c = rot ? c2 * rc : 1.0;
+    const double x = fabs(e) * p.r2;
+    double ta, ca, sa;
+    if (x <= 0x1p-15) {
+        ta = fma(-(x * x), x, x);
+        ca = fma(-0.5 * ta, ta, 1.0);
+        sa = ta * ca;
+    } else {
+        const double f = fmax(fabs(d), fabs(e));
+        if (rot && (f > 1.0e150 || f < 1.0e-150)) {
+            const int k = ilogb(f);
+            d = scalbn(d, -k);
+            e = scalbn(e, -k);
+        }
+        const double rho = rsqrt(fma(d, d, e * e));
+        const double c2 = fma(0.5 * fabs(d), rho, 0.5);
+        const double hs = (0.5 * fabs(e)) * rho;  // sin 2theta / 2
+        const double rc = rsqrt(c2);              // 1 / c
+        ca = c2 * rc;
+        sa = hs * rc;
+        ta = sa * rc;
+    }
+    c = rot ? ca : 1.0;
     s = rot ? sg * sa : 0.0;
-    t = rot ? sg * (sa * rc) : 0.0;
+    t = rot ? sg * ta : 0.0;
     return rot;
 }
 
@@ -553,9 +582,10 @@ __device__ __forceinline__ int evd_next_slot(int s)
 // G is symmetric and only its upper triangle (in slot coordinates) is kept.
 __device__ __forceinline__ int evd_upper(int s, int t) { return s <= t ? s * kEvdLD + t : t * kEvdLD + s; }
 
-// W in registers, in slots.  Row `row` of W is held by four consecutive
-// lanes: quarter q owns pairs 8q .. 8q+7 (slots 16q .. 16q+15, local index
-// j <-> pair 8q + j), w[2j] = first, w[2j+1] = second.
+// W in registers, in slots.  Warp w < 8 holds rows 32 (w & 1) + lane of
+// quarter q = w >> 1 of the slots (pairs 8q .. 8q+7, slots 16q .. 16q+15,
+// local index j <-> pair 8q + j), w[2j] = first, w[2j+1] = second: every
+// lane of a warp applies the same eight rotations (one broadcast load each).
 __device__ __forceinline__ void evd_w_rotate(double (&w)[16], const double2 *cs, int q)
 {
 #pragma unroll
@@ -567,13 +597,11 @@ __device__ __forceinline__ void evd_w_rotate(double (&w)[16], const double2 *cs,
     }
 }
 
-// Advance of the circle for one thread's quarter row: first[8q - 1] comes in
-// from the quarter below (lane - 1), second[8q + 8] from the quarter above
-// (lane + 1).
-__device__ __forceinline__ void evd_w_shift(double (&w)[16], int q)
+// Advance of the circle for one quarter row: up = first[8q - 1] of the
+// quarter below, down = second[8q + 8] of the quarter above (both from the
+// warps holding them, through shared memory).
+__device__ __forceinline__ void evd_w_advance(double (&w)[16], int q, double up, double down)
 {
-    const double up = __shfl_up_sync(0xffffffffu, w[14], 1);    // first[8q - 1]
-    const double down = __shfl_down_sync(0xffffffffu, w[1], 1);  // second[8q + 8]
     double f[8], s[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -594,22 +622,26 @@ __device__ __forceinline__ void evd_w_shift(double (&w)[16], int q)
 // 64 x 64 FP64 upper triangle.  Cyclic two-sided Jacobi, at most
 // inner_sweeps sweeps of 63 rounds of 32 disjoint index pairs, in slot
 // coordinates (above), software pipelined so that a round costs one barrier
-// and the angle chain runs beside the update, on three groups of warps:
+// and the angle chain runs beside the update:
 //   * G (upper triangle, slot coordinates) is double-buffered: round r reads
 //     buffer r%2 and writes buffer (r+1)%2 already advanced to round r+1's
 //     slots, so every thread reads and writes the same addresses in every
 //     round (kept in registers, no table lookups);
-//   * warps 8-14 apply round r to G by 2 x 2 blocks of slot pairs (a, b),
-//     a <= b (two 16-byte loads, every output written once, the unrotated
-//     ones copied: c = 1, s = 0 reproduce them);
-//   * warps 0-7 apply it to W (registers, 4 lanes per row);
-//   * warp 15 meanwhile derives the angles of round r+1 from buffer r%2 and
-//     round r's rotations: pair k of round r+1 takes its first index from
-//     pair k-1 of round r (pair 0 for k <= 1) and its second from pair k+1
-//     (pair 31 for k = 31), so its diagonal entries are round r's annihilated
+//   * warps 8-14 (and threads 0-47) apply round r to the off-diagonal 2 x 2
+//     blocks of slot pairs (a, b), a < b (two 16-byte loads, four stores, the
+//     unrotated blocks copied: c = 1, s = 0 reproduce them);
+//   * warps 0-7 apply it to W (registers; the advance of the circle across
+//     quarters goes through shared memory and completes a round later);
+//   * warp 15 (lane k: pair k) writes the diagonal blocks (the annihilated
+//     pairs) and derives the angles of round r+1 from buffer r%2 and round
+//     r's rotations: pair k of round r+1 takes its first index from pair k-1
+//     of round r (pair 0 for k <= 1) and its second from pair k+1 (pair 31
+//     for k = 31), so its diagonal entries are round r's annihilated
 //     diagonals and its off-diagonal entry is one element of one 2 x 2 block
 //     update, computed with the same operations as the update itself
-//     (bit-identical to what lands in the buffer).
+//     (bit-identical to what lands in the buffer).  Everything that depends
+//     on round r's angles only (the new diagonals, the neighbours' angles,
+//     the diagonal part of the rotation) is done before round r's barrier.
 // Writes W (64 x 64, column-major) and flags[pair] = 1 when some pair
 // rotated (else flags[pair] = 0 and W is left as it was).  stats[0] (as
 // double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over the input
@@ -623,7 +655,8 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     double *const G0 = dsm;                 // [64][66], buffer 0
     double *const G1 = dsm + kW * kEvdLD;   // [64][66], buffer 1
     __shared__ double2 cs[2][kW / 2];       // (c, s) of the 32 pairs, by round parity
-    __shared__ double cs_t[2][kW / 2];      // t
+    __shared__ double xf[2][4][kW];         // W advance: first[8q + 7] of quarter q, by row
+    __shared__ double xs[2][4][kW];         // W advance: second[8q] of quarter q, by row
     __shared__ unsigned rot_mask[2];
     __shared__ int sweep_any[kEvdMaxInner + 1];
     __shared__ int out_col[kW];
@@ -701,8 +734,8 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             }
         }
     }
-    // W rows: thread tid < 256 holds row tid/4, quarter tid&3 (slot layout above)
-    const int wrow = (tid >> 2) & 63, quarter = tid & 3;
+    // W: warp w < 8 holds rows 32 (w & 1) + lane, quarter w >> 1 of the slots
+    const int wrow = 32 * (warp & 1) + lane, quarter = (warp >> 1) & 3;
     double w[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) w[j] = (evd_slot_column(16 * quarter + j) == wrow) ? 1.0 : 0.0;
@@ -728,52 +761,84 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         }
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
-    // the 2 x 2 blocks a G thread updates in every round: pair indices
-    // (a | b << 8), the offset of the block's first row, and the four
-    // destinations (slot coordinates of round r+1, upper triangle), two per int
-    int blk[kEvdBulkIters], rd[kEvdBulkIters], wr01[kEvdBulkIters], wr23[kEvdBulkIters];
+    // the off-diagonal 2 x 2 blocks a thread updates in every round (G threads
+    // two, threads 0-47 one): pair indices (a | b << 8), the offset of the
+    // block's first row, and the destinations of its four entries (slot
+    // coordinates of round r+1, upper triangle)
+    int blk[kEvdBulkIters], rd[kEvdBulkIters], w11[kEvdBulkIters], w12[kEvdBulkIters], w21[kEvdBulkIters],
+        w22[kEvdBulkIters];
 #pragma unroll
     for (int j = 0; j < kEvdBulkIters; ++j) {
-        const int bt = tid - kEvdBulkFirst;
-        int e = bt + j * kEvdBulkThreads;
+        int e = -1;
+        if (tid >= kEvdBulkFirst && tid < kEvdBulkFirst + kEvdBulkThreads)
+            e = tid - kEvdBulkFirst + j * kEvdBulkThreads;
+        else if (j == 0 && tid < kOffBlocks - kEvdBulkIters * kEvdBulkThreads)
+            e = kEvdBulkIters * kEvdBulkThreads + tid;
         blk[j] = -1;
-        rd[j] = wr01[j] = wr23[j] = 0;
-        if (bt >= 0 && bt < kEvdBulkThreads && e < kTriBlocks) {
+        rd[j] = w11[j] = w12[j] = w21[j] = w22[j] = 0;
+        if (e >= 0) {
             int a = 0;
-            while (e >= kW / 2 - a) {  // row-major over a <= b
-                e -= kW / 2 - a;
+            while (e >= kW / 2 - 1 - a) {  // row-major over a < b
+                e -= kW / 2 - 1 - a;
                 ++a;
             }
-            const int b = a + e;
+            const int b = a + 1 + e;
             const int pa = evd_next_slot(2 * a), qa = evd_next_slot(2 * a + 1);
             const int pb = evd_next_slot(2 * b), qb = evd_next_slot(2 * b + 1);
             blk[j] = a | (b << 8);
             rd[j] = 2 * a * kEvdLD + 2 * b;
-            if (a == b) {  // (pp, pq) and qq
-                wr01[j] = evd_upper(pa, pa) | (evd_upper(pa, qa) << 16);
-                wr23[j] = evd_upper(qa, qa);
-            } else {       // (11, 12) and (21, 22)
-                wr01[j] = evd_upper(pa, pb) | (evd_upper(pa, qb) << 16);
-                wr23[j] = evd_upper(qa, pb) | (evd_upper(qa, qb) << 16);
-            }
+            w11[j] = evd_upper(pa, pb);
+            w12[j] = evd_upper(pa, qb);
+            w21[j] = evd_upper(qa, pb);
+            w22[j] = evd_upper(qa, qb);
         }
     }
     const bool work = __syncthreads_or(need) != 0;
-    // warp 15: round 0's angles from buffer 0; it keeps its pair's input
-    // entries and rotation in registers from round to round
-    double a_pp = 0.0, a_qq = 0.0, a_pq = 0.0, a_c = 1.0, a_s = 0.0, a_t = 0.0;
+    // warp 15, lane k = pair k: its diagonal block's destinations, the block
+    // (A, B) holding the off-diagonal entry of its next pair, and its state
+    // from round to round: the pair's entries and rotation (pp, qq, pq, c, s,
+    // t, rotated), the rotated diagonals nd0, nd1, the next pair's diagonal
+    // part of the rotation (pre) and the angles of pairs A and B
+    const int A = lane <= 1 ? 0 : lane - 1, RA = lane == 1 ? 1 : 0;
+    const int B = lane <= 30 ? lane + 1 : 31, RB = lane <= 30 ? 1 : 0;
+    const int dpp = evd_upper(evd_next_slot(2 * lane), evd_next_slot(2 * lane));
+    const int dqq = evd_upper(evd_next_slot(2 * lane + 1), evd_next_slot(2 * lane + 1));
+    const int dpq = evd_upper(evd_next_slot(2 * lane), evd_next_slot(2 * lane + 1));
+    const int rab = 2 * A * kEvdLD + 2 * B;
+    double a_pq = 0.0, a_c = 1.0, a_s = 0.0, a_t = 0.0, nd0 = 0.0, nd1 = 0.0, ca = 1.0, sa = 0.0, cb = 1.0, sb = 0.0;
+    double n_pp = 0.0, n_qq = 0.0;
+    bool me = false;
+    EvdPre pre{0.0, 0.0, 0.0};
+    // after the angles of a round are known: the rotated diagonals, the next
+    // pair's diagonal entries and diagonal part, and the angles of A and B
+    auto prepare_next = [&](double pp, double qq) {
+        nd0 = fma(-a_t, a_pq, pp);
+        nd1 = fma(a_t, a_pq, qq);
+        // first index of pair k: pair k-1's first (k >= 2), pair 0's second
+        // (k = 1), its own (k = 0); second index: pair k+1's second (k <= 30),
+        // its own first (k = 31)
+        const double up = __shfl_up_sync(0xffffffffu, lane == 0 ? nd1 : nd0, 1);
+        const double dn = __shfl_down_sync(0xffffffffu, nd1, 1);
+        ca = __shfl_sync(0xffffffffu, a_c, A);
+        sa = __shfl_sync(0xffffffffu, a_s, A);
+        cb = __shfl_sync(0xffffffffu, a_c, B);
+        sb = __shfl_sync(0xffffffffu, a_s, B);
+        n_pp = lane == 0 ? nd0 : up;
+        n_qq = lane == 31 ? nd0 : dn;
+        pre = evd_prepare(n_pp, n_qq, tau);
+    };
     if (warp == 15 && work) {
-        a_pp = G0[2 * lane * kEvdLD + 2 * lane];
-        a_qq = G0[(2 * lane + 1) * kEvdLD + 2 * lane + 1];
+        const double pp = G0[2 * lane * kEvdLD + 2 * lane];
+        const double qq = G0[(2 * lane + 1) * kEvdLD + 2 * lane + 1];
         a_pq = G0[2 * lane * kEvdLD + 2 * lane + 1];
-        const bool rot = evd_rotation(a_pp, a_qq, a_pq, tau, a_c, a_s, a_t);
+        me = evd_rotation(evd_prepare(pp, qq, tau), a_pq, a_c, a_s, a_t);
         cs[0][lane] = make_double2(a_c, a_s);
-        cs_t[0][lane] = a_t;
-        const unsigned m = __ballot_sync(0xffffffffu, rot);
+        const unsigned m = __ballot_sync(0xffffffffu, me);
         if (lane == 0) {
             rot_mask[0] = m;
             if (m) sweep_any[0] = 1;
         }
+        prepare_next(pp, qq);
     }
     bool rotated_any = false;
     int gr = 0;  // rounds executed so far (buffer parity)
@@ -783,78 +848,68 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             const int cur = gr & 1;
             const double *Gin = cur ? G1 : G0;
             double *Gout = cur ? G0 : G1;
-            const unsigned rot = rot_mask[cur];
             if (warp < 8) {
-                if (rot) evd_w_rotate(w, cs[cur], quarter);
-                evd_w_shift(w, quarter);
-            } else if (warp < 15) {
+                if (gr > 0) {  // the advance after round gr - 1 (its boundary values are published)
+                    const int pb = gr & 1;
+                    const double up = quarter > 0 ? xf[pb][quarter - 1][wrow] : 0.0;
+                    const double down = quarter < 3 ? xs[pb][quarter + 1][wrow] : 0.0;
+                    evd_w_advance(w, quarter, up, down);
+                }
+                if (rot_mask[cur]) evd_w_rotate(w, cs[cur], quarter);
+                xf[cur ^ 1][quarter][wrow] = w[14];
+                xs[cur ^ 1][quarter][wrow] = w[1];
+            }
+            if (warp < 15) {
 #pragma unroll
                 for (int j = 0; j < kEvdBulkIters; ++j) {
                     if (blk[j] < 0) continue;
-                    const int a = blk[j] & 255, b = blk[j] >> 8;
-                    const double2 A = cs[cur][a], B = cs[cur][b];
+                    const double2 P = cs[cur][blk[j] & 255], Q = cs[cur][blk[j] >> 8];
                     const double2 x1 = *reinterpret_cast<const double2 *>(Gin + rd[j]);
-                    if (a == b) {
-                        // annihilated pair: g_pp - t g_pq, g_qq + t g_pq, 0
-                        const double gqq = Gin[rd[j] + kEvdLD + 1];
-                        const double t = cs_t[cur][a];
-                        const bool ra = (rot >> a) & 1u;
-                        Gout[wr01[j] & 0xffff] = fma(-t, x1.y, x1.x);
-                        Gout[wr01[j] >> 16] = ra ? 0.0 : x1.y;
-                        Gout[wr23[j]] = fma(t, x1.y, gqq);
-                        continue;
-                    }
                     const double2 x2 = *reinterpret_cast<const double2 *>(Gin + rd[j] + kEvdLD);
                     const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
-                    const double ca = A.x, sa = A.y, cb = B.x, sb = B.y;
                     // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
-                    const double h11 = fma(cb, g11, -(sb * g12)), h12 = fma(sb, g11, cb * g12);
-                    const double h21 = fma(cb, g21, -(sb * g22)), h22 = fma(sb, g21, cb * g22);
+                    const double h11 = fma(Q.x, g11, -(Q.y * g12)), h12 = fma(Q.y, g11, Q.x * g12);
+                    const double h21 = fma(Q.x, g21, -(Q.y * g22)), h22 = fma(Q.y, g21, Q.x * g22);
                     // rows (on the left, pair a)
-                    Gout[wr01[j] & 0xffff] = fma(ca, h11, -(sa * h21));
-                    Gout[wr01[j] >> 16] = fma(ca, h12, -(sa * h22));
-                    Gout[wr23[j] & 0xffff] = fma(sa, h11, ca * h21);
-                    Gout[wr23[j] >> 16] = fma(sa, h12, ca * h22);
+                    Gout[w11[j]] = fma(P.x, h11, -(P.y * h21));
+                    Gout[w12[j]] = fma(P.x, h12, -(P.y * h22));
+                    Gout[w21[j]] = fma(P.y, h11, P.x * h21);
+                    Gout[w22[j]] = fma(P.y, h12, P.x * h22);
                 }
             } else {
-                // warp 15: the angles of round gr + 1, from G_in and round gr's
-                // rotations (lane k held pair k of round gr)
-                const double nd0 = fma(-a_t, a_pq, a_pp);  // new diagonal of my first slot
-                const double nd1 = fma(a_t, a_pq, a_qq);   // ... of my second slot
-                // first index of pair k: pair k-1's first (k >= 2), pair 0's
-                // second (k = 1), its own (k = 0); second index: pair k+1's
-                // second (k <= 30), its own first (k = 31)
-                const double up = __shfl_up_sync(0xffffffffu, lane == 0 ? nd1 : nd0, 1);
-                const double dn = __shfl_down_sync(0xffffffffu, nd1, 1);
-                const int A = lane <= 1 ? 0 : lane - 1, RA = lane == 1 ? 1 : 0;
-                const int B = lane <= 30 ? lane + 1 : 31, RB = lane <= 30 ? 1 : 0;
-                const double ca = __shfl_sync(0xffffffffu, a_c, A), sa = __shfl_sync(0xffffffffu, a_s, A);
-                const double cb = __shfl_sync(0xffffffffu, a_c, B), sb = __shfl_sync(0xffffffffu, a_s, B);
                 // block (A, B), A < B: rows 2A and 2A+1, columns 2B and 2B+1
-                const double2 x1 = *reinterpret_cast<const double2 *>(Gin + 2 * A * kEvdLD + 2 * B);
-                const double2 x2 = *reinterpret_cast<const double2 *>(Gin + (2 * A + 1) * kEvdLD + 2 * B);
-                const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
+                const double2 x1 = *reinterpret_cast<const double2 *>(Gin + rab);
+                const double2 x2 = *reinterpret_cast<const double2 *>(Gin + rab + kEvdLD);
+                // round gr's diagonal block of pair k: g_pp - t g_pq, g_qq + t g_pq, 0
+                Gout[dpp] = nd0;
+                Gout[dqq] = nd1;
+                Gout[dpq] = me ? 0.0 : a_pq;
                 // element (RA, RB) of block (A, B) of G_out, as the update computes it
+                const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
                 const double h1 = RB ? fma(sb, g11, cb * g12) : fma(cb, g11, -(sb * g12));  // h1RB
                 const double h2 = RB ? fma(sb, g21, cb * g22) : fma(cb, g21, -(sb * g22));  // h2RB
                 a_pq = RA ? fma(sa, h1, ca * h2) : fma(ca, h1, -(sa * h2));
-                a_pp = lane == 0 ? nd0 : up;
-                a_qq = lane == 31 ? nd0 : dn;
-                const bool rot_next = evd_rotation(a_pp, a_qq, a_pq, tau, a_c, a_s, a_t);
+                me = evd_rotation(pre, a_pq, a_c, a_s, a_t);
                 cs[cur ^ 1][lane] = make_double2(a_c, a_s);
-                cs_t[cur ^ 1][lane] = a_t;
-                const unsigned m = __ballot_sync(0xffffffffu, rot_next);
+                const unsigned m = __ballot_sync(0xffffffffu, me);
                 if (lane == 0) {
                     rot_mask[cur ^ 1] = m;
                     if (m) sweep_any[r + 1 < kEvdRounds ? sw : sw + 1] = 1;
                 }
+                prepare_next(n_pp, n_qq);
             }
         }
         // sweep_any[sw] was last written before this sweep's final barrier
         if (!sweep_any[sw]) break;  // the same value in every thread
         rotated_any = true;
     }
-    __syncthreads();  // the last round's output buffer is complete
+    __syncthreads();  // the last round's output buffer and W boundary values are complete
+    if (warp < 8 && gr > 0) {  // the advance after the last round
+        const int pb = gr & 1;
+        const double up = quarter > 0 ? xf[pb][quarter - 1][wrow] : 0.0;
+        const double down = quarter < 3 ? xs[pb][quarter + 1][wrow] : 0.0;
+        evd_w_advance(w, quarter, up, down);
+    }
     const double *Gf = (gr & 1) ? G1 : G0;
     // Output order of W's columns.  With `sort`, the eigenvalues (G's
     // diagonal) are ranked and the lower-numbered block of the pair receives
