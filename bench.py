@@ -260,13 +260,20 @@ def oracle_sigma_check(wl, sigma) -> dict | None:
 def mixed_roofline(mst, hbm_peak: float, peak_kind: str, step_ms: float) -> dict:
     """Roofline of the mixed path's dominant kernel from the block rounds
     sampled inside the timed solves (events around each launch; rounds 0 and
-    rounds/2 of every sweep).  Algorithmic bytes per launch: a Gram launch
-    reads the whole swept factor once (rows_pad x cols_pad elements, 8 bytes
-    each: FP64, or the TF32 head and tail); a rotation launch reads and
-    writes the 64 columns of X and of V of every block pair that rotated
-    ((rows_pad + cols_pad) x 64 x 16 bytes per pair).  The eigen-solve moves
-    no DRAM bytes of note (a 64 x 64 Gram per pair): it is latency-bound, and
-    its share of the sampled time is reported beside."""
+    rounds/2 of every sweep).  Algorithmic work per launch:
+      * Gram: reads the whole swept factor once (rows_pad x cols_pad
+        elements, 8 bytes each: FP64, or the TF32 head and tail) - HBM bound;
+      * rotation: reads and writes the 64 columns of X and of V of every
+        block pair that rotated ((rows_pad + cols_pad) x 64 x 16 bytes per
+        pair) - HBM bound;
+      * eigen-solve: FP64 flops of the 64 x 64 two-sided Jacobi rounds of
+        every block pair (per inner round: 496 off-diagonal 2 x 2 blocks of
+        G at 24 flops, 32 diagonal blocks at 4, 64 x 32 rotations of W rows
+        at 6; 63 rounds per inner sweep) against the measured FP64 FMA
+        throughput - it is latency-bound, far below that peak.
+    The kernel with the largest sampled time share is reported."""
+    import jsvd
+
     k = {}
     for ph, g, e, r, n, pairs in (("tc", mst.tc_gram_ms, mst.tc_evd_ms, mst.tc_rot_ms, mst.tc_sampled_rounds,
                                    mst.tc_sampled_pairs),
@@ -277,28 +284,42 @@ def mixed_roofline(mst, hbm_peak: float, peak_kind: str, step_ms: float) -> dict
                      "rot_pairs_per_launch": pairs / n, "rounds": int(n)}
     rp, cp = mst.rows_pad, mst.cols_pad
     total = {name: sum(v[name + "_us"] * v["rounds"] for v in k.values()) for name in ("gram", "evd", "rot")}
-    cands = []
-    for ph, v in k.items():
-        gb = rp * cp * 8.0
-        cands.append((v["gram_us"] * v["rounds"], {"kernel": "mx_gram_tc" if ph == "tc" else "mx_gram_f64",
-                                                     "bytes": gb, "us": v["gram_us"]}))
-        rb = v["rot_pairs_per_launch"] * (rp + cp) * 64 * 16.0
-        cands.append((v["rot_us"] * v["rounds"], {"kernel": "mx_rot_tc" if ph == "tc" else "mx_rot_f64",
-                                                    "bytes": rb, "us": v["rot_us"]}))
-    if not cands:
+    if not k:
         return {"bound": "hbm", "kernel": None, "achieved": 0.0, "peak": hbm_peak, "unit": "GB/s", "frac": 0.0,
                 "traffic": None}
-    _, top = max(cands, key=lambda x: x[0])
-    achieved = top["bytes"] / (top["us"] * 1e-6) / 1e9
+    inner = int(jsvd.mixed_options().inner_sweeps)
+    evd_flops = mst.block_pairs * inner * 63 * (496 * 24 + 32 * 4 + 64 * 32 * 6)
+    kernels = {}
+    for ph, v in k.items():
+        tcp = ph == "tc"
+        kernels["mx_gram_tc" if tcp else "mx_gram_f64"] = {
+            "bound": "hbm", "us": v["gram_us"], "work": rp * cp * 8.0, "share": v["gram_us"] * v["rounds"]}
+        kernels["mx_rot_tc" if tcp else "mx_rot_f64"] = {
+            "bound": "hbm", "us": v["rot_us"], "work": v["rot_pairs_per_launch"] * (rp + cp) * 64 * 16.0,
+            "share": v["rot_us"] * v["rounds"]}
+        e = kernels.setdefault("mx_evd", {"bound": "fp64", "us": 0.0, "work": float(evd_flops), "share": 0.0,
+                                          "rounds": 0})
+        e["share"] += v["evd_us"] * v["rounds"]
+        e["rounds"] += v["rounds"]
+    kernels["mx_evd"]["us"] = kernels["mx_evd"]["share"] / max(1, kernels["mx_evd"]["rounds"])
     tsum = max(1e-9, sum(total.values()))
-    return {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-            "peak_kind": peak_kind, "frac": achieved / hbm_peak,
-            "traffic": PROFILED_TRAFFIC.get((top["kernel"], rp, cp)),
-            "avg_launch_us": top["us"], "algorithmic_bytes_per_launch": top["bytes"],
-            "sampled_kernel_share": {kk: vv / tsum for kk, vv in total.items()},
-            "per_phase": k, "note": "the eigen-solve (mx_evd) is latency-bound (64 x 64 FP64 Jacobi per block "
-                                    "pair, no DRAM traffic); its share of the sampled kernel time is under "
-                                    "sampled_kernel_share"}
+    name, top = max(kernels.items(), key=lambda kv: kv[1]["share"])
+    common = {"kernel": name, "avg_launch_us": top["us"], "sampled_kernel_share": {kk: vv / tsum for kk, vv in
+                                                                                    total.items()},
+              "per_phase": k}
+    if top["bound"] == "fp64":
+        fp64_peak = jsvd.probe_fp64_tflops()
+        achieved = top["work"] / (top["us"] * 1e-6) / 1e12
+        return {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "peak_kind": "measured FP64 FMA probe (jsvd_probe_fp64_tflops)", "frac": achieved / fp64_peak,
+                "traffic": None, "algorithmic_flops_per_launch": top["work"], **common,
+                "note": "the block eigen-solve is latency-bound: one CTA per block pair runs 63 dependent "
+                        "rounds per inner sweep (one barrier and one angle chain each); its DRAM traffic is "
+                        "the 64 x 64 Gram partials in and W out"}
+    achieved = top["work"] / (top["us"] * 1e-6) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "peak_kind": peak_kind,
+            "frac": achieved / hbm_peak, "traffic": PROFILED_TRAFFIC.get((name, rp, cp)),
+            "algorithmic_bytes_per_launch": top["work"], **common}
 
 
 def run_ours(args, rank: int, world: int, device):
@@ -1091,6 +1112,16 @@ def main():
         line = run_serve(args, rank, world, device)
     elif args.workload == "large":
         line = run_large(args, rank, world, device)
+    elif args.workload == "large_device":
+        # the large graded/clustered matrix solved from device memory only
+        # (no file pipeline): the form the kernel profiles are captured on
+        path = args.path if args.path in ("mixed", "precond") else "mixed"
+        res = run_large_device(args, device, path, steps=args.steps, warmup=args.warmup)
+        line = {"metric": "SVDs/s", "value": res["value"], "unit": "SVD/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * res["s_per_svd"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, on device)",
+                "config": {"workload": f"{args.large_m}x{args.large_n} FP64 graded + clustered sigma, device-resident",
+                           "path": path}, **{k: v for k, v in res.items() if k not in ("value", "unit")}}
     else:
         line = run_ours(args, rank, world, device)
     if world > 1:
