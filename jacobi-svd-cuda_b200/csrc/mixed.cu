@@ -485,14 +485,16 @@ __global__ void __launch_bounds__(kRot64Threads)
 
 constexpr int kEvdThreads = 512;      // warps 0-7: W (and 48 blocks of G); warps 8-14: G; warp 15: the angles
 constexpr int kEvdWThreads = 256;     // a warp per (half of the rows, quarter of the slots) of W
-constexpr int kEvdBulkFirst = 256;    // first thread of the G update
 constexpr int kEvdBulkThreads = 224;  // warps 8-14
-constexpr int kEvdLD = kW + 2;        // even: every row starts on a 16-byte boundary (vector loads of slot pairs)
+constexpr int kEvdQ = kW / 2 + 1;     // row stride of a quadrant of G (odd: column accesses hit distinct banks)
+constexpr int kEvdQuad = (kW / 2) * kEvdQ;  // one 32 x 33 quadrant
+constexpr int kEvdG = 3 * kEvdQuad;   // G: first-first, first-second, second-second quadrants
+constexpr int kEvdTmpLD = kW + 1;     // the input Gram in column coordinates (set-up only)
 constexpr int kOffBlocks = (kW / 2) * (kW / 2 - 1) / 2;  // 2x2 blocks (a < b) of the 32 x 32 block grid
 constexpr int kEvdBulkIters = 2;      // blocks per G thread (the last 48 go to W threads 0-47)
 constexpr int kEvdRounds = kW - 1;
 constexpr int kEvdMaxInner = 8;
-constexpr size_t kEvdSmem = sizeof(double) * 2 * kW * kEvdLD;
+constexpr size_t kEvdSmem = sizeof(double) * (kEvdG + kW * kEvdTmpLD);  // G0, then G1 / the set-up buffer
 static_assert(kOffBlocks - kEvdBulkIters * kEvdBulkThreads <= kEvdWThreads, "G blocks left for the W warps");
 
 // Rotation of [pp pq; pq qq] that annihilates pq, with the reference's
@@ -503,11 +505,12 @@ static_assert(kOffBlocks - kEvdBulkIters * kEvdBulkThreads <= kEvdWThreads, "G b
 //   zeta = (qq - pp) / (2 pq) (Rutishauser's choice), c = 1 / sqrt(1 + t^2),
 //   s = t c, sign(t) = sign(e) for d = qq - pp >= 0 and -sign(e) otherwise
 //   (e = 2 pq).
-// Small angles (x = |e| / (2 |d|) <= 2^-15): the series t = x - x^3 + 2x^5
-// and c = 1 - t^2/2 + 3t^4/8 are exact to rounding without their last
-// terms (relative size below 2^-59), so t = x (1 - x^2), c = 1 - t^2 / 2:
-// one multiplication by the precomputed 1 / (2 |d|) and three fused
-// operations.  Otherwise, with rho = 1 / sqrt(d^2 + e^2), cos 2theta =
+// Small angles (x = |e| / (2 |d|) <= 2^-6): t = (sqrt(1 + 4x^2) - 1) / (2x)
+// = x - x^3 + 2x^5 - 5x^7 + 14x^9 - ... (Catalan-number coefficients) and
+// c = (1 + t^2)^(-1/2) = 1 - z/2 + 3z^2/8 - 5z^3/16 + 35z^4/128 - ...
+// (z = t^2): the terms left out are below 2^-54 relative, so both series,
+// evaluated by Horner's rule from the precomputed 1 / (2 |d|), are exact to
+// rounding: ten fused operations and no square root or division.  Otherwise, with rho = 1 / sqrt(d^2 + e^2), cos 2theta =
 // |d| rho and sin 2theta = |e| rho, and the half-angle identities give
 //   c^2 = (1 + cos 2theta) / 2 in [1/2, 1],  c = c^2 / sqrt(c^2),
 //   |s| = sin 2theta / (2c),  |t| = |s| / c:
@@ -516,7 +519,7 @@ static_assert(kOffBlocks - kEvdBulkIters * kEvdBulkThreads <= kEvdWThreads, "G b
 struct EvdPre {
     double d;    // qq - pp
     double thr;  // tau^2 max(pp, 0) max(qq, 0)
-    double r2;   // 1 / (2 |d|) (infinite for d = 0)
+    double r2;   // 1 / (2 |d|) (infinite for d = 0), to about one ulp
 };
 
 __device__ __forceinline__ EvdPre evd_prepare(double pp, double qq, double tau)
@@ -524,7 +527,18 @@ __device__ __forceinline__ EvdPre evd_prepare(double pp, double qq, double tau)
     EvdPre p;
     p.d = qq - pp;
     p.thr = (tau * tau) * (fmax(pp, 0.0) * fmax(qq, 0.0));
-    p.r2 = 0.5 / fabs(p.d);
+    // 1 / (2 |d|) by Newton's iteration r <- r (2 - |d| r) from a
+    // single-precision reciprocal (two steps: 2^-23 -> 2^-46 -> rounding);
+    // outside the single-precision range, by division
+    const double ad = fabs(p.d);
+    if (ad > 1.0e-30 && ad < 1.0e30) {
+        double r = (double)__frcp_rn((float)ad);
+        r = r * fma(-ad, r, 2.0);
+        r = r * fma(-ad, r, 2.0);
+        p.r2 = 0.5 * r;
+    } else {
+        p.r2 = 0.5 / ad;
+    }
     return p;
 }
 
@@ -535,9 +549,18 @@ __device__ __forceinline__ bool evd_rotation(const EvdPre &p, double pq, double 
     const double sg = ((d >= 0.0) == (e >= 0.0)) ? 1.0 : -1.0;
     const double x = fabs(e) * p.r2;
     double ta, ca, sa;
-    if (x <= 0x1p-15) {
-        ta = fma(-(x * x), x, x);
-        ca = fma(-0.5 * ta, ta, 1.0);
+    if (x <= 0x1p-6) {
+        const double y = x * x;
+        double p = fma(14.0, y, -5.0);
+        p = fma(p, y, 2.0);
+        p = fma(p, y, -1.0);
+        p = fma(p, y, 1.0);
+        ta = x * p;
+        const double z = ta * ta;
+        double q = fma(35.0 / 128.0, z, -5.0 / 16.0);
+        q = fma(q, z, 3.0 / 8.0);
+        q = fma(q, z, -0.5);
+        ca = fma(q, z, 1.0);
         sa = ta * ca;
     } else {
         const double f = fmax(fabs(d), fabs(e));
@@ -579,8 +602,37 @@ __device__ __forceinline__ int evd_next_slot(int s)
     if (s == 62) return 63;
     return (s & 1) ? s - 2 : s + 2;
 }
-// G is symmetric and only its upper triangle (in slot coordinates) is kept.
-__device__ __forceinline__ int evd_upper(int s, int t) { return s <= t ? s * kEvdLD + t : t * kEvdLD + s; }
+// G is symmetric; it is kept as three 32 x 33 quadrants indexed by pair:
+// FF[k][l] = G(first k, first l) and SS[k][l] = G(second k, second l) for
+// k <= l, FS[k][l] = G(first k, second l) for all k, l.  The update of block
+// (a, b) reads FF[a][b], FS[a][b], FS[b][a], SS[a][b] and, after the circle's
+// advance (first k -> first k+1, second k -> second k-1), writes
+// FF[a+1][b+1], FS[a+1][b-1], FS[b+1][a-1], SS[a-1][b-1] (except at the
+// circle's ends): with the odd row stride every one of those eight addresses
+// falls in bank (a + b + constant) mod 16, so a warp whose 32 blocks cover
+// each residue of a + b twice accesses G without bank conflicts.
+__device__ __forceinline__ int evd_off(int s, int t)
+{
+    const int ks = s >> 1, kt = t >> 1;
+    if ((s & 1) == (t & 1)) return ((s & 1) ? 2 * kEvdQuad : 0) + min(ks, kt) * kEvdQ + max(ks, kt);
+    return (s & 1) ? kEvdQuad + kt * kEvdQ + ks : kEvdQuad + ks * kEvdQ + kt;
+}
+
+// The k-th off-diagonal block (a < b) with (a + b) mod 16 == r, in order of
+// a + b, then a.  Residues r even have 30 blocks, odd 32.
+__device__ __forceinline__ int2 evd_block_of(int r, int k)
+{
+    for (int d = r; d <= kW - 3; d += 16) {
+        if (d < 1) continue;
+        const int lo = max(0, d - (kW / 2 - 1)), hi = (d - 1) >> 1;
+        const int cnt = hi - lo + 1;
+        if (cnt > 0) {
+            if (k < cnt) return make_int2(lo + k, d - lo - k);
+            k -= cnt;
+        }
+    }
+    return make_int2(-1, -1);
+}
 
 // W in registers, in slots.  Warp w < 8 holds rows 32 (w & 1) + lane of
 // quarter q = w >> 1 of the slots (pairs 8q .. 8q+7, slots 16q .. 16q+15,
@@ -653,7 +705,7 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
 {
     extern __shared__ __align__(16) double dsm[];
     double *const G0 = dsm;                 // [64][66], buffer 0
-    double *const G1 = dsm + kW * kEvdLD;   // [64][66], buffer 1
+    double *const G1 = dsm + kEvdG;         // buffer 1 (and, at set-up, the Gram in column coordinates)
     __shared__ double2 cs[2][kW / 2];       // (c, s) of the 32 pairs, by round parity
     __shared__ double xf[2][4][kW];         // W advance: first[8q + 7] of quarter q, by row
     __shared__ double xs[2][4][kW];         // W advance: second[8q] of quarter q, by row
@@ -726,10 +778,10 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
             for (int k = 0; k < 4; ++k) {
                 const int r = 4 * j + k;
                 if (kind == 0) {
-                    G1[r * kEvdLD + c] = acc[i][k];
+                    G1[r * kEvdTmpLD + c] = acc[i][k];
                 } else if (r <= c) {  // the FP64 Gram kernel writes the upper triangle only: mirror it
-                    G1[r * kEvdLD + c] = acc[i][k];
-                    G1[c * kEvdLD + r] = acc[i][k];
+                    G1[r * kEvdTmpLD + c] = acc[i][k];
+                    G1[c * kEvdTmpLD + r] = acc[i][k];
                 }
             }
         }
@@ -750,10 +802,10 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     for (int e = tid; e < kW * kW; e += kEvdThreads) {
         const int r = e >> 6, c = e & 63;
         if (r <= c) {
-            const double g = r < c ? 0.5 * (G1[r * kEvdLD + c] + G1[c * kEvdLD + r]) : G1[r * kEvdLD + r];
-            G0[evd_upper(evd_column_slot(r), evd_column_slot(c))] = g;
+            const double g = r < c ? 0.5 * (G1[r * kEvdTmpLD + c] + G1[c * kEvdTmpLD + r]) : G1[r * kEvdTmpLD + r];
+            G0[evd_off(evd_column_slot(r), evd_column_slot(c))] = g;
             if (r < c) {
-                const double a = fmax(G1[r * kEvdLD + r], 0.0) * fmax(G1[c * kEvdLD + c], 0.0);
+                const double a = fmax(G1[r * kEvdTmpLD + r], 0.0) * fmax(G1[c * kEvdTmpLD + c], 0.0);
                 const double d = sqrt(a);
                 if (d > 0.0) off = fmax(off, fabs(g) / d);
                 if (fabs(g) > 1.0e-300 && g * g > (tau * tau) * a) need = 1;
@@ -761,36 +813,32 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         }
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
-    // the off-diagonal 2 x 2 blocks a thread updates in every round (G threads
-    // two, threads 0-47 one): pair indices (a | b << 8), the offset of the
-    // block's first row, and the destinations of its four entries (slot
-    // coordinates of round r+1, upper triangle)
-    int blk[kEvdBulkIters], rd[kEvdBulkIters], w11[kEvdBulkIters], w12[kEvdBulkIters], w21[kEvdBulkIters],
-        w22[kEvdBulkIters];
+    // the off-diagonal 2 x 2 blocks a thread updates in every round: a group
+    // of 32 blocks per warp and iteration holding each residue of a + b mod 16
+    // twice (groups 0-13: G warps 8-14, two each; group 14: warp 0; group 15,
+    // 16 blocks: lanes 0-15 of warp 1).  Per block: the pair indices
+    // (a | b << 8), the offsets of FF[a][b] (FS[a][b] and SS[a][b] follow at
+    // fixed distances) and of FS[b][a], and the destinations of its four
+    // entries after the advance, two per int
+    int blk[kEvdBulkIters], rof[kEvdBulkIters], w01[kEvdBulkIters], w23[kEvdBulkIters];
 #pragma unroll
     for (int j = 0; j < kEvdBulkIters; ++j) {
-        int e = -1;
-        if (tid >= kEvdBulkFirst && tid < kEvdBulkFirst + kEvdBulkThreads)
-            e = tid - kEvdBulkFirst + j * kEvdBulkThreads;
-        else if (j == 0 && tid < kOffBlocks - kEvdBulkIters * kEvdBulkThreads)
-            e = kEvdBulkIters * kEvdBulkThreads + tid;
+        int g = -1;
+        if (warp >= 8 && warp < 15) g = 2 * (warp - 8) + j;
+        else if (j == 0 && warp == 0) g = 14;
+        else if (j == 0 && warp == 1 && lane < 16) g = 15;
         blk[j] = -1;
-        rd[j] = w11[j] = w12[j] = w21[j] = w22[j] = 0;
-        if (e >= 0) {
-            int a = 0;
-            while (e >= kW / 2 - 1 - a) {  // row-major over a < b
-                e -= kW / 2 - 1 - a;
-                ++a;
-            }
-            const int b = a + 1 + e;
+        rof[j] = w01[j] = w23[j] = 0;
+        if (g >= 0) {
+            const int2 ab = g < 15 ? evd_block_of(lane >> 1, 2 * g + (lane & 1))
+                                   : evd_block_of(2 * (lane >> 1) + 1, 30 + (lane & 1));
+            const int a = ab.x, b = ab.y;
             const int pa = evd_next_slot(2 * a), qa = evd_next_slot(2 * a + 1);
             const int pb = evd_next_slot(2 * b), qb = evd_next_slot(2 * b + 1);
             blk[j] = a | (b << 8);
-            rd[j] = 2 * a * kEvdLD + 2 * b;
-            w11[j] = evd_upper(pa, pb);
-            w12[j] = evd_upper(pa, qb);
-            w21[j] = evd_upper(qa, pb);
-            w22[j] = evd_upper(qa, qb);
+            rof[j] = evd_off(2 * a, 2 * b) | (evd_off(2 * a + 1, 2 * b) << 16);
+            w01[j] = evd_off(pa, pb) | (evd_off(pa, qb) << 16);
+            w23[j] = evd_off(qa, pb) | (evd_off(qa, qb) << 16);
         }
     }
     const bool work = __syncthreads_or(need) != 0;
@@ -801,10 +849,10 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     // part of the rotation (pre) and the angles of pairs A and B
     const int A = lane <= 1 ? 0 : lane - 1, RA = lane == 1 ? 1 : 0;
     const int B = lane <= 30 ? lane + 1 : 31, RB = lane <= 30 ? 1 : 0;
-    const int dpp = evd_upper(evd_next_slot(2 * lane), evd_next_slot(2 * lane));
-    const int dqq = evd_upper(evd_next_slot(2 * lane + 1), evd_next_slot(2 * lane + 1));
-    const int dpq = evd_upper(evd_next_slot(2 * lane), evd_next_slot(2 * lane + 1));
-    const int rab = 2 * A * kEvdLD + 2 * B;
+    const int dpp = evd_off(evd_next_slot(2 * lane), evd_next_slot(2 * lane));
+    const int dqq = evd_off(evd_next_slot(2 * lane + 1), evd_next_slot(2 * lane + 1));
+    const int dpq = evd_off(evd_next_slot(2 * lane), evd_next_slot(2 * lane + 1));
+    const int rab = evd_off(2 * A, 2 * B), rba = evd_off(2 * A + 1, 2 * B);
     double a_pq = 0.0, a_c = 1.0, a_s = 0.0, a_t = 0.0, nd0 = 0.0, nd1 = 0.0, ca = 1.0, sa = 0.0, cb = 1.0, sb = 0.0;
     double n_pp = 0.0, n_qq = 0.0;
     bool me = false;
@@ -828,9 +876,9 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         pre = evd_prepare(n_pp, n_qq, tau);
     };
     if (warp == 15 && work) {
-        const double pp = G0[2 * lane * kEvdLD + 2 * lane];
-        const double qq = G0[(2 * lane + 1) * kEvdLD + 2 * lane + 1];
-        a_pq = G0[2 * lane * kEvdLD + 2 * lane + 1];
+        const double pp = G0[evd_off(2 * lane, 2 * lane)];
+        const double qq = G0[evd_off(2 * lane + 1, 2 * lane + 1)];
+        a_pq = G0[evd_off(2 * lane, 2 * lane + 1)];
         me = evd_rotation(evd_prepare(pp, qq, tau), a_pq, a_c, a_s, a_t);
         cs[0][lane] = make_double2(a_c, a_s);
         const unsigned m = __ballot_sync(0xffffffffu, me);
@@ -864,28 +912,26 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
                 for (int j = 0; j < kEvdBulkIters; ++j) {
                     if (blk[j] < 0) continue;
                     const double2 P = cs[cur][blk[j] & 255], Q = cs[cur][blk[j] >> 8];
-                    const double2 x1 = *reinterpret_cast<const double2 *>(Gin + rd[j]);
-                    const double2 x2 = *reinterpret_cast<const double2 *>(Gin + rd[j] + kEvdLD);
-                    const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
+                    const double *f = Gin + (rof[j] & 0xffff);
+                    const double g11 = f[0], g12 = f[kEvdQuad], g22 = f[2 * kEvdQuad], g21 = Gin[rof[j] >> 16];
                     // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
                     const double h11 = fma(Q.x, g11, -(Q.y * g12)), h12 = fma(Q.y, g11, Q.x * g12);
                     const double h21 = fma(Q.x, g21, -(Q.y * g22)), h22 = fma(Q.y, g21, Q.x * g22);
                     // rows (on the left, pair a)
-                    Gout[w11[j]] = fma(P.x, h11, -(P.y * h21));
-                    Gout[w12[j]] = fma(P.x, h12, -(P.y * h22));
-                    Gout[w21[j]] = fma(P.y, h11, P.x * h21);
-                    Gout[w22[j]] = fma(P.y, h12, P.x * h22);
+                    Gout[w01[j] & 0xffff] = fma(P.x, h11, -(P.y * h21));
+                    Gout[w01[j] >> 16] = fma(P.x, h12, -(P.y * h22));
+                    Gout[w23[j] & 0xffff] = fma(P.y, h11, P.x * h21);
+                    Gout[w23[j] >> 16] = fma(P.y, h12, P.x * h22);
                 }
             } else {
-                // block (A, B), A < B: rows 2A and 2A+1, columns 2B and 2B+1
-                const double2 x1 = *reinterpret_cast<const double2 *>(Gin + rab);
-                const double2 x2 = *reinterpret_cast<const double2 *>(Gin + rab + kEvdLD);
+                // block (A, B), A < B: FF[A][B], FS[A][B], FS[B][A], SS[A][B]
+                const double g11 = Gin[rab], g12 = Gin[rab + kEvdQuad], g22 = Gin[rab + 2 * kEvdQuad];
+                const double g21 = Gin[rba];
                 // round gr's diagonal block of pair k: g_pp - t g_pq, g_qq + t g_pq, 0
                 Gout[dpp] = nd0;
                 Gout[dqq] = nd1;
                 Gout[dpq] = me ? 0.0 : a_pq;
                 // element (RA, RB) of block (A, B) of G_out, as the update computes it
-                const double g11 = x1.x, g12 = x1.y, g21 = x2.x, g22 = x2.y;
                 const double h1 = RB ? fma(sb, g11, cb * g12) : fma(cb, g11, -(sb * g12));  // h1RB
                 const double h2 = RB ? fma(sb, g21, cb * g22) : fma(cb, g21, -(sb * g22));  // h2RB
                 a_pq = RA ? fma(sa, h1, ca * h2) : fma(ca, h1, -(sa * h2));
@@ -928,7 +974,7 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         auto real = [&](int c) { return c < kB ? c < real0 : c - kB < real1; };
         auto lam = [&](int c) {
             const int s = evd_column_slot(c);
-            return Gf[s * kEvdLD + s];
+            return Gf[evd_off(s, s)];
         };
         const bool desc = bp.x < bp.y;  // local order follows global order when bp.x < bp.y
         const double l1 = lam(col);
