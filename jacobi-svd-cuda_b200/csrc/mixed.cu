@@ -510,7 +510,8 @@ static_assert(kOffBlocks - kEvdBulkIters * kEvdBulkThreads <= kEvdWThreads, "G b
 // c = (1 + t^2)^(-1/2) = 1 - z/2 + 3z^2/8 - 5z^3/16 + 35z^4/128 - ...
 // (z = t^2): the terms left out are below 2^-54 relative, so both series,
 // evaluated by Horner's rule from the precomputed 1 / (2 |d|), are exact to
-// rounding: ten fused operations and no square root or division.  Otherwise, with rho = 1 / sqrt(d^2 + e^2), cos 2theta =
+// rounding: ten fused operations and no square root or division.  Called by
+// a full warp; the path is chosen for the whole warp.  Otherwise, with rho = 1 / sqrt(d^2 + e^2), cos 2theta =
 // |d| rho and sin 2theta = |e| rho, and the half-angle identities give
 //   c^2 = (1 + cos 2theta) / 2 in [1/2, 1],  c = c^2 / sqrt(c^2),
 //   |s| = sin 2theta / (2c),  |t| = |s| / c:
@@ -549,7 +550,9 @@ __device__ __forceinline__ bool evd_rotation(const EvdPre &p, double pq, double 
     const double sg = ((d >= 0.0) == (e >= 0.0)) ? 1.0 : -1.0;
     const double x = fabs(e) * p.r2;
     double ta, ca, sa;
-    if (x <= 0x1p-6) {
+    // one path for the whole warp (the caller's 32 lanes are all active): the
+    // series when every rotating lane's angle is small, else the exact form
+    if (__all_sync(0xffffffffu, x <= 0x1p-6 || !rot)) {
         const double y = x * x;
         double p = fma(14.0, y, -5.0);
         p = fma(p, y, 2.0);
@@ -706,7 +709,8 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     extern __shared__ __align__(16) double dsm[];
     double *const G0 = dsm;                 // [64][66], buffer 0
     double *const G1 = dsm + kEvdG;         // buffer 1 (and, at set-up, the Gram in column coordinates)
-    __shared__ double2 cs[2][kW / 2];       // (c, s) of the 32 pairs, by round parity
+    __shared__ double2 cs[2][kW / 2];       // (c, s) of the 32 pairs, by round parity (W: broadcast loads)
+    __shared__ double cs_c[2][kW / 2], cs_s[2][kW / 2];  // the same, apart (G: 8-byte loads of many pairs)
     __shared__ double xf[2][4][kW];         // W advance: first[8q + 7] of quarter q, by row
     __shared__ double xs[2][4][kW];         // W advance: second[8q] of quarter q, by row
     __shared__ unsigned rot_mask[2];
@@ -814,9 +818,10 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
     }
     if (off > 0.0) atomicMax(&off_bits, (unsigned long long)__double_as_longlong(off));
     // the off-diagonal 2 x 2 blocks a thread updates in every round: a group
-    // of 32 blocks per warp and iteration holding each residue of a + b mod 16
-    // twice (groups 0-13: G warps 8-14, two each; group 14: warp 0; group 15,
-    // 16 blocks: lanes 0-15 of warp 1).  Per block: the pair indices
+    // of 32 blocks per warp and iteration in which each half-warp holds every
+    // residue of a + b mod 16 once (shared memory serves a half-warp's 8-byte
+    // accesses per wavefront; groups 0-13: G warps 8-14, two each; group 14:
+    // warp 0; group 15, 16 blocks of odd residue: lanes 0-15 of warp 1).  Per block: the pair indices
     // (a | b << 8), the offsets of FF[a][b] (FS[a][b] and SS[a][b] follow at
     // fixed distances) and of FS[b][a], and the destinations of its four
     // entries after the advance, two per int
@@ -830,8 +835,8 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         blk[j] = -1;
         rof[j] = w01[j] = w23[j] = 0;
         if (g >= 0) {
-            const int2 ab = g < 15 ? evd_block_of(lane >> 1, 2 * g + (lane & 1))
-                                   : evd_block_of(2 * (lane >> 1) + 1, 30 + (lane & 1));
+            const int2 ab = g < 15 ? evd_block_of(lane & 15, 2 * g + (lane >> 4))
+                                   : evd_block_of(2 * (lane & 7) + 1, 30 + (lane >> 3));
             const int a = ab.x, b = ab.y;
             const int pa = evd_next_slot(2 * a), qa = evd_next_slot(2 * a + 1);
             const int pb = evd_next_slot(2 * b), qb = evd_next_slot(2 * b + 1);
@@ -881,6 +886,8 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         a_pq = G0[evd_off(2 * lane, 2 * lane + 1)];
         me = evd_rotation(evd_prepare(pp, qq, tau), a_pq, a_c, a_s, a_t);
         cs[0][lane] = make_double2(a_c, a_s);
+        cs_c[0][lane] = a_c;
+        cs_s[0][lane] = a_s;
         const unsigned m = __ballot_sync(0xffffffffu, me);
         if (lane == 0) {
             rot_mask[0] = m;
@@ -911,7 +918,9 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
 #pragma unroll
                 for (int j = 0; j < kEvdBulkIters; ++j) {
                     if (blk[j] < 0) continue;
-                    const double2 P = cs[cur][blk[j] & 255], Q = cs[cur][blk[j] >> 8];
+                    const int ia = blk[j] & 255, ib = blk[j] >> 8;
+                    const double2 P = make_double2(cs_c[cur][ia], cs_s[cur][ia]);
+                    const double2 Q = make_double2(cs_c[cur][ib], cs_s[cur][ib]);
                     const double *f = Gin + (rof[j] & 0xffff);
                     const double g11 = f[0], g12 = f[kEvdQuad], g22 = f[2 * kEvdQuad], g21 = Gin[rof[j] >> 16];
                     // columns: [p' q'] = [c p - s q, s p + c q] (on the right, pair b)
@@ -937,6 +946,8 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
                 a_pq = RA ? fma(sa, h1, ca * h2) : fma(ca, h1, -(sa * h2));
                 me = evd_rotation(pre, a_pq, a_c, a_s, a_t);
                 cs[cur ^ 1][lane] = make_double2(a_c, a_s);
+                cs_c[cur ^ 1][lane] = a_c;
+                cs_s[cur ^ 1][lane] = a_s;
                 const unsigned m = __ballot_sync(0xffffffffu, me);
                 if (lane == 0) {
                     rot_mask[cur ^ 1] = m;
