@@ -287,7 +287,7 @@ def mixed_roofline(mst, hbm_peak: float, peak_kind: str, step_ms: float) -> dict
     if not k:
         return {"bound": "hbm", "kernel": None, "achieved": 0.0, "peak": hbm_peak, "unit": "GB/s", "frac": 0.0,
                 "traffic": None}
-    inner = int(jsvd.mixed_options().inner_sweeps)
+    inner = int(jsvd.mixed_resolved_options(mst.cols_pad).inner_sweeps)
     evd_flops = mst.block_pairs * inner * 63 * (496 * 24 + 32 * 4 + 64 * 32 * 6)
     kernels = {}
     for ph, v in k.items():

@@ -384,17 +384,28 @@ void jsvd_precond_stats_reset(void);
 typedef struct jsvd_mixed_options {
     int precondition;   /* 1 (default): blocked sweeps on X = P^T after the two QRs; 0: on A   */
     int tc_max_sweeps;  /* tensor-core sweeps at most; 0 = FP64 blocked sweeps only; -1 (default) =
-                           automatic: 4 for at most 2048 columns, else 10                       */
+                           automatic (the built-in tuning table, by column count)              */
     double tc_tol;      /* phase 1 ends when no pair's |g_pq| / sqrt(g_pp g_qq) exceeds this    */
-    int inner_sweeps;   /* two-sided sweeps per 64 x 64 block eigen-solve (default 1)           */
+    int inner_sweeps;   /* two-sided sweeps per 64 x 64 block eigen-solve; 0 (default) =
+                           automatic (the built-in tuning table)                               */
     int refine;         /* refinement: 0 = blocked FP64 sweeps (default), 1 = plain scalar sweep */
     int f64_max_sweeps; /* cap on refinement sweeps; 0 = the config's max_sweeps                  */
-    int gram_splits;    /* row splits of each block-pair Gram; 0 = automatic                      */
+    int gram_splits;    /* row splits of each block-pair Gram; 0 = automatic (the table's value,
+                           else enough CTAs to cover the GPU twice)                           */
     int sort;           /* 1 (default): each block eigen-solve gives the larger eigenvalues to the
                            lower-numbered block (decreasing column norms, de Rijk's ordering)   */
 } jsvd_mixed_options;
 
 void jsvd_mixed_options_default(jsvd_mixed_options *o);
+/* The mixed path's built-in tuning table (csrc/mixed_tuning_table.h, made by
+ * jacobi-svd-cuda_b200/mixed_autotune.py on a B200): entry i is out[4i..4i+3]
+ * = {largest column count it covers (0 = any), tc_max_sweeps, inner_sweeps,
+ * gram_splits (0 = automatic)}; the first covering entry resolves a solve's
+ * automatic options.  Writes at most `capacity` entries (out may be NULL)
+ * and returns the number of entries.  No counterpart in the reference (its
+ * only tuner is auto_tune_layout_transpose_threshold, src/kernels.cu:1078-1126,
+ * which this table's role extends to the blocked path). */
+int jsvd_mixed_builtin_tuning(int *out, int capacity);
 /* Options of later jsvd_mixed_svd* calls on the calling thread (NULL: defaults). */
 void jsvd_mixed_set_options(const jsvd_mixed_options *o);
 

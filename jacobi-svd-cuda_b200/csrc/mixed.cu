@@ -48,6 +48,7 @@
 #include "internal.hpp"
 #include "jsvd.h"
 #include "mixed.hpp"
+#include "mixed_tuning_table.h"
 #include "plain.hpp"
 #include "ptx.cuh"
 
@@ -1281,7 +1282,7 @@ jsvd_mixed_options default_options()
     o.precondition = 1;
     o.tc_max_sweeps = -1;
     o.tc_tol = 2e-5;
-    o.inner_sweeps = 1;
+    o.inner_sweeps = 0;
     o.refine = 0;
     o.f64_max_sweeps = 0;
     o.gram_splits = 0;
@@ -1602,16 +1603,40 @@ const jsvd_mixed_options &mixed_options() { return thread_options(); }
 
 void mixed_release_thread_cache() { work_cache().clear(); }
 
-int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const jsvd_mixed_options &o, double *u,
-                double *sigma, double *v, int *sweeps, cudaStream_t st)
+struct MixedTuning {
+    int max_cols;  // largest column count the entry covers (0 = any)
+    int tc_max_sweeps, inner_sweeps, gram_splits;
+};
+constexpr MixedTuning kMixedTuning[] = JSVD_MIXED_TUNING_TABLE;
+constexpr int kMixedTuningCount = (int)(sizeof(kMixedTuning) / sizeof(kMixedTuning[0]));
+
+// The automatic options (tc_max_sweeps < 0, inner_sweeps <= 0, gram_splits
+// <= 0) resolved from the built-in table by the input's width: on narrow
+// inputs (few block pairs per round) a round costs about the same in either
+// phase, the block eigen-solves dominating, so the FP64 phase, which
+// converges quadratically, takes over early; on wide ones the 3xTF32 rounds
+// are the cheaper and phase 1 runs until tc_tol.
+jsvd_mixed_options resolve_options(const jsvd_mixed_options &o, int cols)
+{
+    const MixedTuning *t = &kMixedTuning[kMixedTuningCount - 1];
+    for (int i = 0; i < kMixedTuningCount; ++i)
+        if (kMixedTuning[i].max_cols == 0 || cols <= kMixedTuning[i].max_cols) {
+            t = &kMixedTuning[i];
+            break;
+        }
+    jsvd_mixed_options e = o;
+    if (e.tc_max_sweeps < 0) e.tc_max_sweeps = t->tc_max_sweeps;
+    if (e.inner_sweeps <= 0) e.inner_sweeps = t->inner_sweeps;
+    if (e.gram_splits <= 0) e.gram_splits = t->gram_splits;
+    return e;
+}
+
+int mixed_solve(const double *x, int rows, int cols, const jsvd_config &c, const jsvd_mixed_options &o_in,
+                double *u, double *sigma, double *v, int *sweeps, cudaStream_t st)
 {
     if (int rc = init_kernel_attributes(); rc != JSVD_OK) return rc;
-    // automatic cap on the tensor-core sweeps: on narrow inputs (few block
-    // pairs per round) a round costs about the same in either phase, the
-    // block eigen-solves dominating, so the FP64 phase, which converges
-    // quadratically, takes over early; on wide ones the 3xTF32 rounds are
-    // the cheaper and phase 1 runs until tc_tol
-    const int tc_max = o.tc_max_sweeps >= 0 ? o.tc_max_sweeps : (cols <= 2048 ? 4 : 10);
+    const jsvd_mixed_options o = resolve_options(o_in, cols);
+    const int tc_max = o.tc_max_sweeps;
     const bool tc = tc_max > 0;
     Work owned;
     ScopeExit release([&] { free_work(owned, st); });
@@ -1798,6 +1823,18 @@ extern "C" int jsvd_mixed_test_round(int kind, double *d_x, int rows, int cols, 
 extern "C" void jsvd_mixed_options_default(jsvd_mixed_options *o)
 {
     if (o) *o = default_options();
+}
+
+extern "C" int jsvd_mixed_builtin_tuning(int *out, int capacity)
+{
+    if (out != nullptr)
+        for (int i = 0; i < kMixedTuningCount && i < capacity; ++i) {
+            out[4 * i] = kMixedTuning[i].max_cols;
+            out[4 * i + 1] = kMixedTuning[i].tc_max_sweeps;
+            out[4 * i + 2] = kMixedTuning[i].inner_sweeps;
+            out[4 * i + 3] = kMixedTuning[i].gram_splits;
+        }
+    return kMixedTuningCount;
 }
 
 extern "C" void jsvd_mixed_set_options(const jsvd_mixed_options *o) { thread_options() = o ? *o : default_options(); }

@@ -198,7 +198,7 @@ def exported_symbols() -> list[str]:
         "jsvd_round_robin_schedule", "jsvd_plain_set_vpass_in_global", "jsvd_server_poll",
         "jsvd_mixed_options_default", "jsvd_mixed_set_options", "jsvd_mixed_svd", "jsvd_mixed_svd_device",
         "jsvd_mixed_stats_get", "jsvd_mixed_stats_reset", "jsvd_dgemm_device", "jsvd_mixed_test_round",
-        "jsvd_test_wait_limit",
+        "jsvd_test_wait_limit", "jsvd_mixed_builtin_tuning",
         "jsvd_mixed_sweep_history",
     ]
 
@@ -307,6 +307,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_mixed_test_round.restype = I
         L.jsvd_test_wait_limit.argtypes = [I, I, I, ctypes.POINTER(I), ctypes.POINTER(D)]
         L.jsvd_test_wait_limit.restype = I
+        L.jsvd_mixed_builtin_tuning.argtypes = [ctypes.POINTER(I), I]
+        L.jsvd_mixed_builtin_tuning.restype = I
         L.jsvd_mixed_sweep_history.argtypes = [ctypes.POINTER(I), ctypes.POINTER(ctypes.c_double),
                                                ctypes.POINTER(ctypes.c_ulonglong), I]
         L.jsvd_mixed_sweep_history.restype = I
@@ -528,6 +530,33 @@ def mixed_sweep_history() -> list[tuple[int, float, int]]:
 def mixed_test_round(kind: int, d_x, rows: int, cols: int, rnd: int, d_gw) -> None:
     """One block round of the mixed engine's kernels (0 TC Gram, 1 FP64 Gram, 2 TC rotation, 3 FP64 rotation)."""
     check(lib().jsvd_mixed_test_round(kind, d_x, rows, cols, rnd, d_gw))
+
+
+def mixed_builtin_tuning() -> list[tuple[int, int, int, int]]:
+    """The mixed path's built-in tuning table: (max_cols (0 = any),
+    tc_max_sweeps, inner_sweeps, gram_splits) per entry, in lookup order."""
+    n = lib().jsvd_mixed_builtin_tuning(None, 0)
+    buf = (ctypes.c_int * (4 * n))()
+    lib().jsvd_mixed_builtin_tuning(buf, n)
+    return [tuple(buf[4 * i:4 * i + 4]) for i in range(n)]
+
+
+def mixed_resolved_options(cols: int, opts: MixedOptions | None = None) -> MixedOptions:
+    """The options a mixed solve of `cols` columns runs with: the automatic
+    fields of `opts` (defaults when None) filled from the built-in table, as
+    the library does."""
+    o = opts if opts is not None else mixed_options()
+    table = mixed_builtin_tuning()
+    t = next((e for e in table if e[0] == 0 or cols <= e[0]), table[-1])
+    r = MixedOptions()
+    ctypes.memmove(ctypes.byref(r), ctypes.byref(o), ctypes.sizeof(MixedOptions))
+    if r.tc_max_sweeps < 0:
+        r.tc_max_sweeps = t[1]
+    if r.inner_sweeps <= 0:
+        r.inner_sweeps = t[2]
+    if r.gram_splits <= 0:
+        r.gram_splits = t[3]
+    return r
 
 
 def test_wait_limit(which: int, limit_ms: int, preset: bool = False) -> tuple[int, int, float]:
