@@ -11,8 +11,10 @@ jsvd_mixed_svd_device, over a grid of the tunable options:
   * the Gram row splits for the best pair.
 A candidate counts only if its sigma is within 1e-12 normwise of the
 analytic sigma.  Each candidate runs --reps times after one warm-up solve;
-the minimum is kept.  Entry i of the table covers widths up to shape i's
-width (the last covers all).  Rebuild the library (make) after writing.
+the minimum is kept.  A candidate replaces the library's current choice for
+that width only when it is more than 2% faster.  Entry i of the table covers
+widths up to shape i's width (the last covers all).  Rebuild the library
+(make) after writing.
 """
 from __future__ import annotations
 
@@ -45,7 +47,8 @@ def render_table(entries: list[tuple[int, int, int, int]], notes: list[str], met
         f" * Generated by jacobi-svd-cuda_b200/mixed_autotune.py on {meta['device']},",
         f" * {meta['date']}: {meta['workload']}; {meta['reps']} timed solves per",
         " * candidate after a warm-up, minimum kept; candidates with sigma off by",
-        " * more than 1e-12 normwise rejected.",
+        " * more than 1e-12 normwise rejected; a candidate replaces the previous",
+        " * choice only when it is more than 2% faster.",
         " *",
     ]
     lines += [" * " + n for n in notes]
@@ -115,6 +118,8 @@ def tune_shape(m: int, n: int, reps: int = 2, tc_caps=TC_CAPS, inner=INNER, spli
     'tried', 'rejected'."""
     import torch
 
+    import jsvd
+
     device = device or torch.device("cuda", torch.cuda.current_device())
     da, sig = test_matrix(m, n, device)
     outs = (torch.empty((m, n), dtype=torch.float64, device=device), torch.empty(n, dtype=torch.float64, device=device),
@@ -143,7 +148,13 @@ def tune_shape(m: int, n: int, reps: int = 2, tc_caps=TC_CAPS, inner=INNER, spli
         results[(cap, inn, sp)] = ms
     best = min(results, key=results.get)
     default_ms, _ = time_candidate(da, m, n, sig, outs, {}, reps)
-    return {"best": best, "best_ms": results[best], "default_ms": default_ms, "tried": tried, "rejected": rejected}
+    r = jsvd.mixed_resolved_options(n)
+    current = (int(r.tc_max_sweeps), int(r.inner_sweeps), int(r.gram_splits))
+    if results[best] > default_ms / 1.02:  # not clearly faster: keep the current choice
+        best, best_ms = current, default_ms
+    else:
+        best_ms = results[best]
+    return {"best": best, "best_ms": best_ms, "default_ms": default_ms, "tried": tried, "rejected": rejected}
 
 
 def main() -> int:
