@@ -473,25 +473,29 @@ int jsvd_dgemm_device(char op_a, char op_b, int m, int n, int k, double alpha, c
  * Continuous batching of SVD requests on the current device.  Replaces the
  * reference's thread-pool dispatch of one_sided_jacobi_svd per testcase
  * (src/pipeline.cpp:234-394, 754-863): requests are admitted against a
- * device-memory budget, small ones are gathered into batched launches while
- * earlier batches run, large ones run concurrently on worker streams.  Results
- * do not depend on what else is in flight (every path keeps the plain
- * arithmetic). */
+ * device-memory budget.  Small ones (A's FP64 copy fits a CTA's shared
+ * memory) are batched at sweep granularity: each admitted request keeps A and
+ * V on the device, every step runs one sweep of all active requests, the
+ * converged ones retire after it and queued ones join before the next step.
+ * Large ones run concurrently on worker streams.  Results do not depend on
+ * what else is in flight (every path keeps the plain arithmetic). */
 
 typedef struct jsvd_server jsvd_server;
 
 typedef struct jsvd_server_options {
     size_t device_budget_bytes; /* admission budget (0 = 40 GiB)                    */
-    int small_workers;          /* concurrent batched launches (0 = 2)             */
+    int small_workers;          /* sweep-stepping workers, each with its own active
+                                   set and stream (0 = 2)                           */
     int large_workers;          /* concurrent large solves, one stream each (0 = 4) */
-    int max_batch;              /* requests per batched launch (0 = 4096)           */
+    int max_batch;              /* active small requests per worker (0 = 4096)      */
     jsvd_config cfg;            /* epsilon, max_sweeps, threads_per_block           */
     int large_path;             /* 0 = plain sweep, 1 = QR-preconditioned, 2 = mixed  */
 } jsvd_server_options;
 
 typedef struct jsvd_server_stats {
     unsigned long long submitted, completed, failed;
-    unsigned long long batches, batched_requests, large_solves;
+    unsigned long long batches;          /* sweep steps of the small-request workers */
+    unsigned long long batched_requests, large_solves;
     double p50_ms, p99_ms, mean_ms; /* submit-to-completion latency */
     size_t peak_device_bytes, device_bytes_in_use;
 } jsvd_server_stats;

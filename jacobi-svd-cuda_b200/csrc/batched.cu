@@ -124,6 +124,54 @@ __device__ __forceinline__ double warp_norm2(const double *x, int m, int lane)
 __host__ __device__ constexpr int round_half(int n) { return (n / 2 + 2) & ~1; }
 __host__ __device__ constexpr size_t round_scratch_doubles(int n) { return (size_t)5 * round_half(n); }
 
+// One sweep (every round of the circle) of an m x n member whose columns
+// colA(c) and V live wherever the caller keeps them, by the whole CTA; true
+// when some pair rotated.  s_rot must be 0 on entry and is 0 again on return.
+// The same phases and operations as one sweep of batch_kernel (which keeps
+// its own copy of the loop: sharing it raised that kernel's register spills).
+template <class ColA>
+__device__ __forceinline__ bool batch_sweep(ColA colA, double *V, int m, int n, double eps, double *st_pp,
+                                            double *st_qq, double *st_pq, double2 *st_cs, int &s_rot)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int ne = n + (n & 1);
+    const int rounds = n >= 2 ? ne - 1 : 0;
+    const int npairs = n / 2;
+    for (int r = 0; r < rounds; ++r) {
+        // phase 1: dot products, one warp per pair
+        for (int k = warp; k < npairs; k += nwarps) {
+            const int2 pq = round_robin_pair(n, r, k);
+            double pp, qq, pqv;
+            warp_pair_stats(colA(pq.x), colA(pq.y), m, lane, pp, qq, pqv);
+            if (lane == 0) {
+                st_pp[k] = pp;
+                st_qq[k] = qq;
+                st_pq[k] = pqv;
+            }
+        }
+        __syncthreads();
+        // phase 2: angles, one thread per pair
+        for (int k = threadIdx.x; k < npairs; k += blockDim.x) {
+            double c, s;
+            if (rotation_params(st_pp[k], st_qq[k], st_pq[k], eps, c, s)) s_rot = 1;
+            st_cs[k] = make_double2(c, s);
+        }
+        __syncthreads();
+        // phase 3: rotations, one warp per pair
+        for (int k = warp; k < npairs; k += nwarps) {
+            const double2 g = st_cs[k];
+            if (g.x == 0.0) continue;
+            const int2 pq = round_robin_pair(n, r, k);
+            warp_rotate(colA(pq.x), colA(pq.y), m, V + (size_t)pq.x * n, V + (size_t)pq.y * n, n, lane, g.x, g.y);
+        }
+        __syncthreads();
+    }
+    const bool any = s_rot != 0;
+    __syncthreads();  // every thread has read the flag before it is reset
+    if (threadIdx.x == 0) s_rot = 0;
+    return any;
+}
+
 template <bool kAShared, bool kVShared>
 __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict__ descs, int count,
                                                     int *__restrict__ next, const void *__restrict__ a_all,
@@ -243,6 +291,77 @@ __global__ void __launch_bounds__(512) batch_kernel(const BatchDesc *__restrict_
         }
         if (sweeps_all != nullptr && threadIdx.x == 0) sweeps_all[idx] = sweeps;
         __syncthreads();  // the working copies are reused by the next matrix
+    }
+}
+
+// One sweep step of the sweep-granular batch (serving core): CTA i runs one
+// sweep of member i, whose state (A and V, FP64, column-major) stays in
+// global memory between steps.  On its first step (in != null) a member
+// starts from its row-major FP64 input with V = I, as batch_kernel does.  A
+// is worked on in shared memory, and V too when kVShared (else in place in
+// the state).  rotated[i] = 1 when some pair of the sweep rotated: a member
+// whose sweep did not rotate has converged, exactly where batch_kernel's
+// loop over sweeps stops.
+template <bool kVShared>
+__global__ void __launch_bounds__(256, 2) batch_step_kernel(const StepDesc *__restrict__ descs, double eps,
+                                                            int *__restrict__ rotated)
+{
+    extern __shared__ double smem[];
+    __shared__ int s_rot;
+    const StepDesc d = descs[blockIdx.x];
+    const int m = d.m, n = d.n;
+    const int half = round_half(n);
+    double *st_pp = smem, *st_qq = smem + half, *st_pq = smem + 2 * half;
+    double2 *st_cs = reinterpret_cast<double2 *>(smem + 3 * half);
+    double *A = smem + round_scratch_doubles(n);
+    double *gA = d.a, *gV = d.v;
+    double *V = kVShared ? A + (size_t)m * n : gV;
+    const size_t mn = (size_t)m * n, nn = (size_t)n * n;
+    if (d.in != nullptr) {
+        const double *src = d.in;
+        for (size_t e = threadIdx.x; e < mn; e += blockDim.x) {
+            const size_t r = e / n, c = e - r * n;
+            A[c * m + r] = src[e];
+        }
+        for (size_t e = threadIdx.x; e < nn; e += blockDim.x) V[e] = (e / n == e % n) ? 1.0 : 0.0;
+    } else {
+        for (size_t e = threadIdx.x; e < mn; e += blockDim.x) A[e] = gA[e];
+        if (kVShared)
+            for (size_t e = threadIdx.x; e < nn; e += blockDim.x) V[e] = gV[e];
+    }
+    if (threadIdx.x == 0) s_rot = 0;
+    __syncthreads();
+    bool any = false;
+    if (n >= 2) any = batch_sweep([&](int c) { return A + (size_t)c * m; }, V, m, n, eps, st_pp, st_qq, st_pq, st_cs, s_rot);
+    for (size_t e = threadIdx.x; e < mn; e += blockDim.x) gA[e] = A[e];
+    if (kVShared)
+        for (size_t e = threadIdx.x; e < nn; e += blockDim.x) gV[e] = V[e];
+    if (threadIdx.x == 0) rotated[blockIdx.x] = any ? 1 : 0;
+}
+
+// Outputs of retired members of the sweep-granular batch: sigma, V
+// (row-major) and optionally U (row-major) from the state, with
+// batch_kernel's formulas (CTA i: member i).
+__global__ void __launch_bounds__(256) batch_finish_kernel(const StepDesc *__restrict__ descs, double eps)
+{
+    const StepDesc d = descs[blockIdx.x];
+    const int m = d.m, n = d.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const double *gA = d.a, *gV = d.v;
+    double *sg = d.s_out;
+    for (int c = warp; c < n; c += nwarps) {
+        const double *x = gA + (size_t)c * m;
+        const double sc = sqrt(fmax(warp_norm2(x, m, lane), 0.0));
+        if (lane == 0) sg[c] = sc;
+        if (d.u_out != nullptr) {
+            double *u = d.u_out;
+            for (int i = lane; i < m; i += 32) u[(size_t)i * n + c] = (sc > eps) ? (x[i] / sc) : 0.0;
+        }
+    }
+    double *vo = d.v_out;
+    for (size_t e = threadIdx.x; e < (size_t)n * n; e += blockDim.x) {
+        const size_t r = e / n, c = e - r * n;
+        vo[e] = gV[c * n + r];
     }
 }
 
@@ -499,6 +618,110 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         if (first[c + 1] > first[c] && cudaEventElapsedTime(&cms, ts->c0[c], ts->c1[c]) == cudaSuccess)
             st.class_ms[c] += cms;
     }
+    return JSVD_OK;
+}
+
+}  // namespace jsvd
+
+using namespace jsvd;
+
+namespace jsvd {
+
+size_t step_smem(int m, int n, bool v_shared)
+{
+    return sizeof(double) * (round_scratch_doubles(n) + (size_t)m * n + (v_shared ? (size_t)n * n : 0));
+}
+
+bool step_fits(int m, int n, size_t *smem_cap_out)
+{
+    int dev = 0;
+    size_t cap = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || batch_smem_cap(dev, &cap) != JSVD_OK) return false;
+    if (smem_cap_out) *smem_cap_out = cap;
+    return step_smem(m, n, false) <= cap;
+}
+
+int StepScratch::ensure(int count)
+{
+    if (count <= cap) return JSVD_OK;
+    if (d_descs) cudaFree(d_descs);
+    if (d_rot) cudaFree(d_rot);
+    if (h_rot) cudaFreeHost(h_rot);
+    d_descs = nullptr;
+    d_rot = nullptr;
+    h_rot = nullptr;
+    cap = 0;
+    const int c = std::max(count, 256);
+    JSVD_CUDA_TRY(cudaMalloc((void **)&d_descs, sizeof(StepDesc) * 2 * c));
+    JSVD_CUDA_TRY(cudaMalloc((void **)&d_rot, sizeof(int) * c));
+    JSVD_CUDA_TRY(cudaMallocHost((void **)&h_rot, sizeof(int) * c));
+    cap = c;
+    return JSVD_OK;
+}
+
+StepScratch::~StepScratch()
+{
+    if (d_descs) cudaFree(d_descs);
+    if (d_rot) cudaFree(d_rot);
+    if (h_rot) cudaFreeHost(h_rot);
+}
+
+int batch_step(const std::vector<StepDesc> &descs, double eps, int *rotated, StepScratch &sc, cudaStream_t st)
+{
+    const int count = (int)descs.size();
+    if (count == 0) return JSVD_OK;
+    int dev = 0;
+    size_t cap = 0;
+    JSVD_CUDA_TRY(cudaGetDevice(&dev));
+    if (int rc = batch_smem_cap(dev, &cap); rc != JSVD_OK) return rc;
+    if (int rc = sc.ensure(count); rc != JSVD_OK) return rc;
+    // members whose V fits beside A in shared memory first, the others after
+    std::vector<int> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_partition(order.begin(), order.end(),
+                          [&](int i) { return step_smem(descs[i].m, descs[i].n, true) <= cap; });
+    std::vector<StepDesc> sorted(count);
+    size_t smem_vs = 0, smem_vg = 0;
+    int n_vs = 0;
+    for (int i = 0; i < count; ++i) {
+        const StepDesc &d = descs[order[i]];
+        sorted[i] = d;
+        if (step_smem(d.m, d.n, true) <= cap) {
+            smem_vs = std::max(smem_vs, step_smem(d.m, d.n, true));
+            ++n_vs;
+        } else {
+            if (step_smem(d.m, d.n, false) > cap) return invalid_argument("A step member does not fit shared memory.");
+            smem_vg = std::max(smem_vg, step_smem(d.m, d.n, false));
+        }
+    }
+    JSVD_CUDA_TRY(cudaMemcpyAsync(sc.d_descs, sorted.data(), sizeof(StepDesc) * count, cudaMemcpyHostToDevice, st));
+    static thread_local unsigned long long attr_done = 0;
+    if (dev < 64 && !(attr_done & (1ull << dev))) {
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(batch_step_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)cap));
+        JSVD_CUDA_TRY(cudaFuncSetAttribute(batch_step_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)cap));
+        attr_done |= 1ull << dev;
+    }
+    if (n_vs > 0) batch_step_kernel<true><<<n_vs, 256, smem_vs, st>>>(sc.d_descs, eps, sc.d_rot);
+    if (count > n_vs)
+        batch_step_kernel<false><<<count - n_vs, 256, smem_vg, st>>>(sc.d_descs + n_vs, eps, sc.d_rot + n_vs);
+    JSVD_CUDA_TRY(cudaGetLastError());
+    JSVD_CUDA_TRY(cudaMemcpyAsync(sc.h_rot, sc.d_rot, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+    JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < count; ++i) rotated[order[i]] = sc.h_rot[i];
+    return JSVD_OK;
+}
+
+int batch_finish(const std::vector<StepDesc> &descs, double eps, StepScratch &sc, cudaStream_t st)
+{
+    const int count = (int)descs.size();
+    if (count == 0) return JSVD_OK;
+    if (int rc = sc.ensure(count); rc != JSVD_OK) return rc;
+    StepDesc *d2 = sc.d_descs + sc.cap;  // the second half: the step's descriptors may still be read
+    JSVD_CUDA_TRY(cudaMemcpyAsync(d2, descs.data(), sizeof(StepDesc) * count, cudaMemcpyHostToDevice, st));
+    batch_finish_kernel<<<count, 256, 0, st>>>(d2, eps);
+    JSVD_CUDA_TRY(cudaGetLastError());
     return JSVD_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <vector>
 
 #include "jsvd.h"
 
@@ -40,5 +41,33 @@ struct BatchStats {
 
 BatchStats &batch_stats();
 int batch_solve(const BatchRequest &req, cudaStream_t stream);
+
+// Sweep-granular batching (the serving core's small requests).  A member's
+// state, A (m x n) and V (n x n), FP64 column-major, lives in device memory
+// between steps.
+struct StepDesc {
+    int m, n;
+    double *a, *v;        // state
+    const double *in;     // row-major FP64 input for the first step, else null
+    double *s_out, *v_out, *u_out;  // outputs written by batch_finish (u_out null: none)
+};
+
+// Device descriptors and flags reused from step to step (one per thread).
+struct StepScratch {
+    StepDesc *d_descs = nullptr;  // 2 * cap
+    int *d_rot = nullptr, *h_rot = nullptr;
+    int cap = 0;
+    int ensure(int count);
+    ~StepScratch();
+};
+
+// Whether an m x n member can take part (A and the round scratch fit one
+// CTA's shared memory).
+bool step_fits(int m, int n, size_t *smem_cap = nullptr);
+// One sweep of every member of `descs` (one CTA each); rotated[i] = 1 when
+// member i's sweep rotated a pair (0: converged).  Synchronises `st`.
+int batch_step(const std::vector<StepDesc> &descs, double eps, int *rotated, StepScratch &sc, cudaStream_t st);
+// sigma, V and U of retired members into `out` (asynchronous on `st`).
+int batch_finish(const std::vector<StepDesc> &descs, double eps, StepScratch &sc, cudaStream_t st);
 
 }  // namespace jsvd

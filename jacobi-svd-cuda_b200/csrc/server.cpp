@@ -7,9 +7,12 @@
 //   * admission reserves the request's device footprint against a memory
 //     budget and waits while the budget is exhausted;
 //   * "small" requests (the working copy of A fits a CTA's shared memory) are
-//     gathered by two batch workers: whatever is queued when a worker becomes
-//     free forms its next batch, so requests that arrive while a batch is on
-//     the GPU join the next one and two batches overlap on the device;
+//     batched at sweep granularity: a worker keeps every request it admitted
+//     on the device (A and V stay resident), runs one sweep of all of them per
+//     step (one CTA each), retires the ones whose sweep rotated nothing and,
+//     before the next step, admits queued requests into the room they freed -
+//     a request that arrives while others are on the GPU joins at the next
+//     sweep, not after the whole batch; two such workers overlap on the device;
 //   * "large" requests go to worker threads that each drive their own stream
 //     (plain path, per-thread plan cache), so several large solves overlap;
 //   * every path uses the plain path's arithmetic, so a request's result does
@@ -45,8 +48,8 @@ bool is_small(size_t m, size_t n) { return sizeof(double) * (m * n + 5 * (n / 2 
 
 size_t small_footprint(size_t m, size_t n, bool want_u)
 {
-    // A (FP64 input) + sigma + V + optional U + global V workspace
-    return sizeof(double) * (m * n + n + 2 * n * n + (want_u ? m * n : 0));
+    // state (A, V) + the FP64 input + outputs (sigma, V, optional U)
+    return sizeof(double) * (2 * m * n + n + 2 * n * n + (want_u ? m * n : 0));
 }
 
 size_t large_footprint(size_t m, size_t n, int path)
@@ -279,6 +282,22 @@ private:
         return got;
     }
 
+    // Takes queued requests while their footprints fit the budget, up to
+    // max_count, without waiting.
+    std::vector<Request *> try_admit(std::deque<Request *> &q, size_t max_count)
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        std::vector<Request *> got;
+        while (!stopping_ && !q.empty() && got.size() < max_count &&
+               in_use_ + q.front()->footprint <= opt_.device_budget_bytes) {
+            in_use_ += q.front()->footprint;
+            got.push_back(q.front());
+            q.pop_front();
+        }
+        peak_bytes_ = std::max(peak_bytes_, in_use_);
+        return got;
+    }
+
     void finish(const std::vector<Request *> &rs, int status, const std::string &err)
     {
         const auto now = Clock::now();
@@ -302,64 +321,105 @@ private:
         cv_done_.notify_all();
     }
 
-    int run_batch(const std::vector<Request *> &rs, cudaStream_t st, Pinned &stage)
-    {
-        const int count = (int)rs.size();
-        std::vector<int> rows(count), cols(count);
-        std::vector<long long> aoff(count);
-        size_t a_total = 0, s_total = 0, v_total = 0, u_total = 0;
-        bool any_u = false;
-        for (int i = 0; i < count; ++i) {
-            rows[i] = (int)rs[i]->m;
-            cols[i] = (int)rs[i]->n;
-            aoff[i] = (long long)a_total;
-            a_total += rs[i]->m * rs[i]->n;
-            s_total += rs[i]->n;
-            v_total += rs[i]->n * rs[i]->n;
-            any_u = any_u || rs[i]->want_u;
-        }
-        if (any_u) u_total = a_total;
-        const size_t doubles = a_total + s_total + v_total + u_total;
-        int rc = stage.ensure(sizeof(double) * doubles);
-        if (rc != JSVD_OK) return rc;
-        double *h = static_cast<double *>(stage.p);
-        for (int i = 0; i < count; ++i)
-            std::memcpy(h + aoff[i], rs[i]->a.data(), sizeof(double) * rs[i]->a.size());
+    // A small request on the device: one allocation holding its state (A,
+    // V), its input and its outputs (sigma, V, U).
+    struct Slot {
+        Request *r = nullptr;
         double *d = nullptr;
-        JSVD_CUDA_TRY(cudaMallocAsync((void **)&d, sizeof(double) * doubles, st));
-        ScopeExit free_d([&] { cudaFreeAsync(d, st); });  // stream-ordered, on every path
-        JSVD_CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(double) * a_total, cudaMemcpyHostToDevice, st));
-        BatchRequest req;
-        req.count = count;
-        req.rows = rows.data();
-        req.cols = cols.data();
-        req.a_offsets = aoff.data();
-        req.a = d;
-        req.a_is_f32 = 0;
-        req.eps = opt_.cfg.epsilon;
-        req.max_sweeps = opt_.cfg.max_sweeps;
-        req.sigma = d + a_total;
-        req.v = d + a_total + s_total;
-        req.u = any_u ? d + a_total + s_total + v_total : nullptr;
-        std::vector<int> sweeps(count);
-        req.sweeps = sweeps.data();
-        rc = batch_solve(req, st);
-        if (rc != JSVD_OK) return rc;
-        JSVD_CUDA_TRY(cudaMemcpyAsync(h + a_total, d + a_total, sizeof(double) * (s_total + v_total + u_total),
-                                      cudaMemcpyDeviceToHost, st));
-        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
-        size_t so = 0, vo = 0;
-        for (int i = 0; i < count; ++i) {
-            Request *r = rs[i];
-            r->sigma.assign(h + a_total + so, h + a_total + so + r->n);
-            r->v.assign(h + a_total + s_total + vo, h + a_total + s_total + vo + r->n * r->n);
-            if (r->want_u) {
-                const double *us = h + a_total + s_total + v_total + aoff[i];
-                r->u.assign(us, us + r->m * r->n);
+        int sweeps = 0;
+        bool first = true;
+    };
+
+    StepDesc slot_desc(const Slot &s) const
+    {
+        const size_t m = s.r->m, n = s.r->n;
+        StepDesc d{};
+        d.m = (int)m;
+        d.n = (int)n;
+        d.a = s.d;
+        d.v = s.d + m * n;
+        d.in = s.first ? s.d + m * n + n * n : nullptr;
+        d.s_out = s.d + 2 * m * n + n * n;
+        d.v_out = d.s_out + n;
+        d.u_out = s.r->want_u ? d.v_out + n * n : nullptr;
+        return d;
+    }
+
+    // Uploads the fresh requests (they join `active`), runs one sweep of every
+    // active request, then collects the ones that converged or reached
+    // max_sweeps into `done` (their outputs are on the host, their device
+    // memory released).
+    int step_once(std::vector<Slot> &active, std::vector<Request *> &fresh, std::vector<Slot> &done,
+                  cudaStream_t st, Pinned &stage, StepScratch &sc)
+    {
+        size_t up = 0;
+        for (Request *r : fresh) up += r->m * r->n;
+        if (up > 0) {
+            if (int rc = stage.ensure(sizeof(double) * up); rc != JSVD_OK) return rc;
+            JSVD_CUDA_TRY(cudaStreamSynchronize(st));  // the staging buffer is free again
+        }
+        size_t off = 0;
+        double *h = static_cast<double *>(stage.p);
+        while (!fresh.empty()) {
+            Request *r = fresh.back();
+            const size_t m = r->m, n = r->n;
+            Slot s;
+            s.r = r;
+            JSVD_CUDA_TRY(cudaMallocAsync((void **)&s.d, sizeof(double) * (3 * m * n + n + 2 * n * n), st));
+            fresh.pop_back();
+            active.push_back(s);
+            std::memcpy(h + off, r->a.data(), sizeof(double) * m * n);
+            JSVD_CUDA_TRY(cudaMemcpyAsync(s.d + m * n + n * n, h + off, sizeof(double) * m * n,
+                                          cudaMemcpyHostToDevice, st));
+            off += m * n;
+        }
+        std::vector<StepDesc> descs(active.size());
+        for (size_t i = 0; i < active.size(); ++i) descs[i] = slot_desc(active[i]);
+        std::vector<int> rotated(active.size());
+        if (int rc = batch_step(descs, opt_.cfg.epsilon, rotated.data(), sc, st); rc != JSVD_OK) return rc;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            ++batches_;
+        }
+        std::vector<Slot> keep;
+        std::vector<StepDesc> fin;
+        for (size_t i = 0; i < active.size(); ++i) {
+            Slot &s = active[i];
+            s.first = false;
+            ++s.sweeps;
+            if (rotated[i] == 0 || s.sweeps >= opt_.cfg.max_sweeps) {
+                done.push_back(s);
+                fin.push_back(slot_desc(s));
+            } else {
+                keep.push_back(s);
             }
-            r->sweeps = sweeps[i];
-            so += r->n;
-            vo += r->n * r->n;
+        }
+        active.swap(keep);
+        if (done.empty()) return JSVD_OK;
+        if (int rc = batch_finish(fin, opt_.cfg.epsilon, sc, st); rc != JSVD_OK) return rc;
+        size_t out = 0;
+        for (const Slot &s : done) out += s.r->n + s.r->n * s.r->n + (s.r->want_u ? s.r->m * s.r->n : 0);
+        if (int rc = stage.ensure(sizeof(double) * out); rc != JSVD_OK) return rc;
+        h = static_cast<double *>(stage.p);
+        off = 0;
+        for (const Slot &s : done) {
+            const size_t m = s.r->m, n = s.r->n, k = n + n * n + (s.r->want_u ? m * n : 0);
+            JSVD_CUDA_TRY(cudaMemcpyAsync(h + off, s.d + 2 * m * n + n * n, sizeof(double) * k,
+                                          cudaMemcpyDeviceToHost, st));
+            off += k;
+        }
+        JSVD_CUDA_TRY(cudaStreamSynchronize(st));
+        off = 0;
+        for (Slot &s : done) {
+            Request *r = s.r;
+            const size_t m = r->m, n = r->n;
+            r->sigma.assign(h + off, h + off + n);
+            r->v.assign(h + off + n, h + off + n + n * n);
+            if (r->want_u) r->u.assign(h + off + n + n * n, h + off + n + n * n + m * n);
+            r->sweeps = s.sweeps;
+            off += n + n * n + (r->want_u ? m * n : 0);
+            cudaFreeAsync(s.d, st);
+            s.d = nullptr;
         }
         return JSVD_OK;
     }
@@ -370,17 +430,43 @@ private:
         cudaStream_t st = nullptr;
         cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
         Pinned stage;
+        StepScratch sc;
+        std::vector<Slot> active;
         for (;;) {
-            std::vector<Request *> rs = admit(small_q_, (size_t)opt_.max_batch);
-            if (rs.empty()) break;
+            const size_t cap = (size_t)std::max(1, opt_.max_batch);
+            const size_t room = cap > active.size() ? cap - active.size() : 0;
+            // with nothing on the device, block for work; else take what is queued
+            std::vector<Request *> fresh = active.empty() ? admit(small_q_, room) : try_admit(small_q_, room);
+            if (active.empty() && fresh.empty()) break;
+            std::vector<Slot> done;
             // a C++ exception (a host allocation) fails these requests, not the process
-            const int rc = c_entry([&] { return run_batch(rs, st, stage); });
-            {
-                std::lock_guard<std::mutex> lk(mu_);
-                ++batches_;
-                batched_requests_ += rs.size();
+            const int rc = c_entry([&] { return step_once(active, fresh, done, st, stage, sc); });
+            if (rc != JSVD_OK) {
+                // every request on the device (and any not yet uploaded) fails
+                const std::string err = last_error_message();
+                std::vector<Request *> failed(fresh.begin(), fresh.end());
+                for (Slot &s : active) {
+                    failed.push_back(s.r);
+                    if (s.d) cudaFreeAsync(s.d, st);
+                }
+                for (Slot &s : done) {
+                    failed.push_back(s.r);
+                    if (s.d) cudaFreeAsync(s.d, st);
+                }
+                active.clear();
+                cudaStreamSynchronize(st);
+                finish(failed, rc, err);
+                continue;
             }
-            finish(rs, rc, rc == JSVD_OK ? std::string() : last_error_message());
+            if (!done.empty()) {
+                std::vector<Request *> rs;
+                for (const Slot &s : done) rs.push_back(s.r);
+                {
+                    std::lock_guard<std::mutex> lk(mu_);
+                    batched_requests_ += rs.size();
+                }
+                finish(rs, JSVD_OK, std::string());
+            }
         }
         if (st) cudaStreamDestroy(st);
     }

@@ -67,6 +67,30 @@ def test_server_results_equal_alone_and_in_mix(cuda_device):
         assert sw == ref[3] and np.array_equal(s_, ref[1]) and np.array_equal(v, ref[2])
 
 
+def test_server_small_requests_step_by_sweep(cuda_device):
+    """Sweep-granular batching: a request that converges in a few sweeps and
+    arrives with (or after) one that needs many leaves the device after its
+    own sweeps, not after the other's; both results equal the plain entry
+    point's bit for bit, and the worker counts one step per sweep."""
+    cfg = jsvd.default_config(epsilon=1e-14)
+    big = W.gaussian_splitmix(200, 120, 21)  # small path (A fits shared memory), many sweeps
+    tiny = [W.gaussian_splitmix(16, 4, 30 + i) for i in range(12)]
+    with jsvd.Server(cfg, small_workers=1, large_workers=1) as s:
+        tb = s.submit(big)
+        tt = [s.submit(a) for a in tiny]
+        got_t = [s.wait(t) for t in tt]
+        got_b = s.wait(tb)
+        st = s.stats()
+    ref_b = jsvd.plain_svd(big, cfg)
+    assert got_b[3] == ref_b[3] and np.array_equal(got_b[1], ref_b[1]) and np.array_equal(got_b[2], ref_b[2])
+    for a, g in zip(tiny, got_t):
+        ref = jsvd.plain_svd(a, cfg)
+        assert g[3] == ref[3] and np.array_equal(g[1], ref[1]) and np.array_equal(g[2], ref[2])
+        assert g[3] < got_b[3]
+        assert g[4] < got_b[4]  # latency: retired before the long request
+    assert st.batches >= got_b[3] and st.batched_requests == 13 and st.large_solves == 0
+
+
 def test_server_budget_rejects_oversize(cuda_device):
     with jsvd.Server(budget_bytes=1 << 20) as s:
         with pytest.raises(jsvd.JsvdError) as e:
