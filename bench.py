@@ -856,7 +856,8 @@ def run_serve(args, rank: int, world: int, device):
     sampler.start()
     for rate in rates:
         arrivals = t_unit / rate
-        with jsvd.Server(cfg, budget_bytes=budget, large_path=1, large_workers=args.serve_large_workers) as srv:
+        with jsvd.Server(cfg, budget_bytes=budget, large_path=args.serve_large_path,
+                         large_workers=args.serve_large_workers) as srv:
             # warm the worker plans and kernels
             srv.wait(srv.submit(mats[0]))
             tickets = [None] * len(mats)
@@ -910,7 +911,7 @@ def run_serve(args, rank: int, world: int, device):
         "data": "synthetic (seeded)",
         "config": {"workload": f"serving: Poisson arrivals, {args.serve_count} requests per rate, m log-uniform "
                                f"32..2048, n = m*U(0.25,1), FP64, kappa log-uniform [1e2,1e8], 40 GB budget (seed 4)",
-                   "path": "serving core: batched small requests + QR-preconditioned large requests",
+                   "path": "serving core: small requests batched by sweep, large requests on worker streams (" + {0: "plain", 1: "QR-preconditioned", 2: "blocked mixed precision"}[args.serve_large_path] + " path)",
                    "epsilon": 1e-14, "per_rate": per_rate,
                    "plain_one_at_a_time_svd_s": plain_rate, "plain_sample": k},
         "e2e": {"value": top["svd_s"], "unit": "SVD/s", "h2d_bytes_per_step": in_bytes,
@@ -1067,6 +1068,8 @@ def main():
     ap.add_argument("--serve-count", type=int, default=2000, help="requests per rate of the serve workload")
     ap.add_argument("--serve-plain-sample", type=int, default=40)
     ap.add_argument("--serve-large-workers", type=int, default=0, help="0 = the serving core's default")
+    ap.add_argument("--serve-large-path", type=int, default=2, choices=[0, 1, 2],
+                    help="serve workload: path of the large requests (0 plain, 1 QR-preconditioned, 2 mixed)")
     ap.add_argument("--large-m", type=int, default=16384)
     ap.add_argument("--large-n", type=int, default=8192)
     ap.add_argument("--large-dir", default="")
