@@ -112,15 +112,36 @@ def _check(a, res, kappa):
 
 @pytest.mark.parametrize("name,make,kappa", CASES, ids=[c[0] for c in CASES])
 def test_mixed_accuracy(cuda_device, name, make, kappa):
+    """Both phases (a tensor-core cap of 4 sweeps, whatever the width's
+    automatic choice) on every case."""
     a = make()
-    jsvd.mixed_set_options(None)
+    jsvd.mixed_set_options(tc_max_sweeps=4)
     jsvd.mixed_stats_reset()
-    res = jsvd.mixed_svd(a, jsvd.default_config(epsilon=1e-14))
+    try:
+        res = jsvd.mixed_svd(a, jsvd.default_config(epsilon=1e-14))
+    finally:
+        jsvd.mixed_set_options(None)
     _check(a, res, kappa)
     st = jsvd.mixed_stats()
     if a.shape[1] >= 128:
         assert st.solves == 1 and st.tc_sweeps >= 1 and st.f64_sweeps >= 1, (st.tc_sweeps, st.f64_sweeps)
         assert st.tc_discarded == 0
+
+
+@pytest.mark.parametrize("m,n", [(600, 200), (1024, 384), (2048, 1024), (3000, 1500)])
+def test_mixed_automatic_options(cuda_device, m, n):
+    """The default (automatic) options, resolved from the built-in tuning
+    table by width: accurate, and the tensor-core phase runs exactly when the
+    width's entry gives it sweeps."""
+    a = W.spectrum_matrix(m, n, W.geometric_sigma(n, 1e-6), 60 + n)
+    jsvd.mixed_set_options(None)
+    jsvd.mixed_stats_reset()
+    res = jsvd.mixed_svd(a, jsvd.default_config(epsilon=1e-14))
+    _check(a, res, 1e6)
+    st = jsvd.mixed_stats()
+    r = jsvd.mixed_resolved_options(n)
+    assert st.solves == 1 and st.f64_sweeps >= 1
+    assert (st.tc_sweeps >= 1) == (r.tc_max_sweeps > 0) and st.tc_sweeps <= r.tc_max_sweeps
 
 
 @pytest.mark.parametrize("opts", [dict(tc_max_sweeps=0), dict(precondition=0), dict(inner_sweeps=1),
