@@ -118,10 +118,23 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
     double(*a)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);
     double(*x)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm + kNb * (kNb + 1));
     const int t = threadIdx.x;
-    for (int e = t; e < kNb * kNb; e += kDiagThreads) {
-        const int i = e % kNb, k = e / kNb;  // consecutive threads read consecutive rows of column k
-        a[i][k] = (i < kb && k < kb) ? (i >= k ? G[(size_t)(k0 + k) * n + k0 + i] : 0.0) : (i == k ? 1.0 : 0.0);
-        x[i][k] = (i == k) ? 1.0 : 0.0;
+    {
+        // all of a thread's loads in flight before its stores
+        constexpr int kPer = kNb * kNb / kDiagThreads;
+        double g[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int e = t + u * kDiagThreads;
+            const int i = e % kNb, k = e / kNb;  // consecutive threads read consecutive rows of column k
+            g[u] = (i < kb && k < kb) ? (i >= k ? G[(size_t)(k0 + k) * n + k0 + i] : 0.0) : (i == k ? 1.0 : 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int e = t + u * kDiagThreads;
+            const int i = e % kNb, k = e / kNb;
+            a[i][k] = g[u];
+            x[i][k] = (i == k) ? 1.0 : 0.0;
+        }
     }
     __syncthreads();
     // ---- G = L D L^T ----
@@ -133,7 +146,17 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
                 const double d0 = a[cj][cj];
                 const bool ok = d0 > 0.0 && d0 < INFINITY;
                 const double d = ok ? d0 : 1.0;
-                const double rd = 1.0 / d;
+                // 1 / d by Newton's iteration r <- r (2 - d r) from the
+                // single-precision reciprocal (2^-23 -> 2^-46 -> rounding),
+                // by division outside the single-precision range
+                double rd;
+                if (d > 1.0e-30 && d < 1.0e30) {
+                    rd = (double)__frcp_rn((float)d);
+                    rd = rd * fma(-d, rd, 2.0);
+                    rd = rd * fma(-d, rd, 2.0);
+                } else {
+                    rd = 1.0 / d;
+                }
                 if (lane == 0) {
                     if (!ok) atomicExch(status, 1);
                     dvec[cj] = d;
