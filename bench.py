@@ -562,8 +562,10 @@ def run_extras(args, path: str, device, stream, flush) -> dict:
     line (device-resident inputs, L2 flushed between steps, CUDA events):
     the other fast path on the same 4096 x 1024 input, config 1 (512 x 512
     N(0,1), plain drop-in, checked bit for bit against the reference's own
-    output), config 3 (the 20,000-matrix batch) and the 16384 x 8192 graded
-    and clustered matrix through the mixed path."""
+    output), config 3 (the 20,000-matrix batch), the 16384 x 8192 graded
+    and clustered matrix through the mixed path, the plain drop-in on the
+    4096 x 1024 input, and config 4 at one arrival rate (serve_1000; the
+    serving core's throughput is host wall clock)."""
     import jsvd
 
     out = {}
@@ -584,6 +586,18 @@ def run_extras(args, path: str, device, stream, flush) -> dict:
                               "sweeps_per_svd": s_sw[0], "epsilon": wl1["eps"],
                               "sigma_bitwise_equal_to_reference": bool(np.array_equal(s_sig, g["sigma"])) if float(
                                   g["eps"]) == wl1["eps"] else None}
+    # config 4, briefly: one arrival rate, 500 requests, large ones on the mixed path
+    sargs = argparse.Namespace(**vars(args))
+    sargs.rates, sargs.serve_count, sargs.serve_plain_sample, sargs.serve_large_path = "1000", 500, 20, 2
+    sl = run_serve(sargs, 0, 1, device)
+    r = sl["config"]["per_rate"][0]
+    out["serve_1000"] = {"value": sl["value"], "unit": "SVD/s", "rate_req_s": r["rate_req_s"],
+                         "requests": r["requests"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+                         "sweep_steps": r["batches"], "small_requests": r["batched_requests"],
+                         "large_solves": r["large_solves"],
+                         "plain_one_at_a_time_svd_s": sl["config"]["plain_one_at_a_time_svd_s"],
+                         "note": "the serve workload's trace, first 500 requests; bench.py --workload serve runs "
+                                 "five rates x 2000"}
     bargs = argparse.Namespace(**vars(args))
     bargs.steps, bargs.warmup, bargs.no_cpu_baseline = 2, 1, True
     b = run_batch(bargs, 0, 1, device)
