@@ -603,9 +603,36 @@ def run_extras(args, path: str, device, stream, flush) -> dict:
     b = run_batch(bargs, 0, 1, device)
     out["batch"] = {"value": b["value"], "unit": "SVD/s", "ms_per_step": b["ms_per_step"],
                     "matrices": BATCH_COUNT if bargs.batch_count == BATCH_COUNT else bargs.batch_count,
-                    "class_ms_per_step": b["config"]["classes"]["ms_per_step"], "roofline": b["roofline"]}
+                    "class_ms_per_step": b["config"]["classes"]["ms_per_step"], "roofline": b["roofline"],
+                    "plain_one_at_a_time_svd_s": batch_plain_rate(device, 40), "plain_sample": 40}
+    # config 1 through the blocked mixed-precision path (accuracy against the
+    # reference's own sigma for this input)
+    m_ms, m_sw, _, m_sig, _ = time_single(args, wl1, "mixed", device, stream, 3, 1, flush, 1)
+    ref1 = np.sort(np.asarray(g["sigma"]))[::-1]
+    got1 = np.sort(np.asarray(m_sig))[::-1]
+    out["square512_mixed"] = {"value": 3 / (m_ms / 1e3), "unit": "SVD/s", "ms_per_step": m_ms / 3,
+                              "sweeps_per_svd": m_sw[0],
+                              "sigma_normwise_vs_reference": float(np.max(np.abs(got1 - ref1)) / ref1[0]),
+                              "sigma_max_rel_vs_reference": float(np.max(np.abs(got1 - ref1) / ref1))}
     out["large_mixed"] = run_large_device(args, device, "mixed")
     return out
+
+
+def batch_plain_rate(device, k: int) -> float:
+    """The plain drop-in one matrix at a time (host buffers, as a caller of
+    one_sided_jacobi_svd would) on k matrices drawn from the config-3
+    distribution (seed 3), promoted to FP64: SVD/s."""
+    import jsvd
+    import workloads as W
+
+    mats = W.batch_workload_torch(k, seed=3, device=device)
+    cfg = jsvd.default_config(epsilon=1e-14)
+    a64 = [np.asarray(a, dtype=np.float64) for a in mats]
+    jsvd.plain_svd(a64[0], cfg)  # warm-up
+    t0 = time.perf_counter()
+    for a in a64:
+        jsvd.plain_svd(a, cfg)
+    return k / (time.perf_counter() - t0)
 
 
 def run_large_device(args, device, path: str, steps: int = 1, warmup: int = 1) -> dict:
