@@ -195,11 +195,41 @@ constexpr size_t kRotTcSmem = 1024 + 98304 + 64;
 // is 32 K rows (columns of P) of 128 bytes (32 rows of P), groups of 4 K rows
 // 512 bytes apart (SBO), the four 32-row atoms of the tile 4096 bytes apart
 // (LBO).
+// Entry W(k, n) of a pair's rotation in the rotation kernel's B operand
+// image: row n (head) and row 64 + n (tail) hold column n of W along K (K
+// major, 128-byte swizzle, two 32-float K atoms), 32 KB per pair, laid out
+// exactly as the kernel's shared-memory B region.
+__device__ __forceinline__ void rot_b_store(float *img, int k, int n, double wv)
+{
+    float h, l;
+    split_tf32((float)wv, h, l);
+    const int atom = k >> 5, kk = k & 31;
+#pragma unroll
+    for (int hl = 0; hl < 2; ++hl) {
+        const int row = n + hl * 64;
+        const int off = atom * 16384 + row * 128 + (((kk >> 2) ^ (row & 7)) << 4) + (kk & 3) * 4;
+        img[off >> 2] = hl ? l : h;
+    }
+}
+
+constexpr int kRotImgFloats = 8192;  // 32 KB per block pair
+
+// B operand images of the pairs that rotate, from W (the eigen-solve writes
+// them itself; this builds them from a given W).
+__global__ void __launch_bounds__(256) mx_rot_image(const double *__restrict__ W, float *__restrict__ img,
+                                                    const int *__restrict__ flags)
+{
+    const int pair = blockIdx.x;
+    if (flags[pair] == 0) return;
+    for (int e = threadIdx.x; e < kW * kW; e += blockDim.x)
+        rot_b_store(img + (size_t)pair * kRotImgFloats, e & 63, e >> 6, W[(size_t)pair * kW * kW + e]);
+}
+
 __global__ void __launch_bounds__(kRotTcThreads)
     mx_rot_tc(const __grid_constant__ CUtensorMap mxh, const __grid_constant__ CUtensorMap mxl,
               const __grid_constant__ CUtensorMap mvh, const __grid_constant__ CUtensorMap mvl,
               float *__restrict__ xh, float *__restrict__ xl, long ldx, int x_tiles, float *__restrict__ vh,
-              float *__restrict__ vl, long ldv, int nb, int round, const double *__restrict__ W,
+              float *__restrict__ vl, long ldv, int nb, int round, const float *__restrict__ Wimg,
               const int *__restrict__ flags, int *__restrict__ status)
 {
     const int pair = blockIdx.y;
@@ -231,7 +261,8 @@ __global__ void __launch_bounds__(kRotTcThreads)
     const uint32_t tmem = *tslot;
 
     if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(full, 65536);
+        // the A tiles (64 KB) and the pair's B image, [W_h | W_l] (32 KB)
+        mbar_arrive_expect_tx(full, 65536 + 32768);
 #pragma unroll
         for (int hl = 0; hl < 2; ++hl)
 #pragma unroll
@@ -240,22 +271,7 @@ __global__ void __launch_bounds__(kRotTcThreads)
                 for (int g = 0; g < 4; ++g)
                     tma_load_2d(sm + kRotAOff + hl * 32768 + half * 16384 + g * 4096, hl ? ml : mh, full,
                                 row0 + g * 32, (half ? bp.y : bp.x) * kB);
-    }
-    __syncwarp();
-    // B = [W_h | W_l]: row n (0..63 head, 64..127 tail) holds column n of W
-    // along K (K-major, 128-byte swizzle, two 32-float K atoms).
-    const double *wp = W + (size_t)pair * kW * kW;
-    for (int e = threadIdx.x; e < kW * kW; e += kRotTcThreads) {
-        const int k = e & 63, n = e >> 6;  // W(k, n) at k + 64 n: consecutive threads read consecutive k
-        float h, l;
-        split_tf32((float)wp[e], h, l);
-        const int atom = k >> 5, kk = k & 31;
-#pragma unroll
-        for (int hl = 0; hl < 2; ++hl) {
-            const int row = n + hl * 64;
-            const uint32_t off = kRotBOff + atom * 16384 + row * 128 + (((kk >> 2) ^ (row & 7)) << 4) + (kk & 3) * 4;
-            *reinterpret_cast<float *>(sm + off) = hl ? l : h;
-        }
+        bulk_load(sm + kRotBOff, Wimg + (size_t)pair * kRotImgFloats, 32768, full);
     }
     fence_proxy_async_smem();
     __syncthreads();
@@ -698,13 +714,14 @@ __device__ __forceinline__ void evd_w_advance(double (&w)[16], int q, double up,
 //     (bit-identical to what lands in the buffer).  Everything that depends
 //     on round r's angles only (the new diagonals, the neighbours' angles,
 //     the diagonal part of the rotation) is done before round r's barrier.
-// Writes W (64 x 64, column-major) and flags[pair] = 1 when some pair
-// rotated (else flags[pair] = 0 and W is left as it was).  stats[0] (as
+// Writes W (64 x 64, column-major) - and, when Wimg is not null, its 3xTF32
+// operand image for the tensor-core rotation - and flags[pair] = 1 when some
+// pair rotated (else flags[pair] = 0 and W is left as it was).  stats[0] (as
 // double bits) = running max of |g_pq| / sqrt(g_pp g_qq) over the input
 // Grams, stats[1] = number of block pairs that rotated.
 __global__ void __launch_bounds__(kEvdThreads, 1)
     mx_evd(const void *__restrict__ part, int kind, int splits, double tau, int inner_sweeps, int nb, int round,
-           int sort, int ncols, double *__restrict__ Wout, int *__restrict__ flags,
+           int sort, int ncols, double *__restrict__ Wout, float *__restrict__ Wimg, int *__restrict__ flags,
            unsigned long long *__restrict__ stats)
 {
     extern __shared__ __align__(16) double dsm[];
@@ -1013,7 +1030,11 @@ __global__ void __launch_bounds__(kEvdThreads, 1)
         // every sweep ran all 63 rounds: slot s holds column evd_slot_column(s)
         double *wo = Wout + (size_t)pair * kW * kW;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) wo[(size_t)out_col[evd_slot_column(16 * quarter + j)] * kW + wrow] = w[j];
+        for (int j = 0; j < 16; ++j) {
+            const int col = out_col[evd_slot_column(16 * quarter + j)];
+            wo[(size_t)col * kW + wrow] = w[j];
+            if (Wimg != nullptr) rot_b_store(Wimg + (size_t)pair * kRotImgFloats, wrow, col, w[j]);
+        }
     }
     if (tid == 0) {
         flags[pair] = rotated_any ? 1 : 0;
@@ -1306,6 +1327,7 @@ struct Work {
     float *xh = nullptr, *xl = nullptr, *vh = nullptr, *vl = nullptr;
     void *part = nullptr;
     double *W = nullptr, *sg = nullptr;
+    float *wimg = nullptr;  // the tensor-core rotation's B operand images (phase 1)
     int *flags = nullptr, *status = nullptr;
     // [0] max off (double bits) [1] rotated pairs [2] orth max [4..7] rotated
     // pairs before/after the eigen-solve of the two sampled rounds
@@ -1358,6 +1380,7 @@ int make_work(int rows, int cols, const jsvd_mixed_options &o, bool tc, cudaStre
                  o_e = take(nn * 8);
     const size_t o_xh = tc ? take(mn * 4) : 0, o_xl = tc ? take(mn * 4) : 0, o_vh = tc ? take(nn * 4) : 0,
                  o_vl = tc ? take(nn * 4) : 0;
+    const size_t o_wimg = tc ? take((size_t)w.npairs * kRotImgFloats * 4) : 0;
     const size_t o_part = take(part_bytes), o_w = take((size_t)w.npairs * kW * kW * 8), o_sg = take(w.cols_pad * 8),
                  o_flags = take(w.npairs * 4), o_status = take(4), o_stats = take(8 * 8);
     JSVD_CUDA_TRY(cudaMallocAsync(&w.block, bytes, st));
@@ -1372,6 +1395,7 @@ int make_work(int rows, int cols, const jsvd_mixed_options &o, bool tc, cudaStre
         w.xl = reinterpret_cast<float *>(b + o_xl);
         w.vh = reinterpret_cast<float *>(b + o_vh);
         w.vl = reinterpret_cast<float *>(b + o_vl);
+        w.wimg = reinterpret_cast<float *>(b + o_wimg);
     }
     w.part = b + o_part;
     w.W = reinterpret_cast<double *>(b + o_w);
@@ -1430,13 +1454,13 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
                 cudaMemcpyAsync(w.stats + 4 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
             }
             mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 0, w.tc_splits, tau, inner, w.nb, r, sort, w.cols,
-                                                            w.W, w.flags, w.stats);
+                                                            w.W, w.wimg, w.flags, w.stats);
             if (si >= 0) {
                 cudaMemcpyAsync(w.stats + 5 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
                 cudaEventRecord(w.tev[si][2], st);
             }
             mx_rot_tc<<<dim3(w.x_tiles + w.v_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
-                w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, w.rows_pad, w.x_tiles, w.vh, w.vl, w.cols_pad, w.nb, r, w.W,
+                w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, w.rows_pad, w.x_tiles, w.vh, w.vl, w.cols_pad, w.nb, r, w.wimg,
                 w.flags, w.status);
             ms.tc_gram += 1;
             ms.tc_rot += 1;
@@ -1448,7 +1472,7 @@ int run_sweep(Work &w, bool tc, double tau, int inner, int sort, cudaStream_t st
                 cudaMemcpyAsync(w.stats + 4 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
             }
             mx_evd<<<w.npairs, kEvdThreads, kEvdSmem, st>>>(w.part, 1, w.f64_splits, tau, inner, w.nb, r, sort,
-                                                            w.cols, w.W, w.flags, w.stats);
+                                                            w.cols, w.W, nullptr, w.flags, w.stats);
             if (si >= 0) {
                 cudaMemcpyAsync(w.stats + 5 + 2 * si, w.stats + 1, 8, cudaMemcpyDeviceToDevice, st);
                 cudaEventRecord(w.tev[si][2], st);
@@ -1799,8 +1823,9 @@ extern "C" int jsvd_mixed_test_round(int kind, double *d_x, int rows, int cols, 
         } else {
             mx_fill_int<<<1, 256, 0, st>>>(w.flags, w.npairs, 1);
             if (kind == 2) {
+                mx_rot_image<<<w.npairs, 256, 0, st>>>(d_gw, w.wimg, w.flags);
                 mx_rot_tc<<<dim3(w.x_tiles, w.npairs), kRotTcThreads, kRotTcSmem, st>>>(
-                    w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, rows, w.x_tiles, w.vh, w.vl, cols, w.nb, round, d_gw,
+                    w.rxh, w.rxl, w.rvh, w.rvl, w.xh, w.xl, rows, w.x_tiles, w.vh, w.vl, cols, w.nb, round, w.wimg,
                     w.flags, w.status);
                 mx_join<<<grid_for(mn), 256, 0, st>>>(w.xh, w.xl, mn, d_x);
             } else {

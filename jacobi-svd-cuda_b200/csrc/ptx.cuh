@@ -104,6 +104,17 @@ __device__ __forceinline__ void tma_load_2d(void *smem_dst, const void *tensor_m
         "l"(tensor_map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
         : "memory");
 }
+// Bulk copy of `bytes` contiguous bytes from global to shared memory (no
+// tensor map, no multicast), completing on an mbarrier; both addresses 16-byte
+// aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void *smem_dst, const void *gmem_src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(smem_dst)),
+        "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
 __device__ __forceinline__ void tma_prefetch_desc(const void *tensor_map)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(tensor_map) : "memory");
