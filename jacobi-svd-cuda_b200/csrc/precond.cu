@@ -88,36 +88,24 @@ __global__ void __launch_bounds__(256) pc_shift_diagonal(double *__restrict__ G,
 // factor into Linv (column-major, ld = kNb).  The block is padded to kNb x kNb
 // with the identity.
 //
-// G = L D L^T (L unit lower), the square roots taken at the end (Cholesky
-// factor L sqrt(D), inverse D^{-1/2} L^{-1}, where L^{-1} needs no division).
-// Thread t works with row (or column) t / 4 and the quarter k = t (mod 4) of
-// every inner product; the four partial sums of a group meet by shuffles:
-//   factorisation, left-looking, one column j at a time: each group forms
-//     its row's sum s_i = sum_k L(i,k) d_k L(j,k) and the pivot's s_j, so
-//     d_j = g_jj - s_j is known to every group without a further barrier,
-//     and L(i,j) = (g_ij - s_i) / d_j; one barrier per column;
-//   inverse of L: column c of L^{-1} by forward substitution in group c,
-//     rows one after another, the column's entries in the group's registers
-//     (lane q holds rows k = q mod 4): no block-wide barrier.
-// An earlier form (warp 0 factoring 8-column panels while the block waited at
-// barriers) measured 51 us per block on B200 (ncu).
+// The factor is computed as G = L D L^T (L unit lower): each column costs one
+// reciprocal of its pivot on the serial chain, and the square roots are taken
+// afterwards, all at once (Cholesky factor L sqrt(D), inverse
+// D^{-1/2} L^{-1}, where L^{-1} needs no division).  Panels of kPanel columns:
+//   factorisation: warp 0 factors the panel's columns (right-looking inside
+//     the panel, __syncwarp between columns; each lane owns two rows and reads
+//     the pivot column's panel entries before they are rescaled), then all
+//     threads apply the panel's update to the trailing triangle,
+//     a[i][k] -= sum_j L(i,j) d_j L(k,j);
+//   inverse of L: block forward substitution of [L | I], kPanel rows at a
+//     time: thread c solves column c through the panel's unit triangle, then
+//     all threads subtract the panel's contribution from the rows below.
+// A form with a square root and a reciprocal per column measured about 60 us
+// per block on B200 (ncu), set by that serial chain of 64 pivots.
 // status <- 1 on a pivot that is not positive and finite.
+constexpr int kPanel = 8;
 constexpr int kDiagThreads = 256;
-static_assert(kDiagThreads == 4 * kNb, "four threads per row / column");
-constexpr size_t kDiagSmem = sizeof(double) * kNb * (kNb + 1);
-
-// 1 / d for d > 0: Newton's iteration r <- r (2 - d r) from the
-// single-precision reciprocal (2^-23 -> 2^-46 -> rounding); by division
-// outside the single-precision range.
-__device__ __forceinline__ double pc_recip(double d)
-{
-    if (d > 1.0e-30 && d < 1.0e30) {
-        double r = (double)__frcp_rn((float)d);
-        r = r * fma(-d, r, 2.0);
-        return r * fma(-d, r, 2.0);
-    }
-    return 1.0 / d;
-}
+constexpr size_t kDiagSmem = sizeof(double) * 2 * kNb * (kNb + 1);
 
 __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *__restrict__ G,
                                                                  double *__restrict__ Lm, int n, int k0, int kb,
@@ -125,12 +113,13 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
 {
     extern __shared__ double dsm[];
     __shared__ double dvec[kNb];  // pivots d_i
+    __shared__ double sq[kNb];    // sqrt(d_i)
     __shared__ double isq[kNb];   // 1 / sqrt(d_i)
-    double(*a)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);  // G's lower triangle, then L below it
-    const int t = threadIdx.x, grp = t >> 2, q = t & 3;
+    double(*a)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm);
+    double(*x)[kNb + 1] = reinterpret_cast<double(*)[kNb + 1]>(dsm + kNb * (kNb + 1));
+    const int t = threadIdx.x;
     {
-        // all of a thread's loads in flight before its stores; the upper
-        // triangle is zero
+        // all of a thread's loads in flight before its stores
         constexpr int kPer = kNb * kNb / kDiagThreads;
         double g[kPer];
 #pragma unroll
@@ -142,67 +131,104 @@ __global__ void __launch_bounds__(kDiagThreads) pc_chol_inv_diag(const double *_
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
             const int e = t + u * kDiagThreads;
-            a[e % kNb][e / kNb] = g[u];
+            const int i = e % kNb, k = e / kNb;
+            a[i][k] = g[u];
+            x[i][k] = (i == k) ? 1.0 : 0.0;
         }
     }
     __syncthreads();
-    // ---- G = L D L^T, column by column ----
-    const int i = grp;
-    for (int j = 0; j < kNb; ++j) {
-        double si = 0.0, sj = 0.0;
-        for (int k = q; k < j; k += 4) {
-            const double ljk = a[j][k];
-            const double w = ljk * dvec[k];
-            si = fma(a[i][k], w, si);
-            sj = fma(ljk, w, sj);
+    // ---- G = L D L^T ----
+    for (int c0 = 0; c0 < kNb; c0 += kPanel) {
+        if (t < 32) {
+            const int lane = t;
+            for (int j = 0; j < kPanel; ++j) {
+                const int cj = c0 + j;
+                const double d0 = a[cj][cj];
+                const bool ok = d0 > 0.0 && d0 < INFINITY;
+                const double d = ok ? d0 : 1.0;
+                // 1 / d by Newton's iteration r <- r (2 - d r) from the
+                // single-precision reciprocal (2^-23 -> 2^-46 -> rounding),
+                // by division outside the single-precision range
+                double rd;
+                if (d > 1.0e-30 && d < 1.0e30) {
+                    rd = (double)__frcp_rn((float)d);
+                    rd = rd * fma(-d, rd, 2.0);
+                    rd = rd * fma(-d, rd, 2.0);
+                } else {
+                    rd = 1.0 / d;
+                }
+                if (lane == 0) {
+                    if (!ok) atomicExch(status, 1);
+                    dvec[cj] = d;
+                }
+                double colk[kPanel];  // a[k][cj] = L(k,cj) d_cj of the panel rows below cj
+#pragma unroll
+                for (int kk = 0; kk < kPanel; ++kk) colk[kk] = (kk > j) ? a[c0 + kk][cj] : 0.0;
+                __syncwarp();
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int i = c0 + lane + 32 * h;
+                    if (i >= kNb || i <= cj) continue;
+                    const double lij = a[i][cj] * rd;
+                    a[i][cj] = lij;
+#pragma unroll
+                    for (int kk = 0; kk < kPanel; ++kk) {
+                        const int k = c0 + kk;
+                        if (kk > j && k <= i) a[i][k] = fma(-lij, colk[kk], a[i][k]);
+                    }
+                }
+                __syncwarp();
+            }
         }
-        si += __shfl_xor_sync(0xffffffffu, si, 1);
-        si += __shfl_xor_sync(0xffffffffu, si, 2);
-        sj += __shfl_xor_sync(0xffffffffu, sj, 1);
-        sj += __shfl_xor_sync(0xffffffffu, sj, 2);
-        const double d0 = a[j][j] - sj;
-        const bool ok = d0 > 0.0 && d0 < INFINITY;
-        const double d = ok ? d0 : 1.0;
-        if (t == 0) {
-            dvec[j] = d;
-            if (!ok) atomicExch(status, 1);
+        __syncthreads();
+        const int base = c0 + kPanel, w = kNb - base;
+        for (int e = t; e < w * w; e += kDiagThreads) {
+            const int i = base + e / w, k = base + e % w;
+            if (k > i) continue;
+            double acc = a[i][k];
+#pragma unroll
+            for (int jj = 0; jj < kPanel; ++jj) acc = fma(-a[i][c0 + jj], a[k][c0 + jj] * dvec[c0 + jj], acc);
+            a[i][k] = acc;
         }
-        if (q == 0 && i > j) a[i][j] = (a[i][j] - si) * pc_recip(d);
         __syncthreads();
     }
-    if (t < kNb) isq[t] = 1.0 / sqrt(dvec[t]);
-    // ---- column c = grp of L^{-1} (unit lower): x_r = -sum_{c <= k < r} L(r,k) x_k ----
-    const int c = grp;
-    double xr[kNb / 4];  // x_k for k = q + 4 m
-#pragma unroll
-    for (int m = 0; m < kNb / 4; ++m) xr[m] = (q + 4 * m == c) ? 1.0 : 0.0;
-    // the same rows for every lane of a warp (the shuffles need all 32): a
-    // group keeps its column's entries above and on the diagonal as they are
-    for (int r = 1; r < kNb; ++r) {
-        double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-        for (int m = 0; m < kNb / 4; m += 2) {
-            const int ka = q + 4 * m, kb2 = ka + 4;
-            if (ka < r) s0 = fma(a[r][ka], xr[m], s0);
-            if (kb2 < r) s1 = fma(a[r][kb2], xr[m + 1], s1);
-        }
-        double sr = s0 + s1;
-        sr += __shfl_xor_sync(0xffffffffu, sr, 1);
-        sr += __shfl_xor_sync(0xffffffffu, sr, 2);
-#pragma unroll
-        for (int m = 0; m < kNb / 4; ++m)
-            if (q + 4 * m == r && r > c) xr[m] = -sr;
+    if (t < kNb) {
+        sq[t] = sqrt(dvec[t]);
+        isq[t] = 1.0 / sq[t];
     }
-    __syncthreads();  // isq complete
+    // ---- L^{-1}: forward substitution of [L | I] (unit diagonal) ----
+    for (int r0 = 0; r0 < kNb; r0 += kPanel) {
+        const int cols = r0 + kPanel;  // columns 0 .. cols-1 can be non-zero in these rows
+        if (t < cols) {
+            const int c = t;
+#pragma unroll
+            for (int r = 0; r < kPanel; ++r) {
+                const int i = r0 + r;
+                double val = x[i][c];
+#pragma unroll
+                for (int rr = 0; rr < r; ++rr) val = fma(-a[i][r0 + rr], x[r0 + rr][c], val);
+                x[i][c] = val;
+            }
+        }
+        __syncthreads();
+        const int below = kNb - cols;
+        for (int e = t; e < below * cols; e += kDiagThreads) {
+            const int i = cols + e / cols, c = e % cols;
+            double acc = x[i][c];
+#pragma unroll
+            for (int r = 0; r < kPanel; ++r) acc = fma(-a[i][r0 + r], x[r0 + r][c], acc);
+            x[i][c] = acc;
+        }
+        __syncthreads();
+    }
     // Cholesky factor L sqrt(D) and its inverse D^{-1/2} L^{-1}
     for (int e = t; e < kb * kb; e += kDiagThreads) {
-        const int ii = e % kb, k = e / kb;
-        if (ii >= k) Lm[(size_t)(k0 + k) * n + k0 + ii] = (ii == k) ? sqrt(dvec[ii]) : a[ii][k] * sqrt(dvec[k]);
+        const int i = e % kb, k = e / kb;
+        if (i >= k) Lm[(size_t)(k0 + k) * n + k0 + i] = (i == k) ? sq[i] : a[i][k] * sq[k];
     }
-#pragma unroll
-    for (int m = 0; m < kNb / 4; ++m) {
-        const int rr = q + 4 * m;
-        Linv[rr + (size_t)c * kNb] = (rr < kb && c < kb && c <= rr) ? xr[m] * isq[rr] : 0.0;
+    for (int e = t; e < kNb * kNb; e += kDiagThreads) {
+        const int i = e % kNb, k = e / kNb;
+        Linv[i + (size_t)k * kNb] = (i < kb && k < kb && k <= i) ? x[i][k] * isq[i] : 0.0;
     }
 }
 
