@@ -228,6 +228,15 @@ int jsvd_batch_svd_device(int count, const int *rows, const int *cols, const lon
                           int a_is_f32, const jsvd_config *cfg, double *d_sigma, double *d_v, double *d_u,
                           int *sweeps, const jsvd_batch_tuning *tuning, void *stream);
 
+/* Size classes whose members are solved by a thread-block cluster (2, 4 or 8
+ * CTAs, the smallest whose distributed shared memory holds A and V with at
+ * least two column pairs per CTA) instead of by one CTA: bit c = class c,
+ * classes 2, 3 and 4 only (default: 3 and 4).  A member that fits no cluster
+ * stays with its class's own kernel, which is also the only one the class's
+ * tuning entry shapes.  Results are the same bytes either way.
+ * Process-wide; *previous (optional) gets the old mask. */
+int jsvd_batch_set_cluster_classes(int mask, int *previous);
+
 /* Result of jsvd_batch_autotune, per size class. */
 typedef struct jsvd_batch_autotune_report {
     jsvd_batch_tuning best[5];    /* chosen shape (the built-in one unless another is > 2% faster) */

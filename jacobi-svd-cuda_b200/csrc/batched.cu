@@ -9,6 +9,10 @@
 //   class 3  : A in shared memory, V in a per-CTA slice of global memory
 //   class 4  : A and V in global memory (L2-resident per-CTA slices), the
 //              leading columns of A that fit in shared memory kept there
+// By default the members of classes 3 and 4 are instead solved by a
+// thread-block cluster each (batch_cluster_kernel: A and V in the cluster's
+// distributed shared memory; see the section "cluster classes"); a member no
+// cluster holds stays with its class's kernel.
 // Launch shapes per class (threads, CTAs per SM, grid cap) come from the
 // compiled-in table batch_tuning_table.h, which batch_autotune.py writes from
 // jsvd_batch_autotune (defined at the end of this file).
@@ -20,9 +24,11 @@
 //   2. one thread per pair: the rotation angle (the long sqrt/div chain runs
 //      for all pairs of the round in parallel instead of serially per warp);
 //   3. one warp per pair: rotation of the A and V columns.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -365,6 +371,295 @@ __global__ void __launch_bounds__(256) batch_finish_kernel(const StepDesc *__res
     }
 }
 
+// ---- cluster classes ----------------------------------------------------------
+// A member whose A and V do not fit one CTA's shared memory is solved by a
+// cluster of C CTAs (C = 2, 4, 8) with A and V spread over the cluster's
+// distributed shared memory, laid out as the round-robin circle itself.
+// CTA i owns the contiguous pair slots [k0, k1) of the circle (slot k =
+// positions k and ne-1-k, the pair (top, bottom)) and one warp works a slot.
+// Between rounds the top row moves one slot right and the bottom row one slot
+// left (position 0 stays; ne-1 goes to 1, half-1 to half), so inside a CTA no
+// column moves at all: the top slots live in a ring of S+1 column buffers
+// indexed (j - g) mod (S+1) at round g, the bottom slots in a ring indexed
+// (j + g) mod (S+1), and the spare buffer of each ring receives the one
+// column that arrives for round g+1.  Per round a CTA sends two columns: its
+// last top column to the right neighbour's spare top buffer and its first
+// bottom column to the left neighbour's spare bottom buffer (both written
+// straight from the rotation's registers over distributed shared memory; the
+// two end CTAs send one of them to themselves).  One cluster barrier per
+// round.  A buffer holds a column of A (m) followed by the same column of V
+// (n), rotated together.  Pair arithmetic is batch_kernel's (warp-per-pair
+// dot products in the T = 256 order, Rutishauser angle, rot_p / rot_q), so
+// every member stays bit-identical to the plain path.
+
+constexpr int kClusterThreads = 512;
+constexpr int kClusterSlotsPerWarp = 4;  // a CTA holds at most 4 * 16 pair slots
+
+__host__ __device__ constexpr int cluster_slots_max(int n, int C) { return ((n + (n & 1)) / 2 + C - 1) / C; }
+
+// Column buffer length: A's m rows, then V's n rows, padded to whole warps
+// (the padding rows are rotated and moved like the others and never read).
+__host__ __device__ constexpr int cluster_ld(int m, int n) { return (m + n + 31) & ~31; }
+
+// Shared memory of one CTA: column 0's fixed buffer and two rings.
+__host__ __device__ constexpr size_t cluster_smem_bytes(int m, int n, int C)
+{
+    return sizeof(double) * (size_t)(2 * cluster_slots_max(n, C) + 3) * (size_t)cluster_ld(m, n);
+}
+
+__device__ __forceinline__ int pmod(int a, int b)
+{
+    const int r = a % b;
+    return r < 0 ? r + b : r;
+}
+
+// Address of this CTA's shared-memory location `p` in the shared memory of
+// CTA `rank` of the cluster (a shared::cluster address).
+__device__ __forceinline__ uint32_t cluster_addr(const void *p, int rank)
+{
+    uint32_t out;
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(a), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void st_cluster(uint32_t addr, double v)
+{
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+
+// Rotation of a column pair held in this CTA's buffers (x, y: ld rows, a
+// multiple of 32), written to (xo, yo): shared::cluster addresses of the same
+// buffers or of a neighbour's.  Every 256-row chunk is loaded before it is
+// stored, so in-place use is safe.  c = 0: the columns are only moved.
+__device__ __forceinline__ void warp_rotate_cl(const double *x, const double *y, uint32_t xo, uint32_t yo, int ld,
+                                               int lane, double c, double s, bool rotate)
+{
+    int r0 = 0;
+    for (; r0 + kLanes <= ld; r0 += kLanes) {
+        double xa[kW], ya[kW];
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            xa[j] = x[r0 + 32 * j + lane];
+            ya[j] = y[r0 + 32 * j + lane];
+        }
+#pragma unroll
+        for (int j = 0; j < kW; ++j) {
+            const uint32_t off = 8u * (uint32_t)(r0 + 32 * j + lane);
+            st_cluster(xo + off, rotate ? rot_p(c, s, xa[j], ya[j]) : xa[j]);
+            st_cluster(yo + off, rotate ? rot_q(c, s, xa[j], ya[j]) : ya[j]);
+        }
+    }
+    for (; r0 < ld; r0 += 32) {
+        const double xv = x[r0 + lane], yv = y[r0 + lane];
+        const uint32_t off = 8u * (uint32_t)(r0 + lane);
+        st_cluster(xo + off, rotate ? rot_p(c, s, xv, yv) : xv);
+        st_cluster(yo + off, rotate ? rot_q(c, s, xv, yv) : yv);
+    }
+}
+
+// Moves one column (ld rows) to a shared::cluster address.
+__device__ __forceinline__ void warp_move_cl(const double *x, uint32_t xo, int ld, int lane)
+{
+    for (int r = lane; r < ld; r += 32) st_cluster(xo + 8u * (uint32_t)r, x[r]);
+}
+
+template <int C>
+__global__ void __launch_bounds__(kClusterThreads, 1)
+    batch_cluster_kernel(const BatchDesc *__restrict__ descs, int count, int *__restrict__ next,
+                         const void *__restrict__ a_all, int a_is_f32, double eps, int max_sweeps,
+                         double *__restrict__ sigma_all, double *__restrict__ v_all, double *__restrict__ u_all,
+                         int *__restrict__ sweeps_all)
+{
+    namespace cg = cooperative_groups;
+    extern __shared__ double smem[];
+    __shared__ int s_idx;
+    __shared__ int s_rot;
+    __shared__ unsigned long long s_stamp;  // rank 0's copy: last (member, sweep) stamp that rotated
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int *idx0 = cluster.map_shared_rank(&s_idx, 0);
+    unsigned long long *stamp0 = cluster.map_shared_rank(&s_stamp, 0);
+    // shared::cluster addresses of the start of the dynamic shared memory:
+    // this CTA's own and its neighbours' (same layout in every CTA)
+    const uint32_t sm_self = cluster_addr(smem, rank);
+    const uint32_t sm_right = cluster_addr(smem, rank < C - 1 ? rank + 1 : rank);
+    const uint32_t sm_left = cluster_addr(smem, rank > 0 ? rank - 1 : rank);
+    if (threadIdx.x == 0) {
+        s_rot = 0;
+        s_stamp = 0;
+    }
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) s_idx = atomicAdd(next, 1);
+        cluster.sync();  // (the first one also orders the initialisation above)
+        const int idx = *(volatile const int *)idx0;
+        // every CTA has read the index and finished the previous member's
+        // outputs before any CTA writes into another's buffers or exits
+        cluster.sync();
+        if (idx >= count) return;
+        const BatchDesc d = descs[idx];
+        const int m = d.m, n = d.n;
+        const int ne = n + (n & 1), half = ne / 2, L = ne - 1;
+        const int rounds = n >= 2 ? L : 0;
+        const int ld = cluster_ld(m, n);
+        const int smax = cluster_slots_max(n, C);
+        const int k0 = rank * half / C, k1 = (rank + 1) * half / C, S = k1 - k0;  // S >= 2 (host: half >= 2C)
+        // buffers (offsets in doubles): column 0's fixed one (CTA 0 only), the
+        // top ring, the bottom ring
+        const int top_off = ld, bot_off = (smax + 2) * ld;
+        const int jt0 = rank == 0 ? 1 : 0;  // first top slot that moves
+        const int rt = S - jt0 + 1, rb = S + 1;
+        const int s_right = rank < C - 1 ? (rank + 2) * half / C - k1 : 0;
+        const int s_left = rank > 0 ? k0 - (rank - 1) * half / C : 0;
+        // top slot j is in top buffer (j - jt0 - g) mod rt at round g, bottom
+        // slot j in bottom buffer (j + g) mod rb
+        auto top_at = [&](int j, int g) { return (rank == 0 && j == 0) ? 0 : top_off + pmod(j - jt0 - g, rt) * ld; };
+        auto bot_at = [&](int j, int g) { return bot_off + pmod(j + g, rb) * ld; };
+        // round 0: position p holds column p; V = I
+        const int ncl = 2 * S;
+        for (int e = threadIdx.x; e < m * ncl; e += blockDim.x) {
+            const int row = e / ncl, cc = e - row * ncl;
+            const int j = cc < S ? cc : cc - S;
+            const int col = cc < S ? k0 + j : ne - 1 - (k0 + j);
+            if (col >= n) continue;  // the dummy column of an odd n
+            const size_t src = (size_t)d.a_off + (size_t)row * n + col;
+            smem[(cc < S ? top_at(j, 0) : bot_at(j, 0)) + row] =
+                a_is_f32 ? (double)reinterpret_cast<const float *>(a_all)[src]
+                         : reinterpret_cast<const double *>(a_all)[src];
+        }
+        for (int e = threadIdx.x; e < n * ncl; e += blockDim.x) {
+            const int row = e / ncl, cc = e - row * ncl;
+            const int j = cc < S ? cc : cc - S;
+            const int col = cc < S ? k0 + j : ne - 1 - (k0 + j);
+            if (col >= n) continue;
+            smem[(cc < S ? top_at(j, 0) : bot_at(j, 0)) + m + row] = row == col ? 1.0 : 0.0;
+        }
+        __syncthreads();
+        // This warp's slots j = warp + t * nwarps, tracked from round to round:
+        // the circle values at their two positions (n = the dummy) and their
+        // ring buffers.  Position values fall by one per round (1 -> L).
+        int pv[kClusterSlotsPerWarp], qv[kClusterSlotsPerWarp], tb[kClusterSlotsPerWarp], bb[kClusterSlotsPerWarp];
+#pragma unroll
+        for (int t = 0; t < kClusterSlotsPerWarp; ++t) {
+            const int j = warp + t * nwarps, k = k0 + j;
+            pv[t] = k;
+            qv[t] = ne - 1 - k;
+            tb[t] = (rank == 0 && j == 0) ? -1 : j - jt0;
+            bb[t] = j;
+        }
+        // ring buffers that receive this CTA's outgoing columns in round g:
+        // the right neighbour's spare top buffer (the last CTA: its own spare
+        // bottom one) and the left neighbour's spare bottom buffer (CTA 0: its
+        // own spare top one)
+        int o_top = rank < C - 1 ? s_right : S;
+        int o_bot = rank > 0 ? s_left : rt - 1;
+        int g = 0, sweeps = 1;
+        if (rounds > 0) {
+            for (int sw = 0; sw < max_sweeps; ++sw) {
+                for (int r = 0; r < rounds; ++r, ++g) {
+#pragma unroll
+                    for (int t = 0; t < kClusterSlotsPerWarp; ++t) {
+                        const int j = warp + t * nwarps;
+                        if (j < S) {
+                            const int xo = tb[t] < 0 ? 0 : top_off + tb[t] * ld;
+                            const int yo = bot_off + bb[t] * ld;
+                            const double *xt = smem + xo;
+                            const double *xb = smem + yo;
+                            const uint32_t dt = j == S - 1
+                                                    ? (rank < C - 1 ? sm_right + 8u * (uint32_t)(top_off + o_top * ld)
+                                                                    : sm_self + 8u * (uint32_t)(bot_off + o_top * ld))
+                                                    : sm_self + 8u * (uint32_t)xo;
+                            const uint32_t db = j == 0
+                                                    ? (rank > 0 ? sm_left + 8u * (uint32_t)(bot_off + o_bot * ld)
+                                                                : sm_self + 8u * (uint32_t)(top_off + o_bot * ld))
+                                                    : sm_self + 8u * (uint32_t)yo;
+                            const bool real = pv[t] != n && qv[t] != n;
+                            double c = 0.0, s = 0.0;
+                            if (real) {
+                                double pp, qq, pqv;
+                                warp_pair_stats(xt, xb, m, lane, pp, qq, pqv);
+                                if (lane == 0 && rotation_params(pp, qq, pqv, eps, c, s)) s_rot = 1;
+                                c = __shfl_sync(0xffffffffu, c, 0);
+                                s = __shfl_sync(0xffffffffu, s, 0);
+                            }
+                            if (c != 0.0) {
+                                warp_rotate_cl(xt, xb, dt, db, ld, lane, c, s, true);
+                            } else {  // no rotation (or the dummy's slot): the columns only move
+                                if (j == S - 1 && pv[t] != n) warp_move_cl(xt, dt, ld, lane);
+                                if (j == 0 && qv[t] != n) warp_move_cl(xb, db, ld, lane);
+                            }
+                            if (pv[t] != 0) pv[t] = pv[t] == 1 ? L : pv[t] - 1;
+                            qv[t] = qv[t] == 1 ? L : qv[t] - 1;
+                            if (tb[t] >= 0) tb[t] = tb[t] == 0 ? rt - 1 : tb[t] - 1;
+                            bb[t] = bb[t] == rb - 1 ? 0 : bb[t] + 1;
+                        }
+                    }
+                    if (rank < C - 1) o_top = o_top == 0 ? s_right : o_top - 1;
+                    else o_top = o_top == rb - 1 ? 0 : o_top + 1;
+                    if (rank > 0) o_bot = o_bot == s_left ? 0 : o_bot + 1;
+                    else o_bot = o_bot == 0 ? rt - 1 : o_bot - 1;
+                    cluster.sync();
+                }
+                // sweep test over the cluster: a CTA that rotated raises rank 0's stamp
+                const unsigned long long stamp = (unsigned long long)idx * (unsigned)(max_sweeps + 1) + sw + 1;
+                if (threadIdx.x == 0) {
+                    if (s_rot) atomicMax(stamp0, stamp);
+                    s_rot = 0;
+                }
+                cluster.sync();
+                const bool any = *(volatile const unsigned long long *)stamp0 == stamp;
+                sweeps = sw + 1;
+                if (!any) break;
+            }
+        }
+        // every sweep is a whole turn of the circle: position p holds column p again
+        double *sg = sigma_all + d.s_off;
+        for (int cc = warp; cc < ncl; cc += nwarps) {
+            const int j = cc < S ? cc : cc - S;
+            const int col = cc < S ? k0 + j : ne - 1 - (k0 + j);
+            if (col >= n) continue;
+            const double *x = smem + (cc < S ? top_at(j, g) : bot_at(j, g));
+            const double sc = sqrt(fmax(warp_norm2(x, m, lane), 0.0));
+            if (lane == 0) sg[col] = sc;
+            if (u_all != nullptr) {
+                double *u = u_all + d.u_off;
+                for (int i = lane; i < m; i += 32) u[(size_t)i * n + col] = (sc > eps) ? (x[i] / sc) : 0.0;
+            }
+            if (v_all != nullptr) {
+                double *vo = v_all + d.v_off;
+                for (int i = lane; i < n; i += 32) vo[(size_t)i * n + col] = x[m + i];
+            }
+        }
+        if (rank == 0 && threadIdx.x == 0 && sweeps_all != nullptr) sweeps_all[idx] = sweeps;
+    }
+}
+
+using ClusterFn = void (*)(const BatchDesc *, int, int *, const void *, int, double, int, double *, double *, double *,
+                           int *);
+
+ClusterFn cluster_fn(int C)
+{
+    return C == 2 ? batch_cluster_kernel<2> : (C == 4 ? batch_cluster_kernel<4> : batch_cluster_kernel<8>);
+}
+
+// Size classes whose members go to clusters where one fits (bit c = class c;
+// classes 2-4 only).  Process-wide.
+std::atomic<int> g_cluster_mask{(1 << 3) | (1 << 4)};
+int batch_cluster_mask() { return g_cluster_mask.load(std::memory_order_relaxed); }
+
+// Smallest cluster (2, 4, 8 CTAs) whose shared memory holds an m x n member
+// with at least two and at most 64 pair slots per CTA; 0 when none does.
+int cluster_size_for(int m, int n, size_t smem_cap)
+{
+    const int half = (n + (n & 1)) / 2;
+    for (int C : {2, 4, 8})
+        if (half >= 2 * C && cluster_slots_max(n, C) <= kClusterSlotsPerWarp * (kClusterThreads / 32) &&
+            cluster_smem_bytes(m, n, C) <= smem_cap)
+            return C;
+    return 0;
+}
+
 using BatchFn = void (*)(const BatchDesc *, int, int *, const void *, int, double, int, double *, double *,
                          double *, int *, double *, size_t, int);
 
@@ -524,35 +819,80 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         all[i] = d;
         members[member_class(d.m, d.n, smem_cap, &need_smem[i])].push_back(i);
     }
-    // Largest work first inside each class (tail balance of the work queue).
+    // Launch groups in launch order: per class, largest first, the members
+    // solved by clusters of 8, 4 and 2 CTAs (classes whose bit is set in the
+    // cluster mask), then the rest by the class's own kernel.  Largest work
+    // first inside each group (tail balance of the work queue).
+    struct Group {
+        int cls, csize, first, count;
+        size_t smem, gws;
+        int grid;
+    };
     auto work = [&](int i) { return member_work(all[i].m, all[i].n); };
+    const int mask = batch_cluster_mask();
+    std::vector<Group> groups;
     std::vector<BatchDesc> ordered;
     ordered.reserve(count);
-    std::vector<int> first(kClasses + 1, 0), order_index;
+    std::vector<int> order_index;
     order_index.reserve(count);
-    size_t smem_of[kClasses] = {}, gws_of[kClasses] = {};
-    for (int c = 0; c < kClasses; ++c) {
+    for (int c = kClasses - 1; c >= 0; --c) {
         std::sort(members[c].begin(), members[c].end(), [&](int x, int y) { return work(x) > work(y); });
-        first[c] = (int)ordered.size();
+        std::vector<int> sub[4];  // own kernel, clusters of 2, 4, 8
         for (int i : members[c]) {
-            ordered.push_back(all[i]);
-            order_index.push_back(i);
-            smem_of[c] = std::max(smem_of[c], need_smem[i]);
-            size_t g = 0;
-            if (!classes[c].a_shared) g += (size_t)all[i].m * all[i].n;
-            if (!classes[c].v_shared) g += (size_t)all[i].n * all[i].n;
-            gws_of[c] = std::max(gws_of[c], g);
+            const int C = ((mask >> c) & 1) ? cluster_size_for(all[i].m, all[i].n, smem_cap) : 0;
+            sub[C == 0 ? 0 : (C == 2 ? 1 : (C == 4 ? 2 : 3))].push_back(i);
+        }
+        for (int s : {3, 2, 1, 0}) {
+            if (sub[s].empty()) continue;
+            Group g{c, s == 0 ? 0 : (1 << s), (int)ordered.size(), (int)sub[s].size(), 0, 0, 0};
+            for (int i : sub[s]) {
+                ordered.push_back(all[i]);
+                order_index.push_back(i);
+                if (g.csize > 0) {
+                    g.smem = std::max(g.smem, cluster_smem_bytes(all[i].m, all[i].n, g.csize));
+                } else {
+                    g.smem = std::max(g.smem, need_smem[i]);
+                    size_t w = 0;
+                    if (!classes[c].a_shared) w += (size_t)all[i].m * all[i].n;
+                    if (!classes[c].v_shared) w += (size_t)all[i].n * all[i].n;
+                    g.gws = std::max(g.gws, w);
+                }
+            }
+            groups.push_back(g);
         }
     }
-    first[kClasses] = (int)ordered.size();
-    int grid_of[kClasses] = {};
-    size_t gws_total = 0, gws_base[kClasses] = {};
-    for (int c = 0; c < kClasses; ++c) {
-        const int cnt = first[c + 1] - first[c];
-        grid_of[c] = std::min(cnt, sms * classes[c].ctas_per_sm);
-        if (max_ctas[c] > 0) grid_of[c] = std::min(grid_of[c], max_ctas[c]);
-        gws_base[c] = gws_total;
-        gws_total += gws_of[c] * (size_t)grid_of[c];
+    std::vector<size_t> gws_base(groups.size(), 0);
+    size_t gws_total = 0;
+    for (size_t k = 0; k < groups.size(); ++k) {
+        Group &g = groups[k];
+        if (g.csize > 0) {
+            JSVD_CUDA_TRY(cudaFuncSetAttribute(cluster_fn(g.csize), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem_cap));
+            cudaLaunchConfig_t lc = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = (unsigned)g.csize;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            lc.gridDim = dim3((unsigned)g.csize);
+            lc.blockDim = dim3(kClusterThreads);
+            lc.dynamicSmemBytes = g.smem;
+            lc.attrs = at;
+            lc.numAttrs = 1;
+            int clusters = 0;
+            JSVD_CUDA_TRY(cudaOccupancyMaxActiveClusters(&clusters, cluster_fn(g.csize), &lc));
+            if (clusters <= 0) {
+                set_last_error(JSVD_ERR_RUNTIME, "No cluster of the batched solver fits the device.");
+                return JSVD_ERR_RUNTIME;
+            }
+            g.grid = std::min(g.count, clusters) * g.csize;
+        } else {
+            const Class &cl = classes[g.cls];
+            g.grid = std::min(g.count, sms * cl.ctas_per_sm);
+            if (max_ctas[g.cls] > 0) g.grid = std::min(g.grid, max_ctas[g.cls]);
+            gws_base[k] = gws_total;
+            gws_total += g.gws * (size_t)g.grid;
+        }
     }
 
     BatchDesc *d_desc = nullptr;
@@ -564,35 +904,56 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
         if (d_sweeps) cudaFreeAsync(d_sweeps, stream);
         if (d_ws) cudaFreeAsync(d_ws, stream);
     });
+    const size_t ngroups = std::max<size_t>(groups.size(), 1);
     JSVD_CUDA_TRY(cudaMallocAsync(&d_desc, sizeof(BatchDesc) * ordered.size(), stream));
-    JSVD_CUDA_TRY(cudaMallocAsync(&d_next, sizeof(int) * kClasses, stream));
+    JSVD_CUDA_TRY(cudaMallocAsync(&d_next, sizeof(int) * ngroups, stream));
     JSVD_CUDA_TRY(cudaMallocAsync(&d_sweeps, sizeof(int) * (size_t)count, stream));
     if (gws_total > 0) JSVD_CUDA_TRY(cudaMallocAsync(&d_ws, sizeof(double) * gws_total, stream));
     JSVD_CUDA_TRY(cudaMemcpyAsync(d_desc, ordered.data(), sizeof(BatchDesc) * ordered.size(), cudaMemcpyHostToDevice,
                                   stream));
-    JSVD_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int) * kClasses, stream));
+    JSVD_CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int) * ngroups, stream));
     for (BatchFn fn : {(BatchFn)batch_kernel<true, true>, (BatchFn)batch_kernel<true, false>,
                        (BatchFn)batch_kernel<false, false>})
         JSVD_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
     JSVD_CUDA_TRY(cudaEventRecord(ts->t0, stream));
     int launches = 0;
-    for (int c = kClasses - 1; c >= 0; --c) {
-        const int cnt = first[c + 1] - first[c];
-        if (cnt == 0) continue;
-        const Class &cl = classes[c];
+    std::vector<int> class_count(kClasses, 0);
+    for (size_t k = 0; k < groups.size(); ++k) {
+        const Group &g = groups[k];
+        const int c = g.cls;
         // The classes run one after another on one stream: persistent CTAs of
         // a class hold their SMs until its queue drains, and concurrent classes
         // starved each other (a 512-thread CTA of the global class fills an
         // SM's register file).
-        JSVD_CUDA_TRY(cudaEventRecord(ts->c0[c], stream));
-        // The global class keeps leading columns of A in the shared memory left over.
-        const size_t dyn = (!cl.a_shared && !cl.v_shared) ? (smem_cap & ~(size_t)7) : smem_of[c];
-        cl.fn<<<grid_of[c], cl.threads, dyn, stream>>>(d_desc + first[c], cnt, d_next + c, req.a, req.a_is_f32,
+        if (k == 0 || groups[k - 1].cls != c) JSVD_CUDA_TRY(cudaEventRecord(ts->c0[c], stream));
+        class_count[c] += g.count;
+        if (g.csize > 0) {
+            cudaLaunchConfig_t lc = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = (unsigned)g.csize;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            lc.gridDim = dim3((unsigned)g.grid);
+            lc.blockDim = dim3(kClusterThreads);
+            lc.dynamicSmemBytes = g.smem;
+            lc.stream = stream;
+            lc.attrs = at;
+            lc.numAttrs = 1;
+            JSVD_CUDA_TRY(cudaLaunchKernelEx(&lc, cluster_fn(g.csize), (const BatchDesc *)(d_desc + g.first), g.count,
+                                             d_next + k, req.a, req.a_is_f32, req.eps, req.max_sweeps, req.sigma,
+                                             req.v, req.u, d_sweeps + g.first));
+        } else {
+            const Class &cl = classes[c];
+            // The global class keeps leading columns of A in the shared memory left over.
+            const size_t dyn = (!cl.a_shared && !cl.v_shared) ? (smem_cap & ~(size_t)7) : g.smem;
+            cl.fn<<<g.grid, cl.threads, dyn, stream>>>(d_desc + g.first, g.count, d_next + k, req.a, req.a_is_f32,
                                                        req.eps, req.max_sweeps, req.sigma, req.v, req.u,
-                                                       d_sweeps + first[c], d_ws + gws_base[c], gws_of[c],
+                                                       d_sweeps + g.first, d_ws + gws_base[k], g.gws,
                                                        (int)(dyn / sizeof(double)));
-        JSVD_CUDA_TRY(cudaGetLastError());
-        JSVD_CUDA_TRY(cudaEventRecord(ts->c1[c], stream));
+            JSVD_CUDA_TRY(cudaGetLastError());
+        }
+        if (k + 1 == groups.size() || groups[k + 1].cls != c) JSVD_CUDA_TRY(cudaEventRecord(ts->c1[c], stream));
         ++launches;
     }
     JSVD_CUDA_TRY(cudaEventRecord(ts->t1, stream));
@@ -613,9 +974,9 @@ int batch_solve(const BatchRequest &req, cudaStream_t stream)
     st.sweeps += total_sweeps;
     st.matrices += (unsigned long long)count;
     for (int c = 0; c < kClasses; ++c) {
-        st.class_count[c] += (unsigned long long)(first[c + 1] - first[c]);
+        st.class_count[c] += (unsigned long long)class_count[c];
         float cms = 0.f;
-        if (first[c + 1] > first[c] && cudaEventElapsedTime(&cms, ts->c0[c], ts->c1[c]) == cudaSuccess)
+        if (class_count[c] > 0 && cudaEventElapsedTime(&cms, ts->c0[c], ts->c1[c]) == cudaSuccess)
             st.class_ms[c] += cms;
     }
     return JSVD_OK;
@@ -777,6 +1138,15 @@ extern "C" void jsvd_batch_stats_get(jsvd_batch_stats *out)
 }
 
 extern "C" void jsvd_batch_stats_reset(void) { batch_stats() = BatchStats{}; }
+
+extern "C" int jsvd_batch_set_cluster_classes(int mask, int *previous)
+{
+    if (mask & ~((1 << 2) | (1 << 3) | (1 << 4)))
+        return invalid_argument("Only size classes 2, 3 and 4 can be solved by clusters.");
+    const int old = g_cluster_mask.exchange(mask);
+    if (previous) *previous = old;
+    return JSVD_OK;
+}
 
 extern "C" void jsvd_batch_builtin_tuning(jsvd_batch_tuning *out)
 {

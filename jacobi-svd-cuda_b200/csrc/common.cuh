@@ -82,6 +82,16 @@ __host__ __device__ __forceinline__ int2 round_robin_pair(int n, int r, int k)
     return make_int2(p, q);
 }
 
+// Column at circle position pos (0 <= pos < ne) in round r of the same
+// schedule, L = ne - 1; -1 for the dummy column of an odd n.  Slot k of a
+// round pairs positions k and ne-1-k.
+__host__ __device__ __forceinline__ int circle_col(int n, int L, int r, int pos)
+{
+    if (pos == 0) return 0;
+    const int c = 1 + ((pos - 1 - r) % L + L) % L;
+    return c == n ? -1 : c;
+}
+
 // Rutishauser rotation for the 2x2 Gram [pp pq; pq qq]; returns true when the
 // pair rotates.  A pair that does not rotate reports c = 0, s = 0 (a real
 // rotation always has c >= 1/sqrt(2)), which is how the deferred V update

@@ -418,14 +418,6 @@ __global__ void wait_limit_check_kernel(const int *flags, long long limit_ns, in
     if (threadIdx.x == 0 && !wait_for_rounds(flags, 0, 0, false, 1, limit_ns)) atomicExch(status, (int)kDevWaitTimeout);
 }
 
-// Column of circle position pos in round r (-1 for the dummy of an odd n).
-__device__ __forceinline__ int circle_col(int n, int L, int r, int pos)
-{
-    if (pos == 0) return 0;
-    const int c = 1 + ((pos - 1 - r) % L + L) % L;
-    return c == n ? -1 : c;
-}
-
 template <int T, int K>
 __global__ void __launch_bounds__(T) plain_sweep_persistent(double *__restrict__ a, long lda, int m, int n,
                                                              int rounds, int slots_per_cta, double2 *__restrict__ cs,

@@ -199,7 +199,7 @@ def exported_symbols() -> list[str]:
         "jsvd_mixed_options_default", "jsvd_mixed_set_options", "jsvd_mixed_svd", "jsvd_mixed_svd_device",
         "jsvd_mixed_stats_get", "jsvd_mixed_stats_reset", "jsvd_dgemm_device", "jsvd_mixed_test_round",
         "jsvd_test_wait_limit", "jsvd_mixed_builtin_tuning",
-        "jsvd_mixed_sweep_history",
+        "jsvd_mixed_sweep_history", "jsvd_batch_set_cluster_classes",
     ]
 
 
@@ -237,6 +237,8 @@ def lib() -> ctypes.CDLL:
         L.jsvd_residuals.restype = I
         L.jsvd_batch_builtin_tuning.argtypes = [ctypes.POINTER(BatchTuning)]
         L.jsvd_batch_builtin_tuning.restype = None
+        L.jsvd_batch_set_cluster_classes.argtypes = [I, ctypes.POINTER(I)]
+        L.jsvd_batch_set_cluster_classes.restype = I
         L.jsvd_batch_autotune.argtypes = [I, P, P, P, P, I, ctypes.POINTER(Config), I, I, I, I,
                                           ctypes.POINTER(BatchAutotuneReport), P]
         L.jsvd_batch_autotune.restype = I
@@ -713,6 +715,14 @@ def batch_builtin_tuning() -> list[tuple[int, int, int]]:
     out = (BatchTuning * 5)()
     lib().jsvd_batch_builtin_tuning(out)
     return [(t.threads, t.ctas_per_sm, t.max_ctas) for t in out]
+
+
+def batch_set_cluster_classes(mask: int) -> int:
+    """Size classes (bit c = class c; 2, 3, 4 only) whose members the batched
+    solver runs on thread-block clusters; returns the previous mask."""
+    old = ctypes.c_int(0)
+    check(lib().jsvd_batch_set_cluster_classes(int(mask), ctypes.byref(old)))
+    return old.value
 
 
 def probe_fp64_tflops() -> float:

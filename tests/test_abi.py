@@ -187,3 +187,18 @@ def test_integration_guide_covers_every_declared_function():
     guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     missing = [name for name in _declared_functions() if name not in guide]
     assert missing == [], missing
+
+
+def test_batch_cluster_classes_setter():
+    """Only classes 2-4 may go to clusters; the setter reports the previous
+    mask and needs no GPU."""
+    old = jsvd.batch_set_cluster_classes((1 << 3) | (1 << 4))
+    try:
+        assert jsvd.batch_set_cluster_classes(1 << 2) == (1 << 3) | (1 << 4)
+        for bad in (1, 1 << 1, 1 << 5, -1):
+            with pytest.raises(jsvd.JsvdError) as e:
+                jsvd.batch_set_cluster_classes(bad)
+            assert e.value.code == jsvd.JSVD_ERR_INVALID_ARGUMENT
+        assert jsvd.batch_set_cluster_classes(0) == 1 << 2
+    finally:
+        jsvd.batch_set_cluster_classes(old)

@@ -42,6 +42,39 @@ def test_batch_bitwise_vs_oracle(cuda_device, f32):
         assert np.array_equal(u, eu), a.shape
 
 
+# members of the three classes that clusters can take, odd and even n; each
+# needs a different cluster size (2, 4 or 8 CTAs) or none
+CLUSTER_SHAPES = [(100, 90), (120, 100), (129, 64), (160, 120), (161, 117), (170, 110), (200, 150), (250, 131),
+                  (256, 200), (255, 255), (256, 256), (231, 229), (240, 15), (256, 9)]
+
+
+def test_batch_cluster_classes_bitwise(cuda_device):
+    """Members solved by thread-block clusters (classes 3 and 4 by default,
+    class 2 as well, or none) give the same bytes and sweep counts, and they
+    are the oracle's."""
+    rng = np.random.default_rng(31)
+    mats = [rng.standard_normal(s) for s in CLUSTER_SHAPES]
+    cfg = jsvd.default_config(epsilon=1e-13)
+    runs = []
+    old = jsvd.batch_set_cluster_classes(0)
+    try:
+        for mask in (0, (1 << 3) | (1 << 4), (1 << 2) | (1 << 3) | (1 << 4)):
+            jsvd.batch_set_cluster_classes(mask)
+            b = jsvd.DeviceBatch(mats, cuda_device, want_u=True)
+            b.solve(cfg)
+            runs.append(b.results())
+    finally:
+        jsvd.batch_set_cluster_classes(old)
+    for k, a in enumerate(mats):
+        for other in runs[1:]:
+            assert runs[0][k][3] == other[k][3], a.shape
+            for x, y in zip(runs[0][k][:3], other[k][:3]):
+                assert np.array_equal(x, y), a.shape
+    for a, (u, s, v, sw) in list(zip(mats, runs[1]))[::3]:
+        eu, es, ev, esw = O.plain_svd(a, eps=1e-13, variant=jsvd.arith_variant(), threads=4)
+        assert sw == esw and np.array_equal(s, es) and np.array_equal(v, ev) and np.array_equal(u, eu), a.shape
+
+
 def test_batch_workload_sample_accuracy(cuda_device):
     """A sample of the mixed-size FP32 batch workload: sigma against LAPACK on
     the FP32-promoted input and orthogonality of V."""
