@@ -71,6 +71,8 @@ def test_reference_arm_json_line():
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "SVD/s" and d["n_gpus"] == 1
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # a step is the bounded sample actually timed: its time fits the run
+    assert 0 < d["ms_per_step"] <= 1e3 * (0.5 * 4 + 5) and "step" in d
 
 
 def test_nominal_rate_model():
