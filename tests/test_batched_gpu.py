@@ -42,10 +42,11 @@ def test_batch_bitwise_vs_oracle(cuda_device, f32):
         assert np.array_equal(u, eu), a.shape
 
 
-# members of the three classes that clusters can take, odd and even n; each
-# needs a different cluster size (2, 4 or 8 CTAs) or none
+# members of the three classes that clusters can take, odd and even n, and
+# columns longer than the 256-row reduction chunk; each needs a different
+# cluster size (2, 4 or 8 CTAs) or none
 CLUSTER_SHAPES = [(100, 90), (120, 100), (129, 64), (160, 120), (161, 117), (170, 110), (200, 150), (250, 131),
-                  (256, 200), (255, 255), (256, 256), (231, 229), (240, 15), (256, 9)]
+                  (256, 200), (255, 255), (256, 256), (231, 229), (240, 15), (256, 9), (600, 120), (517, 131)]
 
 
 def test_batch_cluster_classes_bitwise(cuda_device):
