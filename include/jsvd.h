@@ -231,7 +231,8 @@ int jsvd_batch_svd_device(int count, const int *rows, const int *cols, const lon
 /* Size classes whose members are solved by a thread-block cluster (2, 4 or 8
  * CTAs, the smallest whose distributed shared memory holds A and V with at
  * least two column pairs per CTA) instead of by one CTA: bit c = class c,
- * classes 2, 3 and 4 only (default: 3 and 4).  A member that fits no cluster
+ * classes 2, 3 and 4 only (default: the compiled-in tuning table's choice,
+ * JSVD_BATCH_CLUSTER_CLASSES, which batch_autotune.py measures: 3 and 4).  A member that fits no cluster
  * stays with its class's own kernel, which is also the only one the class's
  * tuning entry shapes.  Results are the same bytes either way.
  * Process-wide; *previous (optional) gets the old mask. */

@@ -12,8 +12,20 @@
  *   2 (A and V in <= ~226 KiB of shared memory): 844 / 844, 3 shapes, 46.86 -> 46.86
  *   3 (A in shared memory, V in global memory): 485 / 485, 9 shapes, 76.49 -> 76.49
  *   4 (A and V in global memory): 506 / 506, 9 shapes, 240.89 -> 240.89
+ *
+ * CTAs per matrix: the classes whose bit is set in JSVD_BATCH_CLUSTER_CLASSES
+ * are solved by a thread-block cluster per matrix (2, 4 or 8 CTAs, the
+ * smallest that holds it), the others by one CTA per matrix; a class goes
+ * over only when that is more than 2% faster.
+ * Timed on NVIDIA B200 (148 SMs), 2026-12-04, over 20000 FP32-stored matrices (seed 3), all classes, mean of 3 runs, L2 flushed.
+ * class: ms one CTA per matrix, ms clusters -> chosen
+ *   2: 209.9, 220.0 -> one CTA
+ *   3: 362.9, 334.5 -> clusters
+ *   4: 1134.1, 956.9 -> clusters
  */
 #pragma once
 
 #define JSVD_BATCH_TUNING_TABLE \
     { {256, 4, 0}, {256, 2, 0}, {512, 1, 0}, {512, 1, 0}, {512, 1, 0} }
+
+#define JSVD_BATCH_CLUSTER_CLASSES 0x18

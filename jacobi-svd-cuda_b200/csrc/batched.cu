@@ -644,8 +644,12 @@ ClusterFn cluster_fn(int C)
 }
 
 // Size classes whose members go to clusters where one fits (bit c = class c;
-// classes 2-4 only).  Process-wide.
-std::atomic<int> g_cluster_mask{(1 << 3) | (1 << 4)};
+// classes 2-4 only), initially the compiled-in tuning table's choice.
+// Process-wide.
+#ifndef JSVD_BATCH_CLUSTER_CLASSES
+#define JSVD_BATCH_CLUSTER_CLASSES ((1 << 3) | (1 << 4))
+#endif
+std::atomic<int> g_cluster_mask{JSVD_BATCH_CLUSTER_CLASSES};  // the tuning table's choice
 int batch_cluster_mask() { return g_cluster_mask.load(std::memory_order_relaxed); }
 
 // Smallest cluster (2, 4, 8 CTAs) whose shared memory holds an m x n member

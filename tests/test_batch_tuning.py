@@ -47,14 +47,44 @@ def _fake_report():
     }
 
 
+_FAKE_CLUSTER = {"mask": 0x14, "single_ms": [1.0, 2.0, 30.0, 40.0, 100.0], "cluster_ms": [0, 0, 20.0, 41.0, 60.0],
+                 "note": "Timed on the same batch."}
+
+
 def test_render_parse_round_trip():
     rep = _fake_report()
     text = BA.render_table(rep, {"device": "NVIDIA B200", "sms": 148, "date": "2026-01-01", "reps": 2,
-                                 "workload": "test batch"})
+                                 "workload": "test batch"}, _FAKE_CLUSTER)
     got = BA.parse_table(text)
     # a class without members keeps its built-in shape
     assert got == [rep["best"][0], rep["best"][1], rep["best"][2], rep["builtin"][3], rep["best"][4]]
     assert "#pragma once" in text and "NVIDIA B200" in text and "2.00 -> 1.50" in text
+    assert BA.parse_cluster_mask(text) == 0x14
+    assert " *   2: 30.0, 20.0 -> clusters" in text and " *   3: 40.0, 41.0 -> one CTA" in text
+
+
+def test_library_default_cluster_classes_are_the_committed_table():
+    with open(TABLE) as f:
+        mask = BA.parse_cluster_mask(f.read())
+    assert mask & ~BA.CLUSTER_CAPABLE == 0
+    old = jsvd.batch_set_cluster_classes(mask)
+    jsvd.batch_set_cluster_classes(old)
+    # nothing else in this process has changed it, or the change was undone
+    assert old == mask
+
+
+def test_cluster_choice_needs_a_two_percent_gain():
+    members = [5, 5, 5, 5, 5]
+    single = [1.0, 1.0, 100.0, 100.0, 100.0]
+    # clusters 1% faster for class 2, 10% faster for 3, 5% slower for 4
+    clus = [1.0, 1.0, 99.0, 90.0, 105.0]
+    assert BA.choose_cluster_mask(single, clus, members, previous=0) == 1 << 3
+    # from all on: class 2 stays (single not > 2% faster), class 4 goes back to one CTA
+    assert BA.choose_cluster_mask(single, clus, members, previous=0x1C) == (1 << 2) | (1 << 3)
+    # a class without members keeps its previous choice
+    assert BA.choose_cluster_mask(single, clus, [5, 5, 5, 0, 5], previous=0) == 0
+    # bits outside the cluster-capable classes are dropped
+    assert BA.choose_cluster_mask(single, single, members, previous=0x3) == 0
 
 
 def test_parse_rejects_wrong_entry_count():
